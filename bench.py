@@ -1,0 +1,325 @@
+"""Benchmark: Born voxel-iterations per second of the batched CBS forward solve.
+
+Workload (one step): the multi-illumination forward solve of a seeded
+128^3 multi-sphere phantom (0.1 um voxels, RI 1.34-1.46 in 1.3355, default
+6-wavelength boundary -> 152^3 padded grid), 49 plane waves (normal + 48 on
+rings at NA 0.3/0.6/0.9), transmitted field returned.  Synthetic data stand in
+for the reference's experimental holograms.
+
+  value : voxel-iterations/s with inputs resident in HBM (device API), CUDA
+          events on the solve stream, max over ranks
+  e2e   : the same metric through the C-ABI host path (pinned host buffers,
+          H2D of the input fields and D2H of the transmitted fields inside the
+          timed region), wall clock around synchronous calls
+
+usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Born voxel-iter/s"
+UNIT = "voxel-iter/s"
+GRID = [128, 128, 128]
+N_ILL = 49
+SEED = 0
+# algorithmic HBM bytes per voxel and launch of each Born kernel kind
+# (complex64 = 8 B): born_x reads T, Field_n, Field, V and
+# writes T, Field_n, Field; born_y / born_z read and write T once.
+ALG_BYTES_PER_VOXEL = {"born_x": 56, "born_y": 16, "born_z": 16}
+
+
+def workload_params():
+    from inverse_solver_b200.forward import CBSHostSetup
+
+    return CBSHostSetup.get_default_parameters(dict(
+        size=list(GRID), wavelength=0.532, NA=1.2, RI_bg=1.3355, resolution=[0.1] * 3,
+        vector_simulation=False, return_transmission=True))
+
+
+def workload_inputs(p):
+    from inverse_solver_b200.inputs import ring_illumination, sphere_phantom
+
+    RI = sphere_phantom(GRID, [0.1] * 3, 1.3355, seed=SEED)
+    fields = ring_illumination(p)
+    assert fields.shape[3] == N_ILL
+    return RI, fields
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(p, RI, fields, n_iter):
+    """The oracle's single-precision restatement of the reference's Born loop
+    (unfused sweeps + full 3D FFTs, scipy.fft with all host threads), timed on
+    a bounded sample: one illumination, first n_iter Born iterations."""
+    from oracle import cbs
+
+    o = cbs.ForwardSolverCBS(p, single=True)
+    o.set_RI(RI)
+    inp = o.transform_field_3D(cbs.fftc2(fields[:, :, :, :1].astype(np.complex64)))
+    n_iter = min(n_iter, o.Bornmax)
+    t0 = time.perf_counter()
+    o.solve_raw(inp[:, :, :, 0], n_iter=n_iter)
+    dt = time.perf_counter() - t0
+    vox = int(np.prod(o.V.shape)) * n_iter
+    return {"value": vox / dt, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": f"1 of {N_ILL} illuminations, Born iterations 1-{n_iter} of {o.Bornmax} "
+                      f"on the {list(o.V.shape)} padded grid ({dt:.1f} s)"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    p = workload_params()
+    RI, fields = workload_inputs(p)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(p, RI, fields, args.ref_iters)
+        if i >= args.warmup:
+            vals.append(r["value"])
+    v = float(np.mean(vals))
+    r["value"] = v
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+           "dtype": "fp32", "data": "synthetic",
+           "config": {"workload": workload_name(), "grid": GRID, "n_ill": N_ILL},
+           "cpu_baseline": r,
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "vs_baseline": None}
+    print(json.dumps(out))
+
+
+def workload_name():
+    return ("cbs_forward: 128^3 RI grid, 0.1 um voxels, seeded multi-sphere phantom (seed 0), "
+            "49 plane waves (normal + rings NA 0.3/0.6/0.9), padded 152^3, transmitted field")
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    from inverse_solver_b200 import FORWARD_SOLVER_CONVERGENT_BORN
+
+    p = workload_params()
+    p["used_gpu"] = local_rank
+    RI, fields = workload_inputs(p)
+    s = FORWARD_SOLVER_CONVERGENT_BORN(p)
+    s.set_RI(RI)
+    F = s.field_size
+    vox_step = s.voxel_iterations(N_ILL)
+    dev = torch.device("cuda", local_rank)
+    fin = torch.from_numpy(np.ascontiguousarray(fields[:, :, 0, :].transpose(2, 1, 0))).to(dev)
+    tout = torch.empty((N_ILL, F[1], F[0]), dtype=torch.complex64, device=dev)
+    stream = torch.cuda.current_stream()
+
+    for _ in range(args.warmup):
+        s.solve_device(fin, tout, stream=stream)
+    torch.cuda.synchronize()
+
+    # ---- per-kernel times and launch counts (one profiled step, not timed)
+    s.set_profiling(True)
+    s.solve_device(fin, tout, stream=stream)
+    torch.cuda.synchronize()
+    kt = s.kernel_times()
+    s.set_profiling(False)
+    launches_per_step = sum(n for _, n in kt.values())
+
+    # ---- timed region (device-resident inputs)
+    clk = ClockSampler(local_rank)
+    clk.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    evs[0].record(stream)
+    for i in range(args.steps):
+        s.solve_device(fin, tout, stream=stream)
+        evs[i + 1].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = clk.stop()
+    total_ms = evs[0].elapsed_time(evs[-1])
+    step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * vox_step * args.steps / (total_ms / 1e3)
+
+    # ---- e2e through the host C-ABI path with pinned buffers
+    hin = torch.from_numpy(np.ascontiguousarray(fields[:, :, 0, :].transpose(2, 1, 0))).pin_memory()
+    hout = torch.empty((N_ILL, F[1], F[0]), dtype=torch.complex64).pin_memory()
+    s.solve_ptrs(hin.data_ptr(), N_ILL, trans=hout.data_ptr())
+    if dist:
+        dist.barrier()
+    e2e_steps = max(1, args.steps)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s.solve_ptrs(hin.data_ptr(), N_ILL, trans=hout.data_ptr())
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_val = world * vox_step * e2e_steps / float(te.item())
+
+    if rank != 0:
+        s.delete()
+        return
+    peak, peak_kind = load_peaks()
+    born = {k: v for k, v in kt.items() if k in ALG_BYTES_PER_VOXEL}
+    dom = max(born, key=lambda k: born[k][0])
+    dom_ms, dom_n = born[dom]
+    vox_launch = int(np.prod(s.sim_size)) * s.batch()
+    alg_bytes = ALG_BYTES_PER_VOXEL[dom] * vox_launch
+    achieved = alg_bytes / (dom_ms / dom_n / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        tj = json.load(open(tpath)).get(workload_key(), {})
+        if dom in tj:
+            traffic = tj[dom]
+    born_ms = sum(v[0] for v in born.values())
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": workload_name(), "grid": GRID, "padded_grid": s.sim_size,
+                   "n_ill": N_ILL, "bornmax": s.Bornmax, "voxel_iters_per_step": vox_step,
+                   "batch": s.batch(), "l2": "inputs larger than L2 (per-step working set "
+                   f"{3 * 8 * int(np.prod(s.sim_size)) * s.batch() / 1e9:.1f} GB)",
+                   "parallelism": f"dp{world} (illuminations, replicas)"},
+        "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
+                       "p99": float(np.percentile(step_ms, 99))},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic,
+                     "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": dom_ms / dom_n,
+                     "iteration_frac": (72.0 * vox_step / (born_ms / 1e3) / 1e9) / peak},
+        "kernel_ms_per_step": {k: v[0] for k, v in kt.items()},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clocks,
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(hin.numel() * 8),
+                "d2h_bytes_per_step": int(hout.numel() * 8)},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(p, RI, fields, args.ref_iters)
+    s.delete()
+    print(json.dumps(out))
+
+
+def workload_key():
+    return "cbs_forward_128cube_49ill"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-iters", type=int, default=16,
+                    help="Born iterations in the bounded CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,166 @@
+/*
+ * odt.h -- C ABI of the B200 convergent-Born-series (CBS) library (libodt).
+ *
+ * Drop-in replacement for the `CudaBorn` MEX of BMOLKAIST/Inverse_solver
+ * (Codes/CUDA_CODE/main.cpp:27-213) and for the Born loop of the MATLAB class
+ * FORWARD_SOLVER_CONVERGENT_BORN (Codes/FORWARD_SOLVER_CONVERGENT_BORN.m).
+ * A MATLAB gateway, a Python ctypes binding or C++ code call these functions;
+ * the host side keeps computing the geometry-dependent setup (Green's
+ * kernels, pupil filters, potential) exactly as the MATLAB class does and the
+ * library runs everything per illumination on the GPU.
+ *
+ * Conventions
+ *  - All arrays are column-major (MATLAB order: first index fastest) and
+ *    complex values are interleaved single precision (odt_cfloat), i.e. the
+ *    MATLAB -R2018a interleaved-complex layout.
+ *  - Every function returns an odt_status (0 = ODT_OK), never throws across
+ *    the ABI and never exits; odt_last_error() describes the last failure of
+ *    the calling thread.
+ *  - A handle owns its device memory.  Calls on one handle must not overlap;
+ *    different handles may be used from different threads (a mutex guards
+ *    the handle table).
+ */
+#ifndef ODT_H_
+#define ODT_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ODT_ABI_VERSION 1
+
+typedef enum odt_status {
+  ODT_OK = 0,
+  ODT_ERR_INVALID_ARGUMENT = 1, /* bad sizes, NULL where required, bad flags  */
+  ODT_ERR_BAD_HANDLE = 2,       /* unknown or destroyed handle                */
+  ODT_ERR_CUDA = 3,             /* a CUDA runtime call failed                 */
+  ODT_ERR_OUT_OF_MEMORY = 4,    /* device allocation or memory budget exceeded */
+  ODT_ERR_NOT_READY = 5,        /* odt_solve before odt_set_potential         */
+  ODT_ERR_UNSUPPORTED = 6,      /* grid length with a prime factor > 31, ...  */
+  ODT_ERR_NUMERIC = 7,          /* NaN/Inf in the inputs or the result        */
+  ODT_ERR_INTERNAL = 8
+} odt_status;
+
+typedef struct odt_cfloat {
+  float re;
+  float im;
+} odt_cfloat;
+
+typedef uint32_t odt_handle; /* like CudaBorn's uint32 id; 0 is never valid */
+
+/* Memory space of the pointers passed to odt_solve. */
+#define ODT_MEM_HOST 0
+#define ODT_MEM_DEVICE 1
+
+/*
+ * Geometry of one solver instance.  Mirrors the struct of CudaBorn action 0
+ * (FORWARD_SOLVER_CONVERGENT_BORN_CUDA.m:23-32): simulation_size (padded
+ * grid), RI_size, field_size, conv_size.
+ */
+typedef struct odt_geometry {
+  int32_t sim_size[3];   /* padded grid P = RI_size + 2*boundary_thickness_pixel */
+  int32_t ri_size[3];    /* RI grid (ROI inside the padded grid)                 */
+  int32_t field_size[2]; /* 2D field (params.size(1:2)); must equal ri_size(1:2) */
+  int32_t conv_size[2];  /* field_size + ri_size(1:2): 2D convolution plane      */
+  int32_t device;        /* CUDA device ordinal (CudaBorn's used_gpu)            */
+  int32_t max_batch;     /* illuminations resident on the device at once; 0=auto */
+  int64_t mem_budget;    /* bytes this handle may allocate; 0 = 90% of free HBM */
+} odt_geometry;
+
+/*
+ * Per-potential parameters.  Mirrors CudaBorn action 1
+ * (FORWARD_SOLVER_CONVERGENT_BORN_CUDA.m:50-61: k0_nm, eps_imag, fourier_res,
+ * ROI, Bornmax, dV) plus the separable tables the MATLAB class builds in
+ * create_boundary_RI / init (FORWARD_SOLVER_CONVERGENT_BORN.m:251-271,
+ * :299-377), passed as computed by the host so the float semantics are the
+ * host's:
+ *   mask[a]   : attenuation mask factor along axis a (length sim_size[a])
+ *   ramp[a]   : phase-ramp factor along axis a (complex, length sim_size[a])
+ *   kq2[a]    : squared shifted k-coordinate along axis a in FFT (ifftshifted)
+ *               order, (fourier_coor + fourier_res/4)^2 (length sim_size[a])
+ * The Green's function of iteration jj is evaluated on the fly as
+ *   G = 1 / (green_scale * (kq2x + kq2y + kq2z) - green_offset - i*eps_imag)
+ * with kq2 read at the frequency-negated index on odd jj when acyclic != 0
+ * (fft_flip, FORWARD_SOLVER_CONVERGENT_BORN.m:579-585).
+ */
+typedef struct odt_potential_params {
+  float eps_imag;       /* h.eps_imag                                         */
+  float green_scale;    /* single(4*pi^2)                                     */
+  float green_offset;   /* single((2*pi*k0_nm)^2)                             */
+  float dV;             /* single(utility_border.dV)                          */
+  int32_t roi[6];       /* h.ROI, 1-based inclusive [x0 x1 y0 y1 z0 z1]       */
+  int32_t bornmax;      /* h.Bornmax (>= 0)                                   */
+  int32_t acyclic;      /* params.acyclic                                     */
+  const float* mask[3];
+  const odt_cfloat* ramp[3];
+  const float* kq2[3];
+} odt_potential_params;
+
+/* Outputs of odt_solve; any pointer may be NULL to skip that output. */
+typedef struct odt_solve_args {
+  const odt_cfloat* fields_in; /* [F_x, F_y, n_ill] spatial input fields      */
+  int32_t n_ill;
+  odt_cfloat* trans;           /* [F_x, F_y, n_ill] transmitted field          */
+  odt_cfloat* ref;             /* [F_x, F_y, n_ill] reflected field            */
+  odt_cfloat* field3d;         /* [ri_x, ri_y, ri_z, n_ill] total 3D field     */
+  int32_t memory;              /* ODT_MEM_HOST or ODT_MEM_DEVICE               */
+  void* stream;                /* cudaStream_t for ODT_MEM_DEVICE; NULL=own    */
+} odt_solve_args;
+
+/*
+ * Create a solver (CudaBorn action 0, main.cpp:57-101).
+ *   refocus      : refocusing_util  [conv_x, conv_y, ri_z]
+ *                  (FORWARD_SOLVER_CONVERGENT_BORN.m:80-92)
+ *   kernel_trans : fft2(conj G)     [conv_x, conv_y, ri_z] (:114), may be NULL
+ *   kernel_ref   : fft2(G)          [conv_x, conv_y, ri_z] (:115), may be NULL
+ *   pupil_in     : [F_x, F_y] real, NA_circle and Abbe factor of
+ *                  transform_field_3D (FORWARD_SOLVER.m:38-48)
+ *   pupil_out    : [F_x, F_y] real, NA_circle*sqrt(cos_theta) of
+ *                  transform_field_2D (FORWARD_SOLVER.m:69-77)
+ */
+odt_status odt_create(const odt_geometry* geom, const odt_cfloat* refocus,
+                      const odt_cfloat* kernel_trans, const odt_cfloat* kernel_ref,
+                      const float* pupil_in, const float* pupil_out, odt_handle* out);
+
+/* Upload the scattering potential V = RI2potential(RI) - i*eps_imag on the
+ * padded grid [sim_size] (CudaBorn action 1, main.cpp:102-138;
+ * FORWARD_SOLVER_CONVERGENT_BORN.m:199-222). */
+odt_status odt_set_potential(odt_handle h, const odt_potential_params* pp,
+                             const odt_cfloat* V);
+
+/* Solve n_ill illuminations (CudaBorn action 4, main.cpp:175-210, plus the
+ * MATLAB pre/post-processing of FORWARD_SOLVER_CONVERGENT_BORN.solve,
+ * :397-520): fft2 + pupil_in, refocus into the volume, Born series, emitter
+ * projection, + incident field, pupil_out, ifft2.  Synchronous for host
+ * pointers; for device pointers the work is ordered on `stream` and the call
+ * returns after enqueueing it. */
+odt_status odt_solve(odt_handle h, const odt_solve_args* args);
+
+/* Free a solver (CudaBorn action 3, main.cpp:164-174). */
+odt_status odt_destroy(odt_handle h);
+
+/* Number of illuminations the handle keeps resident per batch. */
+odt_status odt_get_batch(odt_handle h, int32_t* batch);
+
+/* Per-kernel timing (CUDA events around every launch on the solve stream).
+ * When enabled, odt_get_kernel_times fills up to `cap` entries of names
+ * (static strings), accumulated milliseconds and launch counts since the
+ * last reset, and returns the number of kernel kinds in *n. */
+odt_status odt_set_profiling(odt_handle h, int32_t enable);
+odt_status odt_get_kernel_times(odt_handle h, const char** names, double* ms,
+                                int64_t* launches, int32_t cap, int32_t* n);
+
+/* Last error message of the calling thread ("" if none). */
+const char* odt_last_error(void);
+
+/* ODT_ABI_VERSION of the loaded library. */
+int32_t odt_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ODT_H_ */

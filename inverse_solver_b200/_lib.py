@@ -1,0 +1,132 @@
+"""ctypes binding of libodt.so (the C ABI declared in include/odt.h).
+
+The shared library is built in-tree (``inverse_solver_b200/libodt.so``).  If
+it is missing or does not load, every entry point raises ``OdtError`` -- there
+is no CPU fallback for the Born loop.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libodt.so")
+
+ODT_MEM_HOST = 0
+ODT_MEM_DEVICE = 1
+
+STATUS_NAMES = {
+    0: "ODT_OK",
+    1: "ODT_ERR_INVALID_ARGUMENT",
+    2: "ODT_ERR_BAD_HANDLE",
+    3: "ODT_ERR_CUDA",
+    4: "ODT_ERR_OUT_OF_MEMORY",
+    5: "ODT_ERR_NOT_READY",
+    6: "ODT_ERR_UNSUPPORTED",
+    7: "ODT_ERR_NUMERIC",
+    8: "ODT_ERR_INTERNAL",
+}
+
+
+class OdtError(RuntimeError):
+    """A libodt call failed; ``status`` is the odt_status code."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+
+
+class Geometry(C.Structure):
+    _fields_ = [
+        ("sim_size", C.c_int32 * 3),
+        ("ri_size", C.c_int32 * 3),
+        ("field_size", C.c_int32 * 2),
+        ("conv_size", C.c_int32 * 2),
+        ("device", C.c_int32),
+        ("max_batch", C.c_int32),
+        ("mem_budget", C.c_int64),
+    ]
+
+
+class PotentialParams(C.Structure):
+    _fields_ = [
+        ("eps_imag", C.c_float),
+        ("green_scale", C.c_float),
+        ("green_offset", C.c_float),
+        ("dV", C.c_float),
+        ("roi", C.c_int32 * 6),
+        ("bornmax", C.c_int32),
+        ("acyclic", C.c_int32),
+        ("mask", C.c_void_p * 3),
+        ("ramp", C.c_void_p * 3),
+        ("kq2", C.c_void_p * 3),
+    ]
+
+
+class SolveArgs(C.Structure):
+    _fields_ = [
+        ("fields_in", C.c_void_p),
+        ("n_ill", C.c_int32),
+        ("trans", C.c_void_p),
+        ("ref", C.c_void_p),
+        ("field3d", C.c_void_p),
+        ("memory", C.c_int32),
+        ("stream", C.c_void_p),
+    ]
+
+
+# every symbol include/odt.h declares: name -> (restype, argtypes)
+SIGNATURES = {
+    "odt_create": (C.c_int, [C.POINTER(Geometry), C.c_void_p, C.c_void_p, C.c_void_p,
+                             C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]),
+    "odt_set_potential": (C.c_int, [C.c_uint32, C.POINTER(PotentialParams), C.c_void_p]),
+    "odt_solve": (C.c_int, [C.c_uint32, C.POINTER(SolveArgs)]),
+    "odt_destroy": (C.c_int, [C.c_uint32]),
+    "odt_get_batch": (C.c_int, [C.c_uint32, C.POINTER(C.c_int32)]),
+    "odt_set_profiling": (C.c_int, [C.c_uint32, C.c_int32]),
+    "odt_get_kernel_times": (C.c_int, [C.c_uint32, C.POINTER(C.c_char_p),
+                                       C.POINTER(C.c_double), C.POINTER(C.c_int64),
+                                       C.c_int32, C.POINTER(C.c_int32)]),
+    "odt_last_error": (C.c_char_p, []),
+    "odt_abi_version": (C.c_int32, []),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load():
+    """Load libodt.so once and attach signatures; raises OdtError if absent."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise OdtError(8, f"{LIB_PATH} not built (run __graft_entry__.build() or make -C "
+                              "inverse_solver_b200/csrc)")
+        try:
+            lib = C.CDLL(LIB_PATH)
+        except OSError as e:
+            raise OdtError(8, f"cannot load {LIB_PATH}: {e}") from e
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def check(status: int):
+    if status != 0:
+        msg = load().odt_last_error()
+        raise OdtError(status, msg.decode() if msg else "")
+
+
+def ptr(a) -> int:
+    """Address of a numpy array or torch tensor (contiguous)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data

@@ -1,0 +1,91 @@
+// Kernel launchers of the CBS solver (implemented in cbs_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fft_core.cuh"
+
+namespace odt {
+
+// A transform length ready for launch: plan + device twiddle table.
+struct DevFft {
+  FftPlan plan;
+  const float2* tw;  // n entries, device
+  int lgW;           // log2 of pencils per tile
+};
+
+// Everything the Born-loop kernels read.
+struct BornArgs {
+  int px, py, pz;          // padded grid
+  int rx0, ry0, rz0;       // ROI start (0-based)
+  int rx, ry, rz;          // ROI extents
+  long long nvox;          // px*py*pz
+  int nbatch;              // illuminations in flight
+  const float* mask[3];
+  const float2* ramp[3];
+  const float* kq2[3];
+  float eps, c_im, g_scale, g_off, inv_n;
+  int acyclic;
+  float2* T;               // spectral work array  [nvox, nbatch]
+  float2* Fn;              // Field_n             [nvox, nbatch]
+  float2* F;               // Field (running sum)  [nvox, nbatch]
+  const float2* V;         // potential            [nvox]
+  const float2* Einc;      // incident field       [rx*ry*rz, nbatch]
+  float2* Fout;            // Field(ROI)+incident  [rx*ry*rz, nbatch]
+};
+
+enum BornXMode { kBornFirst = 0, kBornMid = 1, kBornLast = 2 };
+
+// x-pass of iteration jj: inverse x-FFT + update of iteration jj-1 (Mid/Last)
+// and source term + forward x-FFT of iteration jj (First/Mid).
+cudaError_t launch_born_x(const BornArgs& a, int mode, int jj, const DevFft& fx, cudaStream_t s);
+// z-pass of iteration jj: forward z-FFT, Green's multiply, inverse z-FFT.
+cudaError_t launch_born_z(const BornArgs& a, int jj, const DevFft& fz, cudaStream_t s);
+
+// Batched FFT along contiguous lines of an [n, nlines] array.  Input element
+// i is gathered from (i + in_shift) % n, output element k scattered to
+// (k + out_shift) % n (in_shift = out_shift = n/2 gives MATLAB's
+// fftshift(fft(ifftshift(x)))).  In-place allowed.
+cudaError_t launch_fft_lines(const float2* in, float2* out, long long nlines, int in_shift,
+                             int out_shift, float scale, bool inverse, const DevFft& f,
+                             cudaStream_t s);
+// Batched FFT along the middle axis of an [n0, n, n2] array.
+cudaError_t launch_fft_cols(const float2* in, float2* out, long long n0, long long n2,
+                            int in_shift, int out_shift, float scale, bool inverse,
+                            const DevFft& f, cudaStream_t s);
+
+// ---- elementwise stages of the field input/output paths
+// out[i] = in[i] * filt[i % plane] ; also copies the product to `keep` if non-null
+cudaError_t launch_mul_plane(const float2* in, float2* out, float2* keep, const float* filt,
+                             long long plane, long long total, cudaStream_t s);
+// zero-padded copy [n0, n1, nb] -> [m0, m1, nb], source element (x, y) lands
+// at (x + o0, y + o1)
+cudaError_t launch_pad2d(const float2* in, float2* out, int n0, int n1, int m0, int m1, int o0,
+                         int o1, long long nb, cudaStream_t s);
+// crop [m0, m1, nb] -> [n0, n1, nb]: out(x, y) = in(x + o0, y + o1)
+cudaError_t launch_crop2d(const float2* in, float2* out, int n0, int n1, int m0, int m1, int o0,
+                          int o1, long long nb, cudaStream_t s);
+// conv[X, Y, z, b] = sk[X, Y, b] * refocus[X, Y, z]
+cudaError_t launch_refocus_expand(const float2* sk, const float2* refocus, float2* conv, int c0,
+                                  int c1, int rz, long long nb, cudaStream_t s);
+// Einc[x, y, z, b] = conv[x + o0, y + o1, z, b]
+cudaError_t launch_crop_volume(const float2* conv, float2* einc, int c0, int c1, int rx, int ry,
+                               int rz, int o0, int o1, long long nb, cudaStream_t s);
+// conv[X, Y, z, b] = (Fout * (V_roi + i eps)) * dV inside the RI footprint, 0 elsewhere
+cudaError_t launch_emitter(const BornArgs& a, float2* conv, int c0, int c1, int o0, int o1,
+                           float dV, cudaStream_t s);
+// tk[X, Y, b] = sum_z conv * Kt ; rk likewise with Kr (either output may be null)
+cudaError_t launch_zreduce(const float2* conv, const float2* Kt, const float2* Kr, float2* tk,
+                           float2* rk, int c0, int c1, int rz, long long nb, cudaStream_t s);
+// out[i] = (x[i] + add[i]) * filt[i % plane]   (add may be null)
+cudaError_t launch_combine(const float2* x, const float2* add, const float* filt, float2* out,
+                           long long plane, long long total, cudaStream_t s);
+// count of non-finite values in [n] (for the numeric watchdog); result on device
+cudaError_t launch_count_nonfinite(const float2* x, long long n, unsigned int* count,
+                                   cudaStream_t s);
+
+// shared-memory bytes a tile kernel needs for length n with 2^lgW pencils
+size_t fft_smem_bytes(int n, int lgW);
+int pick_lgW(int n);
+
+}  // namespace odt

@@ -1,0 +1,282 @@
+// Mixed-radix Stockham FFT building blocks for the CBS hot path.
+//
+// Every 1D transform in the solver runs through these device functions.  A
+// "tile" is a block of W independent pencils of length n held in shared
+// memory as rows: element (i, c) of pencil c lives at s[i * ld + c], with the
+// row pitch ld = W + 1 so that both the column-wise butterfly accesses and the
+// transposed global<->shared staging are bank-conflict free for 8-byte
+// elements.  One pass of radix R reads the tile from `src`, applies the
+// inter-pass twiddles and an R-point DFT in registers, and writes the
+// self-sorting (Stockham) output to `dst`; passes ping-pong between two tiles,
+// so no bit reversal is ever needed and the result is in natural order.
+//
+// Twiddles come from a table tw[k] = exp(-2*pi*i*k/n), k < n, computed in
+// double on the host and rounded once to float (the accuracy of the table
+// bounds the accuracy of the transform; nothing here calls sin/cos).
+//
+// Radices: 2, 4, 8 (closed-form butterflies) and any odd R <= 31 through the
+// symmetric real-coefficient DFT (pairs v[m], v[R-m] so that an odd R-point
+// DFT costs (R-1)^2 real multiply-adds instead of R^2 complex products).
+//
+// The functions are usable from host code as well (plain C++ when not
+// compiled by nvcc) so the pass logic can be checked on a CPU by running each
+// pass with one "thread" -- every pass is a pure src -> dst map, so the
+// sequential schedule is exact.
+#pragma once
+
+#include <cuda_runtime.h>  // float2 / make_float2 for host and device code
+#if defined(__CUDACC__)
+#define ODT_HD __host__ __device__ __forceinline__
+#else
+#define ODT_HD inline
+#endif
+
+namespace odt {
+
+constexpr int kMaxPasses = 8;
+
+// One transform length: radix sequence and where its twiddles live.
+struct FftPlan {
+  int n;
+  int npass;
+  int radix[kMaxPasses];
+  int rclass;  // radix class (largest radix: 0 -> <= 8, 1 -> <= 15, 2 -> <= 31)
+};
+
+ODT_HD float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+ODT_HD float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+ODT_HD float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+ODT_HD float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+ODT_HD float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+// multiply by -i (forward) or +i (inverse)
+template <bool INV>
+ODT_HD float2 rot90(float2 a) {
+  return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+// ---------------------------------------------------------------- butterflies
+template <int R, bool INV>
+struct Butterfly;
+
+template <bool INV>
+struct Butterfly<2, INV> {
+  ODT_HD static void run(float2* v, const float2*, int) {
+    float2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  }
+};
+
+template <bool INV>
+struct Butterfly<4, INV> {
+  ODT_HD static void run(float2* v, const float2*, int) {
+    float2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+    float2 s13 = cadd(v[1], v[3]), d13 = rot90<INV>(csub(v[1], v[3]));
+    v[0] = cadd(s02, s13);
+    v[2] = csub(s02, s13);
+    v[1] = cadd(d02, d13);
+    v[3] = csub(d02, d13);
+  }
+};
+
+template <bool INV>
+struct Butterfly<8, INV> {
+  ODT_HD static void run(float2* v, const float2*, int) {
+    const float h = 0.70710678118654752440f;
+    float2 e[4] = {v[0], v[2], v[4], v[6]};
+    float2 o[4] = {v[1], v[3], v[5], v[7]};
+    Butterfly<4, INV>::run(e, nullptr, 0);
+    Butterfly<4, INV>::run(o, nullptr, 0);
+    // W8^k, k = 1..3 applied to the odd half
+    float2 o1 = INV ? make_float2(h * (o[1].x - o[1].y), h * (o[1].x + o[1].y))
+                    : make_float2(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
+    float2 o2 = rot90<INV>(o[2]);
+    float2 o3 = INV ? make_float2(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y))
+                    : make_float2(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
+    v[0] = cadd(e[0], o[0]);
+    v[4] = csub(e[0], o[0]);
+    v[1] = cadd(e[1], o1);
+    v[5] = csub(e[1], o1);
+    v[2] = cadd(e[2], o2);
+    v[6] = csub(e[2], o2);
+    v[3] = cadd(e[3], o3);
+    v[7] = csub(e[3], o3);
+  }
+};
+
+// Odd R: X[k] = v0 + sum_m a_m cos(2 pi m k / R) -/+ i sum_m b_m sin(2 pi m k / R)
+// with a_m = v[m] + v[R-m], b_m = v[m] - v[R-m]; the cosines and sines are
+// read from the transform's table at multiples of n / R.
+template <int R, bool INV>
+struct OddButterfly {
+  ODT_HD static void run(float2* v, const float2* tw, int n) {
+    constexpr int H = (R - 1) / 2;
+    const int step = n / R;
+    float cs[H + 1], sn[H + 1];
+    cs[0] = 1.f;  // m*k can be a multiple of R when R is composite (9, 15, ...)
+    sn[0] = 0.f;
+#pragma unroll
+    for (int t = 1; t <= H; ++t) {
+      float2 w = tw[t * step];  // exp(-2 pi i t / R)
+      cs[t] = w.x;
+      sn[t] = -w.y;
+    }
+    float2 a[H + 1], b[H + 1];
+    float2 x0 = v[0];
+    float2 sum = v[0];
+#pragma unroll
+    for (int m = 1; m <= H; ++m) {
+      a[m] = cadd(v[m], v[R - m]);
+      b[m] = csub(v[m], v[R - m]);
+      sum = cadd(sum, a[m]);
+    }
+    v[0] = sum;
+#pragma unroll
+    for (int k = 1; k <= H; ++k) {
+      float2 re = x0, im = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int m = 1; m <= H; ++m) {
+        const int t = (m * k) % R;
+        const float c = (t <= H) ? cs[t] : cs[R - t];
+        const float s = (t <= H) ? sn[t] : -sn[R - t];
+        re.x += a[m].x * c;
+        re.y += a[m].y * c;
+        im.x += b[m].x * s;
+        im.y += b[m].y * s;
+      }
+      // forward: X[k] = re - i*im, X[R-k] = re + i*im
+      float2 jim = make_float2(-im.y, im.x);  // i * im
+      if (INV) {
+        v[k] = cadd(re, jim);
+        v[R - k] = csub(re, jim);
+      } else {
+        v[k] = csub(re, jim);
+        v[R - k] = cadd(re, jim);
+      }
+    }
+  }
+};
+
+#define ODT_ODD_BUTTERFLY(R)                                      \
+  template <bool INV>                                             \
+  struct Butterfly<R, INV> {                                      \
+    ODT_HD static void run(float2* v, const float2* tw, int n) {  \
+      OddButterfly<R, INV>::run(v, tw, n);                        \
+    }                                                             \
+  };
+ODT_ODD_BUTTERFLY(3)
+ODT_ODD_BUTTERFLY(5)
+ODT_ODD_BUTTERFLY(7)
+ODT_ODD_BUTTERFLY(9)
+ODT_ODD_BUTTERFLY(11)
+ODT_ODD_BUTTERFLY(13)
+ODT_ODD_BUTTERFLY(15)
+ODT_ODD_BUTTERFLY(17)
+ODT_ODD_BUTTERFLY(19)
+ODT_ODD_BUTTERFLY(23)
+ODT_ODD_BUTTERFLY(25)
+ODT_ODD_BUTTERFLY(27)
+ODT_ODD_BUTTERFLY(29)
+ODT_ODD_BUTTERFLY(31)
+#undef ODT_ODD_BUTTERFLY
+
+// ------------------------------------------------------------------ one pass
+// Stockham radix-R pass over a tile of W pencils (W a power of two, lgW its
+// log2).  ns = product of the radices of the passes already done.  Work item
+// idx -> (column c, butterfly j); thread `tid` of `nthr` takes every nthr-th.
+template <int R, bool INV>
+ODT_HD void stockham_pass(const float2* __restrict__ src, float2* __restrict__ dst,
+                          int n, int ns, int lgW, int ld, const float2* __restrict__ tw,
+                          int tid, int nthr) {
+  const int W = 1 << lgW;
+  const int nb = n / R;
+  const int total = nb << lgW;
+  const int tstride = n / (ns * R);
+  for (int idx = tid; idx < total; idx += nthr) {
+    const int c = idx & (W - 1);
+    const int j = idx >> lgW;
+    const int k = j % ns;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * ld + c];
+    if (ns > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 w = tw[r * k * tstride];
+        if (INV) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    Butterfly<R, INV>::run(v, tw, n);
+    const int d = (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[(d + r * ns) * ld + c] = v[r];
+  }
+}
+
+// Radix classes: a kernel instantiated for class K only contains the
+// butterflies of that class, so its register budget is set by the largest
+// radix it can meet (class 0: <= 8, 1: <= 15, 2: 17 and 19, 3: <= 31).
+constexpr int kNumRadixClasses = 4;
+inline int radix_class_of(int r) { return r <= 8 ? 0 : (r <= 15 ? 1 : (r <= 19 ? 2 : 3)); }
+
+template <int CLS, bool INV>
+ODT_HD void run_pass(int R, const float2* src, float2* dst, int n, int ns, int lgW, int ld,
+                     const float2* tw, int tid, int nthr) {
+  switch (R) {
+#define ODT_CASE(r) \
+  case r: stockham_pass<r, INV>(src, dst, n, ns, lgW, ld, tw, tid, nthr); break;
+    ODT_CASE(2) ODT_CASE(3) ODT_CASE(4) ODT_CASE(5) ODT_CASE(8)
+#undef ODT_CASE
+    default:
+      if (CLS >= 1) {
+        switch (R) {
+#define ODT_CASE(r) \
+  case r: stockham_pass<(CLS >= 1 ? r : 2), INV>(src, dst, n, ns, lgW, ld, tw, tid, nthr); break;
+          ODT_CASE(7) ODT_CASE(9) ODT_CASE(11) ODT_CASE(13) ODT_CASE(15)
+#undef ODT_CASE
+          default:
+            if (CLS >= 2) {
+              switch (R) {
+#define ODT_CASE(r) \
+  case r: stockham_pass<(CLS >= 2 ? r : 2), INV>(src, dst, n, ns, lgW, ld, tw, tid, nthr); break;
+                ODT_CASE(17) ODT_CASE(19)
+#undef ODT_CASE
+                default:
+                  if (CLS >= 3) {
+                    switch (R) {
+#define ODT_CASE(r) \
+  case r: stockham_pass<(CLS >= 3 ? r : 2), INV>(src, dst, n, ns, lgW, ld, tw, tid, nthr); break;
+                      ODT_CASE(23) ODT_CASE(25) ODT_CASE(27) ODT_CASE(29) ODT_CASE(31)
+#undef ODT_CASE
+                      default: break;  // unreachable: plans are validated on the host
+                    }
+                  }
+                  break;
+              }
+            }
+            break;
+        }
+      }
+      break;
+  }
+}
+
+// Host-side dispatch helper (the CPU check runs every radix).
+template <bool INV>
+inline void run_pass_any(int R, const float2* src, float2* dst, int n, int ns, int lgW, int ld,
+                         const float2* tw, int tid, int nthr) {
+  run_pass<3, INV>(R, src, dst, n, ns, lgW, ld, tw, tid, nthr);
+}
+
+inline bool radix_supported(int r) {
+  switch (r) {
+    case 2: case 3: case 4: case 5: case 7: case 8: case 9: case 11: case 13: case 15:
+    case 17: case 19: case 23: case 25: case 27: case 29: case 31: return true;
+    default: return false;
+  }
+}
+
+}  // namespace odt

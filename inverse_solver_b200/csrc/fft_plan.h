@@ -1,0 +1,19 @@
+// Host-side FFT planning: radix factorisation and twiddle tables.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "fft_core.cuh"
+
+namespace odt {
+
+// Factor n into supported radices (8s, then 4, then 2, then odd factors,
+// merging small odd primes while the product stays <= 15).  Returns false when
+// n has a prime factor > 31 (those lengths are rejected with a clear error).
+bool make_plan(int n, FftPlan* plan, std::string* why);
+
+// tw[k] = exp(-2 pi i k / n), k = 0..n-1, evaluated in double, rounded once.
+std::vector<float2> make_twiddles(int n);
+
+}  // namespace odt

@@ -1,0 +1,629 @@
+// C ABI of libodt: handle table, device memory plan and the per-batch
+// orchestration of one forward CBS solve (include/odt.h).
+//
+// Data layout in HBM (column-major, interleaved complex64):
+//   static per handle : refocus / kernel_trans / kernel_ref [conv_x, conv_y, ri_z],
+//                       pupils [F_x, F_y], twiddle tables, V [sim] + 1D tables
+//   per batch slot    : one block of max(3*sim, conv_x*conv_y*ri_z) elements
+//                       holding T | Field_n | Field during the Born loop and the
+//                       refocus / emitter planes before and after it, plus
+//                       Einc and Fout [ri], and small 2D planes.
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/odt.h"
+#include "cbs_kernels.cuh"
+#include "fft_plan.h"
+
+namespace odt {
+namespace {
+
+thread_local std::string g_last_error;
+
+odt_status fail(odt_status st, const std::string& msg) {
+  g_last_error = msg;
+  return st;
+}
+
+struct CudaError {
+  cudaError_t err;
+  std::string where;
+};
+
+#define ODT_CUDA(call)                                                  \
+  do {                                                                  \
+    cudaError_t e_ = (call);                                            \
+    if (e_ != cudaSuccess) throw CudaError{e_, std::string(#call)};     \
+  } while (0)
+
+struct ApiError {
+  odt_status st;
+  std::string msg;
+};
+
+[[noreturn]] void raise(odt_status st, const std::string& msg) { throw ApiError{st, msg}; }
+
+// RAII guard restoring the caller's current device (CudaBorn does the same,
+// main.cpp:50-53).
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) ODT_CUDA(cudaSetDevice(dev));
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+const char* const kKindNames[] = {"born_x", "born_y", "born_z", "io_fft", "io_elementwise"};
+enum Kind { kKBornX = 0, kKBornY, kKBornZ, kKIoFft, kKIoElem, kNumKinds };
+
+struct Handle {
+  odt_geometry g{};
+  cudaStream_t own_stream = nullptr;
+  std::vector<void*> allocs;
+  size_t static_bytes = 0;
+  size_t batch_bytes = 0;
+  size_t budget = 0;
+
+  // transform lengths
+  DevFft fx{}, fy{}, fz{}, ffx{}, ffy{}, fcx{}, fcy{};
+
+  // static device data
+  float2* refocus = nullptr;
+  float2* ktrans = nullptr;
+  float2* kref = nullptr;
+  float* pupil_in = nullptr;
+  float* pupil_out = nullptr;
+
+  // potential
+  bool have_potential = false;
+  odt_potential_params pp{};
+  float2* V = nullptr;
+  float* mask[3] = {nullptr, nullptr, nullptr};
+  float2* ramp[3] = {nullptr, nullptr, nullptr};
+  float* kq2[3] = {nullptr, nullptr, nullptr};
+
+  // batch buffers
+  int batch = 0;
+  float2* work = nullptr;
+  float2* einc = nullptr;
+  float2* fout = nullptr;
+  float2* in2d = nullptr;
+  float2* kin = nullptr;
+  float2* c2a = nullptr;
+  float2* c2b = nullptr;
+  float2* out_t = nullptr;
+  float2* out_r = nullptr;
+  unsigned int* d_count = nullptr;
+  std::vector<void*> batch_allocs;
+
+  // profiling
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> ev_kind;
+  size_t ev_used = 0;
+  double kind_ms[kNumKinds] = {0};
+  long long kind_launches[kNumKinds] = {0};
+
+  long long nvox() const { return (long long)g.sim_size[0] * g.sim_size[1] * g.sim_size[2]; }
+  long long nri() const { return (long long)g.ri_size[0] * g.ri_size[1] * g.ri_size[2]; }
+  long long nf() const { return (long long)g.field_size[0] * g.field_size[1]; }
+  long long nc2() const { return (long long)g.conv_size[0] * g.conv_size[1]; }
+  long long nc3() const { return nc2() * g.ri_size[2]; }
+  long long work_elems() const { return std::max(3 * nvox(), nc3()); }
+  size_t slot_bytes() const {
+    return sizeof(float2) * (size_t)(work_elems() + 2 * nri() + 4 * nf() + 2 * nc2());
+  }
+
+  // allocate `count` elements; batch buffers go to batch_allocs, the rest to allocs
+  template <typename T>
+  T* dalloc(size_t count, bool batch_buf) {
+    const size_t nb = count * sizeof(T);
+    const size_t bytes = static_bytes + batch_bytes;
+    if (budget && bytes + nb > budget)
+      raise(ODT_ERR_OUT_OF_MEMORY, "memory budget exceeded (" + std::to_string(bytes + nb) +
+                                       " > " + std::to_string(budget) + " bytes)");
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, nb ? nb : 1);
+    if (e == cudaErrorMemoryAllocation) {
+      cudaGetLastError();
+      raise(ODT_ERR_OUT_OF_MEMORY, "cudaMalloc of " + std::to_string(nb) + " bytes failed");
+    }
+    if (e != cudaSuccess) throw CudaError{e, "cudaMalloc"};
+    (batch_buf ? batch_allocs : allocs).push_back(p);
+    (batch_buf ? batch_bytes : static_bytes) += nb;
+    return static_cast<T*>(p);
+  }
+
+  void free_batch() {
+    for (void* p : batch_allocs) cudaFree(p);
+    batch_allocs.clear();
+    batch_bytes = 0;
+    batch = 0;
+  }
+
+  ~Handle() {
+    for (void* p : batch_allocs) cudaFree(p);
+    for (void* p : allocs) cudaFree(p);
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    if (own_stream) cudaStreamDestroy(own_stream);
+  }
+
+  // ---- profiling helpers
+  void mark_begin(int kind, cudaStream_t s) {
+    if (!profiling) return;
+    if (ev_used + 2 > ev.size()) {
+      for (int i = 0; i < 64; ++i) {
+        cudaEvent_t e;
+        ODT_CUDA(cudaEventCreate(&e));
+        ev.push_back(e);
+      }
+    }
+    ODT_CUDA(cudaEventRecord(ev[ev_used], s));
+    if (ev_kind.size() < ev.size()) ev_kind.resize(ev.size());
+    ev_kind[ev_used] = kind;
+  }
+  void mark_end(cudaStream_t s) {
+    if (!profiling) return;
+    ODT_CUDA(cudaEventRecord(ev[ev_used + 1], s));
+    ev_used += 2;
+  }
+  void collect(cudaStream_t s) {
+    if (!profiling || ev_used == 0) return;
+    ODT_CUDA(cudaStreamSynchronize(s));
+    for (size_t i = 0; i < ev_used; i += 2) {
+      float ms = 0.f;
+      ODT_CUDA(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+      kind_ms[ev_kind[i]] += ms;
+      kind_launches[ev_kind[i]] += 1;
+    }
+    ev_used = 0;
+  }
+};
+
+std::mutex g_mu;
+std::map<uint32_t, std::shared_ptr<Handle>> g_handles;
+std::atomic<uint32_t> g_next_id{1};
+
+std::shared_ptr<Handle> lookup(odt_handle h) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_handles.find(h);
+  if (it == g_handles.end()) raise(ODT_ERR_BAD_HANDLE, "unknown handle " + std::to_string(h));
+  return it->second;
+}
+
+template <typename F>
+odt_status guarded(F&& f) {
+  try {
+    g_last_error.clear();
+    f();
+    return ODT_OK;
+  } catch (const ApiError& e) {
+    return fail(e.st, e.msg);
+  } catch (const CudaError& e) {
+    cudaGetLastError();
+    return fail(e.err == cudaErrorMemoryAllocation ? ODT_ERR_OUT_OF_MEMORY : ODT_ERR_CUDA,
+                e.where + ": " + cudaGetErrorString(e.err));
+  } catch (const std::exception& e) {
+    return fail(ODT_ERR_INTERNAL, e.what());
+  } catch (...) {
+    return fail(ODT_ERR_INTERNAL, "unknown exception");
+  }
+}
+
+DevFft make_dev_fft(Handle& H, int n, const char* what) {
+  DevFft f{};
+  std::string why;
+  if (!make_plan(n, &f.plan, &why)) raise(ODT_ERR_UNSUPPORTED, std::string(what) + ": " + why);
+  f.lgW = pick_lgW(n);
+  int dev = 0;
+  ODT_CUDA(cudaGetDevice(&dev));
+  int max_smem = 0;
+  ODT_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (fft_smem_bytes(n, f.lgW) > (size_t)max_smem)
+    raise(ODT_ERR_UNSUPPORTED, std::string(what) + ": length " + std::to_string(n) +
+                                   " needs more shared memory than the device offers");
+  auto tw = make_twiddles(n);
+  float2* d = H.dalloc<float2>(n, false);
+  ODT_CUDA(cudaMemcpy(d, tw.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+  f.tw = d;
+  return f;
+}
+
+bool is_device_ptr(const void* p) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+void ensure_batch(Handle& H, int nb) {
+  if (H.batch >= nb) return;
+  ODT_CUDA(cudaDeviceSynchronize());  // buffers may still be in use by queued work
+  H.free_batch();
+  H.work = H.dalloc<float2>((size_t)H.work_elems() * nb, true);
+  H.einc = H.dalloc<float2>((size_t)H.nri() * nb, true);
+  H.fout = H.dalloc<float2>((size_t)H.nri() * nb, true);
+  H.in2d = H.dalloc<float2>((size_t)H.nf() * nb, true);
+  H.kin = H.dalloc<float2>((size_t)H.nf() * nb, true);
+  H.out_t = H.dalloc<float2>((size_t)H.nf() * nb, true);
+  H.out_r = H.dalloc<float2>((size_t)H.nf() * nb, true);
+  H.c2a = H.dalloc<float2>((size_t)H.nc2() * nb, true);
+  H.c2b = H.dalloc<float2>((size_t)H.nc2() * nb, true);
+  H.d_count = H.dalloc<unsigned int>(1, true);
+  H.batch = nb;
+}
+
+int auto_batch(Handle& H) {
+  if (H.g.max_batch > 0) return H.g.max_batch;
+  size_t free_b = 0, total_b = 0;
+  ODT_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  const size_t held = H.static_bytes;  // batch buffers are reallocated, not added
+  size_t avail = H.budget ? (H.budget > held ? H.budget - held : 0) : (free_b + H.batch_bytes) / 2;
+  long long nb = (long long)(avail / std::max<size_t>(1, H.slot_bytes()));
+  if (nb > 64) nb = 64;
+  if (nb < 1) raise(ODT_ERR_OUT_OF_MEMORY, "not enough device memory for one illumination");
+  return (int)nb;
+}
+
+// centred 2D FFT on [n0, n1, nslices] in place (MATLAB fftshift(fft2(ifftshift(x))))
+void fftc2(Handle& H, float2* x, const DevFft& f0, const DevFft& f1, long long nslices,
+           bool inverse, cudaStream_t s) {
+  const int n0 = f0.plan.n, n1 = f1.plan.n;
+  const float sc = inverse ? 1.0f / ((float)n0 * (float)n1) : 1.0f;
+  H.mark_begin(kKIoFft, s);
+  ODT_CUDA(launch_fft_lines(x, x, (long long)n1 * nslices, n0 / 2, n0 / 2, 1.0f, inverse, f0, s));
+  ODT_CUDA(launch_fft_cols(x, x, n0, nslices, n1 / 2, n1 / 2, sc, inverse, f1, s));
+  H.mark_end(s);
+}
+
+void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r) {
+  const odt_geometry& g = H.g;
+  const int Fx = g.field_size[0], Fy = g.field_size[1];
+  const int Cx = g.conv_size[0], Cy = g.conv_size[1];
+  const int Rx = g.ri_size[0], Ry = g.ri_size[1], Rz = g.ri_size[2];
+  const long long nF = H.nf();
+  const int ocx = Cx / 2 - Fx / 2, ocy = Cy / 2 - Fy / 2;   // field <-> conv offsets
+  const int orx = Cx / 2 - Rx / 2, ory = Cy / 2 - Ry / 2;   // RI -> conv (padd_RI2conv)
+  float2* conv = H.work;
+
+  // ---- input: fft2 + pupil, back to space, pad, fft2, refocus, ifft2, crop
+  //      (FORWARD_SOLVER_CONVERGENT_BORN.m:416-418, :543-554)
+  fftc2(H, H.in2d, H.ffx, H.ffy, nb, false, s);
+  H.mark_begin(kKIoElem, s);
+  ODT_CUDA(launch_mul_plane(H.in2d, H.in2d, H.kin, H.pupil_in, nF, nF * nb, s));
+  H.mark_end(s);
+  fftc2(H, H.in2d, H.ffx, H.ffy, nb, true, s);
+  H.mark_begin(kKIoElem, s);
+  ODT_CUDA(launch_pad2d(H.in2d, H.c2a, Fx, Fy, Cx, Cy, ocx, ocy, nb, s));
+  H.mark_end(s);
+  fftc2(H, H.c2a, H.fcx, H.fcy, nb, false, s);
+  H.mark_begin(kKIoElem, s);
+  ODT_CUDA(launch_refocus_expand(H.c2a, H.refocus, conv, Cx, Cy, Rz, nb, s));
+  H.mark_end(s);
+  fftc2(H, conv, H.fcx, H.fcy, (long long)Rz * nb, true, s);
+  H.mark_begin(kKIoElem, s);
+  ODT_CUDA(launch_crop_volume(conv, H.einc, Cx, Cy, Rx, Ry, Rz, ocx, ocy, nb, s));
+  H.mark_end(s);
+
+  // ---- Born series (:577-647)
+  BornArgs a{};
+  a.px = g.sim_size[0];
+  a.py = g.sim_size[1];
+  a.pz = g.sim_size[2];
+  a.rx0 = H.pp.roi[0] - 1;
+  a.ry0 = H.pp.roi[2] - 1;
+  a.rz0 = H.pp.roi[4] - 1;
+  a.rx = Rx;
+  a.ry = Ry;
+  a.rz = Rz;
+  a.nvox = H.nvox();
+  a.nbatch = nb;
+  for (int i = 0; i < 3; ++i) {
+    a.mask[i] = H.mask[i];
+    a.ramp[i] = H.ramp[i];
+    a.kq2[i] = H.kq2[i];
+  }
+  a.eps = H.pp.eps_imag;
+  a.c_im = 1.0f / H.pp.eps_imag;
+  a.g_scale = H.pp.green_scale;
+  a.g_off = H.pp.green_offset;
+  a.inv_n = (float)(1.0 / (double)H.nvox());
+  a.acyclic = H.pp.acyclic;
+  a.T = H.work;
+  a.Fn = H.work + (size_t)H.nvox() * nb;
+  a.F = H.work + 2 * (size_t)H.nvox() * nb;
+  a.V = H.V;
+  a.Einc = H.einc;
+  a.Fout = H.fout;
+  const int B = H.pp.bornmax;
+  for (int jj = 1; jj <= B; ++jj) {
+    H.mark_begin(kKBornX, s);
+    ODT_CUDA(launch_born_x(a, jj == 1 ? kBornFirst : kBornMid, jj, H.fx, s));
+    H.mark_end(s);
+    H.mark_begin(kKBornY, s);
+    ODT_CUDA(launch_fft_cols(a.T, a.T, a.px, (long long)a.pz * nb, 0, 0, 1.0f, false, H.fy, s));
+    H.mark_end(s);
+    H.mark_begin(kKBornZ, s);
+    ODT_CUDA(launch_born_z(a, jj, H.fz, s));
+    H.mark_end(s);
+    H.mark_begin(kKBornY, s);
+    ODT_CUDA(launch_fft_cols(a.T, a.T, a.px, (long long)a.pz * nb, 0, 0, 1.0f, true, H.fy, s));
+    H.mark_end(s);
+  }
+  H.mark_begin(kKBornX, s);
+  ODT_CUDA(launch_born_x(a, kBornLast, B + 1, H.fx, s));
+  H.mark_end(s);
+
+  // ---- output projection (:445-511)
+  if (want_t || want_r) {
+    H.mark_begin(kKIoElem, s);
+    ODT_CUDA(launch_emitter(a, conv, Cx, Cy, orx, ory, H.pp.dV, s));
+    H.mark_end(s);
+    fftc2(H, conv, H.fcx, H.fcy, (long long)Rz * nb, false, s);
+    H.mark_begin(kKIoElem, s);
+    ODT_CUDA(launch_zreduce(conv, want_t ? H.ktrans : nullptr, want_r ? H.kref : nullptr,
+                            want_t ? H.c2a : nullptr, want_r ? H.c2b : nullptr, Cx, Cy, Rz, nb, s));
+    H.mark_end(s);
+    for (int w = 0; w < 2; ++w) {
+      if ((w == 0 && !want_t) || (w == 1 && !want_r)) continue;
+      float2* c2 = w == 0 ? H.c2a : H.c2b;
+      float2* o = w == 0 ? H.out_t : H.out_r;
+      fftc2(H, c2, H.fcx, H.fcy, nb, true, s);
+      H.mark_begin(kKIoElem, s);
+      ODT_CUDA(launch_crop2d(c2, o, Fx, Fy, Cx, Cy, ocx, ocy, nb, s));
+      H.mark_end(s);
+      fftc2(H, o, H.ffx, H.ffy, nb, false, s);
+      H.mark_begin(kKIoElem, s);
+      ODT_CUDA(launch_combine(o, w == 0 ? H.kin : nullptr, H.pupil_out, o, nF, nF * nb, s));
+      H.mark_end(s);
+      fftc2(H, o, H.ffx, H.ffy, nb, true, s);
+    }
+  }
+}
+
+}  // namespace
+}  // namespace odt
+
+using namespace odt;
+
+extern "C" {
+
+int32_t odt_abi_version(void) { return ODT_ABI_VERSION; }
+
+const char* odt_last_error(void) { return g_last_error.c_str(); }
+
+odt_status odt_create(const odt_geometry* geom, const odt_cfloat* refocus,
+                      const odt_cfloat* kernel_trans, const odt_cfloat* kernel_ref,
+                      const float* pupil_in, const float* pupil_out, odt_handle* out) {
+  return guarded([&] {
+    if (!geom || !out || !refocus || !pupil_in || !pupil_out)
+      raise(ODT_ERR_INVALID_ARGUMENT, "odt_create: NULL argument");
+    *out = 0;
+    const odt_geometry& g = *geom;
+    for (int i = 0; i < 3; ++i) {
+      if (g.sim_size[i] < 1 || g.ri_size[i] < 1 || g.ri_size[i] > g.sim_size[i])
+        raise(ODT_ERR_INVALID_ARGUMENT, "odt_create: sim_size / ri_size out of range");
+    }
+    for (int i = 0; i < 2; ++i) {
+      if (g.field_size[i] != g.ri_size[i])
+        raise(ODT_ERR_INVALID_ARGUMENT,
+              "odt_create: field_size must equal ri_size(1:2) (the reference's crop_field2RI "
+              "and V(ROI).*source require it)");
+      if (g.conv_size[i] != g.field_size[i] + g.ri_size[i])
+        raise(ODT_ERR_INVALID_ARGUMENT, "odt_create: conv_size must be field_size + ri_size");
+    }
+    if (g.max_batch < 0 || g.mem_budget < 0)
+      raise(ODT_ERR_INVALID_ARGUMENT, "odt_create: negative max_batch / mem_budget");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      raise(ODT_ERR_CUDA, "odt_create: no CUDA device");
+    }
+    if (g.device < 0 || g.device >= ndev)
+      raise(ODT_ERR_INVALID_ARGUMENT, "odt_create: device ordinal out of range");
+    DeviceGuard dg(g.device);
+    auto H = std::make_shared<Handle>();
+    H->g = g;
+    H->budget = (size_t)g.mem_budget;
+    ODT_CUDA(cudaStreamCreateWithFlags(&H->own_stream, cudaStreamNonBlocking));
+    H->fx = make_dev_fft(*H, g.sim_size[0], "sim_size(1)");
+    H->fy = make_dev_fft(*H, g.sim_size[1], "sim_size(2)");
+    H->fz = make_dev_fft(*H, g.sim_size[2], "sim_size(3)");
+    H->ffx = make_dev_fft(*H, g.field_size[0], "field_size(1)");
+    H->ffy = make_dev_fft(*H, g.field_size[1], "field_size(2)");
+    H->fcx = make_dev_fft(*H, g.conv_size[0], "conv_size(1)");
+    H->fcy = make_dev_fft(*H, g.conv_size[1], "conv_size(2)");
+    const size_t n3 = (size_t)H->nc3();
+    H->refocus = H->dalloc<float2>(n3, false);
+    ODT_CUDA(cudaMemcpy(H->refocus, refocus, n3 * sizeof(float2), cudaMemcpyHostToDevice));
+    if (kernel_trans) {
+      H->ktrans = H->dalloc<float2>(n3, false);
+      ODT_CUDA(cudaMemcpy(H->ktrans, kernel_trans, n3 * sizeof(float2), cudaMemcpyHostToDevice));
+    }
+    if (kernel_ref) {
+      H->kref = H->dalloc<float2>(n3, false);
+      ODT_CUDA(cudaMemcpy(H->kref, kernel_ref, n3 * sizeof(float2), cudaMemcpyHostToDevice));
+    }
+    const size_t nf = (size_t)H->nf();
+    H->pupil_in = H->dalloc<float>(nf, false);
+    H->pupil_out = H->dalloc<float>(nf, false);
+    ODT_CUDA(cudaMemcpy(H->pupil_in, pupil_in, nf * sizeof(float), cudaMemcpyHostToDevice));
+    ODT_CUDA(cudaMemcpy(H->pupil_out, pupil_out, nf * sizeof(float), cudaMemcpyHostToDevice));
+    H->V = H->dalloc<float2>((size_t)H->nvox(), false);
+    for (int i = 0; i < 3; ++i) {
+      H->mask[i] = H->dalloc<float>(g.sim_size[i], false);
+      H->ramp[i] = H->dalloc<float2>(g.sim_size[i], false);
+      H->kq2[i] = H->dalloc<float>(g.sim_size[i], false);
+    }
+    const uint32_t id = g_next_id++;
+    {
+      std::lock_guard<std::mutex> lk(g_mu);
+      g_handles[id] = H;
+    }
+    *out = id;
+  });
+}
+
+odt_status odt_set_potential(odt_handle h, const odt_potential_params* pp, const odt_cfloat* V) {
+  return guarded([&] {
+    auto H = lookup(h);
+    if (!pp || !V) raise(ODT_ERR_INVALID_ARGUMENT, "odt_set_potential: NULL argument");
+    const odt_geometry& g = H->g;
+    for (int i = 0; i < 3; ++i) {
+      const int lo = pp->roi[2 * i], hi = pp->roi[2 * i + 1];
+      if (lo < 1 || hi > g.sim_size[i] || hi - lo + 1 != g.ri_size[i])
+        raise(ODT_ERR_INVALID_ARGUMENT, "odt_set_potential: ROI does not match ri_size");
+      if (!pp->mask[i] || !pp->kq2[i] || (pp->acyclic && !pp->ramp[i]))
+        raise(ODT_ERR_INVALID_ARGUMENT, "odt_set_potential: NULL table");
+    }
+    if (pp->bornmax < 0) raise(ODT_ERR_INVALID_ARGUMENT, "odt_set_potential: bornmax < 0");
+    if (!(pp->eps_imag > 0.f) || !std::isfinite(pp->eps_imag))
+      raise(ODT_ERR_INVALID_ARGUMENT, "odt_set_potential: eps_imag must be positive and finite");
+    if (!std::isfinite(pp->green_scale) || !std::isfinite(pp->green_offset) ||
+        !std::isfinite(pp->dV))
+      raise(ODT_ERR_INVALID_ARGUMENT, "odt_set_potential: non-finite scalar");
+    DeviceGuard dg(g.device);
+    const size_t nv = (size_t)H->nvox();
+    ODT_CUDA(cudaMemcpy(H->V, V, nv * sizeof(float2), cudaMemcpyHostToDevice));
+    std::vector<float2> one;
+    for (int i = 0; i < 3; ++i) {
+      const size_t n = g.sim_size[i];
+      ODT_CUDA(cudaMemcpy(H->mask[i], pp->mask[i], n * sizeof(float), cudaMemcpyHostToDevice));
+      ODT_CUDA(cudaMemcpy(H->kq2[i], pp->kq2[i], n * sizeof(float), cudaMemcpyHostToDevice));
+      if (pp->acyclic) {
+        ODT_CUDA(cudaMemcpy(H->ramp[i], pp->ramp[i], n * sizeof(float2), cudaMemcpyHostToDevice));
+      } else {
+        one.assign(n, make_float2(1.f, 0.f));
+        ODT_CUDA(cudaMemcpy(H->ramp[i], one.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+      }
+    }
+    H->pp = *pp;
+    for (int i = 0; i < 3; ++i) {  // do not keep caller pointers
+      H->pp.mask[i] = nullptr;
+      H->pp.ramp[i] = nullptr;
+      H->pp.kq2[i] = nullptr;
+    }
+    H->have_potential = true;
+  });
+}
+
+odt_status odt_solve(odt_handle h, const odt_solve_args* args) {
+  return guarded([&] {
+    auto H = lookup(h);
+    if (!args) raise(ODT_ERR_INVALID_ARGUMENT, "odt_solve: NULL args");
+    if (!H->have_potential) raise(ODT_ERR_NOT_READY, "odt_solve: call odt_set_potential first");
+    const odt_solve_args& A = *args;
+    if (A.n_ill < 0) raise(ODT_ERR_INVALID_ARGUMENT, "odt_solve: n_ill < 0");
+    if (A.n_ill == 0) return;
+    if (!A.fields_in) raise(ODT_ERR_INVALID_ARGUMENT, "odt_solve: fields_in is NULL");
+    if (A.memory != ODT_MEM_HOST && A.memory != ODT_MEM_DEVICE)
+      raise(ODT_ERR_INVALID_ARGUMENT, "odt_solve: memory must be ODT_MEM_HOST or ODT_MEM_DEVICE");
+    const bool want_t = A.trans != nullptr, want_r = A.ref != nullptr;
+    if (want_t && !H->ktrans) raise(ODT_ERR_INVALID_ARGUMENT, "odt_solve: created without kernel_trans");
+    if (want_r && !H->kref) raise(ODT_ERR_INVALID_ARGUMENT, "odt_solve: created without kernel_ref");
+    DeviceGuard dg(H->g.device);
+    const bool dev = A.memory == ODT_MEM_DEVICE;
+    if (dev) {
+      if (!is_device_ptr(A.fields_in) || (want_t && !is_device_ptr(A.trans)) ||
+          (want_r && !is_device_ptr(A.ref)) || (A.field3d && !is_device_ptr(A.field3d)))
+        raise(ODT_ERR_INVALID_ARGUMENT, "odt_solve: ODT_MEM_DEVICE with a non-device pointer");
+    }
+    cudaStream_t s = (dev && A.stream) ? (cudaStream_t)A.stream : H->own_stream;
+    const int want_batch = std::min<int>(A.n_ill, auto_batch(*H));
+    ensure_batch(*H, want_batch);
+    const cudaMemcpyKind kin = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const cudaMemcpyKind kout = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    const long long nF = H->nf(), nR = H->nri();
+    ODT_CUDA(cudaMemsetAsync(H->d_count, 0, sizeof(unsigned int), s));
+    for (int b0 = 0; b0 < A.n_ill; b0 += H->batch) {
+      const int nb = std::min(H->batch, A.n_ill - b0);
+      ODT_CUDA(cudaMemcpyAsync(H->in2d, A.fields_in + (size_t)b0 * nF,
+                               (size_t)nb * nF * sizeof(float2), kin, s));
+      run_chunk(*H, nb, s, want_t, want_r);
+      ODT_CUDA(launch_count_nonfinite(H->fout, nR * nb, H->d_count, s));
+      if (A.field3d)
+        ODT_CUDA(cudaMemcpyAsync(A.field3d + (size_t)b0 * nR, H->fout,
+                                 (size_t)nb * nR * sizeof(float2), kout, s));
+      if (want_t)
+        ODT_CUDA(cudaMemcpyAsync(A.trans + (size_t)b0 * nF, H->out_t,
+                                 (size_t)nb * nF * sizeof(float2), kout, s));
+      if (want_r)
+        ODT_CUDA(cudaMemcpyAsync(A.ref + (size_t)b0 * nF, H->out_r,
+                                 (size_t)nb * nF * sizeof(float2), kout, s));
+      if (!dev) ODT_CUDA(cudaStreamSynchronize(s));
+      H->collect(s);
+    }
+    if (!dev) {
+      unsigned int cnt = 0;
+      ODT_CUDA(cudaMemcpy(&cnt, H->d_count, sizeof(cnt), cudaMemcpyDeviceToHost));
+      if (cnt) raise(ODT_ERR_NUMERIC, "odt_solve: " + std::to_string(cnt) +
+                                          " non-finite values in the 3D field (NaN/Inf input?)");
+    }
+  });
+}
+
+odt_status odt_destroy(odt_handle h) {
+  return guarded([&] {
+    std::shared_ptr<Handle> H;
+    {
+      std::lock_guard<std::mutex> lk(g_mu);
+      auto it = g_handles.find(h);
+      if (it == g_handles.end()) raise(ODT_ERR_BAD_HANDLE, "unknown handle " + std::to_string(h));
+      H = it->second;
+      g_handles.erase(it);
+    }
+    DeviceGuard dg(H->g.device);
+    cudaStreamSynchronize(H->own_stream);
+    H.reset();
+  });
+}
+
+odt_status odt_get_batch(odt_handle h, int32_t* batch) {
+  return guarded([&] {
+    auto H = lookup(h);
+    if (!batch) raise(ODT_ERR_INVALID_ARGUMENT, "odt_get_batch: NULL");
+    *batch = H->batch;
+  });
+}
+
+odt_status odt_set_profiling(odt_handle h, int32_t enable) {
+  return guarded([&] {
+    auto H = lookup(h);
+    H->profiling = enable != 0;
+    for (int i = 0; i < kNumKinds; ++i) {
+      H->kind_ms[i] = 0;
+      H->kind_launches[i] = 0;
+    }
+    H->ev_used = 0;
+  });
+}
+
+odt_status odt_get_kernel_times(odt_handle h, const char** names, double* ms, int64_t* launches,
+                                int32_t cap, int32_t* n) {
+  return guarded([&] {
+    auto H = lookup(h);
+    if (!n) raise(ODT_ERR_INVALID_ARGUMENT, "odt_get_kernel_times: NULL count");
+    DeviceGuard dg(H->g.device);
+    H->collect(H->own_stream);
+    *n = kNumKinds;
+    for (int i = 0; i < kNumKinds && i < cap; ++i) {
+      if (names) names[i] = kKindNames[i];
+      if (ms) ms[i] = H->kind_ms[i];
+      if (launches) launches[i] = H->kind_launches[i];
+    }
+  });
+}
+
+}  // extern "C"

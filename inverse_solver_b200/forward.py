@@ -1,0 +1,360 @@
+"""FORWARD_SOLVER_CONVERGENT_BORN on the B200 library.
+
+Same constructor / ``set_RI`` / ``solve`` surface and parameter struct as
+Codes/FORWARD_SOLVER_CONVERGENT_BORN.m; the geometry-dependent setup is done
+on the host in MATLAB single semantics (as the reference's CUDA variant does,
+FORWARD_SOLVER_CONVERGENT_BORN_CUDA.m:18-63) and every illumination is solved
+by libodt (include/odt.h) on the GPU.  There is no CPU path for the solve: if
+the library is missing the constructor raises.
+
+Arrays are numpy arrays indexed like MATLAB, ``a[x, y, z, pol, ill]``.
+"""
+from __future__ import annotations
+
+import copy
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from .optics import (C64, F32, OpticalTool, basic_optical_parameter, centered_fft2,
+                     centered_fftn, mround, potential2ri, ri2potential, truncated_green_plus,
+                     update_struct)
+
+
+def _f32(x):
+    return np.asfortranarray(np.asarray(x, dtype=F32))
+
+
+def _c64(x):
+    return np.asfortranarray(np.asarray(x, dtype=C64))
+
+
+class CBSHostSetup:
+    """Host-side part of FORWARD_SOLVER_CONVERGENT_BORN: everything the MATLAB
+    class computes before the GPU takes over (Green's kernels, pupils, the
+    padded potential and its separable tables).  Needs no GPU."""
+
+    @staticmethod
+    def get_default_parameters(init_params=None):
+        """FORWARD_SOLVER.m:9-20 + FORWARD_SOLVER_CONVERGENT_BORN.m:32-45, plus
+        the CUDA class's ``used_gpu`` (device ordinal) and this library's
+        ``max_batch`` (illuminations resident per launch, 0 = automatic) and
+        ``mem_budget`` (bytes, 0 = half of free HBM)."""
+        p = basic_optical_parameter()
+        p.update(return_transmission=True, return_reflection=False, return_3D=False,
+                 use_GPU=True)
+        p.update(iterations_number=-1, boundary_thickness=[6, 6, 6], boundary_sharpness=1,
+                 verbose=False, acyclic=True, RI_xy_size=[0, 0], RI_center=[0, 0])
+        p.update(used_gpu=0, max_batch=0, mem_budget=0)
+        return update_struct(p, init_params) if init_params else p
+
+    # ------------------------------------------------------------ ctor
+    def __init__(self, params):
+        """Constructor (FORWARD_SOLVER_CONVERGENT_BORN.m:48-133)."""
+        p = self.parameters = copy.deepcopy(params)
+        if p.get("vector_simulation", True):
+            raise NotImplementedError(
+                "vector_simulation=true (dyadic Green's function) is not supported by this "
+                "library yet; pass vector_simulation=false")
+        for key, val in (("used_gpu", 0), ("max_batch", 0), ("mem_budget", 0)):
+            p.setdefault(key, val)
+        self.utility = u = OpticalTool(p)
+        p["RI_xy_size"] = list(p["RI_xy_size"])
+        for i in range(2):
+            if p["RI_xy_size"][i] == 0:
+                p["RI_xy_size"][i] = p["size"][i]
+        self.expected_RI_size = [int(p["RI_xy_size"][0]), int(p["RI_xy_size"][1]), int(p["size"][2])]
+        bt = [float(b) for b in p["boundary_thickness"]]
+        if len(bt) != 3:
+            raise ValueError('Boundary in only one direction is not precise; enter '
+                             '"boundary_thickness" as an array of size 3')
+        self.cyclic_boundary_xy = (bt[0] == 0 and bt[1] == 0
+                                   and self.expected_RI_size[0] == p["size"][0]
+                                   and self.expected_RI_size[1] == p["size"][1])
+        rc = [int(c) for c in p["RI_center"]]
+        if self.cyclic_boundary_xy:                                   # :65-72
+            ru = np.exp(u.refocusing_kernel[:, :, None] * u.image_coor[2][None, None, :])
+            ru = ru * u.NA_circle[:, :, None]
+            fsg = ru / (1j * 4 * math.pi)
+            fsg = fsg * (u.NA_circle / (u.k3 + (~u.NA_circle)))[:, :, None]
+            fsg = fsg / (u.image_res[0] * u.image_res[1])
+            fsg = centered_fft2(fsg, inverse=True)
+        else:                                                         # :74-108
+            ptg = copy.deepcopy(p)
+            ptg["size"] = [p["size"][0] + self.expected_RI_size[0] + rc[0],
+                           p["size"][1] + self.expected_RI_size[1] + rc[1], p["size"][2]]
+            ru = self._crop_shift(truncated_green_plus(ptg, True), rc)
+            ru = centered_fft2(centered_fftn(ru, inverse=True))
+            ru = ru * (u.image_res[0] * u.image_res[1])
+            fsg = self._crop_shift(truncated_green_plus(ptg, False), rc)
+            fsg = centered_fftn(fsg, inverse=True)
+        self.refocusing_util = ru.astype(C64)
+        self.kernel_trans = centered_fft2(np.conj(fsg)).astype(C64)   # :114
+        self.kernel_ref = centered_fft2(fsg).astype(C64)              # :115
+        self.boundary_thickness_pixel = mround(
+            (np.asarray(bt) * p["wavelength"] / p["RI_bg"]) / (np.asarray(p["resolution"], dtype=np.float64) * 2)
+        ).astype(int)                                                 # :129
+        ri = self.expected_RI_size
+        self.sim_size = [ri[i] + 2 * int(self.boundary_thickness_pixel[i]) for i in range(3)]
+        self.field_size = [int(p["size"][0]), int(p["size"][1])]
+        self.conv_size = (list(self.field_size) if self.cyclic_boundary_xy
+                          else [self.field_size[0] + ri[0], self.field_size[1] + ri[1]])
+        self.pupil_in, self.pupil_out = self._pupils()
+
+    @staticmethod
+    def _crop_shift(a, rc):
+        a = a[-min(0, rc[0]):a.shape[0] - max(0, rc[0]), -min(0, rc[1]):a.shape[1] - max(0, rc[1]), :]
+        return np.roll(a, (-rc[0], -rc[1]), axis=(0, 1))
+
+    def _pupils(self):
+        """transform_field_3D / transform_field_2D filters (FORWARD_SOLVER.m:38-97),
+        scalar case, as one real factor each."""
+        u = self.utility
+        NA = u.NA_circle
+        pin = NA.astype(F32)
+        pout = NA.astype(F32)
+        if self.parameters["use_abbe_sine"]:
+            pin[NA] = pin[NA] / np.sqrt(u.cos_theta[NA])
+            pout = (pout * np.sqrt(u.cos_theta)) * NA
+        return pin, pout
+
+    # ------------------------------------------------------------ set_RI
+    def prepare_potential(self, RI):
+        """condition_RI -> create_boundary_RI -> init
+        (FORWARD_SOLVER_CONVERGENT_BORN.m:180-396): fills V, the separable
+        tables and the scalars, and returns the PotentialParams struct plus
+        the arrays it points into (keep them alive until the call returns)."""
+        RI = np.asarray(RI)
+        if list(RI.shape[:3]) != list(self.expected_RI_size) or (RI.ndim > 3 and RI.shape[3] > 1):
+            raise ValueError("The refractive index does not have the expected size : %d %d %d"
+                             % tuple(self.expected_RI_size))
+        RI = RI.reshape(RI.shape[:3]).astype(C64 if np.iscomplexobj(RI) else F32)
+        p = self.parameters
+        lam, nm = p["wavelength"], p["RI_bg"]
+        # condition_RI :199-222
+        self.eps_imag = F32(np.abs(ri2potential(RI.ravel(), lam, nm)).max() * 1.01)
+        btp = [int(b) for b in self.boundary_thickness_pixel]
+        old = RI.shape
+        # create_boundary_RI :223-279
+        RIp = np.pad(ri2potential(RI, lam, nm), [(btp[0], btp[0]), (btp[1], btp[1]), (btp[2], btp[2])])
+        RIp = potential2ri(RIp, lam, nm)
+        self.ROI = [btp[0] + 1, btp[0] + old[0], btp[1] + 1, btp[1] + old[1], btp[2] + 1, btp[2] + old[2]]
+        V_temp = ri2potential(RIp, lam, nm)
+        masks = []
+        for j in range(3):
+            n = V_temp.shape[j]
+            x = (np.abs(np.arange(1, n + 1) - math.floor(n / 2 + 1) + 0.5) - 0.5).astype(F32)
+            x = np.roll(x, -(n // 2)) / (btp[j] - 0.5)
+            v0 = x.copy()
+            v0[np.abs(x) >= 1] = 1
+            v0 = 1 - np.abs(v0)
+            sh = p["boundary_sharpness"]
+            v0[v0 > sh] = sh
+            v0 = v0 / sh
+            if btp[j] == 0:
+                v0[:] = 0
+            masks.append((1 - v0 * 1).astype(F32))
+        self.RI = potential2ri(V_temp, lam, nm)
+        V = (ri2potential(self.RI, lam, nm) - 1j * self.eps_imag).astype(C64)
+        # init :280-396
+        pb = copy.deepcopy(p)
+        pb["size"] = list(V.shape)
+        ub = self.utility_border = OpticalTool(pb)
+        if p["acyclic"] and self.cyclic_boundary_xy:
+            sc = [ub.fourier_coor[0], ub.fourier_coor[1], ub.fourier_coor[2] + ub.fourier_res[2] / 4]
+        elif p["acyclic"]:
+            sc = [ub.fourier_coor[i] + ub.fourier_res[i] / 4 for i in range(3)]
+        else:
+            sc = list(ub.fourier_coor)
+        kq2 = [np.fft.ifftshift(c * c).astype(F32) for c in sc]
+        step = F32(abs(2 * (2 * math.pi * ub.k0_nm) / self.eps_imag))
+        nrm = float(np.linalg.norm(np.asarray(V.shape, dtype=np.float64) * np.asarray(p["resolution"], dtype=np.float64)))
+        bopt = int(math.ceil(float(F32(F32(nrm / step) / 2 + 1)))) * 2
+        it = p["iterations_number"]
+        self.Bornmax = 0 if it == 0 else (bopt * abs(int(it)) if it < 0 else int(it))
+        ramps = []
+        if p["acyclic"]:
+            for j in range(3):
+                n = V.shape[j]
+                if self.boundary_thickness_pixel[0] == 0 and self.boundary_thickness_pixel[1] == 0:
+                    if j < 2:
+                        ramps.append(np.ones(n, dtype=C64))
+                        continue
+                    x = np.exp(-1j * math.pi * (np.arange(1, n + 1) - 1) / n / 2)
+                    ramps.append((x / x[n // 2]).astype(C64))
+                else:
+                    x = np.exp(-1j * math.pi * (np.arange(1, n + 1) - 1) / n / 2).astype(C64)
+                    ramps.append(x / x[n // 2])
+        else:
+            ramps = [np.ones(V.shape[j], dtype=C64) for j in range(3)]
+        pp = _lib.PotentialParams()
+        pp.eps_imag = float(self.eps_imag)
+        pp.green_scale = float(F32(4 * math.pi ** 2))
+        pp.green_offset = float(F32((2 * math.pi * ub.k0_nm) ** 2))
+        pp.dV = float(F32(ub.dV))
+        pp.roi[:] = [int(r) for r in self.ROI]
+        pp.bornmax = int(self.Bornmax)
+        pp.acyclic = 1 if p["acyclic"] else 0
+        keep = [_f32(m) for m in masks] + [_c64(r) for r in ramps] + [_f32(k) for k in kq2]
+        for j in range(3):
+            pp.mask[j] = _lib.ptr(keep[j])
+            pp.ramp[j] = _lib.ptr(keep[3 + j])
+            pp.kq2[j] = _lib.ptr(keep[6 + j])
+        self.V = V
+        self.attenuation_mask1d = masks
+        self.ramp1d = ramps
+        self.kq2 = kq2
+        return pp, keep + [_c64(V)]
+
+    def voxel_iterations(self, n_ill):
+        """Born voxel-iterations of one solve of n_ill illuminations."""
+        return int(np.prod(self.sim_size)) * int(self.Bornmax) * int(n_ill)
+
+
+class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
+    """Convergent Born series forward solver (scalar Green's function) whose
+    per-illumination work runs in libodt on the GPU."""
+
+    def __init__(self, params):
+        """Constructor + CudaBorn action 0 (FORWARD_SOLVER_CONVERGENT_BORN_CUDA.m:18-41)."""
+        self._handle = 0
+        self.lib = _lib.load()
+        super().__init__(params)
+        self._create_handle()
+
+    def _create_handle(self):
+        p = self.parameters
+        ri, sim, field, conv = self.expected_RI_size, self.sim_size, self.field_size, self.conv_size
+        if p["RI_center"][0] != 0 or p["RI_center"][1] != 0 or ri[0] != field[0] or ri[1] != field[1]:
+            raise ValueError("RI_xy_size must equal size(1:2) and RI_center must be [0 0] "
+                             "(the reference's crop_field2RI / V(ROI).*source need it)")
+        g = _lib.Geometry()
+        g.sim_size[:] = sim
+        g.ri_size[:] = ri
+        g.field_size[:] = field
+        g.conv_size[:] = conv
+        g.device = int(p["used_gpu"])
+        g.max_batch = int(p["max_batch"])
+        g.mem_budget = int(p["mem_budget"])
+        self._keep = [_c64(self.refocusing_util), _c64(self.kernel_trans), _c64(self.kernel_ref),
+                      _f32(self.pupil_in), _f32(self.pupil_out)]
+        h = C.c_uint32(0)
+        _lib.check(self.lib.odt_create(C.byref(g), *[_lib.ptr(a) for a in self._keep], C.byref(h)))
+        self._handle = h.value
+        self._keep = None
+
+    def set_RI(self, RI):
+        """set_RI (FORWARD_SOLVER_CONVERGENT_BORN.m:180-198) + CudaBorn action 1
+        (FORWARD_SOLVER_CONVERGENT_BORN_CUDA.m:42-63)."""
+        pp, keep = self.prepare_potential(RI)
+        _lib.check(self.lib.odt_set_potential(self._handle, C.byref(pp), _lib.ptr(keep[-1])))
+
+    # ------------------------------------------------------------ solve
+    def _outputs(self, n_ill, on_device=False):
+        p = self.parameters
+        F = self.field_size
+        R = self.expected_RI_size
+        shp_t = (F[0], F[1], 1, n_ill)
+        shp_3 = (R[0], R[1], R[2], 1, n_ill)
+        mk = (lambda s: np.empty(s, dtype=C64, order="F"))
+        return (mk(shp_t) if p["return_transmission"] else None,
+                mk(shp_t) if p["return_reflection"] else None,
+                mk(shp_3) if p["return_3D"] else None)
+
+    def solve(self, input_field):
+        """solve (FORWARD_SOLVER_CONVERGENT_BORN.m:397-520): input_field is the
+        spatial field [F_x, F_y, 1, n_ill]; returns (fields_trans, fields_ref,
+        fields_3D), each None when its return_* flag is false."""
+        x = np.asarray(input_field)
+        if x.ndim == 2:
+            x = x[:, :, None, None]
+        elif x.ndim == 3:
+            x = x[:, :, :, None]
+        if x.shape[2] > 1:
+            raise ValueError("the source is 2D but parameter indicate a vectorial simulation")
+        if list(x.shape[:2]) != list(self.field_size):
+            raise ValueError("input field must be %d x %d" % tuple(self.field_size))
+        n_ill = x.shape[3]
+        xin = _c64(x)
+        ft, fr, f3 = self._outputs(n_ill)
+        a = _lib.SolveArgs()
+        a.fields_in = _lib.ptr(xin)
+        a.n_ill = n_ill
+        a.trans = _lib.ptr(ft)
+        a.ref = _lib.ptr(fr)
+        a.field3d = _lib.ptr(f3)
+        a.memory = _lib.ODT_MEM_HOST
+        a.stream = None
+        _lib.check(self.lib.odt_solve(self._handle, C.byref(a)))
+        return ft, fr, f3
+
+    def solve_device(self, fields_in, trans=None, ref=None, field3d=None, stream=None):
+        """Device-resident solve: arguments are CUDA tensors (torch) whose memory
+        is the column-major MATLAB layout, e.g. a contiguous complex64 tensor of
+        shape (n_ill, F_y, F_x) for [F_x, F_y, n_ill].  Work is queued on
+        ``stream`` (a torch.cuda.Stream or raw handle; default: the current
+        torch stream) and the call returns without synchronising."""
+        import torch
+
+        if stream is None:
+            stream = torch.cuda.current_stream()
+        sh = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        nF = self.field_size[0] * self.field_size[1]
+        n_ill = fields_in.numel() // nF
+        for t in (fields_in, trans, ref, field3d):
+            if t is not None and (not t.is_cuda or not t.is_contiguous() or t.dtype != torch.complex64):
+                raise ValueError("solve_device expects contiguous complex64 CUDA tensors")
+        a = _lib.SolveArgs()
+        a.fields_in = fields_in.data_ptr()
+        a.n_ill = n_ill
+        a.trans = trans.data_ptr() if trans is not None else None
+        a.ref = ref.data_ptr() if ref is not None else None
+        a.field3d = field3d.data_ptr() if field3d is not None else None
+        a.memory = _lib.ODT_MEM_DEVICE
+        a.stream = sh
+        _lib.check(self.lib.odt_solve(self._handle, C.byref(a)))
+
+    def solve_ptrs(self, fields_in, n_ill, trans=None, ref=None, field3d=None, device=False,
+                   stream=None):
+        """odt_solve on raw addresses (e.g. pinned host tensors); column-major
+        [F_x, F_y, n_ill] / [ri, n_ill] complex64 buffers."""
+        a = _lib.SolveArgs()
+        a.fields_in = fields_in
+        a.n_ill = int(n_ill)
+        a.trans, a.ref, a.field3d = trans, ref, field3d
+        a.memory = _lib.ODT_MEM_DEVICE if device else _lib.ODT_MEM_HOST
+        a.stream = stream
+        _lib.check(self.lib.odt_solve(self._handle, C.byref(a)))
+
+    # ------------------------------------------------------------ misc
+    def batch(self):
+        b = C.c_int32(0)
+        _lib.check(self.lib.odt_get_batch(self._handle, C.byref(b)))
+        return b.value
+
+    def set_profiling(self, on: bool):
+        _lib.check(self.lib.odt_set_profiling(self._handle, 1 if on else 0))
+
+    def kernel_times(self):
+        """{kind: (total ms, launches)} accumulated while profiling was on."""
+        cap = 16
+        names = (C.c_char_p * cap)()
+        ms = (C.c_double * cap)()
+        nl = (C.c_int64 * cap)()
+        n = C.c_int32(0)
+        _lib.check(self.lib.odt_get_kernel_times(self._handle, names, ms, nl, cap, C.byref(n)))
+        return {names[i].decode(): (ms[i], nl[i]) for i in range(min(n.value, cap))}
+
+    def delete(self):
+        """CudaBorn action 3 (FORWARD_SOLVER_CONVERGENT_BORN_CUDA.m:64-68)."""
+        if getattr(self, "_handle", 0):
+            h, self._handle = self._handle, 0
+            _lib.check(self.lib.odt_destroy(h))
+
+    def __del__(self):
+        try:
+            self.delete()
+        except Exception:
+            pass

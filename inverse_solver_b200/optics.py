@@ -1,0 +1,262 @@
+"""Host-side optical setup in MATLAB ``single`` semantics.
+
+These are the geometry-dependent quantities the MATLAB classes compute before
+handing work to the GPU (in the reference's CUDA variant they are computed on
+the host as well: FORWARD_SOLVER_CONVERGENT_BORN_CUDA.m:20 sets use_GPU=false
+for the setup).  Everything runs in float32 / complex64 with double scalars
+converted to single before each operation, which is what MATLAB does for
+single arrays (numpy's weak Python-scalar rule gives the same behaviour).
+
+Arrays are indexed ``a[x, y, z]`` (axis 0 = MATLAB's first dimension).
+"""
+from __future__ import annotations
+
+import copy
+import math
+import os
+
+import numpy as np
+import scipy.fft as sfft
+import scipy.special as ssp
+
+F32 = np.float32
+C64 = np.complex64
+_WORKERS = os.cpu_count() or 1
+
+
+def basic_optical_parameter(init=None):
+    """BASIC_OPTICAL_PARAMETER (sub_code/BASIC_OPTICAL_PARAMETER.m:1-15)."""
+    p = {"size": [100, 100, 100], "wavelength": 0.532, "NA": 1.2, "RI_bg": 1.336,
+         "resolution": [0.1, 0.1, 0.1], "vector_simulation": True, "use_abbe_sine": True}
+    return update_struct(p, init) if init else p
+
+
+def update_struct(base, update):
+    """update_struct (sub_code/update_struct.m:1-16): unknown fields are kept."""
+    out = copy.deepcopy(base)
+    if update:
+        for k, v in update.items():
+            out[k] = copy.deepcopy(v)
+    return out
+
+
+def mround(x):
+    """MATLAB round (half away from zero)."""
+    x = np.asarray(x, dtype=np.float64)
+    return np.sign(x) * np.floor(np.abs(x) + 0.5)
+
+
+def centered_fft2(x, inverse=False):
+    """fftshift(fft2(ifftshift(x))) over the first two axes, single precision."""
+    y = np.fft.ifftshift(x, axes=(0, 1))
+    y = (sfft.ifft2 if inverse else sfft.fft2)(y, axes=(0, 1), workers=_WORKERS)
+    return np.fft.fftshift(y, axes=(0, 1))
+
+
+def centered_fft_axis(x, axis, inverse=False):
+    y = np.fft.ifftshift(x, axes=(axis,))
+    y = (sfft.ifft if inverse else sfft.fft)(y, axis=axis, workers=_WORKERS)
+    return np.fft.fftshift(y, axes=(axis,))
+
+
+def centered_fftn(x, inverse=False):
+    y = np.fft.ifftshift(x)
+    y = (sfft.ifftn if inverse else sfft.fftn)(y, workers=_WORKERS)
+    return np.fft.fftshift(y)
+
+
+class OpticalTool:
+    """DERIVE_OPTICAL_TOOL (sub_code/DERIVE_OPTICAL_TOOL.m:1-81)."""
+
+    def __init__(self, params):
+        self.image_res = [float(r) for r in params["resolution"]]
+        self.size = [int(s) for s in params["size"]]
+        self.image_coor, self.fourier_coor, self.fourier_res = [], [], []
+        for i in range(3):
+            n = self.size[i]
+            idx = np.arange(1, n + 1, dtype=F32) - F32(n // 2 + 1)
+            self.image_coor.append(idx * self.image_res[i])
+            fr = 1.0 / (self.image_res[i] * n)
+            self.fourier_res.append(fr)
+            self.fourier_coor.append(idx * fr)
+        c0, c1 = self.fourier_coor[0], self.fourier_coor[1]
+        self.coorxy = np.sqrt(c0[:, None] ** 2 + c1[None, :] ** 2)
+        lam = float(params["wavelength"])
+        self.k0 = 1.0 / lam
+        self.k0_nm = self.k0 * float(params["RI_bg"])
+        self.kmax = float(params["NA"]) / lam
+        self.NA_circle = self.coorxy < self.kmax
+        k3 = self.k0_nm ** 2 - self.coorxy ** 2
+        k3[k3 < 0] = 0
+        self.k3 = np.sqrt(k3)
+        self.dV = self.image_res[0] * self.image_res[1] * self.image_res[2]
+        self.refocusing_kernel = (1j * 2 * math.pi) * self.k3
+        self.cos_theta = self.k3 / self.k0_nm
+
+
+def ri2potential(RI, wavelength, base_RI):
+    """RI2potential (sub_code/RI2potential.m:1-5)."""
+    k = 2 * math.pi * base_RI * (1.0 / wavelength)
+    RI = np.asarray(RI)
+    if RI.dtype not in (np.float32, np.complex64):
+        RI = RI.astype(C64 if np.iscomplexobj(RI) else F32)
+    return k ** 2 * (RI ** 2 / base_RI ** 2 - 1)
+
+
+def potential2ri(pot, wavelength, base_RI):
+    """potential2RI (sub_code/potential2RI.m:1-5); sqrt of a negative real
+    argument is complex as in MATLAB."""
+    k = 2 * math.pi * base_RI * (1.0 / wavelength)
+    arg = 1 + pot / k ** 2
+    if not np.iscomplexobj(arg) and np.any(arg < 0):
+        arg = arg.astype(C64)
+    return base_RI * np.sqrt(arg)
+
+
+# ------------------------------------------------ truncated Green's function
+def bessel_j(order, x):
+    if order == 0:
+        return ssp.j0(x)
+    if order == 1:
+        return ssp.j1(x)
+    return ssp.jv(order, x)
+
+
+def bessel_zeros(n, N):
+    """First N positive zeros of J_n by the Gauss-Newton iteration with a
+    finite-difference slope of hankel_transform/JnRoots.m:10-36."""
+    eps = np.finfo(np.float64).eps
+
+    def step(r):
+        lo = (1 - eps / 2) * r
+        hi = (1 + eps) * r
+        with np.errstate(invalid="ignore", divide="ignore"):
+            d = np.real(bessel_j(n, r)) * (hi - lo) / np.real(bessel_j(n, hi) - bessel_j(n, lo))
+        d[np.abs(d) > 0.05] = 0.05
+        d[np.isnan(d)] = 0
+        return r - d
+
+    r = n * math.pi / 2 - math.pi / 4 + math.pi * np.arange(1, N + 1, dtype=np.float64)
+    r = step(r)
+    active = np.ones(N, dtype=bool)
+    for _ in range(100):
+        if not active.any():
+            break
+        nr = step(r[active])
+        changed = r[active] != nr
+        r[active] = nr
+        active[active] = changed
+    if n:
+        r = np.concatenate([[0.0], r[r > 0]])[:N]
+    return r
+
+
+class CroppedHankel:
+    """Discrete Hankel transform restricted to the low-k band
+    (hankel_transform/discrete_hankel_croped_fourier.m:19-65)."""
+
+    def __init__(self, max_r, samples, order, cropping):
+        R = F32(max_r)
+        roots = bessel_zeros(order, samples + 1).astype(F32)
+        C = roots[-1]
+        c = roots[:-1]
+        self.r = R / C * c
+        k = c / R
+        self.pos = int(np.argmin(np.abs(k - k.max() * cropping))) + 1
+        p = self.pos
+        I = np.abs(bessel_j(1 + order, c.astype(np.float64)).astype(F32))
+        self.K = 2 * math.pi * R / C * I
+        self.Rv = I / R
+        I = np.sqrt(F32(2) / C) / I
+        b1 = bessel_j(order, (c[:p, None] / C * c[None, :]).astype(np.float64)).astype(F32)
+        b2 = bessel_j(order, (c[:, None] / C * c[None, :p]).astype(np.float64)).astype(F32)
+        self.fwd = I[:p, None] * I[None, :] * b1
+        self.bwd = I[:, None] * I[None, :p] * b2
+        self.k = k[:p]
+
+    def forward(self, vals):
+        return (self.fwd @ (vals / self.Rv[:, None])) * self.K[:self.pos, None]
+
+    def backward(self, vals):
+        return (self.bwd @ (vals / self.K[:self.pos, None])) * self.Rv[:, None]
+
+
+def _nearest_bins(value, grid):
+    """Bracketing sample indices and linear weight of `value` in the sorted
+    `grid` (truncated_green_plus.m:111-129), 1-based like the reference."""
+    g = grid.ravel()
+    n = g.size
+    near = np.ones(value.shape, dtype=np.int64)
+    step = n
+    while step > 1:
+        step = int(math.ceil(step / 2))
+        up = np.minimum(near + step, n)
+        near = np.where(g[up - 1] < value, up, near)
+    near2 = near.copy()
+    near2[g[near - 1] < value] += 1
+    near2[near2 > n] = n
+    with np.errstate(invalid="ignore", divide="ignore"):
+        w = (value - g[near - 1]) / (g[near2 - 1] - g[near - 1])
+    w[near2 == near] = 1
+    return near, near2, w
+
+
+def truncated_green_plus(params, refocus_version=False):
+    """xy-truncated free-space Green's function (or refocusing kernel) on the
+    [size(1), size(2), size(3)] grid, Fourier in xy and z
+    (sub_code/truncated_green_plus.m:1-110)."""
+    req = basic_optical_parameter()
+    req.update(use_GPU=True, oversize_z=10, oversample_xy=20000, oversample_xy_fourier=2,
+               simultanous_process=30)
+    params = update_struct(req, params)
+    res = np.asarray(params["resolution"], dtype=np.float64)
+    out_px = [int(v) for v in params["size"]]
+    crea = np.asarray(out_px, dtype=np.float64) * np.array([math.sqrt(2) * 1.1, math.sqrt(2) * 1.1, 1.0])
+    crea = crea + params["oversize_z"]
+    size_um = crea * res
+    crea[:2] = np.ceil(size_um[:2].max() / res[:2])
+    params["size"] = [int(round(v)) for v in crea]
+    S1, S2, Nz = params["size"]
+    u = OpticalTool(params)
+    ovf = params["oversample_xy_fourier"]
+    samples = params["oversample_xy"] * ovf
+    if samples < math.sqrt(S1 ** 2 + S2 ** 2) * 5:
+        raise ValueError("truncated_green_plus: grid too large for the Hankel sampling")
+    hk = CroppedHankel(1, samples, 0, (math.sqrt(S1 ** 2 + S2 ** 2) * ovf) / (2 * samples))
+    H = hk.r / hk.r.max()
+    H = H * (u.coorxy.max() * ovf)
+    Hk3 = u.k0_nm ** 2 - H ** 2
+    Hk3[Hk3 < 0] = 0
+    Hk3 = np.sqrt(Hk3)
+    Hin = H < u.kmax
+    ratio = (Nz - params["oversize_z"] / 2) / Nz
+    green = np.sinc((Hk3[:, None] - u.fourier_coor[2][None, :]) / u.fourier_res[2] * ratio) * ratio
+    green = green.astype(F32)
+    if refocus_version:
+        green = green * Hin[:, None]
+    else:
+        green = green * Hin[:, None] / (Hk3 + (~Hin))[:, None]
+        green = green / (1j * 4 * math.pi)
+    img = hk.forward(green)
+    nk = hk.k / hk.k.max()
+    band = (nk < 0.9) + (nk < 1) * (nk > 0.9) * (1 - nk) * 10
+    green = hk.backward(img * band.astype(F32)[:, None])
+    near, near2, w = _nearest_bins(u.coorxy, H)
+    out = np.zeros((out_px[0], out_px[1], Nz), dtype=C64)
+    slices = list(range(1, Nz + 1, params["simultanous_process"]))
+    if len(slices) == 1 or slices[-1] != Nz:
+        slices.append(Nz)
+    scale = Nz / (u.image_res[0] * u.image_res[1])
+    r0 = S1 // 2 - out_px[0] // 2
+    r1 = S2 // 2 - out_px[1] // 2
+    for a, b in zip(slices[:-1], slices[1:]):
+        zi = np.arange(a - 1, b)
+        g = green[:, zi]
+        gs = g[near - 1, :] * w[:, :, None] + g[near2 - 1, :] * (1 - w)[:, :, None]
+        gs = centered_fft2(gs * scale, inverse=True)
+        gs = centered_fft2(gs[r0:r0 + out_px[0], r1:r1 + out_px[1], :])
+        out[:, :, zi] = gs
+    out = centered_fft_axis(out, 2, inverse=True)
+    z0 = Nz // 2 - out_px[2] // 2
+    out = out[:, :, z0:z0 + out_px[2]]
+    return centered_fft_axis(out, 2)

@@ -1,0 +1,682 @@
+"""Oracle: CPU restatement of the convergent-Born-series (CBS) forward solver.
+
+TEST INFRASTRUCTURE ONLY -- imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU baseline legs; never by the product package.
+
+Parity unpinned: the reference is MATLAB R2021a (no MATLAB/Octave here, no
+stored outputs in the reference), so this module restates it line by line and
+is pinned by known-answer properties only (see ``oracle/__init__.py``).
+
+Two precisions:
+
+* ``single=True``  -- MATLAB ``single`` semantics: every array op runs in
+  float32 / complex64 and a double scalar meeting a single array is first
+  converted to single (numpy's NEP-50 weak-scalar rule does exactly this for
+  Python floats).  This is "the reference in single precision".
+* ``single=False`` -- the same code in float64 / complex128: the FP64 oracle.
+
+Array convention: numpy arrays indexed ``a[x, y, z, ...]`` where axis 0 is
+MATLAB's first (fastest) dimension.  Column-major memory is only a concern
+at the C-ABI boundary, not here.
+
+The Born loop (``solve_raw``) is restated literally -- separate elementwise
+sweeps, ``fft_flip`` of the Green's function and conjugation of the phase
+ramp on every iteration, full 3D FFTs -- because that unfused form is also
+what the CPU baseline times.
+"""
+from __future__ import annotations
+
+import copy
+import math
+import os
+
+import numpy as np
+import scipy.fft as sfft
+import scipy.special as ssp
+
+_WORKERS = os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------- precision
+class Prec:
+    """float32 (MATLAB single) or float64 working precision."""
+
+    def __init__(self, single: bool):
+        self.single = bool(single)
+        self.r = np.float32 if single else np.float64
+        self.c = np.complex64 if single else np.complex128
+
+    def R(self, x):
+        return np.asarray(x, dtype=self.r)
+
+    def C(self, x):
+        return np.asarray(x, dtype=self.c)
+
+    def S(self, x):
+        """MATLAB ``single(x)`` in single mode, identity cast otherwise."""
+        x = np.asarray(x)
+        if np.iscomplexobj(x):
+            return x.astype(self.c)
+        return x.astype(self.r)
+
+
+def mround(x):
+    """MATLAB ``round``: half away from zero."""
+    x = np.asarray(x, dtype=np.float64)
+    return np.sign(x) * np.floor(np.abs(x) + 0.5)
+
+
+# ------------------------------------------------------------- FFT helpers
+def fftc2(x, inverse=False):
+    """``fftshift(fft2(ifftshift(x)))`` on the first two axes (MATLAB's
+    shifts over the remaining axes cancel because fft2 does not touch them)."""
+    ax = (0, 1)
+    y = np.fft.ifftshift(x, axes=ax)
+    y = (sfft.ifft2 if inverse else sfft.fft2)(y, axes=ax, workers=_WORKERS)
+    return np.fft.fftshift(y, axes=ax)
+
+
+def fftc_axis(x, axis, inverse=False):
+    y = np.fft.ifftshift(x, axes=(axis,))
+    y = (sfft.ifft if inverse else sfft.fft)(y, axis=axis, workers=_WORKERS)
+    return np.fft.fftshift(y, axes=(axis,))
+
+
+def fftcn(x, inverse=False):
+    y = np.fft.ifftshift(x)
+    y = (sfft.ifftn if inverse else sfft.fftn)(y, workers=_WORKERS)
+    return np.fft.fftshift(y)
+
+
+# ------------------------------------------------------------ parameters
+def basic_optical_parameter(init=None):
+    """``sub_code/BASIC_OPTICAL_PARAMETER.m:1-15``."""
+    p = dict(size=[100, 100, 100], wavelength=0.532, NA=1.2, RI_bg=1.336,
+             resolution=[0.1, 0.1, 0.1], vector_simulation=True,
+             use_abbe_sine=True)
+    if init is not None:
+        p = update_struct(p, init)
+    return p
+
+
+def update_struct(base, update):
+    """``sub_code/update_struct.m:1-16`` (unknown fields are copied too)."""
+    out = copy.deepcopy(base)
+    for k, v in update.items():
+        out[k] = copy.deepcopy(v)
+    return out
+
+
+def cbs_default_parameters(init=None):
+    """``FORWARD_SOLVER.m:9-20`` + ``FORWARD_SOLVER_CONVERGENT_BORN.m:32-45``."""
+    p = basic_optical_parameter()
+    p.update(return_transmission=True, return_reflection=False,
+             return_3D=False, use_GPU=True)
+    p.update(iterations_number=-1, boundary_thickness=[6, 6, 6],
+             boundary_sharpness=1, verbose=False, acyclic=True,
+             RI_xy_size=[0, 0], RI_center=[0, 0])
+    if init is not None:
+        p = update_struct(p, init)
+    return p
+
+
+# ------------------------------------------------------ optical utilities
+def derive_optical_tool(params, P: Prec):
+    """``sub_code/DERIVE_OPTICAL_TOOL.m:1-81``."""
+    res = [float(r) for r in params["resolution"]]
+    size = [int(s) for s in params["size"]]
+    u = {}
+    ci, cf, fres = [], [], []
+    for i in range(3):
+        n = size[i]
+        idx = P.R(np.arange(1, n + 1) - (n // 2 + 1))
+        ci.append(idx * res[i])                       # :22-27
+        fres.append(1.0 / (res[i] * n))               # :34-36
+        cf.append(idx * fres[i])                      # :42-47
+    u["image_coor"] = ci
+    u["fourier_coor"] = cf
+    u["fourier_res"] = fres
+    u["image_res"] = res
+    u["size"] = size
+    coorxy = np.sqrt(cf[0][:, None] ** 2 + cf[1][None, :] ** 2)  # :51-53
+    u["coorxy"] = coorxy
+    lam = float(params["wavelength"])
+    u["k0"] = 1.0 / lam
+    u["k0_nm"] = u["k0"] * float(params["RI_bg"])
+    u["nm"] = float(params["RI_bg"])
+    u["kmax"] = float(params["NA"]) / lam
+    u["NA_circle"] = coorxy < u["kmax"]                           # :60
+    k3 = u["k0_nm"] ** 2 - coorxy ** 2                            # :61
+    k3[k3 < 0] = 0
+    k3 = np.sqrt(k3)
+    u["k3"] = k3
+    u["dV"] = res[0] * res[1] * res[2]                            # :62
+    u["refocusing_kernel"] = (1j * 2 * math.pi) * k3              # :64
+    u["cos_theta"] = k3 / u["k0_nm"]                              # :65
+    return u
+
+
+def ri2potential(RI, wavelength, base_RI, P: Prec):
+    """``sub_code/RI2potential.m:1-5``."""
+    k0 = 1.0 / wavelength
+    k = 2 * math.pi * base_RI * k0
+    return P.S(k ** 2 * (RI ** 2 / base_RI ** 2 - 1))
+
+
+def potential2ri(pot, wavelength, base_RI, P: Prec):
+    """``sub_code/potential2RI.m:1-5`` (MATLAB sqrt of a negative real is
+    complex; the real-valued path is the one the configs use)."""
+    k0 = 1.0 / wavelength
+    k = 2 * math.pi * base_RI * k0
+    arg = 1 + pot / k ** 2
+    if not np.iscomplexobj(arg) and np.any(arg < 0):
+        arg = arg.astype(P.c)
+    return P.S(base_RI * np.sqrt(arg))
+
+
+def fft_flip(a, flip_bool, use_shift):
+    """``sub_code/fft_flip.m:1-11``."""
+    for ii, fb in enumerate(flip_bool):
+        if fb:
+            a = np.flip(a, axis=ii)
+            if a.shape[ii] % 2 == 0 or not use_shift:
+                a = np.roll(a, 1, axis=ii)
+    return a
+
+
+# ------------------------------------------------ truncated Green function
+def jn_roots(n, N):
+    """Roots of J_n: ``hankel_transform/JnRoots.m:10-36`` (Gauss-Newton
+    with a finite-difference slope, 100 rounds at most)."""
+    eps = np.finfo(np.float64).eps
+
+    def jv(order, x):
+        return ssp.j0(x) if order == 0 else (ssp.j1(x) if order == 1 else ssp.jv(order, x))
+
+    def step(r):
+        b = (1 - eps / 2) * r
+        f = (1 + eps) * r
+        with np.errstate(invalid="ignore", divide="ignore"):
+            f = np.real(jv(n, r)) * (f - b) / np.real(jv(n, f) - jv(n, b))
+        f[np.abs(f) > 0.05] = 0.05
+        f[np.isnan(f)] = 0
+        return r - f
+
+    r = n * math.pi / 2 - math.pi / 4 + math.pi * np.arange(1, N + 1, dtype=np.float64)
+    r = step(r)
+    m = np.ones(N, dtype=bool)
+    K = 100
+    while m.any() and K:
+        R = step(r[m])
+        k = r[m] != R
+        r[m] = R
+        m[m] = k
+        K -= 1
+    if n:
+        r = np.concatenate([[0.0], r[r > 0]])[:N]
+    return r
+
+
+def _besselj(order, x):
+    if order == 0:
+        return ssp.j0(x)
+    if order == 1:
+        return ssp.j1(x)
+    return ssp.jv(order, x)
+
+
+class DiscreteHankelCroppedFourier:
+    """``hankel_transform/discrete_hankel_croped_fourier.m:19-65``."""
+
+    def __init__(self, max_r, samples, order, cropping, P: Prec):
+        self.P = P
+        n = order
+        R = P.R(max_r)
+        roots = P.S(jn_roots(n, samples + 1))
+        C = roots[-1]
+        c = roots[:-1]
+        self.r = R / C * c                                        # :31
+        k = c / R                                                 # :32
+        self.pos = int(np.argmin(np.abs(k - k.max() * cropping))) + 1   # :34
+        pos = self.pos
+        I = np.abs(P.S(_besselj(1 + n, c.astype(np.float64))))   # :37
+        self.K = 2 * math.pi * R / C * I                          # :38
+        self.Rv = I / R                                           # :39
+        I = np.sqrt(P.R(2) / C) / I                               # :40
+        bess = P.S(_besselj(n, (c[:pos, None] / C * c[None, :]).astype(np.float64)))   # :41
+        bess2 = P.S(_besselj(n, (c[:, None] / C * c[None, :pos]).astype(np.float64)))  # :42
+        self.I2 = I[:, None] * I[None, :pos] * bess2              # :43
+        self.I = I[:pos, None] * I[None, :] * bess                # :44
+        self.k = k[:pos]                                          # :46
+
+    def forward(self, vals):                                      # :54-59
+        return (self.I @ (vals / self.Rv[:, None])) * self.K[:self.pos, None]
+
+    def backward(self, vals):                                     # :60-65
+        return (self.I2 @ (vals / self.K[:self.pos, None])) * self.Rv[:, None]
+
+
+def _bin_search_nearest(value, searched_pos):
+    """``truncated_green_plus.m:111-129`` (1-based indices returned)."""
+    sp = searched_pos.ravel()
+    nearest = np.ones(value.shape, dtype=np.int64)
+    dist = sp.size
+    step_up = dist
+    while step_up > 1:
+        step_up = int(math.ceil(step_up / 2))
+        upper = nearest + step_up
+        upper[upper > dist] = dist
+        flag = sp[upper - 1] < value
+        nearest = np.where(flag, upper, nearest)
+    nearest2 = nearest.copy()
+    sel = sp[nearest - 1] < value
+    nearest2[sel] += 1
+    nearest2[nearest2 > dist] = dist
+    with np.errstate(invalid="ignore", divide="ignore"):
+        blend = (value - sp[nearest - 1]) / (sp[nearest2 - 1] - sp[nearest - 1])
+    blend[nearest2 == nearest] = 1
+    return nearest, nearest2, blend
+
+
+def truncated_green_plus(params, refocus_version, P: Prec):
+    """``sub_code/truncated_green_plus.m:1-110`` (Vico-Greengard style
+    xy-truncated Green's function through a cropped discrete Hankel
+    transform)."""
+    req = basic_optical_parameter()
+    req.update(use_GPU=True, oversize_z=10, oversample_xy=20000,
+               oversample_xy_fourier=2, simultanous_process=30)
+    params = update_struct(req, params)
+    res = np.asarray(params["resolution"], dtype=np.float64)
+    out_px = np.asarray(params["size"], dtype=np.float64)
+    crea_px = out_px * np.array([math.sqrt(2) * 1.1, math.sqrt(2) * 1.1, 1.0]) + params["oversize_z"]
+    crea = crea_px * res
+    max_size = crea[:2].max()
+    crea_px[:2] = np.ceil(max_size / res[:2])
+    params["size"] = [int(round(v)) for v in crea_px]
+    out_px = [int(v) for v in out_px]
+    u = derive_optical_tool(params, P)
+    samples = params["oversample_xy"] * params["oversample_xy_fourier"]
+    S1, S2, Nz = params["size"]
+    if samples < math.sqrt(S1 ** 2 + S2 ** 2) * 5:
+        raise ValueError("the code might not be valid for such big array")
+    hk = DiscreteHankelCroppedFourier(
+        1, samples, 0,
+        (math.sqrt(S1 ** 2 + S2 ** 2) * params["oversample_xy_fourier"]) / (2 * samples), P)
+    H = hk.r
+    H = H / H.max()
+    H = H * (u["coorxy"].max() * params["oversample_xy_fourier"])   # :43
+    Hk3 = u["k0_nm"] ** 2 - H ** 2
+    Hk3[Hk3 < 0] = 0
+    Hk3 = np.sqrt(Hk3)
+    Hcirc = H < u["kmax"]
+    fz = u["fourier_coor"][2]
+    fres3 = u["fourier_res"][2]
+    ratio = (Nz - params["oversize_z"] / 2) / Nz
+    arg = (Hk3[:, None] - fz[None, :]) / fres3 * ratio
+    green = np.sinc(arg) * ratio                                  # :47-49
+    green = P.S(green)
+    if not refocus_version:
+        green = green * Hcirc[:, None] / (Hk3 + (~Hcirc))[:, None]
+        green = green / (1j * 4 * math.pi)
+    else:
+        green = green * Hcirc[:, None]
+    img = hk.forward(green)
+    nk = hk.k / hk.k.max()
+    mask = (nk < 0.9) + (nk < 1) * (nk > 0.9) * (1 - nk) * 10     # :62
+    img = img * P.S(mask)[:, None]
+    green = hk.backward(img)
+    near, near2, blend = _bin_search_nearest(u["coorxy"], H)
+    green_out = np.zeros((out_px[0], out_px[1], Nz), dtype=P.c)
+    slices = list(range(1, Nz + 1, params["simultanous_process"]))
+    if len(slices) == 1 or slices[-1] != Nz:
+        slices.append(Nz)
+    scale = Nz / (u["image_res"][0] * u["image_res"][1])
+    for ii in range(len(slices) - 1):
+        zi = np.arange(slices[ii], slices[ii + 1] + 1)
+        g = green[:, zi - 1]
+        gs = g[near - 1, :] * blend[:, :, None] + g[near2 - 1, :] * (1 - blend)[:, :, None]
+        gs = gs * scale
+        gs = fftc2(gs, inverse=True)
+        rs = [S1 // 2 + 1 - out_px[0] // 2, S2 // 2 + 1 - out_px[1] // 2]
+        gs = gs[rs[0] - 1:rs[0] - 1 + out_px[0], rs[1] - 1:rs[1] - 1 + out_px[1], :]
+        gs = fftc2(gs)
+        green_out[:, :, zi - 1] = gs
+    green_out = fftc_axis(green_out, 2, inverse=True)
+    zs = Nz // 2 + 1 - out_px[2] // 2
+    green_out = green_out[:, :, zs - 1:zs - 1 + out_px[2]]
+    green_out = fftc_axis(green_out, 2)
+    return green_out
+
+
+# ---------------------------------------------------------- the solver
+class ForwardSolverCBS:
+    """Restatement of ``Codes/FORWARD_SOLVER_CONVERGENT_BORN.m`` (scalar
+    Green's function; ``vector_simulation`` must be false)."""
+
+    def __init__(self, params, single=True):
+        """Constructor ``:48-133``."""
+        self.P = P = Prec(single)
+        self.parameters = p = copy.deepcopy(params)
+        if p.get("vector_simulation", False):
+            raise NotImplementedError("dyadic (vector) CBS is not restated")
+        self.utility = derive_optical_tool(p, P)
+        p["RI_xy_size"] = list(p["RI_xy_size"])
+        if p["RI_xy_size"][0] == 0:
+            p["RI_xy_size"][0] = p["size"][0]
+        if p["RI_xy_size"][1] == 0:
+            p["RI_xy_size"][1] = p["size"][1]
+        self.expected_RI_size = [p["RI_xy_size"][0], p["RI_xy_size"][1], p["size"][2]]
+        bt = p["boundary_thickness"]
+        self.cyclic_boundary_xy = (bt[0] == 0 and bt[1] == 0
+                                   and self.expected_RI_size[0] == p["size"][0]
+                                   and self.expected_RI_size[1] == p["size"][1])
+        u = self.utility
+        rc = p["RI_center"]
+        if self.cyclic_boundary_xy:                                   # :65-72
+            ru = np.exp(u["refocusing_kernel"][:, :, None] * u["image_coor"][2][None, None, :])
+            ru = ru * u["NA_circle"][:, :, None]
+            fsg = ru / (1j * 4 * math.pi)
+            fsg = fsg * (u["NA_circle"] / (u["k3"] + (~u["NA_circle"])))[:, :, None]
+            fsg = fsg / (u["image_res"][0] * u["image_res"][1])
+            fsg = fftc2(fsg, inverse=True)
+            self.refocusing_util = ru
+        else:                                                         # :74-108
+            ptg = copy.deepcopy(p)
+            ptg["size"] = [p["size"][0] + self.expected_RI_size[0] + rc[0],
+                           p["size"][1] + self.expected_RI_size[1] + rc[1],
+                           p["size"][2]]
+            ru = truncated_green_plus(ptg, True, P)
+            ru = self._crop_center_shift(ru, rc)
+            ru = fftcn(ru, inverse=True)
+            ru = fftc2(ru)
+            ru = ru * (u["image_res"][0] * u["image_res"][1])
+            self.refocusing_util = ru
+            fsg = truncated_green_plus(ptg, False, P)
+            fsg = self._crop_center_shift(fsg, rc)
+            fsg = fftcn(fsg, inverse=True)
+        self.kernel_trans = fftc2(np.conj(fsg))                       # :114
+        self.kernel_ref = fftc2(fsg)                                  # :115
+        bt = np.asarray(bt, dtype=np.float64)
+        if bt.size != 3:
+            raise ValueError("boundary_thickness must have 3 entries")
+        self.boundary_thickness_pixel = mround(
+            (bt * p["wavelength"] / p["RI_bg"]) / (np.asarray(p["resolution"], dtype=np.float64) * 2)
+        ).astype(int)                                                 # :129
+
+    @staticmethod
+    def _crop_center_shift(a, rc):
+        a = a[-min(0, rc[0]):a.shape[0] - max(0, rc[0]), -min(0, rc[1]):a.shape[1] - max(0, rc[1]), :]
+        return np.roll(a, (-rc[0], -rc[1]), axis=(0, 1))
+
+    # --- padding / cropping helpers :134-179
+    def _conv_size(self):
+        p = self.parameters
+        return [p["size"][0] + self.expected_RI_size[0], p["size"][1] + self.expected_RI_size[1]]
+
+    def padd_RI2conv(self, m):
+        if self.cyclic_boundary_xy:
+            return m
+        C = self._conv_size()
+        rc = self.parameters["RI_center"]
+        add_start = [-(m.shape[i] // 2 - C[i] // 2) + rc[i] for i in range(2)]
+        add_end = [C[i] - m.shape[i] - add_start[i] for i in range(2)]
+        pad = [(add_start[0], add_end[0]), (add_start[1], add_end[1])] + [(0, 0)] * (m.ndim - 2)
+        return np.pad(m, pad)
+
+    def padd_field2conv(self, m):
+        if self.cyclic_boundary_xy:
+            return m
+        C = self._conv_size()
+        add_start = [-(m.shape[i] // 2 - C[i] // 2) for i in range(2)]
+        add_end = [C[i] - m.shape[i] - add_start[i] for i in range(2)]
+        pad = [(add_start[0], add_end[0]), (add_start[1], add_end[1])] + [(0, 0)] * (m.ndim - 2)
+        return np.pad(m, pad)
+
+    def crop_conv2field(self, m):
+        if self.cyclic_boundary_xy:
+            return m
+        sz = self.parameters["size"]
+        s = [m.shape[i] // 2 + 1 - sz[i] // 2 for i in range(2)]
+        return m[s[0] - 1:s[0] - 1 + sz[0], s[1] - 1:s[1] - 1 + sz[1], ...]
+
+    def crop_field2RI(self, m):
+        sz = self.parameters["size"]
+        rc = self.parameters["RI_center"]
+        s = [m.shape[i] // 2 + 1 - sz[i] // 2 + rc[i] for i in range(2)]
+        return m[s[0] - 1:s[0] - 1 + sz[0], s[1] - 1:s[1] - 1 + sz[1], ...]
+
+    def crop_conv2RI(self, m):
+        return self.crop_field2RI(self.crop_conv2field(m))
+
+    # --- set_RI :180-198
+    def set_RI(self, RI):
+        RI = np.asarray(RI)
+        if list(RI.shape[:3]) != list(self.expected_RI_size):
+            raise ValueError("The refractive index does not have the expected size")
+        self.RI = self.P.S(RI)
+        self.condition_RI()
+        self.init()
+
+    def condition_RI(self):
+        """``:199-222`` (scalar potential)."""
+        P, p = self.P, self.parameters
+        pot = ri2potential(self.RI.ravel(), p["wavelength"], p["RI_bg"], P)
+        self.eps_imag = P.S(np.abs(pot).max() * 1.01)                 # :205
+        self.ROI = self.create_boundary_RI()
+        V = ri2potential(self.RI, p["wavelength"], p["RI_bg"], P)
+        self.V = V - 1j * self.eps_imag                               # :215
+        self.V = P.S(self.V)
+
+    def create_boundary_RI(self):
+        """``:223-279``: zero-potential padding, ROI, attenuation mask."""
+        P, p = self.P, self.parameters
+        btp = [int(b) for b in self.boundary_thickness_pixel]  # Python ints keep single ops single
+        old = self.RI.shape
+        RIp = ri2potential(self.RI, p["wavelength"], p["RI_bg"], P)
+        RIp = np.pad(RIp, [(btp[0], btp[0]), (btp[1], btp[1]), (btp[2], btp[2])])
+        RIp = potential2ri(RIp, p["wavelength"], p["RI_bg"], P)
+        ROI = [btp[0] + 1, btp[0] + old[0], btp[1] + 1, btp[1] + old[1], btp[2] + 1, btp[2] + old[2]]
+        V_temp = ri2potential(RIp, p["wavelength"], p["RI_bg"], P)
+        mask = None
+        self.mask1d = []
+        for j1 in range(3):
+            n = V_temp.shape[j1]
+            x = P.R(np.abs(np.arange(1, n + 1) - math.floor(n / 2 + 1) + 0.5) - 0.5)
+            x = np.roll(x, -(n // 2))
+            x = x / (btp[j1] - 0.5)
+            val0 = x.copy()
+            val0[np.abs(x) >= 1] = 1
+            val0 = np.abs(val0)
+            val0 = 1 - val0
+            sh = p["boundary_sharpness"]
+            val0[val0 > sh] = sh
+            val0 = val0 / sh
+            if btp[j1] == 0:
+                val0[:] = 0
+            fac = 1 - val0 * 1
+            self.mask1d.append(fac)
+            shp = [1, 1, 1]
+            shp[j1] = n
+            mask = fac.reshape(shp) if mask is None else mask * fac.reshape(shp)
+        self.attenuation_mask = mask
+        self.RI = potential2ri(V_temp, p["wavelength"], p["RI_bg"], P)
+        return ROI
+
+    def init(self):
+        """``:280-396``: Green's function, phase ramp, iteration count."""
+        P, p = self.P, self.parameters
+        pb = copy.deepcopy(p)
+        pb["size"] = list(self.RI.shape)
+        ub = self.utility_border = derive_optical_tool(pb, P)
+        self.pole_num = 1
+        fc, fr = ub["fourier_coor"], ub["fourier_res"]
+        if p["acyclic"] and self.cyclic_boundary_xy:
+            sc = [fc[0], fc[1], fc[2] + fr[2] / 4]
+        elif p["acyclic"]:
+            sc = [fc[0] + fr[0] / 4, fc[1] + fr[1] / 4, fc[2] + fr[2] / 4]
+        else:
+            sc = list(fc)
+        self.shifted_coordinate = sc
+        k0nm = ub["k0_nm"]
+        step = P.S(abs(2 * (2 * math.pi * k0nm) / self.eps_imag))     # :326
+        nrm = float(np.linalg.norm(np.asarray(self.RI.shape[:3], dtype=np.float64) * np.asarray(p["resolution"], dtype=np.float64)))
+        Bopt = math.ceil(float(P.S(P.S(nrm / step) / 2 + 1))) * 2      # :327
+        it = p["iterations_number"]
+        if it == 0:
+            self.Bornmax = 0
+        elif it < 0:
+            self.Bornmax = Bopt * abs(it)
+        else:
+            self.Bornmax = int(it)
+        A = (sc[0] ** 2)[:, None, None] + (sc[1] ** 2)[None, :, None] + (sc[2] ** 2)[None, None, :]
+        G = 4 * math.pi ** 2 * np.abs(A) - (2 * math.pi * k0nm) ** 2 - 1j * self.eps_imag
+        self.Greenp = P.S(1 / P.S(G))                                # :347-351
+        if p["acyclic"]:
+            if self.boundary_thickness_pixel[0] == 0 and self.boundary_thickness_pixel[1] == 0:
+                n = self.V.shape[2]
+                x = np.exp(-1j * math.pi * (np.arange(1, n + 1) - 1) / n / 2)
+                x = x / x[n // 2]
+                ramp = x.reshape(1, 1, n)
+                self.ramp1d = [np.ones(self.V.shape[0]), np.ones(self.V.shape[1]), x]
+            else:
+                ramp = None
+                self.ramp1d = []
+                for j1 in range(3):
+                    n = self.V.shape[j1]
+                    x = P.S(np.exp(-1j * math.pi * (np.arange(1, n + 1) - 1) / n / 2))
+                    x = x / x[n // 2]
+                    self.ramp1d.append(x)
+                    shp = [1, 1, 1]
+                    shp[j1] = n
+                    ramp = x.reshape(shp) if ramp is None else ramp * x.reshape(shp)
+            self.phase_ramp = P.S(ramp)
+            self.ramp1d = [P.S(r) for r in self.ramp1d]
+        else:
+            self.phase_ramp = np.ones((1, 1, 1), dtype=P.c)
+            self.ramp1d = None
+        self.Greenp = np.fft.ifftshift(self.Greenp)                  # :384
+
+    # --- solve :397-520
+    def transform_field_3D(self, f):
+        """``FORWARD_SOLVER.m:38-68`` (scalar)."""
+        u = self.utility
+        NA = u["NA_circle"]
+        f = f * NA.reshape(NA.shape + (1,) * (f.ndim - 2))
+        if self.parameters["use_abbe_sine"]:
+            filt = self.P.R(NA)
+            filt[NA] = filt[NA] / np.sqrt(u["cos_theta"][NA])
+            f = f * filt.reshape(filt.shape + (1,) * (f.ndim - 2))
+        return f
+
+    def transform_field_2D(self, f):
+        """``FORWARD_SOLVER.m:69-97`` (scalar; the reflection variant
+        ``:98-128`` is identical for one polarisation)."""
+        u = self.utility
+        NA = u["NA_circle"]
+        sh = NA.shape + (1,) * (f.ndim - 2)
+        f = f * NA.reshape(sh)
+        if self.parameters["use_abbe_sine"]:
+            f = f * np.sqrt(u["cos_theta"]).reshape(sh) * NA.reshape(sh)
+        return f
+
+    def solve(self, input_field):
+        P, p = self.P, self.parameters
+        inp = P.S(np.asarray(input_field))
+        if inp.ndim == 2:
+            inp = inp[:, :, None, None]
+        elif inp.ndim == 3:
+            inp = inp[:, :, :, None]
+        if inp.shape[2] != 1:
+            raise ValueError("the source is 2D but parameter indicate a vectorial simulation")
+        inp = fftc2(inp)
+        inp = self.transform_field_3D(inp)
+        R = self.ROI
+        nx, ny, nz = R[1] - R[0] + 1, R[3] - R[2] + 1, R[5] - R[4] + 1
+        nill = inp.shape[3]
+        ft = np.ones((nx, ny, 1, nill), dtype=P.c) if p["return_transmission"] else None
+        fr = np.ones((nx, ny, 1, nill), dtype=P.c) if p["return_reflection"] else None
+        f3 = np.ones((nx, ny, nz, 1, nill), dtype=P.c) if p["return_3D"] else None
+        for k in range(nill):
+            Field = self.solve_raw(inp[:, :, :, k])
+            if p["return_3D"]:
+                f3[:, :, :, 0, k] = Field
+            if p["return_transmission"] or p["return_reflection"]:
+                pot = ri2potential(self.RI[R[0] - 1:R[1], R[2] - 1:R[3], R[4] - 1:R[5]], p["wavelength"], p["RI_bg"], P)
+                em = Field * pot * self.utility_border["dV"]
+                em = self.padd_RI2conv(em)
+                em = fftc2(em)
+            if p["return_transmission"]:
+                t = self.crop_conv2field(fftc2(np.sum(em * self.kernel_trans, axis=2), inverse=True))
+                t = fftc2(t) + inp[:, :, 0, k]
+                t = self.transform_field_2D(t)
+                ft[:, :, 0, k] = fftc2(t, inverse=True)
+            if p["return_reflection"]:
+                r = self.crop_conv2field(fftc2(np.sum(em * self.kernel_ref, axis=2), inverse=True))
+                r = fftc2(r)
+                r = self.transform_field_2D(r)
+                fr[:, :, 0, k] = fftc2(r, inverse=True)
+        return ft, fr, f3
+
+    def refocus_source(self, source):
+        """``solve_raw :543-554``: 2D input spectrum -> 3D incident field."""
+        s = fftc2(source, inverse=True)
+        s = self.padd_field2conv(s)
+        s = fftc2(s)
+        s = s[:, :, None] * self.refocusing_util
+        s = fftc2(s, inverse=True)
+        return self.crop_conv2RI(s)
+
+    def solve_raw(self, source, n_iter=None):
+        """``:521-654``: the Born loop, restated literally.  ``n_iter``
+        truncates the loop (used only to time a bounded CPU sample)."""
+        P = self.P
+        if source.ndim == 3:
+            source = source[:, :, 0]
+        V = self.V
+        shp = V.shape
+        psi = np.zeros(shp, dtype=P.c)
+        Field = np.zeros(shp, dtype=P.c)
+        Field_n = np.zeros(shp, dtype=P.c)
+        source = self.refocus_source(source)
+        incident = source
+        R = self.ROI
+        roi = (slice(R[0] - 1, R[1]), slice(R[2] - 1, R[3]), slice(R[4] - 1, R[5]))
+        source = (V[roi] + 1j * self.eps_imag) * source               # :566
+        Greenp = self.Greenp
+        ramp = self.phase_ramp
+        acyc = self.parameters["acyclic"]
+        c = 1j / self.eps_imag
+        nB = self.Bornmax if n_iter is None else min(n_iter, self.Bornmax)
+        temp = None
+        for jj in range(1, nB + 1):
+            if acyc:
+                Greenp = fft_flip(Greenp, [1, 1, 1], False)
+                ramp = np.conj(ramp)
+            psi[...] = 0
+            if jj in (1, 2):
+                Field_n[...] = 0
+                psi[roi] = c * source / 2
+            else:
+                psi = c * Field_n * V
+            PSI = Greenp * sfft.fftn(psi * ramp, workers=_WORKERS)
+            PSI = sfft.ifftn(PSI, workers=_WORKERS) * np.conj(ramp)
+            if jj not in (1, 2):
+                Field_n = Field_n - psi
+            Field_n = Field_n + V * PSI
+            Field_n = Field_n * self.attenuation_mask
+            if jj == 2:
+                temp = Field
+            Field = Field + Field_n
+            if jj == 3:
+                Field_n = Field_n + temp
+                temp = None
+        return Field[roi] + incident
+
+
+# ---------------------------------------------------------- convenience
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.complex128)
+    b = np.asarray(b, dtype=np.complex128)
+    d = np.linalg.norm((a - b).ravel())
+    n = np.linalg.norm(b.ravel())
+    return float(d / n) if n > 0 else float(d)

@@ -1,0 +1,53 @@
+"""Shared small CBS cases for the tests (sizes the oracle finishes in seconds)."""
+import numpy as np
+
+from inverse_solver_b200.forward import CBSHostSetup
+from inverse_solver_b200.inputs import FIELD_GENERATOR, bead_RI, ring_illumination, sphere_phantom
+
+NM = 1.3355
+LAM = 0.532
+
+
+def params(size, bt, res=0.1, NA=1.2, **kw):
+    p = CBSHostSetup.get_default_parameters(dict(
+        size=list(size), wavelength=LAM, NA=NA, RI_bg=NM, resolution=[res] * 3,
+        vector_simulation=False, boundary_thickness=list(bt)))
+    p.update(kw)
+    return p
+
+
+def cfg1_params(**kw):
+    """64^3 bead, 16-voxel boundary (bt 8.0331 -> 16 px), 0.1 um voxels."""
+    return params([64, 64, 64], [8.0331] * 3, **kw)
+
+
+def cfg1_RI():
+    return bead_RI([64, 64, 64], 50, NM, 1.4607)
+
+
+def normal_field(size, n=1):
+    return np.ones((size[0], size[1], 1, n), dtype=np.complex64)
+
+
+def circle_fields(p, n, seed=0):
+    fg = FIELD_GENERATOR.get_default_parameters(dict(size=p["size"], wavelength=LAM, NA=p["NA"],
+                                                     RI_bg=NM, resolution=p["resolution"],
+                                                     vector_simulation=False,
+                                                     illumination_style="circle",
+                                                     illumination_number=n, seed=seed))
+    return FIELD_GENERATOR(fg).get_fields()
+
+
+# small non-cubic case with odd and prime-factor lengths:
+# size [30, 26, 21], bt [2, 3, 1.5] -> bt_px [4, 6, 3] -> padded [38, 38, 27]
+SMALL_SIZE = [30, 26, 21]
+SMALL_BT = [2, 3, 1.5]
+
+
+def small_params(**kw):
+    return params(SMALL_SIZE, SMALL_BT, **kw)
+
+
+def small_RI(seed=3):
+    return sphere_phantom(SMALL_SIZE, [0.1] * 3, NM, seed=seed, n_spheres=3,
+                          radius_um=(0.4, 1.0))

@@ -1,0 +1,40 @@
+"""C-ABI library checks that need no GPU: it loads, exports every symbol
+include/odt.h declares, and its argument checks fail cleanly."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from inverse_solver_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "odt.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:odt_status|const char\*|int32_t)\s+(odt_\w+)\s*\(", src, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    names = declared_symbols()
+    assert "odt_create" in names and "odt_solve" in names and len(names) >= 9
+    for n in names:
+        assert hasattr(lib, n), n
+        assert n in _lib.SIGNATURES, n
+    assert lib.odt_abi_version() == 1
+
+
+def test_bad_handle_and_null_arguments():
+    lib = _lib.load()
+    st = lib.odt_destroy(123456)
+    assert st == 2
+    assert b"unknown handle" in lib.odt_last_error()
+    assert lib.odt_create(None, None, None, None, None, None, None) == 1
+    assert b"NULL" in lib.odt_last_error()
+    b = C.c_int32(0)
+    assert lib.odt_get_batch(99, C.byref(b)) == 2
+    with pytest.raises(_lib.OdtError) as e:
+        _lib.check(lib.odt_solve(77, None))
+    assert e.value.status == 2
