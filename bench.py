@@ -48,13 +48,13 @@ def workload_params():
         vector_simulation=False, return_transmission=True))
 
 
-def workload_inputs(p):
+def workload_inputs(p, n_ill=N_ILL):
     from inverse_solver_b200.inputs import ring_illumination, sphere_phantom
 
     RI = sphere_phantom(GRID, [0.1] * 3, 1.3355, seed=SEED)
     fields = ring_illumination(p)
     assert fields.shape[3] == N_ILL
-    return RI, fields
+    return RI, np.ascontiguousarray(fields[:, :, :, :n_ill])
 
 
 def load_peaks():
@@ -175,19 +175,23 @@ def run_ours(args, rank, world, local_rank):
 
     p = workload_params()
     p["used_gpu"] = local_rank
-    RI, fields = workload_inputs(p)
+    n_ill = args.n_ill
+    RI, fields = workload_inputs(p, n_ill)
     s = FORWARD_SOLVER_CONVERGENT_BORN(p)
     s.set_RI(RI)
     F = s.field_size
-    vox_step = s.voxel_iterations(N_ILL)
+    vox_step = s.voxel_iterations(n_ill)
     dev = torch.device("cuda", local_rank)
     fin = torch.from_numpy(np.ascontiguousarray(fields[:, :, 0, :].transpose(2, 1, 0))).to(dev)
-    tout = torch.empty((N_ILL, F[1], F[0]), dtype=torch.complex64, device=dev)
+    tout = torch.empty((n_ill, F[1], F[0]), dtype=torch.complex64, device=dev)
     stream = torch.cuda.current_stream()
 
     for _ in range(args.warmup):
         s.solve_device(fin, tout, stream=stream)
     torch.cuda.synchronize()
+    if args.profile_run:
+        s.delete()
+        return
 
     # ---- per-kernel times and launch counts (one profiled step, not timed)
     s.set_profiling(True)
@@ -224,14 +228,14 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- e2e through the host C-ABI path with pinned buffers
     hin = torch.from_numpy(np.ascontiguousarray(fields[:, :, 0, :].transpose(2, 1, 0))).pin_memory()
-    hout = torch.empty((N_ILL, F[1], F[0]), dtype=torch.complex64).pin_memory()
-    s.solve_ptrs(hin.data_ptr(), N_ILL, trans=hout.data_ptr())
+    hout = torch.empty((n_ill, F[1], F[0]), dtype=torch.complex64).pin_memory()
+    s.solve_ptrs(hin.data_ptr(), n_ill, trans=hout.data_ptr())
     if dist:
         dist.barrier()
     e2e_steps = max(1, args.steps)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        s.solve_ptrs(hin.data_ptr(), N_ILL, trans=hout.data_ptr())
+        s.solve_ptrs(hin.data_ptr(), n_ill, trans=hout.data_ptr())
     e2e_s = time.perf_counter() - t0
     te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
     if dist:
@@ -260,7 +264,7 @@ def run_ours(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
         "config": {"workload": workload_name(), "grid": GRID, "padded_grid": s.sim_size,
-                   "n_ill": N_ILL, "bornmax": s.Bornmax, "voxel_iters_per_step": vox_step,
+                   "n_ill": n_ill, "bornmax": s.Bornmax, "voxel_iters_per_step": vox_step,
                    "batch": s.batch(), "l2": "inputs larger than L2 (per-step working set "
                    f"{3 * 8 * int(np.prod(s.sim_size)) * s.batch() / 1e9:.1f} GB)",
                    "parallelism": f"dp{world} (illuminations, replicas)"},
@@ -296,6 +300,10 @@ def main():
     ap.add_argument("--ref-iters", type=int, default=16,
                     help="Born iterations in the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--n-ill", type=int, default=N_ILL,
+                    help="illuminations per step (profiling runs use fewer)")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="only run --warmup solves (for ncu captures) and exit")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -64,7 +64,8 @@ typedef struct odt_geometry {
   int32_t sim_size[3];   /* padded grid P = RI_size + 2*boundary_thickness_pixel */
   int32_t ri_size[3];    /* RI grid (ROI inside the padded grid)                 */
   int32_t field_size[2]; /* 2D field (params.size(1:2)); must equal ri_size(1:2) */
-  int32_t conv_size[2];  /* field_size + ri_size(1:2): 2D convolution plane      */
+  int32_t conv_size[2];  /* field_size + ri_size(1:2): 2D convolution plane, or
+                            field_size when the xy boundary is cyclic          */
   int32_t device;        /* CUDA device ordinal (CudaBorn's used_gpu)            */
   int32_t max_batch;     /* illuminations resident on the device at once; 0=auto */
   int64_t mem_budget;    /* bytes this handle may allocate; 0 = 90% of free HBM */
@@ -107,7 +108,8 @@ typedef struct odt_solve_args {
   odt_cfloat* ref;             /* [F_x, F_y, n_ill] reflected field            */
   odt_cfloat* field3d;         /* [ri_x, ri_y, ri_z, n_ill] total 3D field     */
   int32_t memory;              /* ODT_MEM_HOST or ODT_MEM_DEVICE               */
-  void* stream;                /* cudaStream_t for ODT_MEM_DEVICE; NULL=own    */
+  void* stream;                /* cudaStream_t for ODT_MEM_DEVICE (NULL = the
+                                  legacy default stream); ignored for host   */
 } odt_solve_args;
 
 /*

@@ -7,12 +7,18 @@
 
 namespace odt {
 
-// A transform length ready for launch: plan + device twiddle table.
+// A transform length ready for launch: plan + device twiddle table + tile
+// shape (pencils per CTA, threads per CTA).
 struct DevFft {
   FftPlan plan;
   const float2* tw;  // n entries, device
-  int lgW;           // log2 of pencils per tile
+  int W;             // pencils per tile (a power of two for column kernels)
+  int lgW;           // log2(W) for column kernels
+  int nthr;          // threads per CTA (a multiple of W for column kernels)
 };
+
+// tile-kernel kinds (shared-memory layouts differ)
+enum FftKind { kKindLines = 0, kKindCols = 1, kKindBornX = 2, kKindBornZ = 3 };
 
 // Everything the Born-loop kernels read.
 struct BornArgs {
@@ -84,8 +90,7 @@ cudaError_t launch_combine(const float2* x, const float2* add, const float* filt
 cudaError_t launch_count_nonfinite(const float2* x, long long n, unsigned int* count,
                                    cudaStream_t s);
 
-// shared-memory bytes a tile kernel needs for length n with 2^lgW pencils
-size_t fft_smem_bytes(int n, int lgW);
-int pick_lgW(int n);
+// shared-memory bytes a tile kernel of `kind` needs for length n and W pencils
+size_t fft_smem_bytes(int n, int W, int kind);
 
 }  // namespace odt

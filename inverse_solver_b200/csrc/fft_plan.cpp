@@ -5,7 +5,7 @@
 
 namespace odt {
 
-bool make_plan(int n, FftPlan* plan, std::string* why) {
+bool make_plan(int n, FftPlan* plan, std::string* why, int order) {
   if (n < 1) {
     if (why) *why = "FFT length must be positive";
     return false;
@@ -36,10 +36,12 @@ bool make_plan(int n, FftPlan* plan, std::string* why) {
       merged.push_back(p);
     }
   }
-  // odd (large) radices first: the first pass has ns == 1 and needs no twiddles
   std::vector<int> all = merged;
   all.insert(all.end(), rad.begin(), rad.end());
   if (all.empty()) all.push_back(1);
+  std::stable_sort(all.begin(), all.end(), [order](int a, int b) {
+    return order == kSmallFirst ? a < b : a > b;
+  });
   if ((int)all.size() > kMaxPasses) {
     if (why) *why = "too many FFT passes for length " + std::to_string(n);
     return false;

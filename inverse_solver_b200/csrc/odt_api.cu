@@ -220,16 +220,29 @@ odt_status guarded(F&& f) {
   }
 }
 
-DevFft make_dev_fft(Handle& H, int n, const char* what) {
+// Tile shape of a transform of length n used by kernels of `kind`: 16 pencils
+// per CTA (8 when n > 512) and 128 threads.
+// Radix order: the fused x-pass applies the CBS update between the last
+// inverse and the first forward pass, i.e. at radix f[0]; a small radix there
+// keeps the update's loads few per thread, and the large radices then sit at
+// the passes that touch global memory (many independent loads in flight).
+DevFft make_dev_fft(Handle& H, int n, int kind, const char* what) {
   DevFft f{};
   std::string why;
-  if (!make_plan(n, &f.plan, &why)) raise(ODT_ERR_UNSUPPORTED, std::string(what) + ": " + why);
-  f.lgW = pick_lgW(n);
+  const int order = kind == kKindBornX ? kSmallFirst : kLargeFirst;
+  if (!make_plan(n, &f.plan, &why, order))
+    raise(ODT_ERR_UNSUPPORTED, std::string(what) + ": " + why);
+  if (f.plan.rclass > 2)
+    raise(ODT_ERR_UNSUPPORTED, std::string(what) + ": length " + std::to_string(n) +
+                                   " has a prime factor > 19 (device kernels take radices <= 19)");
+  f.lgW = n <= 512 ? 4 : 3;
+  f.W = 1 << f.lgW;
+  f.nthr = 128;
   int dev = 0;
   ODT_CUDA(cudaGetDevice(&dev));
   int max_smem = 0;
   ODT_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  if (fft_smem_bytes(n, f.lgW) > (size_t)max_smem)
+  if (fft_smem_bytes(n, f.W, kind) > (size_t)max_smem)
     raise(ODT_ERR_UNSUPPORTED, std::string(what) + ": length " + std::to_string(n) +
                                    " needs more shared memory than the device offers");
   auto tw = make_twiddles(n);
@@ -421,8 +434,10 @@ odt_status odt_create(const odt_geometry* geom, const odt_cfloat* refocus,
         raise(ODT_ERR_INVALID_ARGUMENT,
               "odt_create: field_size must equal ri_size(1:2) (the reference's crop_field2RI "
               "and V(ROI).*source require it)");
-      if (g.conv_size[i] != g.field_size[i] + g.ri_size[i])
-        raise(ODT_ERR_INVALID_ARGUMENT, "odt_create: conv_size must be field_size + ri_size");
+      if (g.conv_size[i] != g.field_size[i] + g.ri_size[i] && g.conv_size[i] != g.field_size[i])
+        raise(ODT_ERR_INVALID_ARGUMENT,
+              "odt_create: conv_size must be field_size + ri_size (or field_size for a "
+              "cyclic xy boundary)");
     }
     if (g.max_batch < 0 || g.mem_budget < 0)
       raise(ODT_ERR_INVALID_ARGUMENT, "odt_create: negative max_batch / mem_budget");
@@ -438,13 +453,13 @@ odt_status odt_create(const odt_geometry* geom, const odt_cfloat* refocus,
     H->g = g;
     H->budget = (size_t)g.mem_budget;
     ODT_CUDA(cudaStreamCreateWithFlags(&H->own_stream, cudaStreamNonBlocking));
-    H->fx = make_dev_fft(*H, g.sim_size[0], "sim_size(1)");
-    H->fy = make_dev_fft(*H, g.sim_size[1], "sim_size(2)");
-    H->fz = make_dev_fft(*H, g.sim_size[2], "sim_size(3)");
-    H->ffx = make_dev_fft(*H, g.field_size[0], "field_size(1)");
-    H->ffy = make_dev_fft(*H, g.field_size[1], "field_size(2)");
-    H->fcx = make_dev_fft(*H, g.conv_size[0], "conv_size(1)");
-    H->fcy = make_dev_fft(*H, g.conv_size[1], "conv_size(2)");
+    H->fx = make_dev_fft(*H, g.sim_size[0], kKindBornX, "sim_size(1)");
+    H->fy = make_dev_fft(*H, g.sim_size[1], kKindCols, "sim_size(2)");
+    H->fz = make_dev_fft(*H, g.sim_size[2], kKindBornZ, "sim_size(3)");
+    H->ffx = make_dev_fft(*H, g.field_size[0], kKindLines, "field_size(1)");
+    H->ffy = make_dev_fft(*H, g.field_size[1], kKindCols, "field_size(2)");
+    H->fcx = make_dev_fft(*H, g.conv_size[0], kKindLines, "conv_size(1)");
+    H->fcy = make_dev_fft(*H, g.conv_size[1], kKindCols, "conv_size(2)");
     const size_t n3 = (size_t)H->nc3();
     H->refocus = H->dalloc<float2>(n3, false);
     ODT_CUDA(cudaMemcpy(H->refocus, refocus, n3 * sizeof(float2), cudaMemcpyHostToDevice));
@@ -540,7 +555,8 @@ odt_status odt_solve(odt_handle h, const odt_solve_args* args) {
           (want_r && !is_device_ptr(A.ref)) || (A.field3d && !is_device_ptr(A.field3d)))
         raise(ODT_ERR_INVALID_ARGUMENT, "odt_solve: ODT_MEM_DEVICE with a non-device pointer");
     }
-    cudaStream_t s = (dev && A.stream) ? (cudaStream_t)A.stream : H->own_stream;
+    // device pointers: the caller's stream as given (NULL = legacy default stream)
+    cudaStream_t s = dev ? (cudaStream_t)A.stream : H->own_stream;
     const int want_batch = std::min<int>(A.n_ill, auto_batch(*H));
     ensure_batch(*H, want_batch);
     const cudaMemcpyKind kin = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;

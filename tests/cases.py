@@ -2,7 +2,7 @@
 import numpy as np
 
 from inverse_solver_b200.forward import CBSHostSetup
-from inverse_solver_b200.inputs import FIELD_GENERATOR, bead_RI, ring_illumination, sphere_phantom
+from inverse_solver_b200.inputs import FIELD_GENERATOR, bead_RI, ring_illumination, sphere_phantom  # noqa: F401
 
 NM = 1.3355
 LAM = 0.532

@@ -2,7 +2,7 @@
 // with a single "thread" on a tile of pencils and prints the result so the
 // Python test can compare it against numpy.  Test infrastructure only.
 //
-// usage: fft_host_check n W inverse   (reads 2*n*W floats from stdin: pencil-
+// usage: fft_host_check n W inverse [order]  (reads 2*n*W floats from stdin: pencil-
 // major interleaved complex input, writes the same layout to stdout)
 #include <cstdio>
 #include <cstdlib>
@@ -12,14 +12,15 @@
 #include "fft_plan.h"
 
 int main(int argc, char** argv) {
-  if (argc != 4) return 2;
+  if (argc != 4 && argc != 5) return 2;
+  const int order = argc == 5 ? std::atoi(argv[4]) : 0;
   int n = std::atoi(argv[1]), W = std::atoi(argv[2]), inv = std::atoi(argv[3]);
   int lgW = 0;
   while ((1 << lgW) < W) ++lgW;
   if ((1 << lgW) != W) return 3;
   odt::FftPlan plan;
   std::string why;
-  if (!odt::make_plan(n, &plan, &why)) {
+  if (!odt::make_plan(n, &plan, &why, order)) {
     std::fprintf(stderr, "%s\n", why.c_str());
     return 4;
   }

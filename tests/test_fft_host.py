@@ -21,10 +21,10 @@ def checker(tmp_path_factory):
     return exe
 
 
-def _run(exe, n, W, inv, x):
+def _run(exe, n, W, inv, x, order=0):
     inp = "\n".join(f"{v.real:.9g} {v.imag:.9g}" for v in x.ravel())
-    r = subprocess.run([exe, str(n), str(W), str(int(inv))], input=inp, capture_output=True,
-                       text=True)
+    r = subprocess.run([exe, str(n), str(W), str(int(inv)), str(order)], input=inp,
+                       capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     return np.array([complex(*map(float, l.split())) for l in r.stdout.split("\n") if l]).reshape(W, n)
 
@@ -35,11 +35,12 @@ SIZES = [1, 2, 3, 5, 8, 9, 12, 16, 19, 24, 27, 29, 31, 64, 88, 96, 120, 128, 144
 
 @pytest.mark.parametrize("n", SIZES)
 @pytest.mark.parametrize("inv", [False, True])
-def test_stockham_matches_numpy(checker, n, inv):
+@pytest.mark.parametrize("order", [0, 1])
+def test_stockham_matches_numpy(checker, n, inv, order):
     rng = np.random.default_rng(n)
     W = 4
     x = (rng.standard_normal((W, n)) + 1j * rng.standard_normal((W, n))).astype(np.complex64)
-    y = _run(checker, n, W, inv, x)
+    y = _run(checker, n, W, inv, x, order)
     xd = x.astype(np.complex128)
     ref = np.fft.ifft(xd, axis=1) * n if inv else np.fft.fft(xd, axis=1)
     err = np.linalg.norm(y - ref) / np.linalg.norm(ref)
