@@ -1,0 +1,140 @@
+// MATLAB MEX gateway over libodt (include/odt.h), call-compatible with the
+// reference's CudaBorn MEX (Codes/CUDA_CODE/main.cpp:27-213):
+//
+//   id = odt_mex(uint32(0), uint32(0), geom, refocus, kernel_trans, kernel_ref, pupil_in, pupil_out)
+//   odt_mex(uint32(1), id, pot, single(V))
+//   [trans, ref, field3d] = odt_mex(uint32(4), id, single complex input [F_x, F_y, 1, n])
+//   odt_mex(uint32(3), id)
+//
+// geom: struct with simulation_size, RI_size, field_size, conv_size, used_gpu
+// (the CudaBorn names), optional max_batch.  pot: struct with eps_imag,
+// green_scale, green_offset, dV, ROI, Bornmax, acyclic, mask1/2/3, ramp1/2/3,
+// kq2_1/2/3.  Complex arrays use the interleaved layout of -R2018a.
+//
+// Build (needs MATLAB's mex.h, not present in this environment):
+//   mex -R2018a odt_mex.cpp -I../../include -L.. -lodt
+#include <mex.h>
+
+#include <cstdint>
+#include <cstring>
+#include <string>
+
+#include "odt.h"
+
+namespace {
+
+double scalar(const mxArray* s, const char* name) {
+  const mxArray* f = mxGetField(s, 0, name);
+  if (!f) mexErrMsgIdAndTxt("odt:param", "missing field %s", name);
+  return mxGetScalar(f);
+}
+
+void ints(const mxArray* s, const char* name, int32_t* out, int n) {
+  const mxArray* f = mxGetField(s, 0, name);
+  if (!f || (int)mxGetNumberOfElements(f) < n) mexErrMsgIdAndTxt("odt:param", "field %s needs %d values", name, n);
+  const double* d = mxGetPr(f);
+  for (int i = 0; i < n; ++i) out[i] = (int32_t)d[i];
+}
+
+const void* array_field(const mxArray* s, const char* name, mxClassID cls, bool cplx) {
+  const mxArray* f = mxGetField(s, 0, name);
+  if (!f || mxGetClassID(f) != cls || (mxIsComplex(f) != cplx))
+    mexErrMsgIdAndTxt("odt:param", "field %s must be %s%s", name, cplx ? "complex " : "",
+                      cls == mxSINGLE_CLASS ? "single" : "double");
+  return cplx ? (const void*)mxGetComplexSingles(f) : (const void*)mxGetSingles(f);
+}
+
+void check(odt_status st) {
+  if (st != ODT_OK) mexErrMsgIdAndTxt("odt:call", "%s", odt_last_error());
+}
+
+uint32_t u32(const mxArray* a) {
+  if (mxGetClassID(a) != mxUINT32_CLASS || mxGetNumberOfElements(a) != 1)
+    mexErrMsgIdAndTxt("odt:arg", "action and id must be uint32 scalars");
+  return *static_cast<const uint32_t*>(mxGetData(a));
+}
+
+const odt_cfloat* csingle(const mxArray* a, const char* what) {
+  if (mxGetClassID(a) != mxSINGLE_CLASS || !mxIsComplex(a))
+    mexErrMsgIdAndTxt("odt:arg", "%s must be complex single", what);
+  return reinterpret_cast<const odt_cfloat*>(mxGetComplexSingles(a));
+}
+
+}  // namespace
+
+void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
+  if (nrhs < 2) mexErrMsgIdAndTxt("odt:arg", "need the action and the id");
+  const uint32_t action = u32(prhs[0]);
+  const uint32_t id = u32(prhs[1]);
+  switch (action) {
+    case 0: {
+      if (nrhs < 8) mexErrMsgIdAndTxt("odt:arg", "create needs geom and five arrays");
+      odt_geometry g{};
+      ints(prhs[2], "simulation_size", g.sim_size, 3);
+      ints(prhs[2], "RI_size", g.ri_size, 3);
+      ints(prhs[2], "field_size", g.field_size, 2);
+      ints(prhs[2], "conv_size", g.conv_size, 2);
+      g.device = (int32_t)scalar(prhs[2], "used_gpu");
+      g.max_batch = mxGetField(prhs[2], 0, "max_batch") ? (int32_t)scalar(prhs[2], "max_batch") : 0;
+      odt_handle h = 0;
+      check(odt_create(&g, csingle(prhs[3], "refocus"), csingle(prhs[4], "kernel_trans"),
+                       csingle(prhs[5], "kernel_ref"), mxGetSingles(prhs[6]), mxGetSingles(prhs[7]), &h));
+      plhs[0] = mxCreateNumericMatrix(1, 1, mxUINT32_CLASS, mxREAL);
+      *static_cast<uint32_t*>(mxGetData(plhs[0])) = h;
+      break;
+    }
+    case 1: {
+      if (nrhs < 4) mexErrMsgIdAndTxt("odt:arg", "set_potential needs pot and V");
+      odt_potential_params pp{};
+      pp.eps_imag = (float)scalar(prhs[2], "eps_imag");
+      pp.green_scale = (float)scalar(prhs[2], "green_scale");
+      pp.green_offset = (float)scalar(prhs[2], "green_offset");
+      pp.dV = (float)scalar(prhs[2], "dV");
+      ints(prhs[2], "ROI", pp.roi, 6);
+      pp.bornmax = (int32_t)scalar(prhs[2], "Bornmax");
+      pp.acyclic = (int32_t)scalar(prhs[2], "acyclic");
+      const char* mk[3] = {"mask1", "mask2", "mask3"};
+      const char* rk[3] = {"ramp1", "ramp2", "ramp3"};
+      const char* kk[3] = {"kq2_1", "kq2_2", "kq2_3"};
+      for (int i = 0; i < 3; ++i) {
+        pp.mask[i] = static_cast<const float*>(array_field(prhs[2], mk[i], mxSINGLE_CLASS, false));
+        pp.ramp[i] = static_cast<const odt_cfloat*>(array_field(prhs[2], rk[i], mxSINGLE_CLASS, true));
+        pp.kq2[i] = static_cast<const float*>(array_field(prhs[2], kk[i], mxSINGLE_CLASS, false));
+      }
+      check(odt_set_potential(id, &pp, csingle(prhs[3], "V")));
+      break;
+    }
+    case 3:
+      check(odt_destroy(id));
+      break;
+    case 4: {
+      if (nrhs < 3) mexErrMsgIdAndTxt("odt:arg", "solve needs the input field");
+      const mwSize* d = mxGetDimensions(prhs[2]);
+      const mwSize nd = mxGetNumberOfDimensions(prhs[2]);
+      const int n_ill = nd >= 4 ? (int)d[3] : 1;
+      int32_t ri[3] = {0, 0, 0};
+      // output sizes follow the input field (field_size == RI_size(1:2))
+      mwSize dt[4] = {d[0], d[1], 1, (mwSize)n_ill};
+      plhs[0] = mxCreateNumericArray(4, dt, mxSINGLE_CLASS, mxCOMPLEX);
+      if (nlhs > 1) plhs[1] = mxCreateNumericArray(4, dt, mxSINGLE_CLASS, mxCOMPLEX);
+      odt_solve_args a{};
+      a.fields_in = csingle(prhs[2], "input field");
+      a.n_ill = n_ill;
+      a.trans = reinterpret_cast<odt_cfloat*>(mxGetComplexSingles(plhs[0]));
+      a.ref = nlhs > 1 ? reinterpret_cast<odt_cfloat*>(mxGetComplexSingles(plhs[1])) : nullptr;
+      if (nlhs > 2) {
+        if (nrhs < 4) mexErrMsgIdAndTxt("odt:arg", "pass RI_size as 4th argument to get field3d");
+        const double* r = mxGetPr(prhs[3]);
+        for (int i = 0; i < 3; ++i) ri[i] = (int32_t)r[i];
+        mwSize d3[5] = {(mwSize)ri[0], (mwSize)ri[1], (mwSize)ri[2], 1, (mwSize)n_ill};
+        plhs[2] = mxCreateNumericArray(5, d3, mxSINGLE_CLASS, mxCOMPLEX);
+        a.field3d = reinterpret_cast<odt_cfloat*>(mxGetComplexSingles(plhs[2]));
+      }
+      a.memory = ODT_MEM_HOST;
+      check(odt_solve(id, &a));
+      break;
+    }
+    default:
+      mexErrMsgIdAndTxt("odt:arg", "unknown action %u", action);
+  }
+}

@@ -30,12 +30,17 @@ def normal_field(size, n=1):
 
 
 def circle_fields(p, n, seed=0):
+    """Normal incidence + plane waves on a circle at 60% of the NA (at 95%,
+    the reference default, the rounded k-pixel of a small grid can fall just
+    outside the NA circle and the pupil removes the illumination)."""
     fg = FIELD_GENERATOR.get_default_parameters(dict(size=p["size"], wavelength=LAM, NA=p["NA"],
                                                      RI_bg=NM, resolution=p["resolution"],
                                                      vector_simulation=False,
                                                      illumination_style="circle",
+                                                     percentage_NA_usage=0.6,
                                                      illumination_number=n, seed=seed))
-    return FIELD_GENERATOR(fg).get_fields()
+    f = FIELD_GENERATOR(fg).get_fields()
+    return f
 
 
 # small non-cubic case with odd and prime-factor lengths:
