@@ -155,6 +155,52 @@ odt_status odt_set_profiling(odt_handle h, int32_t enable);
 odt_status odt_get_kernel_times(odt_handle h, const char** names, double* ms,
                                 int64_t* launches, int32_t cap, int32_t* n);
 
+/*
+ * odt_born_series_noalloc -- no counterpart in the reference.
+ *
+ * The Born-series loop of odt_solve for ONE illumination (the part between
+ * the incident field and Field(ROI) + incident field), for callers that must
+ * not have the library allocate GPU memory: a host framework that owns the
+ * device memory (MATLAB's gpuArray manager, PyTorch's caching allocator) can
+ * see a hidden cudaMalloc fail against its pool or stall every stream on the
+ * device, and a latency-bound request loop must not enter the driver's
+ * allocator mid-request.  This entry point calls no cudaMalloc / cudaFree and
+ * no allocating library routine: every input and output is a caller-owned
+ * device pointer, and the loop's scratch (the spectral array, Field_n, Field
+ * and the FFT twiddles: 3 * prod(sim_size) + sum(sim_size) complex64) lives in
+ * one fixed 64 MiB array that every GPU which loads the library holds until
+ * the process exits.  Grids needing more (more than about 2.79 million padded
+ * voxels, e.g. 152^3) are rejected with ODT_ERR_OUT_OF_MEMORY.
+ *
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * All calls share the one array and it keeps the last call's contents (each
+ * call writes every scratch element before reading it, so nothing needs
+ * clearing); calls that overlap on the GPU -- two host threads, or work on
+ * two streams -- race on it.  The call returns after the work on `stream`
+ * has finished.  Inputs are those odt_set_potential takes (V, the 1D tables,
+ * the scalars), plus the incident field inside the ROI; `fout` receives
+ * Field(ROI) + incident field, as field3d of odt_solve does.
+ */
+typedef struct odt_noalloc_born_args {
+  int32_t sim_size[3];        /* padded grid                                  */
+  int32_t roi[6];             /* 1-based inclusive, as odt_potential_params   */
+  int32_t bornmax;
+  int32_t acyclic;
+  float eps_imag;
+  float green_scale;
+  float green_offset;
+  const float* mask[3];       /* device; length sim_size[a]                   */
+  const odt_cfloat* ramp[3];  /* device; ones when acyclic == 0               */
+  const float* kq2[3];        /* device                                       */
+  const odt_cfloat* V;        /* device [sim_size]                            */
+  const odt_cfloat* einc;     /* device [roi extents] incident field          */
+  odt_cfloat* fout;           /* device [roi extents] result                  */
+  void* stream;               /* cudaStream_t (NULL = legacy default stream)  */
+} odt_noalloc_born_args;
+
+odt_status odt_born_series_noalloc(const odt_noalloc_born_args* args);
+
 /* Last error message of the calling thread ("" if none). */
 const char* odt_last_error(void);
 

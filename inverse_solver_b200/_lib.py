@@ -76,6 +76,25 @@ class SolveArgs(C.Structure):
     ]
 
 
+class NoallocBornArgs(C.Structure):
+    _fields_ = [
+        ("sim_size", C.c_int32 * 3),
+        ("roi", C.c_int32 * 6),
+        ("bornmax", C.c_int32),
+        ("acyclic", C.c_int32),
+        ("eps_imag", C.c_float),
+        ("green_scale", C.c_float),
+        ("green_offset", C.c_float),
+        ("mask", C.c_void_p * 3),
+        ("ramp", C.c_void_p * 3),
+        ("kq2", C.c_void_p * 3),
+        ("V", C.c_void_p),
+        ("einc", C.c_void_p),
+        ("fout", C.c_void_p),
+        ("stream", C.c_void_p),
+    ]
+
+
 # every symbol include/odt.h declares: name -> (restype, argtypes)
 SIGNATURES = {
     "odt_create": (C.c_int, [C.POINTER(Geometry), C.c_void_p, C.c_void_p, C.c_void_p,
@@ -88,6 +107,7 @@ SIGNATURES = {
     "odt_get_kernel_times": (C.c_int, [C.c_uint32, C.POINTER(C.c_char_p),
                                        C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                        C.c_int32, C.POINTER(C.c_int32)]),
+    "odt_born_series_noalloc": (C.c_int, [C.POINTER(NoallocBornArgs)]),
     "odt_last_error": (C.c_char_p, []),
     "odt_abi_version": (C.c_int32, []),
 }

@@ -23,9 +23,18 @@
 #include "fft_plan.h"
 
 namespace odt {
-namespace {
 
+namespace {
 thread_local std::string g_last_error;
+}  // namespace
+
+// used by the entry points defined in other files (noalloc.cu)
+const char* set_last_error(const std::string& msg) {
+  g_last_error = msg;
+  return g_last_error.c_str();
+}
+
+namespace {
 
 odt_status fail(odt_status st, const std::string& msg) {
   g_last_error = msg;
