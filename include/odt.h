@@ -141,6 +141,56 @@ odt_status odt_set_potential(odt_handle h, const odt_potential_params* pp,
  * returns after enqueueing it. */
 odt_status odt_solve(odt_handle h, const odt_solve_args* args);
 
+/*
+ * Adjoint potential for odt_gradient: the potential of conj(flip(RI, 3))
+ * (BACKWARD_SOLVER_MULTI.m:48), same geometry and tables layout as
+ * odt_set_potential.
+ */
+odt_status odt_set_adjoint_potential(odt_handle h, const odt_potential_params* pp,
+                                     const odt_cfloat* V);
+
+/*
+ * Gradient of the transmitted-field misfit (BACKWARD_SOLVER_MULTI.m:30-54),
+ * fused on the device: forward solve (potential of odt_set_potential) ->
+ * diff = trans - fields_meas, err = sum |diff|^2 (accumulated in double) ->
+ * adjoint solve of conj(diff) (potential of odt_set_adjoint_potential) ->
+ * grad = -1i * mean_ill(conj(E_3D) .* flip(conj(A_3D), 3)).
+ * `err` is a host pointer in both memory modes.
+ */
+typedef struct odt_gradient_args {
+  const odt_cfloat* fields_in;    /* [F_x, F_y, n_ill] illuminations            */
+  const odt_cfloat* fields_meas;  /* [F_x, F_y, n_ill] measured transmissions   */
+  int32_t n_ill;
+  odt_cfloat* grad;               /* [ri] output                                 */
+  double* err;                    /* host scalar output                          */
+  int32_t memory;                 /* ODT_MEM_HOST or ODT_MEM_DEVICE              */
+  void* stream;
+} odt_gradient_args;
+
+odt_status odt_gradient(odt_handle h, const odt_gradient_args* args);
+
+/*
+ * Isotropic-TV proximal operator by dual FISTA (sub_code/TV_FISTA_inner_v2.m
+ * :1-53, called from BACKWARD_SOLVER_MULTI.m:152): `inner_itt` iterations on
+ * a [size] array with periodic differences; projections onto
+ * [vmin, vmax] (non_neg), imag >= 0 and imag <= vimag_max.  Real arrays
+ * (is_complex = 0; the reference takes the real part when vimag_max == 0) or
+ * complex64.  Scratch comes from the stream-ordered allocator.
+ */
+typedef struct odt_tv_args {
+  int32_t size[3];
+  const void* in;       /* float or complex64 [size]                         */
+  void* out;            /* same type and size                                */
+  int32_t is_complex;
+  double lambda;        /* tv_param / alpha                                  */
+  double vmin, vmax, vimag_max;
+  int32_t non_neg, dirichlet, inner_itt;
+  int32_t memory;
+  void* stream;
+} odt_tv_args;
+
+odt_status odt_tv_prox(const odt_tv_args* args);
+
 /* Free a solver (CudaBorn action 3, main.cpp:164-174). */
 odt_status odt_destroy(odt_handle h);
 

@@ -95,6 +95,36 @@ class NoallocBornArgs(C.Structure):
     ]
 
 
+class GradientArgs(C.Structure):
+    _fields_ = [
+        ("fields_in", C.c_void_p),
+        ("fields_meas", C.c_void_p),
+        ("n_ill", C.c_int32),
+        ("grad", C.c_void_p),
+        ("err", C.c_void_p),
+        ("memory", C.c_int32),
+        ("stream", C.c_void_p),
+    ]
+
+
+class TVArgs(C.Structure):
+    _fields_ = [
+        ("size", C.c_int32 * 3),
+        ("inp", C.c_void_p),
+        ("out", C.c_void_p),
+        ("is_complex", C.c_int32),
+        ("lam", C.c_double),
+        ("vmin", C.c_double),
+        ("vmax", C.c_double),
+        ("vimag_max", C.c_double),
+        ("non_neg", C.c_int32),
+        ("dirichlet", C.c_int32),
+        ("inner_itt", C.c_int32),
+        ("memory", C.c_int32),
+        ("stream", C.c_void_p),
+    ]
+
+
 # every symbol include/odt.h declares: name -> (restype, argtypes)
 SIGNATURES = {
     "odt_create": (C.c_int, [C.POINTER(Geometry), C.c_void_p, C.c_void_p, C.c_void_p,
@@ -108,6 +138,9 @@ SIGNATURES = {
                                        C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                        C.c_int32, C.POINTER(C.c_int32)]),
     "odt_born_series_noalloc": (C.c_int, [C.POINTER(NoallocBornArgs)]),
+    "odt_set_adjoint_potential": (C.c_int, [C.c_uint32, C.POINTER(PotentialParams), C.c_void_p]),
+    "odt_gradient": (C.c_int, [C.c_uint32, C.POINTER(GradientArgs)]),
+    "odt_tv_prox": (C.c_int, [C.POINTER(TVArgs)]),
     "odt_last_error": (C.c_char_p, []),
     "odt_abi_version": (C.c_int32, []),
 }

@@ -152,6 +152,52 @@ __global__ void count_nonfinite_kernel(const float2* x, long long n, unsigned in
   if (local) atomicAdd(count, local);
 }
 
+__global__ void residual_kernel(const float2* trans, const float2* meas, float2* adj_in,
+                                long long n, double* err) {
+  double local = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float2 d = csub(trans[i], meas[i]);
+    local += (double)d.x * d.x + (double)d.y * d.y;
+    adj_in[i] = cconj(d);
+  }
+  __shared__ double red[kThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = local;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) atomicAdd(err, v);
+  }
+}
+
+__global__ void grad_accumulate_kernel(const float2* E, const float2* A, float2* acc, int rx,
+                                       int ry, int rz, int nb) {
+  const long long n = (long long)rx * ry * rz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long plane = (long long)rx * ry;
+    const long long z = i / plane;
+    const long long iflip = i + (rz - 1 - 2 * z) * plane;  // (x, y, rz-1-z)
+    float2 s = acc[i];
+    for (int b = 0; b < nb; ++b) {
+      const float2 e = E[i + b * n];
+      const float2 a = A[iflip + b * n];
+      s = cadd(s, cmul(cconj(e), cconj(a)));
+    }
+    acc[i] = s;
+  }
+}
+
+__global__ void grad_finalize_kernel(const float2* acc, float2* grad, long long n, float n_ill) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float2 m = make_float2(acc[i].x / n_ill, acc[i].y / n_ill);
+    grad[i] = make_float2(m.y, -m.x);  // -(1i * m)
+  }
+}
+
 int grid_for(long long total) {
   long long g = (total + kThreads - 1) / kThreads;
   const long long cap = 148LL * 16;  // enough resident blocks; grid-stride beyond
@@ -268,6 +314,25 @@ cudaError_t launch_zreduce(const float2* conv, const float2* Kt, const float2* K
 cudaError_t launch_combine(const float2* x, const float2* add, const float* filt, float2* out,
                            long long plane, long long total, cudaStream_t s) {
   combine_kernel<<<grid_for(total), kThreads, 0, s>>>(x, add, filt, out, plane, total);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_residual(const float2* trans, const float2* meas, float2* adj_in, long long n,
+                            double* err, cudaStream_t s) {
+  residual_kernel<<<grid_for(n), kThreads, 0, s>>>(trans, meas, adj_in, n, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grad_accumulate(const float2* E, const float2* A, float2* acc, int rx, int ry,
+                                   int rz, int nb, cudaStream_t s) {
+  const long long n = (long long)rx * ry * rz;
+  grad_accumulate_kernel<<<grid_for(n), kThreads, 0, s>>>(E, A, acc, rx, ry, rz, nb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grad_finalize(const float2* acc, float2* grad, long long n, float n_ill,
+                                 cudaStream_t s) {
+  grad_finalize_kernel<<<grid_for(n), kThreads, 0, s>>>(acc, grad, n, n_ill);
   return cudaGetLastError();
 }
 

@@ -90,6 +90,17 @@ cudaError_t launch_combine(const float2* x, const float2* add, const float* filt
 cudaError_t launch_count_nonfinite(const float2* x, long long n, unsigned int* count,
                                    cudaStream_t s);
 
+// ---- gradient (BACKWARD_SOLVER_MULTI.m:30-54)
+// diff = trans - meas ; *err += sum |diff|^2 (double) ; adj_in = conj(diff)
+cudaError_t launch_residual(const float2* trans, const float2* meas, float2* adj_in, long long n,
+                            double* err, cudaStream_t s);
+// acc[x,y,z] += sum_b conj(E[x,y,z,b]) * conj(A[x,y,rz-1-z,b])   (b in order)
+cudaError_t launch_grad_accumulate(const float2* E, const float2* A, float2* acc, int rx, int ry,
+                                   int rz, int nb, cudaStream_t s);
+// grad = -(1i * (acc / n_ill))
+cudaError_t launch_grad_finalize(const float2* acc, float2* grad, long long n, float n_ill,
+                                 cudaStream_t s);
+
 // shared-memory bytes a tile kernel of `kind` needs for length n and W pencils
 size_t fft_smem_bytes(int n, int W, int kind);
 

@@ -8,6 +8,7 @@
 //                       holding T | Field_n | Field during the Born loop and the
 //                       refocus / emitter planes before and after it, plus
 //                       Einc and Fout [ri], and small 2D planes.
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -93,13 +94,21 @@ struct Handle {
   float* pupil_in = nullptr;
   float* pupil_out = nullptr;
 
-  // potential
-  bool have_potential = false;
-  odt_potential_params pp{};
-  float2* V = nullptr;
-  float* mask[3] = {nullptr, nullptr, nullptr};
-  float2* ramp[3] = {nullptr, nullptr, nullptr};
-  float* kq2[3] = {nullptr, nullptr, nullptr};
+  // potentials: slot 0 = forward (odt_set_potential), slot 1 = adjoint
+  // (odt_set_adjoint_potential, used by odt_gradient)
+  struct PotSlot {
+    bool have = false;
+    bool allocated = false;
+    odt_potential_params pp{};
+    float2* V = nullptr;
+    float* mask[3] = {nullptr, nullptr, nullptr};
+    float2* ramp[3] = {nullptr, nullptr, nullptr};
+    float* kq2[3] = {nullptr, nullptr, nullptr};
+  } pot[2];
+  float2* fout_adj = nullptr;   // adjoint 3D field of a batch (odt_gradient)
+  float2* grad_acc = nullptr;   // gradient accumulator [ri]
+  double* d_err = nullptr;      // misfit accumulator
+  int grad_batch = 0;
 
   // batch buffers
   int batch = 0;
@@ -310,7 +319,9 @@ void fftc2(Handle& H, float2* x, const DevFft& f0, const DevFft& f1, long long n
   H.mark_end(s);
 }
 
-void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r) {
+void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int slot,
+               float2* fout) {
+  const Handle::PotSlot& P = H.pot[slot];
   const odt_geometry& g = H.g;
   const int Fx = g.field_size[0], Fy = g.field_size[1];
   const int Cx = g.conv_size[0], Cy = g.conv_size[1];
@@ -344,32 +355,32 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r) {
   a.px = g.sim_size[0];
   a.py = g.sim_size[1];
   a.pz = g.sim_size[2];
-  a.rx0 = H.pp.roi[0] - 1;
-  a.ry0 = H.pp.roi[2] - 1;
-  a.rz0 = H.pp.roi[4] - 1;
+  a.rx0 = P.pp.roi[0] - 1;
+  a.ry0 = P.pp.roi[2] - 1;
+  a.rz0 = P.pp.roi[4] - 1;
   a.rx = Rx;
   a.ry = Ry;
   a.rz = Rz;
   a.nvox = H.nvox();
   a.nbatch = nb;
   for (int i = 0; i < 3; ++i) {
-    a.mask[i] = H.mask[i];
-    a.ramp[i] = H.ramp[i];
-    a.kq2[i] = H.kq2[i];
+    a.mask[i] = P.mask[i];
+    a.ramp[i] = P.ramp[i];
+    a.kq2[i] = P.kq2[i];
   }
-  a.eps = H.pp.eps_imag;
-  a.c_im = 1.0f / H.pp.eps_imag;
-  a.g_scale = H.pp.green_scale;
-  a.g_off = H.pp.green_offset;
+  a.eps = P.pp.eps_imag;
+  a.c_im = 1.0f / P.pp.eps_imag;
+  a.g_scale = P.pp.green_scale;
+  a.g_off = P.pp.green_offset;
   a.inv_n = (float)(1.0 / (double)H.nvox());
-  a.acyclic = H.pp.acyclic;
+  a.acyclic = P.pp.acyclic;
   a.T = H.work;
   a.Fn = H.work + (size_t)H.nvox() * nb;
   a.F = H.work + 2 * (size_t)H.nvox() * nb;
-  a.V = H.V;
+  a.V = P.V;
   a.Einc = H.einc;
-  a.Fout = H.fout;
-  const int B = H.pp.bornmax;
+  a.Fout = fout;
+  const int B = P.pp.bornmax;
   for (int jj = 1; jj <= B; ++jj) {
     H.mark_begin(kKBornX, s);
     ODT_CUDA(launch_born_x(a, jj == 1 ? kBornFirst : kBornMid, jj, H.fx, s));
@@ -391,7 +402,7 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r) {
   // ---- output projection (:445-511)
   if (want_t || want_r) {
     H.mark_begin(kKIoElem, s);
-    ODT_CUDA(launch_emitter(a, conv, Cx, Cy, orx, ory, H.pp.dV, s));
+    ODT_CUDA(launch_emitter(a, conv, Cx, Cy, orx, ory, P.pp.dV, s));
     H.mark_end(s);
     fftc2(H, conv, H.fcx, H.fcy, (long long)Rz * nb, false, s);
     H.mark_begin(kKIoElem, s);
@@ -413,6 +424,64 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r) {
       fftc2(H, o, H.ffx, H.ffy, nb, true, s);
     }
   }
+}
+
+
+void alloc_slot(Handle& H, int k) {
+  Handle::PotSlot& P = H.pot[k];
+  if (P.allocated) return;
+  const odt_geometry& g = H.g;
+  P.V = H.dalloc<float2>((size_t)H.nvox(), false);
+  for (int i = 0; i < 3; ++i) {
+    P.mask[i] = H.dalloc<float>(g.sim_size[i], false);
+    P.ramp[i] = H.dalloc<float2>(g.sim_size[i], false);
+    P.kq2[i] = H.dalloc<float>(g.sim_size[i], false);
+  }
+  P.allocated = true;
+}
+
+void set_potential_slot(const std::shared_ptr<Handle>& Hp, int k, const odt_potential_params* pp,
+                        const odt_cfloat* V, const char* fn) {
+  Handle& H = *Hp;
+  const std::string who(fn);
+  if (!pp || !V) raise(ODT_ERR_INVALID_ARGUMENT, who + ": NULL argument");
+  const odt_geometry& g = H.g;
+  for (int i = 0; i < 3; ++i) {
+    const int lo = pp->roi[2 * i], hi = pp->roi[2 * i + 1];
+    if (lo < 1 || hi > g.sim_size[i] || hi - lo + 1 != g.ri_size[i])
+      raise(ODT_ERR_INVALID_ARGUMENT, who + ": ROI does not match ri_size");
+    if (!pp->mask[i] || !pp->kq2[i] || (pp->acyclic && !pp->ramp[i]))
+      raise(ODT_ERR_INVALID_ARGUMENT, who + ": NULL table");
+  }
+  if (pp->bornmax < 0) raise(ODT_ERR_INVALID_ARGUMENT, who + ": bornmax < 0");
+  if (!(pp->eps_imag > 0.f) || !std::isfinite(pp->eps_imag))
+    raise(ODT_ERR_INVALID_ARGUMENT, who + ": eps_imag must be positive and finite");
+  if (!std::isfinite(pp->green_scale) || !std::isfinite(pp->green_offset) || !std::isfinite(pp->dV))
+    raise(ODT_ERR_INVALID_ARGUMENT, who + ": non-finite scalar");
+  DeviceGuard dg(g.device);
+  alloc_slot(H, k);
+  Handle::PotSlot& P = H.pot[k];
+  const size_t nv = (size_t)H.nvox();
+  ODT_CUDA(cudaMemcpy(P.V, V, nv * sizeof(float2), cudaMemcpyHostToDevice));
+  std::vector<float2> one;
+  for (int i = 0; i < 3; ++i) {
+    const size_t n = g.sim_size[i];
+    ODT_CUDA(cudaMemcpy(P.mask[i], pp->mask[i], n * sizeof(float), cudaMemcpyHostToDevice));
+    ODT_CUDA(cudaMemcpy(P.kq2[i], pp->kq2[i], n * sizeof(float), cudaMemcpyHostToDevice));
+    if (pp->acyclic) {
+      ODT_CUDA(cudaMemcpy(P.ramp[i], pp->ramp[i], n * sizeof(float2), cudaMemcpyHostToDevice));
+    } else {
+      one.assign(n, make_float2(1.f, 0.f));
+      ODT_CUDA(cudaMemcpy(P.ramp[i], one.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+    }
+  }
+  P.pp = *pp;
+  for (int i = 0; i < 3; ++i) {  // do not keep caller pointers
+    P.pp.mask[i] = nullptr;
+    P.pp.ramp[i] = nullptr;
+    P.pp.kq2[i] = nullptr;
+  }
+  P.have = true;
 }
 
 }  // namespace
@@ -485,12 +554,7 @@ odt_status odt_create(const odt_geometry* geom, const odt_cfloat* refocus,
     H->pupil_out = H->dalloc<float>(nf, false);
     ODT_CUDA(cudaMemcpy(H->pupil_in, pupil_in, nf * sizeof(float), cudaMemcpyHostToDevice));
     ODT_CUDA(cudaMemcpy(H->pupil_out, pupil_out, nf * sizeof(float), cudaMemcpyHostToDevice));
-    H->V = H->dalloc<float2>((size_t)H->nvox(), false);
-    for (int i = 0; i < 3; ++i) {
-      H->mask[i] = H->dalloc<float>(g.sim_size[i], false);
-      H->ramp[i] = H->dalloc<float2>(g.sim_size[i], false);
-      H->kq2[i] = H->dalloc<float>(g.sim_size[i], false);
-    }
+    alloc_slot(*H, 0);
     const uint32_t id = g_next_id++;
     {
       std::lock_guard<std::mutex> lk(g_mu);
@@ -501,53 +565,19 @@ odt_status odt_create(const odt_geometry* geom, const odt_cfloat* refocus,
 }
 
 odt_status odt_set_potential(odt_handle h, const odt_potential_params* pp, const odt_cfloat* V) {
-  return guarded([&] {
-    auto H = lookup(h);
-    if (!pp || !V) raise(ODT_ERR_INVALID_ARGUMENT, "odt_set_potential: NULL argument");
-    const odt_geometry& g = H->g;
-    for (int i = 0; i < 3; ++i) {
-      const int lo = pp->roi[2 * i], hi = pp->roi[2 * i + 1];
-      if (lo < 1 || hi > g.sim_size[i] || hi - lo + 1 != g.ri_size[i])
-        raise(ODT_ERR_INVALID_ARGUMENT, "odt_set_potential: ROI does not match ri_size");
-      if (!pp->mask[i] || !pp->kq2[i] || (pp->acyclic && !pp->ramp[i]))
-        raise(ODT_ERR_INVALID_ARGUMENT, "odt_set_potential: NULL table");
-    }
-    if (pp->bornmax < 0) raise(ODT_ERR_INVALID_ARGUMENT, "odt_set_potential: bornmax < 0");
-    if (!(pp->eps_imag > 0.f) || !std::isfinite(pp->eps_imag))
-      raise(ODT_ERR_INVALID_ARGUMENT, "odt_set_potential: eps_imag must be positive and finite");
-    if (!std::isfinite(pp->green_scale) || !std::isfinite(pp->green_offset) ||
-        !std::isfinite(pp->dV))
-      raise(ODT_ERR_INVALID_ARGUMENT, "odt_set_potential: non-finite scalar");
-    DeviceGuard dg(g.device);
-    const size_t nv = (size_t)H->nvox();
-    ODT_CUDA(cudaMemcpy(H->V, V, nv * sizeof(float2), cudaMemcpyHostToDevice));
-    std::vector<float2> one;
-    for (int i = 0; i < 3; ++i) {
-      const size_t n = g.sim_size[i];
-      ODT_CUDA(cudaMemcpy(H->mask[i], pp->mask[i], n * sizeof(float), cudaMemcpyHostToDevice));
-      ODT_CUDA(cudaMemcpy(H->kq2[i], pp->kq2[i], n * sizeof(float), cudaMemcpyHostToDevice));
-      if (pp->acyclic) {
-        ODT_CUDA(cudaMemcpy(H->ramp[i], pp->ramp[i], n * sizeof(float2), cudaMemcpyHostToDevice));
-      } else {
-        one.assign(n, make_float2(1.f, 0.f));
-        ODT_CUDA(cudaMemcpy(H->ramp[i], one.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
-      }
-    }
-    H->pp = *pp;
-    for (int i = 0; i < 3; ++i) {  // do not keep caller pointers
-      H->pp.mask[i] = nullptr;
-      H->pp.ramp[i] = nullptr;
-      H->pp.kq2[i] = nullptr;
-    }
-    H->have_potential = true;
-  });
+  return guarded([&] { set_potential_slot(lookup(h), 0, pp, V, "odt_set_potential"); });
+}
+
+odt_status odt_set_adjoint_potential(odt_handle h, const odt_potential_params* pp,
+                                     const odt_cfloat* V) {
+  return guarded([&] { set_potential_slot(lookup(h), 1, pp, V, "odt_set_adjoint_potential"); });
 }
 
 odt_status odt_solve(odt_handle h, const odt_solve_args* args) {
   return guarded([&] {
     auto H = lookup(h);
     if (!args) raise(ODT_ERR_INVALID_ARGUMENT, "odt_solve: NULL args");
-    if (!H->have_potential) raise(ODT_ERR_NOT_READY, "odt_solve: call odt_set_potential first");
+    if (!H->pot[0].have) raise(ODT_ERR_NOT_READY, "odt_solve: call odt_set_potential first");
     const odt_solve_args& A = *args;
     if (A.n_ill < 0) raise(ODT_ERR_INVALID_ARGUMENT, "odt_solve: n_ill < 0");
     if (A.n_ill == 0) return;
@@ -576,7 +606,7 @@ odt_status odt_solve(odt_handle h, const odt_solve_args* args) {
       const int nb = std::min(H->batch, A.n_ill - b0);
       ODT_CUDA(cudaMemcpyAsync(H->in2d, A.fields_in + (size_t)b0 * nF,
                                (size_t)nb * nF * sizeof(float2), kin, s));
-      run_chunk(*H, nb, s, want_t, want_r);
+      run_chunk(*H, nb, s, want_t, want_r, 0, H->fout);
       ODT_CUDA(launch_count_nonfinite(H->fout, nR * nb, H->d_count, s));
       if (A.field3d)
         ODT_CUDA(cudaMemcpyAsync(A.field3d + (size_t)b0 * nR, H->fout,
@@ -596,6 +626,68 @@ odt_status odt_solve(odt_handle h, const odt_solve_args* args) {
       if (cnt) raise(ODT_ERR_NUMERIC, "odt_solve: " + std::to_string(cnt) +
                                           " non-finite values in the 3D field (NaN/Inf input?)");
     }
+  });
+}
+
+odt_status odt_gradient(odt_handle h, const odt_gradient_args* args) {
+  return guarded([&] {
+    auto H = lookup(h);
+    if (!args) raise(ODT_ERR_INVALID_ARGUMENT, "odt_gradient: NULL args");
+    const odt_gradient_args& A = *args;
+    if (!H->pot[0].have || !H->pot[1].have)
+      raise(ODT_ERR_NOT_READY, "odt_gradient: set the forward and the adjoint potential first");
+    if (A.n_ill < 1 || !A.fields_in || !A.fields_meas || !A.grad || !A.err)
+      raise(ODT_ERR_INVALID_ARGUMENT, "odt_gradient: NULL buffer or n_ill < 1");
+    if (A.memory != ODT_MEM_HOST && A.memory != ODT_MEM_DEVICE)
+      raise(ODT_ERR_INVALID_ARGUMENT, "odt_gradient: bad memory flag");
+    if (!H->ktrans) raise(ODT_ERR_INVALID_ARGUMENT, "odt_gradient: created without kernel_trans");
+    DeviceGuard dg(H->g.device);
+    const bool dev = A.memory == ODT_MEM_DEVICE;
+    if (dev && (!is_device_ptr(A.fields_in) || !is_device_ptr(A.fields_meas) ||
+                !is_device_ptr(A.grad)))
+      raise(ODT_ERR_INVALID_ARGUMENT, "odt_gradient: ODT_MEM_DEVICE with a non-device pointer");
+    cudaStream_t s = dev ? (cudaStream_t)A.stream : H->own_stream;
+    ensure_batch(*H, std::min<int>(A.n_ill, auto_batch(*H)));
+    const long long nF = H->nf(), nR = H->nri();
+    if (H->grad_batch != H->batch) {
+      for (void** p : {(void**)&H->fout_adj, (void**)&H->grad_acc, (void**)&H->d_err}) {
+        if (*p) {
+          cudaFree(*p);
+          auto& L = H->allocs;
+          L.erase(std::remove(L.begin(), L.end(), *p), L.end());
+          *p = nullptr;
+        }
+      }
+      H->fout_adj = H->dalloc<float2>((size_t)nR * H->batch, false);
+      H->grad_acc = H->dalloc<float2>((size_t)nR, false);
+      H->d_err = H->dalloc<double>(1, false);
+      H->grad_batch = H->batch;
+    }
+    const cudaMemcpyKind kin = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    ODT_CUDA(cudaMemsetAsync(H->grad_acc, 0, nR * sizeof(float2), s));
+    ODT_CUDA(cudaMemsetAsync(H->d_err, 0, sizeof(double), s));
+    for (int b0 = 0; b0 < A.n_ill; b0 += H->batch) {
+      const int nb = std::min(H->batch, A.n_ill - b0);
+      ODT_CUDA(cudaMemcpyAsync(H->in2d, A.fields_in + (size_t)b0 * nF,
+                               (size_t)nb * nF * sizeof(float2), kin, s));
+      ODT_CUDA(cudaMemcpyAsync(H->out_r, A.fields_meas + (size_t)b0 * nF,
+                               (size_t)nb * nF * sizeof(float2), kin, s));
+      run_chunk(*H, nb, s, true, false, 0, H->fout);              // E_3D, trans
+      ODT_CUDA(launch_residual(H->out_t, H->out_r, H->in2d, nF * nb, H->d_err, s));
+      run_chunk(*H, nb, s, false, false, 1, H->fout_adj);         // adjoint 3D field
+      ODT_CUDA(launch_grad_accumulate(H->fout, H->fout_adj, H->grad_acc, H->g.ri_size[0],
+                                      H->g.ri_size[1], H->g.ri_size[2], nb, s));
+      H->collect(s);
+    }
+    if (dev) {
+      ODT_CUDA(launch_grad_finalize(H->grad_acc, reinterpret_cast<float2*>(A.grad), nR,
+                                    (float)A.n_ill, s));
+    } else {
+      ODT_CUDA(launch_grad_finalize(H->grad_acc, H->fout_adj, nR, (float)A.n_ill, s));
+      ODT_CUDA(cudaMemcpyAsync(A.grad, H->fout_adj, nR * sizeof(float2), cudaMemcpyDeviceToHost, s));
+    }
+    ODT_CUDA(cudaMemcpyAsync(A.err, H->d_err, sizeof(double), cudaMemcpyDeviceToHost, s));
+    ODT_CUDA(cudaStreamSynchronize(s));
   });
 }
 

@@ -251,6 +251,48 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
         pp, keep = self.prepare_potential(RI)
         _lib.check(self.lib.odt_set_potential(self._handle, C.byref(pp), _lib.ptr(keep[-1])))
 
+    _STATE = ("eps_imag", "ROI", "RI", "V", "Bornmax", "utility_border", "attenuation_mask1d",
+              "ramp1d", "kq2")
+
+    def set_RI_adjoint(self, RI):
+        """Potential of the adjoint solve, conj(flip(RI, 3))
+        (BACKWARD_SOLVER_MULTI.m:48), uploaded to the adjoint slot; the
+        forward state of this object is left unchanged."""
+        saved = {k: getattr(self, k) for k in self._STATE if hasattr(self, k)}
+        try:
+            pp, keep = self.prepare_potential(np.conj(np.flip(np.asarray(RI), axis=2)))
+            _lib.check(self.lib.odt_set_adjoint_potential(self._handle, C.byref(pp),
+                                                          _lib.ptr(keep[-1])))
+            self.adjoint_Bornmax = self.Bornmax
+        finally:
+            for k, v in saved.items():
+                setattr(self, k, v)
+
+    def gradient(self, input_field, output_field):
+        """Fused forward + adjoint gradient of get_gradiant_static
+        (BACKWARD_SOLVER_MULTI.m:30-54) after set_RI(RI) and
+        set_RI_adjoint(RI): returns (gradient [RI size] complex64, err)."""
+        x = np.asarray(input_field)
+        y = np.asarray(output_field)
+        if x.ndim == 3:
+            x = x[:, :, :, None]
+        if y.ndim == 3:
+            y = y[:, :, :, None]
+        if x.shape != y.shape or x.shape[2] != 1:
+            raise ValueError("input and output fields must be [F_x, F_y, 1, n] alike")
+        xin, yin = _c64(x), _c64(y)
+        g = np.empty(self.expected_RI_size, dtype=C64, order="F")
+        err = C.c_double(0)
+        a = _lib.GradientArgs()
+        a.fields_in, a.fields_meas = _lib.ptr(xin), _lib.ptr(yin)
+        a.n_ill = x.shape[3]
+        a.grad = _lib.ptr(g)
+        a.err = C.addressof(err)
+        a.memory = _lib.ODT_MEM_HOST
+        a.stream = None
+        _lib.check(self.lib.odt_gradient(self._handle, C.byref(a)))
+        return g, err.value
+
     # ------------------------------------------------------------ solve
     def _outputs(self, n_ill, on_device=False):
         p = self.parameters
