@@ -191,6 +191,46 @@ typedef struct odt_tv_args {
 
 odt_status odt_tv_prox(const odt_tv_args* args);
 
+/*
+ * Rytov reconstruction with Ewald-sphere mapping (BACKWARD_SOLVER_RYTOV.m:22-127)
+ * and overlap counting (BACKWARD_SOLVER_RYTOV_precompute.m:87-137,
+ * OVERLAP_COUNTER.m:19-23).  Scalar fields [size1, size2, n_ill]; the tables
+ * are DERIVE_OPTICAL_TOOL's single-precision grids (fourier coor{1}, coor{2},
+ * k3, NA_circle) as the host computed them.  `phase` is the unwrapped phase
+ * of sp./bg (NULL with sp == NULL: overlap counting only).  count_one = 1
+ * counts every Ewald hit (overlap counter); 0 counts hits with Uprime ~= 0
+ * (Rytov).  Count and overlap_field are integer-valued single, bit-exact
+ * with the reference's single-precision index arithmetic.  Any output may be
+ * NULL.  `shifts` (host, 2*n_ill int32, may be NULL) receives the spectrum
+ * shift (rows, cols) of each illumination.  Synchronous.
+ */
+typedef struct odt_rytov_args {
+  int32_t size[3];
+  double resolution[3];
+  double fourier_res[3];
+  double k0_nm, ri_bg, wavelength;
+  const float* coor1;              /* [size1]                                */
+  const float* coor2;              /* [size2]                                */
+  const float* k3;                 /* [size1*size2]                          */
+  const uint8_t* na_circle;        /* [size1*size2]                          */
+  const uint8_t* emask;            /* [size1*size2] coorxy < 2 NA/lambda     */
+  const odt_cfloat* bg;            /* [size1, size2, n_ill]                  */
+  const odt_cfloat* sp;            /* same, or NULL                          */
+  const float* phase;              /* same, or NULL                          */
+  int32_t n_ill;
+  int32_t count_one;
+  int32_t non_negativity_iteration;
+  odt_cfloat* RI;                  /* [size] outputs                          */
+  odt_cfloat* ORytov;
+  float* count;
+  float* overlap_field;            /* [size1, size2, n_ill]                  */
+  int32_t* shifts;
+  int32_t memory;
+  void* stream;
+} odt_rytov_args;
+
+odt_status odt_rytov(const odt_rytov_args* args);
+
 /* Free a solver (CudaBorn action 3, main.cpp:164-174). */
 odt_status odt_destroy(odt_handle h);
 

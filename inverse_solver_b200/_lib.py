@@ -125,6 +125,35 @@ class TVArgs(C.Structure):
     ]
 
 
+class RytovArgs(C.Structure):
+    _fields_ = [
+        ("size", C.c_int32 * 3),
+        ("resolution", C.c_double * 3),
+        ("fourier_res", C.c_double * 3),
+        ("k0_nm", C.c_double),
+        ("ri_bg", C.c_double),
+        ("wavelength", C.c_double),
+        ("coor1", C.c_void_p),
+        ("coor2", C.c_void_p),
+        ("k3", C.c_void_p),
+        ("na_circle", C.c_void_p),
+        ("emask", C.c_void_p),
+        ("bg", C.c_void_p),
+        ("sp", C.c_void_p),
+        ("phase", C.c_void_p),
+        ("n_ill", C.c_int32),
+        ("count_one", C.c_int32),
+        ("non_negativity_iteration", C.c_int32),
+        ("RI", C.c_void_p),
+        ("ORytov", C.c_void_p),
+        ("count", C.c_void_p),
+        ("overlap_field", C.c_void_p),
+        ("shifts", C.c_void_p),
+        ("memory", C.c_int32),
+        ("stream", C.c_void_p),
+    ]
+
+
 # every symbol include/odt.h declares: name -> (restype, argtypes)
 SIGNATURES = {
     "odt_create": (C.c_int, [C.POINTER(Geometry), C.c_void_p, C.c_void_p, C.c_void_p,
@@ -141,6 +170,7 @@ SIGNATURES = {
     "odt_set_adjoint_potential": (C.c_int, [C.c_uint32, C.POINTER(PotentialParams), C.c_void_p]),
     "odt_gradient": (C.c_int, [C.c_uint32, C.POINTER(GradientArgs)]),
     "odt_tv_prox": (C.c_int, [C.POINTER(TVArgs)]),
+    "odt_rytov": (C.c_int, [C.POINTER(RytovArgs)]),
     "odt_last_error": (C.c_char_p, []),
     "odt_abi_version": (C.c_int32, []),
 }

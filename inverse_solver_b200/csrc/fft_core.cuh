@@ -217,10 +217,18 @@ ODT_HD void stockham_pass(const float2* __restrict__ src, float2* __restrict__ d
 }
 
 // Radix classes: a kernel instantiated for class K only contains the
-// butterflies of that class, so its register budget is set by the largest
-// radix it can meet (class 0: <= 8, 1: <= 15, 2: 17 and 19, 3: <= 31).
+// butterflies of classes <= K, so its register budget is set by the largest
+// radix it can meet (class 0: 2, 3, 4, 5, 8; 1: adds 7, 9, 11, 13, 15;
+// 2: adds 17, 19; 3: adds 23-31).
 constexpr int kNumRadixClasses = 4;
-inline int radix_class_of(int r) { return r <= 8 ? 0 : (r <= 15 ? 1 : (r <= 19 ? 2 : 3)); }
+inline int radix_class_of(int r) {
+  switch (r) {
+    case 2: case 3: case 4: case 5: case 8: return 0;  // closed-form / short butterflies
+    case 7: case 9: case 11: case 13: case 15: return 1;
+    case 17: case 19: return 2;
+    default: return 3;
+  }
+}
 
 template <int CLS, bool INV>
 ODT_HD void run_pass(int R, const float2* src, float2* dst, int n, int ns, int lgW, int ld,
@@ -264,11 +272,16 @@ ODT_HD void run_pass(int R, const float2* src, float2* dst, int n, int ns, int l
   }
 }
 
-// Host-side dispatch helper (the CPU check runs every radix).
+// Host-side dispatch by a plan's radix class, as the kernels dispatch.
 template <bool INV>
-inline void run_pass_any(int R, const float2* src, float2* dst, int n, int ns, int lgW, int ld,
-                         const float2* tw, int tid, int nthr) {
-  run_pass<3, INV>(R, src, dst, n, ns, lgW, ld, tw, tid, nthr);
+inline void run_pass_any(int cls, int R, const float2* src, float2* dst, int n, int ns, int lgW,
+                         int ld, const float2* tw, int tid, int nthr) {
+  switch (cls) {
+    case 0: run_pass<0, INV>(R, src, dst, n, ns, lgW, ld, tw, tid, nthr); break;
+    case 1: run_pass<1, INV>(R, src, dst, n, ns, lgW, ld, tw, tid, nthr); break;
+    case 2: run_pass<2, INV>(R, src, dst, n, ns, lgW, ld, tw, tid, nthr); break;
+    default: run_pass<3, INV>(R, src, dst, n, ns, lgW, ld, tw, tid, nthr); break;
+  }
 }
 
 inline bool radix_supported(int r) {

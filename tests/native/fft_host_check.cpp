@@ -38,8 +38,8 @@ int main(int argc, char** argv) {
   int ns = 1;
   for (int p = 0; p < plan.npass; ++p) {
     int R = plan.radix[p];
-    if (inv) odt::run_pass_any<true>(R, src, dst, n, ns, lgW, ld, tw.data(), 0, 1);
-    else odt::run_pass_any<false>(R, src, dst, n, ns, lgW, ld, tw.data(), 0, 1);
+    if (inv) odt::run_pass_any<true>(plan.rclass, R, src, dst, n, ns, lgW, ld, tw.data(), 0, 1);
+    else odt::run_pass_any<false>(plan.rclass, R, src, dst, n, ns, lgW, ld, tw.data(), 0, 1);
     ns *= R;
     std::swap(src, dst);
   }

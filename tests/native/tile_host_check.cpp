@@ -76,23 +76,38 @@ int main(int argc, char** argv) {
   const long long n0z = (long long)a.px * a.py;
   const unsigned bz = (unsigned)(((n0z + (1 << lgWz) - 1) >> lgWz) * a.nbatch);
   const unsigned by = (unsigned)((((long long)a.px + (1 << lgWy) - 1) >> lgWy) * a.pz * a.nbatch);
+  // every body is dispatched on its plan's radix class, as the launchers do
+  if (lx.plan.rclass > 2 || ly.plan.rclass > 2 || lz.plan.rclass > 2) return 6;
   auto born_x = [&](int mode, int jj) {
     for (unsigned blk = 0; blk < bx; ++blk) {
-      if (mode == kBornFirst) born_x_body<2, kBornFirst>(a, jj, lx.plan, lx.tw.data(), Wx, sm.data(), blk, th);
-      else if (mode == kBornMid) born_x_body<2, kBornMid>(a, jj, lx.plan, lx.tw.data(), Wx, sm.data(), blk, th);
-      else born_x_body<2, kBornLast>(a, jj, lx.plan, lx.tw.data(), Wx, sm.data(), blk, th);
+#define BX(C)                                                                                   \
+  if (mode == kBornFirst) born_x_body<C, kBornFirst>(a, jj, lx.plan, lx.tw.data(), Wx, sm.data(), blk, th); \
+  else if (mode == kBornMid) born_x_body<C, kBornMid>(a, jj, lx.plan, lx.tw.data(), Wx, sm.data(), blk, th); \
+  else born_x_body<C, kBornLast>(a, jj, lx.plan, lx.tw.data(), Wx, sm.data(), blk, th);
+      if (lx.plan.rclass == 0) { BX(0) } else if (lx.plan.rclass == 1) { BX(1) } else { BX(2) }
+#undef BX
     }
   };
   auto born_y = [&](bool inv) {
     for (unsigned blk = 0; blk < by; ++blk) {
-      if (inv) fft_cols_body<2, true, false>(a.T, a.T, a.px, 0, 0, 1.f, ly.plan, ly.tw.data(), lgWy, sm.data(), blk, th);
-      else fft_cols_body<2, false, false>(a.T, a.T, a.px, 0, 0, 1.f, ly.plan, ly.tw.data(), lgWy, sm.data(), blk, th);
+#define BY(C)                                                                                                    \
+  if (inv) fft_cols_body<C, true, false>(a.T, a.T, a.px, 0, 0, 1.f, ly.plan, ly.tw.data(), lgWy, sm.data(), blk, th); \
+  else fft_cols_body<C, false, false>(a.T, a.T, a.px, 0, 0, 1.f, ly.plan, ly.tw.data(), lgWy, sm.data(), blk, th);
+      if (ly.plan.rclass == 0) { BY(0) } else if (ly.plan.rclass == 1) { BY(1) } else { BY(2) }
+#undef BY
+    }
+  };
+  auto born_z = [&](int jj) {
+    for (unsigned blk = 0; blk < bz; ++blk) {
+      if (lz.plan.rclass == 0) born_z_body<0>(a, jj, lz.plan, lz.tw.data(), lgWz, sm.data(), blk, th);
+      else if (lz.plan.rclass == 1) born_z_body<1>(a, jj, lz.plan, lz.tw.data(), lgWz, sm.data(), blk, th);
+      else born_z_body<2>(a, jj, lz.plan, lz.tw.data(), lgWz, sm.data(), blk, th);
     }
   };
   for (int jj = 1; jj <= B; ++jj) {
     born_x(jj == 1 ? kBornFirst : kBornMid, jj);
     born_y(false);
-    for (unsigned blk = 0; blk < bz; ++blk) born_z_body<2>(a, jj, lz.plan, lz.tw.data(), lgWz, sm.data(), blk, th);
+    born_z(jj);
     born_y(true);
   }
   born_x(kBornLast, B + 1);

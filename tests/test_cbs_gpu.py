@@ -105,6 +105,25 @@ def test_cyclic_xy_matches_oracle():
     s.delete()
 
 
+def test_radix7_grid_matches_oracle():
+    """Padded grid [56, 38, 24] (radices 7x8, 19x2, 3x8)."""
+    p = cases.params([48, 30, 20], [2, 2, 1], return_reflection=True, return_3D=True)
+    RI = cases.sphere_phantom([48, 30, 20], [0.1] * 3, cases.NM, seed=7, n_spheres=2,
+                              radius_um=(0.3, 0.8))
+    fields = cases.circle_fields(p, 2)
+    s = _solver(p)
+    s.set_RI(RI)
+    assert s.sim_size == [56, 38, 24]
+    t, r, f = s.solve(fields)
+    o = cbs.ForwardSolverCBS(p, single=True)
+    o.set_RI(RI)
+    ot, orr, of = o.solve(fields)
+    assert worst(f, of) < TOL_3D
+    assert worst(t, ot) < TOL_T
+    assert worst(r, orr) < TOL_R
+    s.delete()
+
+
 def test_batch_chunking_is_bit_identical():
     """Illuminations are independent: solving 5 in chunks of 2 or all at once
     gives identical bits."""

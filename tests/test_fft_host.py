@@ -50,3 +50,41 @@ def test_stockham_matches_numpy(checker, n, inv, order):
 def test_unsupported_prime_is_rejected(checker):
     r = subprocess.run([checker, "37", "4", "0"], input="", capture_output=True, text=True)
     assert r.returncode == 4 and "prime factor 37" in r.stderr
+
+
+TILE_SIZES = [3, 7, 9, 15, 16, 19, 21, 24, 26, 27, 35, 38, 52, 56, 88, 96]
+
+
+@pytest.fixture(scope="module")
+def tile_checker(tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("tfft") / "fft_tile_host_check")
+    cuda_inc = os.environ.get("CUDA_HOME", "/usr/local/cuda") + "/include"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I" + cuda_inc, "-I" + CSRC,
+                    os.path.join(ROOT, "tests", "native", "fft_tile_host_check.cpp"),
+                    os.path.join(CSRC, "fft_plan.cpp"), "-o", exe], check=True)
+    return exe
+
+
+@pytest.mark.parametrize("n", TILE_SIZES)
+@pytest.mark.parametrize("kind", [0, 1])
+def test_tile_fft_bodies_with_centring_shifts(tile_checker, n, kind):
+    """The line / column FFT kernel bodies (dispatched on the plan's radix
+    class, as on the GPU) against numpy's centred FFT, both directions."""
+    rng = np.random.default_rng(n + 100 * kind)
+    n0, n2 = 20, 3
+    if kind == 0:
+        x = (rng.standard_normal((n, n0 * n2)) + 1j * rng.standard_normal((n, n0 * n2))).astype(np.complex64)
+        ax = 0
+    else:
+        x = (rng.standard_normal((n0, n, n2)) + 1j * rng.standard_normal((n0, n, n2))).astype(np.complex64)
+        ax = 1
+    inp = "\n".join(f"{v.real:.9g} {v.imag:.9g}" for v in x.ravel(order="F"))
+    for inv in (False, True):
+        r = subprocess.run([tile_checker, str(kind), str(n0), str(n), str(n2), str(int(inv)),
+                            str(n // 2), "0"], input=inp, capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        y = np.array([complex(*map(float, l.split())) for l in r.stdout.split("\n") if l])
+        y = y.reshape(x.shape, order="F")
+        xd = np.fft.ifftshift(x.astype(np.complex128), axes=ax)
+        ref = np.fft.fftshift((np.fft.ifft if inv else np.fft.fft)(xd, axis=ax), axes=ax)
+        assert np.linalg.norm(y - ref) / np.linalg.norm(ref) < 3e-7

@@ -69,6 +69,15 @@ def test_small_case(harness, tmp_path, iters):
     assert cbs.rel_l2(got, ref) < 1e-5
 
 
+def test_radix7_plan(harness, tmp_path):
+    # padded [56, 38, 24]: plans [7,8], [19,2], [8,3]
+    p = cases.params([48, 30, 20], [2, 2, 1])
+    RI = cases.sphere_phantom([48, 30, 20], [0.1] * 3, cases.NM, seed=7, n_spheres=2,
+                              radius_um=(0.3, 0.8))
+    got, ref = run_case(harness, str(tmp_path), p, RI, cases.circle_fields(p, 1))
+    assert cbs.rel_l2(got, ref) < 1e-5
+
+
 def test_one_and_three_pass_plans(harness, tmp_path):
     # padded [48, 38, 19]: plans [3,8,2], [19,2], [19]
     p = cases.params([40, 26, 11], [2, 3, 2])
