@@ -68,7 +68,7 @@ typedef struct odt_geometry {
                             field_size when the xy boundary is cyclic          */
   int32_t device;        /* CUDA device ordinal (CudaBorn's used_gpu)            */
   int32_t max_batch;     /* illuminations resident on the device at once; 0=auto */
-  int64_t mem_budget;    /* bytes this handle may allocate; 0 = 90% of free HBM */
+  int64_t mem_budget;    /* bytes this handle may allocate; 0 = half the free HBM */
 } odt_geometry;
 
 /*
@@ -230,6 +230,53 @@ typedef struct odt_rytov_args {
 } odt_rytov_args;
 
 odt_status odt_rytov(const odt_rytov_args* args);
+
+/*
+ * odt_unwrap_goldstein -- Goldstein branch-cut phase unwrapping of a stack of
+ * 2D phase maps: the whole of unwrapp2_gpu.m (Codes/sub_code/goldstein_GPU/
+ * unwrapp2_gpu.m:1-6), which replaces the chain of MEX calls
+ *   get_residue_gpu          (get_residue_mex.cpp, get_residue_cuda.cu:34-66)
+ *   remove_dipoles_gpu       (remove_dipoles_mex.cpp, remove_dipoles_cuda.cu:52-146)
+ *   goldstein_branch_cut     (goldstein_branch_cut.m:1-100: create_sort_value_gpu,
+ *                             get_lookup_gpu, get_shortest_sort_gpu,
+ *                             get_branches_goldstein_v2, raster_branches_gpu)
+ *   unwrapp_phase_goldstein_gpu (unwrapp_phase_goldstein_cuda.cu:62-157).
+ * `phase_in` / `phase_out` are [size0, size1, size2] single, column-major
+ * (size2 = number of maps, 1 for one map); phase_out may equal phase_in.
+ * The optional outputs (NULL to skip) expose the intermediate products with
+ * the reference's layouts:
+ *   residue_out  [size0-1, size1-1, size2] single: residues after the dipole pass
+ *   step1_out    [size0, size1, size2] int32: the 2*pi steps along dimension 1
+ *   step2_out    [size1, size2] int32: the steps along dimension 2 of row 1
+ *   table_out    [6, residue_cap] int32: sorted residue table (idx, value, box, x, y, z)
+ *   nearest_out  [2, 8, residue_cap] int32: (row, distance) of the 8 nearest
+ *   branches_out [6, branch_cap] int32: (x1, y1, x2, y2, z, jump)
+ * n_residues / n_branches (host, optional) receive the counts; the tables are
+ * written only up to their capacities.  `memory` says where phase_in,
+ * phase_out and the optional arrays live; `link_threads` bounds the host
+ * threads of the branch linker (0: one per hardware thread).  Requires
+ * size0, size1 >= 2 and a total below 2^31 elements.
+ */
+typedef struct odt_unwrap_args {
+  int32_t size[3];
+  const float* phase_in;
+  float* phase_out;
+  float* residue_out;
+  int32_t* step1_out;
+  int32_t* step2_out;
+  int32_t* table_out;
+  int32_t* nearest_out;
+  int64_t residue_cap;
+  int32_t* branches_out;
+  int64_t branch_cap;
+  int64_t* n_residues;
+  int64_t* n_branches;
+  int32_t link_threads;
+  int32_t memory;
+  void* stream;
+} odt_unwrap_args;
+
+odt_status odt_unwrap_goldstein(const odt_unwrap_args* args);
 
 /* Free a solver (CudaBorn action 3, main.cpp:164-174). */
 odt_status odt_destroy(odt_handle h);

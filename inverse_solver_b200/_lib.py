@@ -155,6 +155,27 @@ class RytovArgs(C.Structure):
 
 
 # every symbol include/odt.h declares: name -> (restype, argtypes)
+class UnwrapArgs(C.Structure):
+    _fields_ = [
+        ("size", C.c_int32 * 3),
+        ("phase_in", C.c_void_p),
+        ("phase_out", C.c_void_p),
+        ("residue_out", C.c_void_p),
+        ("step1_out", C.c_void_p),
+        ("step2_out", C.c_void_p),
+        ("table_out", C.c_void_p),
+        ("nearest_out", C.c_void_p),
+        ("residue_cap", C.c_int64),
+        ("branches_out", C.c_void_p),
+        ("branch_cap", C.c_int64),
+        ("n_residues", C.c_void_p),
+        ("n_branches", C.c_void_p),
+        ("link_threads", C.c_int32),
+        ("memory", C.c_int32),
+        ("stream", C.c_void_p),
+    ]
+
+
 SIGNATURES = {
     "odt_create": (C.c_int, [C.POINTER(Geometry), C.c_void_p, C.c_void_p, C.c_void_p,
                              C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]),
@@ -171,6 +192,7 @@ SIGNATURES = {
     "odt_gradient": (C.c_int, [C.c_uint32, C.POINTER(GradientArgs)]),
     "odt_tv_prox": (C.c_int, [C.POINTER(TVArgs)]),
     "odt_rytov": (C.c_int, [C.POINTER(RytovArgs)]),
+    "odt_unwrap_goldstein": (C.c_int, [C.POINTER(UnwrapArgs)]),
     "odt_last_error": (C.c_char_p, []),
     "odt_abi_version": (C.c_int32, []),
 }

@@ -134,6 +134,25 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
       check(odt_solve(id, &a));
       break;
     }
+    case 20: {
+      // Goldstein unwrapping of a single [N1, N2(, n)] host array: the whole
+      // of unwrapp2_gpu.m (the id argument is ignored).
+      if (nrhs < 3 || mxGetClassID(prhs[2]) != mxSINGLE_CLASS || mxIsComplex(prhs[2]))
+        mexErrMsgIdAndTxt("odt:arg", "unwrap needs a real single phase array");
+      const mwSize* d = mxGetDimensions(prhs[2]);
+      const mwSize nd = mxGetNumberOfDimensions(prhs[2]);
+      if (nd > 3) mexErrMsgIdAndTxt("odt:arg", "phase must be 2D or 3D");
+      plhs[0] = mxCreateNumericArray(nd, d, mxSINGLE_CLASS, mxREAL);
+      odt_unwrap_args a{};
+      a.size[0] = (int32_t)d[0];
+      a.size[1] = (int32_t)d[1];
+      a.size[2] = nd == 3 ? (int32_t)d[2] : 1;
+      a.phase_in = mxGetSingles(prhs[2]);
+      a.phase_out = mxGetSingles(plhs[0]);
+      a.memory = ODT_MEM_HOST;
+      check(odt_unwrap_goldstein(&a));
+      break;
+    }
     default:
       mexErrMsgIdAndTxt("odt:arg", "unknown action %u", action);
   }

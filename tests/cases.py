@@ -56,3 +56,18 @@ def small_params(**kw):
 def small_RI(seed=3):
     return sphere_phantom(SMALL_SIZE, [0.1] * 3, NM, seed=seed, n_spheres=3,
                           radius_um=(0.4, 1.0))
+
+
+def wrapped_phase(shape, seed, noise=0.6, amp=25.0):
+    """Seeded wrapped phase maps [N1, N2, n] (single): a tall Gaussian bump
+    (steep enough to wrap many times) at a random centre per slice plus white
+    noise of the given standard deviation, wrapped to (-pi, pi]."""
+    rng = np.random.default_rng(seed)
+    N1, N2, n = shape
+    y, x = np.meshgrid(np.linspace(-1, 1, N1), np.linspace(-1, 1, N2), indexing="ij")
+    out = np.empty(shape, np.float32)
+    for z in range(n):
+        c = rng.uniform(-0.5, 0.5, 2)
+        phi = amp * np.exp(-((x - c[0]) ** 2 + (y - c[1]) ** 2) / 0.2) + rng.normal(0, noise, (N1, N2))
+        out[:, :, z] = np.angle(np.exp(1j * phi)).astype(np.float32)
+    return out

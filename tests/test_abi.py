@@ -38,3 +38,21 @@ def test_bad_handle_and_null_arguments():
     with pytest.raises(_lib.OdtError) as e:
         _lib.check(lib.odt_solve(77, None))
     assert e.value.status == 2
+
+
+def test_unwrap_argument_checks():
+    lib = _lib.load()
+    assert lib.odt_unwrap_goldstein(None) == 1
+    a = _lib.UnwrapArgs()
+    a.size[:] = [1, 8, 1]
+    assert lib.odt_unwrap_goldstein(C.byref(a)) == 1          # NULL phase
+    import numpy as np
+    buf = np.zeros(64, np.float32)
+    a.phase_in = a.phase_out = buf.ctypes.data
+    assert lib.odt_unwrap_goldstein(C.byref(a)) == 1          # size0 < 2
+    assert b"size" in lib.odt_last_error()
+    a.size[:] = [65536, 65536, 1]
+    assert lib.odt_unwrap_goldstein(C.byref(a)) == 1          # 2^32 elements
+    a.size[:] = [8, 8, 1]
+    a.memory = 5
+    assert lib.odt_unwrap_goldstein(C.byref(a)) == 1          # bad memory flag
