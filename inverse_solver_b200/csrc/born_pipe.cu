@@ -1,0 +1,316 @@
+// Pipelined x-pass of the Born iteration for x-lengths n = 8 * R2 (R2 odd):
+// the same arithmetic as born_x_body in mode Mid (inverse x-FFT, update of
+// iteration jj-1 for jj-1 >= 3, source term of iteration jj, forward x-FFT;
+// FORWARD_SOLVER_CONVERGENT_BORN.m:588-605, :616-642), restructured for the
+// B200 memory system:
+//
+//   * persistent CTAs (two per SM) walk the tiles of 16 x-lines; a tile of
+//     consecutive lines is one contiguous block of T, Field_n and Field, so
+//     one thread moves it into shared memory with bulk asynchronous copies
+//     (the TMA engine) completing on an mbarrier;
+//   * T of the next tile is copied while the current one is computed, and
+//     Field_n / Field of the next tile while the current one finishes its
+//     last FFT pass, so DRAM latency overlaps the FFT arithmetic instead of
+//     stalling it;
+//   * the plan is fixed at compile time: inverse radix-R2 pass (in place in
+//     the landing buffer: every thread holds its butterfly in registers across
+//     a barrier), fused inverse-8 / update / forward-8 pass, forward radix-R2
+//     pass written straight to global memory.
+//
+// Shared-memory layouts: landing buffers are the global layout [line][x]
+// (pitch n; with 16 lines and R1 = 8 the radix-R2 passes' accesses are
+// conflict-free for any odd R2), the mid pass writes a [line][x + x/8]
+// buffer with pitch = 8 (mod 16) (conflict-free stride-8 stores).
+#include <cuda_runtime.h>
+
+#include "cbs_kernels.cuh"
+#include "fft_core.cuh"
+#include "fft_tile.cuh"
+#include "tile_launch.cuh"
+#include "tma.cuh"
+
+namespace odt {
+namespace {
+
+constexpr int kW = 16;                 // x-lines per tile
+constexpr int kR1 = 8;
+constexpr int kThreads = kW * kR1;     // one radix-R2 butterfly per thread
+
+struct PipeLine {      // per-line constants of a tile
+  long long g;         // element offset of x = 0 in T / Field_n / Field
+  int v;               // element offset of x = 0 in V
+  int valid;
+  float my, mz;
+  float2 ry, rz;
+};
+
+constexpr size_t a16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+template <int N>
+struct PipeSmem {
+  static constexpr int kLdB = (N + N / 8 + 1) + ((8 - ((N + N / 8 + 1) & 15)) & 15);
+  static constexpr size_t kBars = 0;                                   // 3 mbarriers
+  static constexpr size_t kTw = 64;
+  static constexpr size_t kR0 = kTw + a16(sizeof(float2) * N);
+  static constexpr size_t kM0 = kR0 + a16(sizeof(float2) * N);
+  static constexpr size_t kLines = kM0 + a16(sizeof(float) * N);
+  static constexpr size_t kT0 = kLines + a16(sizeof(PipeLine) * kW);
+  static constexpr size_t kTile = sizeof(float2) * N * kW;
+  static constexpr size_t kT1 = kT0 + kTile;
+  static constexpr size_t kFn = kT1 + kTile;
+  static constexpr size_t kF = kFn + kTile;
+  static constexpr size_t kB = kF + kTile;
+  static constexpr size_t kTotal = kB + sizeof(float2) * kLdB * kW;
+};
+
+template <int R2>
+__global__ void __launch_bounds__(kThreads, 2)
+    born_x_pipe_kernel(const BornArgs a, const int jj, const float2* __restrict__ twg, const int ntiles,
+                       int* __restrict__ fault) {
+#if defined(__CUDA_ARCH__)
+  constexpr int N = kR1 * R2;
+  using L = PipeSmem<N>;
+  extern __shared__ __align__(128) unsigned char sm[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + L::kBars);  // [0], [1]: T stages, [2]: Fn/F
+  float2* tw = reinterpret_cast<float2*>(sm + L::kTw);
+  float2* r0t = reinterpret_cast<float2*>(sm + L::kR0);
+  float* m0t = reinterpret_cast<float*>(sm + L::kM0);
+  PipeLine* lines = reinterpret_cast<PipeLine*>(sm + L::kLines);
+  float2* const sT0 = reinterpret_cast<float2*>(sm + L::kT0);
+  float2* const sT1 = reinterpret_cast<float2*>(sm + L::kT1);
+  float2* sFn = reinterpret_cast<float2*>(sm + L::kFn);
+  float2* sF = reinterpret_cast<float2*>(sm + L::kF);
+  float2* sB = reinterpret_cast<float2*>(sm + L::kB);
+  const int tid = threadIdx.x;
+
+  for (int i = tid; i < N; i += kThreads) {
+    tw[i] = twg[i];
+    r0t[i] = a.acyclic ? a.ramp[0][i] : make_float2(1.f, 0.f);
+    m0t[i] = a.mask[0][i];
+  }
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init(&bar[2], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  int tile = blockIdx.x;
+  if (tile >= ntiles) return;
+
+  const int nty = (a.py + kW - 1) / kW;
+  const long long lineN = N;
+  // tile -> (illumination b fastest, then y-tile, then z): concurrent tiles
+  // share the V lines, which then come from L2
+  auto decode = [&](int t, int& b, int& y0, int& z, int& nl) {
+    b = t % a.nbatch;
+    const int r = t / a.nbatch;
+    const int ty = r % nty;
+    z = r / nty;
+    y0 = ty * kW;
+    nl = min(kW, a.py - y0);
+  };
+  auto tile_off = [&](int b, int y0, int z) {
+    return ((long long)y0 + (long long)a.py * (z + (long long)a.pz * b)) * lineN;
+  };
+  auto issue_T = [&](int t, int stage) {
+    int b, y0, z, nl;
+    decode(t, b, y0, z, nl);
+    const uint32_t bytes = (uint32_t)(nl * N * sizeof(float2));
+    mbar_arrive_expect_tx(&bar[stage], bytes);
+    bulk_g2s(stage ? sT1 : sT0, a.T + tile_off(b, y0, z), bytes, &bar[stage]);
+  };
+  auto issue_F = [&](int t) {
+    int b, y0, z, nl;
+    decode(t, b, y0, z, nl);
+    const uint32_t bytes = (uint32_t)(nl * N * sizeof(float2));
+    const long long o = tile_off(b, y0, z);
+    mbar_arrive_expect_tx(&bar[2], 2 * bytes);
+    bulk_g2s(sFn, a.Fn + o, bytes, &bar[2]);
+    bulk_g2s(sF, a.F + o, bytes, &bar[2]);
+  };
+  if (tid == 0) {
+    issue_T(tile, 0);
+    issue_F(tile);
+  }
+  uint32_t phT0 = 0, phT1 = 0, phF = 0;
+  const int e = jj - 1;  // iteration whose update completes here (>= 3)
+  const float2 cc = make_float2(0.f, a.c_im);
+  const float2 z2 = make_float2(0.f, 0.f);
+
+  for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+    const int s = it & 1;
+    const int next = tile + gridDim.x;
+    if (tid == 0 && next < ntiles) {
+      fence_proxy_async();
+      issue_T(next, s ^ 1);
+    }
+    int b, y0, z, nl;
+    decode(tile, b, y0, z, nl);
+    if (tid < kW) {
+      PipeLine P;
+      P.valid = tid < nl;
+      const int yy = P.valid ? y0 + tid : y0;
+      P.g = tile_off(b, yy, z);
+      P.v = (yy + a.py * z) * N;
+      P.my = a.mask[1][yy];
+      P.mz = a.mask[2][z];
+      P.ry = a.ramp[1][yy];
+      P.rz = a.ramp[2][z];
+      lines[tid] = P;
+    }
+    bool ok = mbar_wait(&bar[s], s ? phT1 : phT0);
+    if (s) phT1 ^= 1; else phT0 ^= 1;
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {  // give up; let this CTA's copies in flight land first
+        atomicCAS(fault, 0, kFaultTimeout);
+        if (next < ntiles) mbar_wait(&bar[s ^ 1], s ? phT0 : phT1);
+        mbar_wait(&bar[2], phF);
+      }
+      return;
+    }
+    float2* T0 = s ? sT1 : sT0;
+    // ---- inverse radix-R2 pass (ns = 1), in place
+    {
+      const int c = tid >> 3, j = tid & 7;
+      float2 v[R2];
+#pragma unroll
+      for (int r = 0; r < R2; ++r) v[r] = T0[c * N + j + kR1 * r];
+      Butterfly<R2, true>::run(v, tw, N);
+      __syncthreads();
+#pragma unroll
+      for (int r = 0; r < R2; ++r) T0[c * N + j * R2 + r] = v[r];
+    }
+    ok = mbar_wait(&bar[2], phF);
+    phF ^= 1;
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicCAS(fault, 0, kFaultTimeout);
+        if (next < ntiles) mbar_wait(&bar[s ^ 1], s ? phT0 : phT1);
+      }
+      return;
+    }
+    // ---- inverse radix-8 (ns = R2) -> update + source -> forward radix-8
+    for (int idx = tid; idx < kW * R2; idx += kThreads) {
+      const int c = idx / R2, j = idx - c * R2;
+      const PipeLine& Ln = lines[c];
+      float2 Vv[kR1];
+#pragma unroll
+      for (int r = 0; r < kR1; ++r) Vv[r] = a.V[Ln.v + j + R2 * r];
+      float2 v[kR1];
+#pragma unroll
+      for (int r = 0; r < kR1; ++r) v[r] = T0[c * N + j + R2 * r];
+#pragma unroll
+      for (int r = 1; r < kR1; ++r) {
+        float2 w = tw[r * j];
+        w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+      Butterfly<kR1, true>::run(v, tw, N);
+#pragma unroll
+      for (int r = 0; r < kR1; ++r) {
+        const int x = j + R2 * r;
+        const float2 V = Vv[r];
+        const float2 r0 = a.acyclic ? cmul(cmul(r0t[x], Ln.ry), Ln.rz) : make_float2(1.f, 0.f);
+        float2 P = v[r];
+        if (a.acyclic) P = cmul(P, (e & 1) ? r0 : cconj(r0));
+        const float m = (m0t[x] * Ln.my) * Ln.mz;
+        const float2 vP = cmul(V, P);
+        const float2 fo = sFn[c * N + x];
+        const float2 fp = sF[c * N + x];
+        const float2 psi = cmul(cmul(cc, fo), V);
+        const float2 fn = cscale(cadd(csub(fo, psi), vP), m);
+        float2 ftot, fn_new;
+        if (e == 3) {  // Field = (Field_n1 + Field_n2) + Field_n3; Field_n = Field_n3 + Field_n1
+          ftot = cadd(cadd(fp, fo), fn);
+          fn_new = cadd(fn, fp);
+        } else {
+          ftot = cadd(fp, fn);
+          fn_new = fn;
+        }
+        if (Ln.valid) {
+          a.F[Ln.g + x] = ftot;
+          a.Fn[Ln.g + x] = fn_new;
+        }
+        float2 src = cmul(cmul(cc, fn_new), V);
+        if (a.acyclic) src = cmul(src, (jj & 1) ? cconj(r0) : r0);
+        v[r] = Ln.valid ? src : z2;
+      }
+      Butterfly<kR1, false>::run(v, tw, N);
+#pragma unroll
+      for (int r = 0; r < kR1; ++r) {
+        const int row = j * kR1 + r;
+        sB[c * L::kLdB + row + (row >> 3)] = v[r];
+      }
+    }
+    __syncthreads();
+    if (tid == 0 && next < ntiles) {
+      fence_proxy_async();
+      issue_F(next);
+    }
+    // ---- forward radix-R2 pass (ns = 8) -> T
+    {
+      const int c = tid >> 3, j = tid & 7;
+      float2 v[R2];
+#pragma unroll
+      for (int r = 0; r < R2; ++r) {
+        const int row = j + kR1 * r;
+        v[r] = sB[c * L::kLdB + row + (row >> 3)];
+      }
+#pragma unroll
+      for (int r = 1; r < R2; ++r) v[r] = cmul(v[r], tw[r * j]);
+      Butterfly<R2, false>::run(v, tw, N);
+      if (c < nl) {
+        float2* out = a.T + tile_off(b, y0 + c, z);
+#pragma unroll
+        for (int r = 0; r < R2; ++r) out[j + kR1 * r] = v[r];
+      }
+    }
+    __syncthreads();
+  }
+#endif
+}
+
+template <int R2>
+cudaError_t launch_r2(const BornArgs& a, int jj, const DevFft& fx, int* fault, cudaStream_t s) {
+  using L = PipeSmem<kR1 * R2>;
+  static int configured = -1;   // per process: attribute set once per device
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (configured != dev) {
+    e = cudaFuncSetAttribute(born_x_pipe_kernel<R2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)L::kTotal);
+    if (e != cudaSuccess) return e;
+    configured = dev;
+  }
+  int nsm = 0;
+  e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  const int nty = (a.py + kW - 1) / kW;
+  const long long ntiles = (long long)nty * a.pz * a.nbatch;
+  const int grid = (int)(ntiles < 2LL * nsm ? ntiles : 2LL * nsm);
+  born_x_pipe_kernel<R2><<<grid, kThreads, L::kTotal, s>>>(a, jj, fx.tw, (int)ntiles, fault);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+bool born_x_pipe_supported(const BornArgs& a, const DevFft& fx) {
+  if (fx.plan.n != a.px || a.px % kR1 != 0) return false;
+  const int r2 = a.px / kR1;
+  if (r2 != 11 && r2 != 15 && r2 != 19) return false;
+  const long long ntiles = (long long)((a.py + kW - 1) / kW) * a.pz * a.nbatch;
+  return ntiles < (1LL << 31);
+}
+
+cudaError_t launch_born_x_pipe(const BornArgs& a, int jj, const DevFft& fx, int* fault, cudaStream_t s) {
+  switch (a.px / kR1) {
+    case 11: return launch_r2<11>(a, jj, fx, fault, s);
+    case 15: return launch_r2<15>(a, jj, fx, fault, s);
+    case 19: return launch_r2<19>(a, jj, fx, fault, s);
+    default: return cudaErrorNotSupported;
+  }
+}
+
+}  // namespace odt

@@ -45,6 +45,12 @@ enum BornXMode { kBornFirst = 0, kBornMid = 1, kBornLast = 2 };
 // x-pass of iteration jj: inverse x-FFT + update of iteration jj-1 (Mid/Last)
 // and source term + forward x-FFT of iteration jj (First/Mid).
 cudaError_t launch_born_x(const BornArgs& a, int mode, int jj, const DevFft& fx, cudaStream_t s);
+// Pipelined x-pass (persistent CTAs, bulk asynchronous copies) for mode Mid
+// with jj >= 4 and x-lengths 8 * {11, 15, 19}; same results as launch_born_x.
+// A wait that times out sets *fault (device int) and ends the kernel.
+bool born_x_pipe_supported(const BornArgs& a, const DevFft& fx);
+cudaError_t launch_born_x_pipe(const BornArgs& a, int jj, const DevFft& fx, int* fault,
+                               cudaStream_t s);
 // z-pass of iteration jj: forward z-FFT, Green's multiply, inverse z-FFT.
 cudaError_t launch_born_z(const BornArgs& a, int jj, const DevFft& fz, cudaStream_t s);
 

@@ -12,6 +12,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -122,7 +123,12 @@ struct Handle {
   float2* out_t = nullptr;
   float2* out_r = nullptr;
   unsigned int* d_count = nullptr;
+  int* d_fault = nullptr;       // set by a pipelined kernel whose wait timed out
   std::vector<void*> batch_allocs;
+
+  // kernel selection: the pipelined x-pass where it applies (ODT_KERNELS=generic
+  // in the environment at odt_create selects the generic tile kernels)
+  bool use_pipe = true;
 
   // profiling
   bool profiling = false;
@@ -293,6 +299,8 @@ void ensure_batch(Handle& H, int nb) {
   H.c2a = H.dalloc<float2>((size_t)H.nc2() * nb, true);
   H.c2b = H.dalloc<float2>((size_t)H.nc2() * nb, true);
   H.d_count = H.dalloc<unsigned int>(1, true);
+  H.d_fault = H.dalloc<int>(1, true);
+  ODT_CUDA(cudaMemset(H.d_fault, 0, sizeof(int)));
   H.batch = nb;
 }
 
@@ -317,6 +325,17 @@ void fftc2(Handle& H, float2* x, const DevFft& f0, const DevFft& f1, long long n
   ODT_CUDA(launch_fft_lines(x, x, (long long)n1 * nslices, n0 / 2, n0 / 2, 1.0f, inverse, f0, s));
   ODT_CUDA(launch_fft_cols(x, x, n0, nslices, n1 / 2, n1 / 2, sc, inverse, f1, s));
   H.mark_end(s);
+}
+
+// A pipelined kernel whose bounded wait ran out leaves a fault code behind.
+void check_fault(Handle& H) {
+  int f = 0;
+  ODT_CUDA(cudaMemcpy(&f, H.d_fault, sizeof(f), cudaMemcpyDeviceToHost));
+  if (f) {
+    ODT_CUDA(cudaMemset(H.d_fault, 0, sizeof(int)));
+    raise(ODT_ERR_INTERNAL, "a pipelined Born kernel timed out waiting for its copies (code " +
+                                std::to_string(f) + ")");
+  }
 }
 
 void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int slot,
@@ -381,9 +400,13 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
   a.Einc = H.einc;
   a.Fout = fout;
   const int B = P.pp.bornmax;
+  const bool pipe_x = H.use_pipe && born_x_pipe_supported(a, H.fx);
   for (int jj = 1; jj <= B; ++jj) {
     H.mark_begin(kKBornX, s);
-    ODT_CUDA(launch_born_x(a, jj == 1 ? kBornFirst : kBornMid, jj, H.fx, s));
+    if (pipe_x && jj >= 4)
+      ODT_CUDA(launch_born_x_pipe(a, jj, H.fx, H.d_fault, s));
+    else
+      ODT_CUDA(launch_born_x(a, jj == 1 ? kBornFirst : kBornMid, jj, H.fx, s));
     H.mark_end(s);
     H.mark_begin(kKBornY, s);
     ODT_CUDA(launch_fft_cols(a.T, a.T, a.px, (long long)a.pz * nb, 0, 0, 1.0f, false, H.fy, s));
@@ -530,6 +553,7 @@ odt_status odt_create(const odt_geometry* geom, const odt_cfloat* refocus,
     auto H = std::make_shared<Handle>();
     H->g = g;
     H->budget = (size_t)g.mem_budget;
+    if (const char* k = std::getenv("ODT_KERNELS")) H->use_pipe = std::string(k) != "generic";
     ODT_CUDA(cudaStreamCreateWithFlags(&H->own_stream, cudaStreamNonBlocking));
     H->fx = make_dev_fft(*H, g.sim_size[0], kKindBornX, "sim_size(1)");
     H->fy = make_dev_fft(*H, g.sim_size[1], kKindCols, "sim_size(2)");
@@ -621,6 +645,7 @@ odt_status odt_solve(odt_handle h, const odt_solve_args* args) {
       H->collect(s);
     }
     if (!dev) {
+      check_fault(*H);
       unsigned int cnt = 0;
       ODT_CUDA(cudaMemcpy(&cnt, H->d_count, sizeof(cnt), cudaMemcpyDeviceToHost));
       if (cnt) raise(ODT_ERR_NUMERIC, "odt_solve: " + std::to_string(cnt) +
@@ -688,6 +713,7 @@ odt_status odt_gradient(odt_handle h, const odt_gradient_args* args) {
     }
     ODT_CUDA(cudaMemcpyAsync(A.err, H->d_err, sizeof(double), cudaMemcpyDeviceToHost, s));
     ODT_CUDA(cudaStreamSynchronize(s));
+    check_fault(*H);
   });
 }
 
