@@ -51,6 +51,15 @@ cudaError_t launch_born_x(const BornArgs& a, int mode, int jj, const DevFft& fx,
 bool born_x_pipe_supported(const BornArgs& a, const DevFft& fx);
 cudaError_t launch_born_x_pipe(const BornArgs& a, int jj, const DevFft& fx, int* fault,
                                cudaStream_t s);
+// Pipelined column passes (persistent CTAs, tiled TMA copies) for lengths
+// 8 * {11, 15, 19} along y / z: the y-FFT of the Born loop in place on a.T,
+// and the z-pass; same results as launch_fft_cols / launch_born_z up to the
+// order of the radix passes of the inverse y-FFT.
+bool cols_pipe_supported(const BornArgs& a, const DevFft& f, bool zpass);
+cudaError_t launch_fft_y_pipe(const BornArgs& a, bool inverse, const DevFft& fy, int* fault,
+                              cudaStream_t s);
+cudaError_t launch_born_z_pipe(const BornArgs& a, int jj, const DevFft& fz, int* fault,
+                               cudaStream_t s);
 // z-pass of iteration jj: forward z-FFT, Green's multiply, inverse z-FFT.
 cudaError_t launch_born_z(const BornArgs& a, int jj, const DevFft& fz, cudaStream_t s);
 

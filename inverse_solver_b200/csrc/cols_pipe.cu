@@ -1,0 +1,334 @@
+// Pipelined column passes of the Born iteration for lengths n = 8 * R2 (R2
+// odd): the y-FFTs (forward / inverse, in place on T) and the z-pass
+// (forward z-FFT, Green's multiply G(k -/+ dk/4) / N, inverse z-FFT;
+// FORWARD_SOLVER_CONVERGENT_BORN.m:606-615) -- the same transforms as
+// fft_cols_body / born_z_body, restructured like the pipelined x-pass:
+//
+//   * persistent CTAs (three per SM) walk tiles of 16 adjacent columns;
+//   * a tile (16 columns x n rows, each row a 128-byte segment at a stride of
+//     px or px*py elements) arrives in shared memory through one tiled TMA
+//     copy (cp.async.bulk.tensor, 3D map for y, 4D for z) on an mbarrier,
+//     while the CTA computes the previous tile from the other stage;
+//   * fixed plan: radix-R2 pass in place in the landing buffer (one butterfly
+//     per thread held in registers across a barrier), then radix-8 with
+//     twiddles (y: straight to global memory; z: Green's multiply and the
+//     first inverse radix-8 pass into a second buffer, then the inverse
+//     radix-R2 pass to global memory).
+//
+// Layout in shared memory: [row][column], 16 columns = 128 bytes per row; the
+// column index is the fastest thread index, so every access of a half-warp
+// covers one row: conflict-free.  Columns past the grid edge arrive as zeros
+// (TMA out-of-bounds fill) and are not stored.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "cbs_kernels.cuh"
+#include "fft_core.cuh"
+#include "tma.cuh"
+
+namespace odt {
+namespace {
+
+constexpr int kW = 16;               // columns per tile
+constexpr int kR1 = 8;
+constexpr int kThreads = kW * kR1;   // one radix-R2 butterfly per thread
+
+constexpr size_t a16(size_t b) { return (b + 15) & ~(size_t)15; }
+constexpr size_t a1k(size_t b) { return (b + 1023) & ~(size_t)1023; }
+
+// Tiled TMA copies need 128-byte aligned shared-memory destinations; the tile
+// buffers start on 1024-byte boundaries (the dynamic window itself is
+// 1024-byte aligned, checked at run time).
+template <int N>
+struct ColSmem {
+  static constexpr size_t kTw = 64;                                  // after 3 mbarriers
+  static constexpr size_t kKz = kTw + a16(sizeof(float2) * N);       // kq2 along z (born_z)
+  static constexpr size_t kGxy = kKz + a16(sizeof(float) * N);
+  static constexpr size_t kTile = sizeof(float2) * N * kW;           // 1024 * R2 bytes
+  static constexpr size_t kS0 = a1k(kGxy + a16(sizeof(float) * kW));
+  static constexpr size_t kS1 = kS0 + kTile;
+  static constexpr size_t kB = kS1 + kTile;
+  static constexpr size_t kTotalY = kB;                             // y-pass: no second buffer
+  static constexpr size_t kTotalZ = kB + kTile;
+};
+
+#if defined(__CUDA_ARCH__)
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(dst)),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                            int c3, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_addr(dst)),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_addr(bar))
+      : "memory");
+}
+#endif
+
+// KIND 0: forward y-FFT, 1: inverse y-FFT, 2: z-pass with Green's multiply.
+// Tile t -> (x-tile fastest, then the outer index o): y-pass o = z + pz*b
+// (3D map {px, py, pz*nb}), z-pass o = y + py*b (4D map {px, py, pz, nb}).
+template <int R2, int KIND>
+__global__ void __launch_bounds__(kThreads, 3)
+    cols_pipe_kernel(const __grid_constant__ CUtensorMap map, const BornArgs a, const int jj,
+                     const float2* __restrict__ twg, const int nxt, const int ntiles,
+                     int* __restrict__ fault) {
+#if defined(__CUDA_ARCH__)
+  constexpr int N = kR1 * R2;
+  constexpr bool kZ = KIND == 2;
+  constexpr bool kInvFirst = KIND == 1;  // direction of the first transform
+  using L = ColSmem<N>;
+  extern __shared__ __align__(128) unsigned char sm[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
+  float2* tw = reinterpret_cast<float2*>(sm + L::kTw);
+  float* kz = reinterpret_cast<float*>(sm + L::kKz);
+  float* gxy = reinterpret_cast<float*>(sm + L::kGxy);
+  float2* const s0 = reinterpret_cast<float2*>(sm + L::kS0);
+  float2* const s1 = reinterpret_cast<float2*>(sm + L::kS1);
+  float2* const sB = reinterpret_cast<float2*>(sm + L::kB);
+  const int tid = threadIdx.x;
+  const bool flip = kZ && a.acyclic && (jj & 1);
+  if ((smem_addr(s0) & 127u) != 0u || (smem_addr(s1) & 127u) != 0u) {  // never issue a misaligned copy
+    if (tid == 0) atomicCAS(fault, 0, kFaultAlign);
+    return;
+  }
+
+  for (int i = tid; i < N; i += kThreads) {
+    tw[i] = twg[i];
+    if (kZ) kz[i] = a.kq2[2][flip ? (i == 0 ? 0 : N - i) : i];
+  }
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  int tile = blockIdx.x;
+  if (tile >= ntiles) return;
+  const long long rstride = kZ ? (long long)a.px * a.py : a.px;   // element stride between rows
+  constexpr uint32_t kBytes = (uint32_t)(sizeof(float2) * N * kW);
+  auto issue = [&](int t, int stage) {
+    const int xt = t % nxt, o = t / nxt;
+    mbar_arrive_expect_tx(&bar[stage], kBytes);
+    float2* dst = stage ? s1 : s0;
+    if (kZ) tma_load_4d(dst, &map, 2 * kW * xt, o % a.py, 0, o / a.py, &bar[stage]);
+    else tma_load_3d(dst, &map, 2 * kW * xt, 0, o, &bar[stage]);
+  };
+  if (tid == 0) issue(tile, 0);
+  uint32_t ph0 = 0, ph1 = 0;
+  const int c = tid & (kW - 1), jr = tid >> 4;   // column, butterfly of the radix-R2 passes
+
+  for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+    const int s = it & 1;
+    const int next = tile + gridDim.x;
+    if (tid == 0 && next < ntiles) {
+      fence_proxy_async();
+      issue(next, s ^ 1);
+    }
+    const int xt = tile % nxt, o = tile / nxt;
+    const int x0 = kW * xt;
+    const int ncol = min(kW, a.px - x0);
+    if (kZ && tid < kW) {
+      const int y = o % a.py;
+      const int kx = min(x0 + tid, a.px - 1);
+      const int ix = flip ? (kx == 0 ? 0 : a.px - kx) : kx;
+      const int iy = flip ? (y == 0 ? 0 : a.py - y) : y;
+      gxy[tid] = a.kq2[0][ix] + a.kq2[1][iy];
+    }
+    const bool ok = mbar_wait(&bar[s], s ? ph1 : ph0);
+    if (s) ph1 ^= 1; else ph0 ^= 1;
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {  // give up; let the copy in flight land first
+        atomicCAS(fault, 0, kFaultTimeout);
+        if (next < ntiles) mbar_wait(&bar[s ^ 1], s ? ph0 : ph1);
+      }
+      return;
+    }
+    float2* S = s ? s1 : s0;
+    // ---- radix-R2 pass (ns = 1), in place: rows jr + 8r -> rows jr*R2 + r
+    {
+      float2 v[R2];
+#pragma unroll
+      for (int r = 0; r < R2; ++r) v[r] = S[(jr + kR1 * r) * kW + c];
+      Butterfly<R2, kInvFirst>::run(v, tw, N);
+      __syncthreads();
+#pragma unroll
+      for (int r = 0; r < R2; ++r) S[(jr * R2 + r) * kW + c] = v[r];
+    }
+    __syncthreads();
+    // global address of (row, column) of this tile
+    long long gbase;
+    if (kZ) {
+      const int y = o % a.py, b = o / a.py;
+      gbase = (long long)b * a.nvox + (long long)y * a.px + x0;
+    } else {
+      gbase = (long long)o * a.px * a.py + x0;
+    }
+    // ---- radix-8 pass (ns = R2): rows j + R2 r, twiddles tw[r j]
+    for (int idx = tid; idx < kW * R2; idx += kThreads) {
+      const int j = idx >> 4;  // c is idx & 15 == tid & 15
+      float2 v[kR1];
+#pragma unroll
+      for (int r = 0; r < kR1; ++r) v[r] = S[(j + R2 * r) * kW + c];
+#pragma unroll
+      for (int r = 1; r < kR1; ++r) {
+        float2 w = tw[r * j];
+        if (kInvFirst) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+      Butterfly<kR1, kInvFirst>::run(v, tw, N);
+      if (!kZ) {
+        if (c < ncol) {
+          float2* out = a.T + gbase + c;
+#pragma unroll
+          for (int r = 0; r < kR1; ++r) out[(j + R2 * r) * rstride] = v[r];
+        }
+      } else {
+        // Green's multiply at kz = j + R2 r, then the first inverse radix-8
+        // pass (ns = 1) into rows 8 j + r of the second buffer
+        const float qxy = gxy[c];
+#pragma unroll
+        for (int r = 0; r < kR1; ++r) {
+          float q = qxy + kz[j + R2 * r];
+          q = a.g_scale * q - a.g_off;
+          const float rden = __frcp_rn(q * q + a.eps * a.eps);
+          const float2 G = make_float2(q * rden, a.eps * rden);  // 1 / (q - i eps)
+          v[r] = cscale(cmul(G, v[r]), a.inv_n);
+        }
+        Butterfly<kR1, true>::run(v, tw, N);
+#pragma unroll
+        for (int r = 0; r < kR1; ++r) sB[(j * kR1 + r) * kW + c] = v[r];
+      }
+    }
+    if (kZ) {
+      __syncthreads();
+      // ---- inverse radix-R2 pass (ns = 8): rows jr + 8 r, twiddles conj(tw[r jr])
+      float2 v[R2];
+#pragma unroll
+      for (int r = 0; r < R2; ++r) v[r] = sB[(jr + kR1 * r) * kW + c];
+#pragma unroll
+      for (int r = 1; r < R2; ++r) {
+        float2 w = tw[r * jr];
+        w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+      Butterfly<R2, true>::run(v, tw, N);
+      if (c < ncol) {
+        float2* out = a.T + gbase + c;
+#pragma unroll
+        for (int r = 0; r < R2; ++r) out[(jr + kR1 * r) * rstride] = v[r];
+      }
+    }
+    __syncthreads();
+  }
+#endif
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// T viewed as float32 pairs: dims (inner first) {2*px, py, pz*nb} (y-pass) or
+// {2*px, py, pz, nb} (z-pass); box 32 floats = 16 complex columns.
+bool make_map(const BornArgs& a, bool zpass, CUtensorMap* m) {
+  auto enc = encoder();
+  if (!enc) return false;
+  const cuuint64_t px2 = 2ull * a.px;
+  const cuuint64_t rowb = (cuuint64_t)a.px * sizeof(float2);
+  const cuuint64_t planeb = rowb * a.py;
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r;
+  if (!zpass) {
+    const cuuint64_t dims[3] = {px2, (cuuint64_t)a.py, (cuuint64_t)a.pz * a.nbatch};
+    const cuuint64_t strides[2] = {rowb, planeb};
+    const cuuint32_t box[3] = {2 * kW, (cuuint32_t)a.py, 1};
+    r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, a.T, dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  } else {
+    const cuuint64_t dims[4] = {px2, (cuuint64_t)a.py, (cuuint64_t)a.pz, (cuuint64_t)a.nbatch};
+    const cuuint64_t strides[3] = {rowb, planeb, planeb * a.pz};
+    const cuuint32_t box[4] = {2 * kW, 1, (cuuint32_t)a.pz, 1};
+    r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, a.T, dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  }
+  return r == CUDA_SUCCESS;
+}
+
+template <int R2, int KIND>
+cudaError_t launch_kind(const BornArgs& a, int jj, const DevFft& f, int* fault, cudaStream_t s) {
+  using L = ColSmem<kR1 * R2>;
+  constexpr size_t smem = KIND == 2 ? L::kTotalZ : L::kTotalY;
+  static int configured = -1;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (configured != dev) {
+    e = cudaFuncSetAttribute(cols_pipe_kernel<R2, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+    if (e != cudaSuccess) return e;
+    configured = dev;
+  }
+  CUtensorMap map;
+  if (!make_map(a, KIND == 2, &map)) return cudaErrorInvalidValue;
+  int nsm = 0;
+  e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  const int nxt = (a.px + kW - 1) / kW;
+  const long long nout = KIND == 2 ? (long long)a.py * a.nbatch : (long long)a.pz * a.nbatch;
+  const long long ntiles = nout * nxt;
+  const int grid = (int)(ntiles < 3LL * nsm ? ntiles : 3LL * nsm);
+  cols_pipe_kernel<R2, KIND><<<grid, kThreads, smem, s>>>(map, a, jj, f.tw, nxt, (int)ntiles, fault);
+  return cudaGetLastError();
+}
+
+template <int KIND>
+cudaError_t dispatch(const BornArgs& a, int jj, const DevFft& f, int* fault, cudaStream_t s) {
+  switch (f.plan.n / kR1) {
+    case 11: return launch_kind<11, KIND>(a, jj, f, fault, s);
+    case 15: return launch_kind<15, KIND>(a, jj, f, fault, s);
+    case 19: return launch_kind<19, KIND>(a, jj, f, fault, s);
+    default: return cudaErrorNotSupported;
+  }
+}
+
+}  // namespace
+
+bool cols_pipe_supported(const BornArgs& a, const DevFft& f, bool zpass) {
+  const int n = f.plan.n;
+  if (n != (zpass ? a.pz : a.py) || n % kR1 != 0) return false;
+  const int r2 = n / kR1;
+  if (r2 != 11 && r2 != 15 && r2 != 19) return false;
+  if (a.px % 2 != 0 || !encoder()) return false;   // row strides must be multiples of 16 bytes
+  const long long nout = zpass ? (long long)a.py * a.nbatch : (long long)a.pz * a.nbatch;
+  return nout * ((a.px + kW - 1) / kW) < (1LL << 31);
+}
+
+cudaError_t launch_fft_y_pipe(const BornArgs& a, bool inverse, const DevFft& fy, int* fault,
+                              cudaStream_t s) {
+  return inverse ? dispatch<1>(a, 0, fy, fault, s) : dispatch<0>(a, 0, fy, fault, s);
+}
+
+cudaError_t launch_born_z_pipe(const BornArgs& a, int jj, const DevFft& fz, int* fault, cudaStream_t s) {
+  return dispatch<2>(a, jj, fz, fault, s);
+}
+
+}  // namespace odt

@@ -401,6 +401,8 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
   a.Fout = fout;
   const int B = P.pp.bornmax;
   const bool pipe_x = H.use_pipe && born_x_pipe_supported(a, H.fx);
+  const bool pipe_y = H.use_pipe && cols_pipe_supported(a, H.fy, false);
+  const bool pipe_z = H.use_pipe && cols_pipe_supported(a, H.fz, true);
   for (int jj = 1; jj <= B; ++jj) {
     H.mark_begin(kKBornX, s);
     if (pipe_x && jj >= 4)
@@ -409,13 +411,22 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
       ODT_CUDA(launch_born_x(a, jj == 1 ? kBornFirst : kBornMid, jj, H.fx, s));
     H.mark_end(s);
     H.mark_begin(kKBornY, s);
-    ODT_CUDA(launch_fft_cols(a.T, a.T, a.px, (long long)a.pz * nb, 0, 0, 1.0f, false, H.fy, s));
+    if (pipe_y)
+      ODT_CUDA(launch_fft_y_pipe(a, false, H.fy, H.d_fault, s));
+    else
+      ODT_CUDA(launch_fft_cols(a.T, a.T, a.px, (long long)a.pz * nb, 0, 0, 1.0f, false, H.fy, s));
     H.mark_end(s);
     H.mark_begin(kKBornZ, s);
-    ODT_CUDA(launch_born_z(a, jj, H.fz, s));
+    if (pipe_z)
+      ODT_CUDA(launch_born_z_pipe(a, jj, H.fz, H.d_fault, s));
+    else
+      ODT_CUDA(launch_born_z(a, jj, H.fz, s));
     H.mark_end(s);
     H.mark_begin(kKBornY, s);
-    ODT_CUDA(launch_fft_cols(a.T, a.T, a.px, (long long)a.pz * nb, 0, 0, 1.0f, true, H.fy, s));
+    if (pipe_y)
+      ODT_CUDA(launch_fft_y_pipe(a, true, H.fy, H.d_fault, s));
+    else
+      ODT_CUDA(launch_fft_cols(a.T, a.T, a.px, (long long)a.pz * nb, 0, 0, 1.0f, true, H.fy, s));
     H.mark_end(s);
   }
   H.mark_begin(kKBornX, s);

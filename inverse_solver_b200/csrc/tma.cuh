@@ -73,6 +73,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 #endif  // __CUDA_ARCH__
 
 // fault codes written by the pipelined kernels (first one wins)
-enum PipeFault { kFaultNone = 0, kFaultTimeout = 1 };
+enum PipeFault { kFaultNone = 0, kFaultTimeout = 1, kFaultAlign = 2 };
 
 }  // namespace odt

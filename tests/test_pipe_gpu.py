@@ -1,9 +1,11 @@
-"""GPU parity of the pipelined x-pass (csrc/born_pipe.cu: persistent CTAs,
-bulk asynchronous copies, compile-time 8 x R2 plans), which the library
-selects for x-lengths 88, 120 and 152 from iteration 4 on.
+"""GPU parity of the pipelined Born passes (csrc/born_pipe.cu, the x-pass;
+csrc/cols_pipe.cu, the y-FFTs and the z-pass: persistent CTAs, bulk / tiled
+asynchronous copies, compile-time 8 x R2 plans), which the library selects
+for grid lengths 88, 120 and 152.
 
-  * against the single-precision oracle at x = 88, 120, 152 (relative L2
-    per illumination 1e-5 for the transmitted and 3D fields, 3e-5 reflected);
+  * against the single-precision oracle on grids that put each of 88, 120
+    and 152 on each axis (relative L2 per illumination 1e-5 for the
+    transmitted and 3D fields, 3e-5 reflected);
   * against the library's generic tile kernels (ODT_KERNELS=generic) on the
     benchmark's 152^3 grid with a partial last y-tile and several batches:
     relative L2 <= 1e-6 (the same operations; only the compiler's
@@ -43,14 +45,15 @@ def _solve(p, RI, fields, kernels=None):
     return out, info
 
 
-@pytest.mark.parametrize("nx", [64, 96, 128])
-def test_pipe_x_pass_matches_oracle(nx):
-    size = [nx, 24, 16]
+@pytest.mark.parametrize("size", [[64, 96, 64], [128, 24, 128], [96, 64, 16]])
+def test_pipe_passes_match_oracle(size):
+    """Padded grids (88, 120, 88), (152, 48, 152), (120, 88, 40)."""
     p = cases.params(size, [6, 6, 6], return_reflection=True, return_3D=True)
-    RI = cases.sphere_phantom(size, [0.1] * 3, cases.NM, seed=nx, n_spheres=3, radius_um=(0.3, 0.8))
-    fields = cases.circle_fields(p, 3)
+    RI = cases.sphere_phantom(size, [0.1] * 3, cases.NM, seed=size[0], n_spheres=3,
+                              radius_um=(0.3, 0.8))
+    fields = cases.circle_fields(p, 2)
     (t, r, f), (sim, bm) = _solve(p, RI, fields)
-    assert sim[0] == nx + 24 and bm >= 4
+    assert sim == [v + 24 for v in size] and bm >= 4
     o = cbs.ForwardSolverCBS(p, single=True)
     o.set_RI(RI)
     ot, orr, of = o.solve(fields)
