@@ -35,9 +35,11 @@ GRID = [128, 128, 128]
 N_ILL = 49
 SEED = 0
 # algorithmic HBM bytes per voxel and launch of each Born kernel kind
-# (complex64 = 8 B): born_x reads T, Field_n, Field, V and
-# writes T, Field_n, Field; born_y / born_z read and write T once.
-ALG_BYTES_PER_VOXEL = {"born_x": 56, "born_y": 16, "born_z": 16}
+# (complex64 = 8 B): born_x reads T, Field_n, Field, V and writes T, Field_n,
+# Field; born_y / born_z read and write T once.  "_pipe" = the pipelined
+# (TMA-fed, persistent) variants of the same passes.
+ALG_BYTES_PER_VOXEL = {"born_x": 56, "born_y": 16, "born_z": 16,
+                       "born_x_pipe": 56, "born_y_pipe": 16, "born_z_pipe": 16}
 
 
 def workload_params():

@@ -74,8 +74,10 @@ struct DeviceGuard {
   }
 };
 
-const char* const kKindNames[] = {"born_x", "born_y", "born_z", "io_fft", "io_elementwise"};
-enum Kind { kKBornX = 0, kKBornY, kKBornZ, kKIoFft, kKIoElem, kNumKinds };
+const char* const kKindNames[] = {"born_x", "born_y", "born_z", "io_fft", "io_elementwise",
+                                  "born_x_pipe", "born_y_pipe", "born_z_pipe"};
+enum Kind { kKBornX = 0, kKBornY, kKBornZ, kKIoFft, kKIoElem, kKBornXPipe, kKBornYPipe, kKBornZPipe,
+            kNumKinds };
 
 struct Handle {
   odt_geometry g{};
@@ -404,25 +406,27 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
   const bool pipe_y = H.use_pipe && cols_pipe_supported(a, H.fy, false);
   const bool pipe_z = H.use_pipe && cols_pipe_supported(a, H.fz, true);
   for (int jj = 1; jj <= B; ++jj) {
-    H.mark_begin(kKBornX, s);
-    if (pipe_x && jj >= 4)
+    if (pipe_x && jj >= 4) {
+      H.mark_begin(kKBornXPipe, s);
       ODT_CUDA(launch_born_x_pipe(a, jj, H.fx, H.d_fault, s));
-    else
+    } else {
+      H.mark_begin(kKBornX, s);
       ODT_CUDA(launch_born_x(a, jj == 1 ? kBornFirst : kBornMid, jj, H.fx, s));
+    }
     H.mark_end(s);
-    H.mark_begin(kKBornY, s);
+    H.mark_begin(pipe_y ? kKBornYPipe : kKBornY, s);
     if (pipe_y)
       ODT_CUDA(launch_fft_y_pipe(a, false, H.fy, H.d_fault, s));
     else
       ODT_CUDA(launch_fft_cols(a.T, a.T, a.px, (long long)a.pz * nb, 0, 0, 1.0f, false, H.fy, s));
     H.mark_end(s);
-    H.mark_begin(kKBornZ, s);
+    H.mark_begin(pipe_z ? kKBornZPipe : kKBornZ, s);
     if (pipe_z)
       ODT_CUDA(launch_born_z_pipe(a, jj, H.fz, H.d_fault, s));
     else
       ODT_CUDA(launch_born_z(a, jj, H.fz, s));
     H.mark_end(s);
-    H.mark_begin(kKBornY, s);
+    H.mark_begin(pipe_y ? kKBornYPipe : kKBornY, s);
     if (pipe_y)
       ODT_CUDA(launch_fft_y_pipe(a, true, H.fy, H.d_fault, s));
     else
