@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define ODT_ABI_VERSION 1
+#define ODT_ABI_VERSION 2
 
 typedef enum odt_status {
   ODT_OK = 0,
@@ -69,6 +69,11 @@ typedef struct odt_geometry {
   int32_t device;        /* CUDA device ordinal (CudaBorn's used_gpu)            */
   int32_t max_batch;     /* illuminations resident on the device at once; 0=auto */
   int64_t mem_budget;    /* bytes this handle may allocate; 0 = half the free HBM */
+  int32_t pol;           /* 0 or 1: scalar Green's function (pole_num = 1);
+                            3: dyadic Green's function (vector_simulation,
+                            pole_num = 3): input / output fields carry 2
+                            polarisations, the 3D field 3 components
+                            (FORWARD_SOLVER_CONVERGENT_BORN.m:293-296) */
 } odt_geometry;
 
 /*
@@ -98,15 +103,22 @@ typedef struct odt_potential_params {
   const float* mask[3];
   const odt_cfloat* ramp[3];
   const float* kq2[3];
+  /* dyadic handles (pol = 3) only: rads(:,:,:,a) = shifted k-coordinate / k0_nm
+   * along axis a in FFT (ifftshifted) order (:316-319, :385), and the
+   * absorptive correction (2 pi k0_nm)^2 / ((2 pi k0_nm)^2 + i eps_imag) of
+   * the dyadic Green's function (:322) */
+  const float* rad[3];
+  odt_cfloat absorb;
 } odt_potential_params;
 
-/* Outputs of odt_solve; any pointer may be NULL to skip that output. */
+/* Outputs of odt_solve; any pointer may be NULL to skip that output.  npol
+ * = 1 for scalar handles, 2 for dyadic ones; ncomp = 1 or 3. */
 typedef struct odt_solve_args {
-  const odt_cfloat* fields_in; /* [F_x, F_y, n_ill] spatial input fields      */
+  const odt_cfloat* fields_in; /* [F_x, F_y, npol, n_ill] spatial input fields */
   int32_t n_ill;
-  odt_cfloat* trans;           /* [F_x, F_y, n_ill] transmitted field          */
-  odt_cfloat* ref;             /* [F_x, F_y, n_ill] reflected field            */
-  odt_cfloat* field3d;         /* [ri_x, ri_y, ri_z, n_ill] total 3D field     */
+  odt_cfloat* trans;           /* [F_x, F_y, npol, n_ill] transmitted field    */
+  odt_cfloat* ref;             /* [F_x, F_y, npol, n_ill] reflected field      */
+  odt_cfloat* field3d;         /* [ri_x, ri_y, ri_z, ncomp, n_ill] 3D field    */
   int32_t memory;              /* ODT_MEM_HOST or ODT_MEM_DEVICE               */
   void* stream;                /* cudaStream_t for ODT_MEM_DEVICE (NULL = the
                                   legacy default stream); ignored for host   */
@@ -126,6 +138,19 @@ typedef struct odt_solve_args {
 odt_status odt_create(const odt_geometry* geom, const odt_cfloat* refocus,
                       const odt_cfloat* kernel_trans, const odt_cfloat* kernel_ref,
                       const float* pupil_in, const float* pupil_out, odt_handle* out);
+
+/*
+ * Polarisation basis of a dyadic handle (polarisation_utility,
+ * FORWARD_SOLVER.m:131-180), per pixel of the [F_x, F_y] field spectrum:
+ *   radial  [F_x, F_y, 2]  Radial_2D      perp    [F_x, F_y, 2]  Perp_2D
+ *   tangent [F_x, F_y, 3]  ewald_TanVec   kmask   [F_x, F_y]     K_mask (0/1)
+ * transform_field_3D (:38-68) maps the two input polarisations onto three
+ * components with them, transform_field_2D (:69-97) maps back (the
+ * reflection variant, :98-128, with the axial tangent component negated).
+ * Required before odt_solve on a handle created with pol = 3.
+ */
+odt_status odt_set_polarisation(odt_handle h, const float* radial, const float* perp,
+                                const float* tangent, const uint8_t* kmask);
 
 /* Upload the scattering potential V = RI2potential(RI) - i*eps_imag on the
  * padded grid [sim_size] (CudaBorn action 1, main.cpp:102-138;

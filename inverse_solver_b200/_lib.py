@@ -46,6 +46,7 @@ class Geometry(C.Structure):
         ("device", C.c_int32),
         ("max_batch", C.c_int32),
         ("mem_budget", C.c_int64),
+        ("pol", C.c_int32),
     ]
 
 
@@ -61,6 +62,8 @@ class PotentialParams(C.Structure):
         ("mask", C.c_void_p * 3),
         ("ramp", C.c_void_p * 3),
         ("kq2", C.c_void_p * 3),
+        ("rad", C.c_void_p * 3),
+        ("absorb", C.c_float * 2),
     ]
 
 
@@ -180,6 +183,7 @@ SIGNATURES = {
     "odt_create": (C.c_int, [C.POINTER(Geometry), C.c_void_p, C.c_void_p, C.c_void_p,
                              C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]),
     "odt_set_potential": (C.c_int, [C.c_uint32, C.POINTER(PotentialParams), C.c_void_p]),
+    "odt_set_polarisation": (C.c_int, [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "odt_solve": (C.c_int, [C.c_uint32, C.POINTER(SolveArgs)]),
     "odt_destroy": (C.c_int, [C.c_uint32]),
     "odt_get_batch": (C.c_int, [C.c_uint32, C.POINTER(C.c_int32)]),

@@ -42,6 +42,29 @@ struct BornArgs {
 
 enum BornXMode { kBornFirst = 0, kBornMid = 1, kBornLast = 2 };
 
+// ---- dyadic (vector) branch: tables of polarisation_utility
+// (FORWARD_SOLVER.m:131-180) on the [F_x, F_y] spectrum, device pointers
+struct PolTables {
+  const float* radial;  // [nF, 2]
+  const float* perp;    // [nF, 2]
+  const float* tan3;    // [nF, 3]
+  const float* kmask;   // [nF] 0 / 1
+};
+// rads per axis in FFT order and the absorptive correction of the dyadic
+// Green's function (FORWARD_SOLVER_CONVERGENT_BORN.m:316-322)
+struct DyadArgs {
+  const float* rad[3];
+  float2 absorb;
+};
+// 2 -> 3 components (optionally also into `keep`) / 3 -> 2 polarisations
+cudaError_t launch_pol23(const float2* in, float2* out, float2* keep, const PolTables& t, long long nF,
+                         long long nb, cudaStream_t s);
+cudaError_t launch_pol32(const float2* in, float2* out, const PolTables& t, bool reflection, long long nF,
+                         long long nb, cudaStream_t s);
+// z-pass with the dyadic Green's function; a.nbatch = 3 * illuminations
+cudaError_t launch_born_z_dyadic(const BornArgs& a, const DyadArgs& d, int jj, const DevFft& fz,
+                                 int max_smem, cudaStream_t s);
+
 // x-pass of iteration jj: inverse x-FFT + update of iteration jj-1 (Mid/Last)
 // and source term + forward x-FFT of iteration jj (First/Mid).
 cudaError_t launch_born_x(const BornArgs& a, int mode, int jj, const DevFft& fx, cudaStream_t s);

@@ -90,6 +90,13 @@ struct Handle {
   // transform lengths
   DevFft fx{}, fy{}, fz{}, ffx{}, ffy{}, fcx{}, fcy{};
 
+  // dyadic (vector) handles: np = 3 field components per illumination (batch
+  // entries 3 b + i), npol = 2 input / output polarisations
+  int np = 1, npol = 1;
+  bool have_pol = false;
+  float* pol_tab = nullptr;     // radial [nF,2] | perp [nF,2] | tan3 [nF,3] | kmask [nF]
+  int max_smem = 0;
+
   // static device data
   float2* refocus = nullptr;
   float2* ktrans = nullptr;
@@ -107,6 +114,7 @@ struct Handle {
     float* mask[3] = {nullptr, nullptr, nullptr};
     float2* ramp[3] = {nullptr, nullptr, nullptr};
     float* kq2[3] = {nullptr, nullptr, nullptr};
+    float* rad[3] = {nullptr, nullptr, nullptr};   // dyadic handles
   } pot[2];
   float2* fout_adj = nullptr;   // adjoint 3D field of a batch (odt_gradient)
   float2* grad_acc = nullptr;   // gradient accumulator [ri]
@@ -122,6 +130,8 @@ struct Handle {
   float2* kin = nullptr;
   float2* c2a = nullptr;
   float2* c2b = nullptr;
+  float2* res_t = nullptr;      // where run_chunk left the transmitted / reflected fields
+  float2* res_r = nullptr;
   float2* out_t = nullptr;
   float2* out_r = nullptr;
   unsigned int* d_count = nullptr;
@@ -147,7 +157,11 @@ struct Handle {
   long long nc3() const { return nc2() * g.ri_size[2]; }
   long long work_elems() const { return std::max(3 * nvox(), nc3()); }
   size_t slot_bytes() const {
-    return sizeof(float2) * (size_t)(work_elems() + 2 * nri() + 4 * nf() + 2 * nc2());
+    return sizeof(float2) * (size_t)np * (size_t)(work_elems() + 2 * nri() + 4 * nf() + 2 * nc2());
+  }
+  PolTables pol_tables() const {
+    const long long n = nf();
+    return PolTables{pol_tab, pol_tab + 2 * n, pol_tab + 4 * n, pol_tab + 7 * n};
   }
 
   // allocate `count` elements; batch buffers go to batch_allocs, the rest to allocs
@@ -291,15 +305,16 @@ void ensure_batch(Handle& H, int nb) {
   if (H.batch >= nb) return;
   ODT_CUDA(cudaDeviceSynchronize());  // buffers may still be in use by queued work
   H.free_batch();
-  H.work = H.dalloc<float2>((size_t)H.work_elems() * nb, true);
-  H.einc = H.dalloc<float2>((size_t)H.nri() * nb, true);
-  H.fout = H.dalloc<float2>((size_t)H.nri() * nb, true);
-  H.in2d = H.dalloc<float2>((size_t)H.nf() * nb, true);
-  H.kin = H.dalloc<float2>((size_t)H.nf() * nb, true);
-  H.out_t = H.dalloc<float2>((size_t)H.nf() * nb, true);
-  H.out_r = H.dalloc<float2>((size_t)H.nf() * nb, true);
-  H.c2a = H.dalloc<float2>((size_t)H.nc2() * nb, true);
-  H.c2b = H.dalloc<float2>((size_t)H.nc2() * nb, true);
+  const size_t nbp = (size_t)nb * H.np;  // field planes of nb illuminations
+  H.work = H.dalloc<float2>((size_t)H.work_elems() * nbp, true);
+  H.einc = H.dalloc<float2>((size_t)H.nri() * nbp, true);
+  H.fout = H.dalloc<float2>((size_t)H.nri() * nbp, true);
+  H.in2d = H.dalloc<float2>((size_t)H.nf() * nbp, true);
+  H.kin = H.dalloc<float2>((size_t)H.nf() * nbp, true);
+  H.out_t = H.dalloc<float2>((size_t)H.nf() * nbp, true);
+  H.out_r = H.dalloc<float2>((size_t)H.nf() * nbp, true);
+  H.c2a = H.dalloc<float2>((size_t)H.nc2() * nbp, true);
+  H.c2b = H.dalloc<float2>((size_t)H.nc2() * nbp, true);
   H.d_count = H.dalloc<unsigned int>(1, true);
   H.d_fault = H.dalloc<int>(1, true);
   ODT_CUDA(cudaMemset(H.d_fault, 0, sizeof(int)));
@@ -353,22 +368,29 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
   float2* conv = H.work;
 
   // ---- input: fft2 + pupil, back to space, pad, fft2, refocus, ifft2, crop
-  //      (FORWARD_SOLVER_CONVERGENT_BORN.m:416-418, :543-554)
-  fftc2(H, H.in2d, H.ffx, H.ffy, nb, false, s);
+  //      (FORWARD_SOLVER_CONVERGENT_BORN.m:416-418, :543-554); a dyadic handle
+  //      maps the two input polarisations onto three components in between
+  //      (transform_field_3D, FORWARD_SOLVER.m:38-68) and carries 3 planes per
+  //      illumination from there on
+  const bool vec = H.np == 3;
+  const long long nbp = (long long)nb * H.np;
+  fftc2(H, H.in2d, H.ffx, H.ffy, (long long)nb * H.npol, false, s);
   H.mark_begin(kKIoElem, s);
-  ODT_CUDA(launch_mul_plane(H.in2d, H.in2d, H.kin, H.pupil_in, nF, nF * nb, s));
+  ODT_CUDA(launch_mul_plane(H.in2d, H.in2d, vec ? nullptr : H.kin, H.pupil_in, nF, nF * nb * H.npol, s));
+  if (vec) ODT_CUDA(launch_pol23(H.in2d, H.out_t, H.kin, H.pol_tables(), nF, nb, s));
   H.mark_end(s);
-  fftc2(H, H.in2d, H.ffx, H.ffy, nb, true, s);
+  float2* src2 = vec ? H.out_t : H.in2d;
+  fftc2(H, src2, H.ffx, H.ffy, nbp, true, s);
   H.mark_begin(kKIoElem, s);
-  ODT_CUDA(launch_pad2d(H.in2d, H.c2a, Fx, Fy, Cx, Cy, ocx, ocy, nb, s));
+  ODT_CUDA(launch_pad2d(src2, H.c2a, Fx, Fy, Cx, Cy, ocx, ocy, nbp, s));
   H.mark_end(s);
-  fftc2(H, H.c2a, H.fcx, H.fcy, nb, false, s);
+  fftc2(H, H.c2a, H.fcx, H.fcy, nbp, false, s);
   H.mark_begin(kKIoElem, s);
-  ODT_CUDA(launch_refocus_expand(H.c2a, H.refocus, conv, Cx, Cy, Rz, nb, s));
+  ODT_CUDA(launch_refocus_expand(H.c2a, H.refocus, conv, Cx, Cy, Rz, nbp, s));
   H.mark_end(s);
-  fftc2(H, conv, H.fcx, H.fcy, (long long)Rz * nb, true, s);
+  fftc2(H, conv, H.fcx, H.fcy, (long long)Rz * nbp, true, s);
   H.mark_begin(kKIoElem, s);
-  ODT_CUDA(launch_crop_volume(conv, H.einc, Cx, Cy, Rx, Ry, Rz, ocx, ocy, nb, s));
+  ODT_CUDA(launch_crop_volume(conv, H.einc, Cx, Cy, Rx, Ry, Rz, ocx, ocy, nbp, s));
   H.mark_end(s);
 
   // ---- Born series (:577-647)
@@ -383,7 +405,7 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
   a.ry = Ry;
   a.rz = Rz;
   a.nvox = H.nvox();
-  a.nbatch = nb;
+  a.nbatch = (int)nbp;
   for (int i = 0; i < 3; ++i) {
     a.mask[i] = P.mask[i];
     a.ramp[i] = P.ramp[i];
@@ -396,15 +418,20 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
   a.inv_n = (float)(1.0 / (double)H.nvox());
   a.acyclic = P.pp.acyclic;
   a.T = H.work;
-  a.Fn = H.work + (size_t)H.nvox() * nb;
-  a.F = H.work + 2 * (size_t)H.nvox() * nb;
+  a.Fn = H.work + (size_t)H.nvox() * nbp;
+  a.F = H.work + 2 * (size_t)H.nvox() * nbp;
   a.V = P.V;
   a.Einc = H.einc;
   a.Fout = fout;
   const int B = P.pp.bornmax;
   const bool pipe_x = H.use_pipe && born_x_pipe_supported(a, H.fx);
   const bool pipe_y = H.use_pipe && cols_pipe_supported(a, H.fy, false);
-  const bool pipe_z = H.use_pipe && cols_pipe_supported(a, H.fz, true);
+  const bool pipe_z = !vec && H.use_pipe && cols_pipe_supported(a, H.fz, true);
+  DyadArgs dy{};
+  if (vec) {
+    for (int i = 0; i < 3; ++i) dy.rad[i] = P.rad[i];
+    dy.absorb = make_float2(P.pp.absorb.re, P.pp.absorb.im);
+  }
   for (int jj = 1; jj <= B; ++jj) {
     if (pipe_x && jj >= 4) {
       H.mark_begin(kKBornXPipe, s);
@@ -418,10 +445,12 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
     if (pipe_y)
       ODT_CUDA(launch_fft_y_pipe(a, false, H.fy, H.d_fault, s));
     else
-      ODT_CUDA(launch_fft_cols(a.T, a.T, a.px, (long long)a.pz * nb, 0, 0, 1.0f, false, H.fy, s));
+      ODT_CUDA(launch_fft_cols(a.T, a.T, a.px, (long long)a.pz * nbp, 0, 0, 1.0f, false, H.fy, s));
     H.mark_end(s);
     H.mark_begin(pipe_z ? kKBornZPipe : kKBornZ, s);
-    if (pipe_z)
+    if (vec)
+      ODT_CUDA(launch_born_z_dyadic(a, dy, jj, H.fz, H.max_smem, s));
+    else if (pipe_z)
       ODT_CUDA(launch_born_z_pipe(a, jj, H.fz, H.d_fault, s));
     else
       ODT_CUDA(launch_born_z(a, jj, H.fz, s));
@@ -430,7 +459,7 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
     if (pipe_y)
       ODT_CUDA(launch_fft_y_pipe(a, true, H.fy, H.d_fault, s));
     else
-      ODT_CUDA(launch_fft_cols(a.T, a.T, a.px, (long long)a.pz * nb, 0, 0, 1.0f, true, H.fy, s));
+      ODT_CUDA(launch_fft_cols(a.T, a.T, a.px, (long long)a.pz * nbp, 0, 0, 1.0f, true, H.fy, s));
     H.mark_end(s);
   }
   H.mark_begin(kKBornX, s);
@@ -442,24 +471,32 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
     H.mark_begin(kKIoElem, s);
     ODT_CUDA(launch_emitter(a, conv, Cx, Cy, orx, ory, P.pp.dV, s));
     H.mark_end(s);
-    fftc2(H, conv, H.fcx, H.fcy, (long long)Rz * nb, false, s);
+    fftc2(H, conv, H.fcx, H.fcy, (long long)Rz * nbp, false, s);
     H.mark_begin(kKIoElem, s);
     ODT_CUDA(launch_zreduce(conv, want_t ? H.ktrans : nullptr, want_r ? H.kref : nullptr,
-                            want_t ? H.c2a : nullptr, want_r ? H.c2b : nullptr, Cx, Cy, Rz, nb, s));
+                            want_t ? H.c2a : nullptr, want_r ? H.c2b : nullptr, Cx, Cy, Rz, nbp, s));
     H.mark_end(s);
     for (int w = 0; w < 2; ++w) {
       if ((w == 0 && !want_t) || (w == 1 && !want_r)) continue;
       float2* c2 = w == 0 ? H.c2a : H.c2b;
       float2* o = w == 0 ? H.out_t : H.out_r;
-      fftc2(H, c2, H.fcx, H.fcy, nb, true, s);
+      fftc2(H, c2, H.fcx, H.fcy, nbp, true, s);
       H.mark_begin(kKIoElem, s);
-      ODT_CUDA(launch_crop2d(c2, o, Fx, Fy, Cx, Cy, ocx, ocy, nb, s));
+      ODT_CUDA(launch_crop2d(c2, o, Fx, Fy, Cx, Cy, ocx, ocy, nbp, s));
       H.mark_end(s);
-      fftc2(H, o, H.ffx, H.ffy, nb, false, s);
+      fftc2(H, o, H.ffx, H.ffy, nbp, false, s);
       H.mark_begin(kKIoElem, s);
-      ODT_CUDA(launch_combine(o, w == 0 ? H.kin : nullptr, H.pupil_out, o, nF, nF * nb, s));
+      ODT_CUDA(launch_combine(o, w == 0 ? H.kin : nullptr, H.pupil_out, o, nF, nF * nbp, s));
       H.mark_end(s);
-      fftc2(H, o, H.ffx, H.ffy, nb, true, s);
+      float2* res = o;
+      if (vec) {  // three components -> two polarisations (transform_field_2D / _reflection)
+        H.mark_begin(kKIoElem, s);
+        ODT_CUDA(launch_pol32(o, c2, H.pol_tables(), w == 1, nF, nb, s));
+        H.mark_end(s);
+        res = c2;
+      }
+      fftc2(H, res, H.ffx, H.ffy, (long long)nb * H.npol, true, s);
+      (w == 0 ? H.res_t : H.res_r) = res;
     }
   }
 }
@@ -474,6 +511,7 @@ void alloc_slot(Handle& H, int k) {
     P.mask[i] = H.dalloc<float>(g.sim_size[i], false);
     P.ramp[i] = H.dalloc<float2>(g.sim_size[i], false);
     P.kq2[i] = H.dalloc<float>(g.sim_size[i], false);
+    if (H.np == 3) P.rad[i] = H.dalloc<float>(g.sim_size[i], false);
   }
   P.allocated = true;
 }
@@ -488,7 +526,7 @@ void set_potential_slot(const std::shared_ptr<Handle>& Hp, int k, const odt_pote
     const int lo = pp->roi[2 * i], hi = pp->roi[2 * i + 1];
     if (lo < 1 || hi > g.sim_size[i] || hi - lo + 1 != g.ri_size[i])
       raise(ODT_ERR_INVALID_ARGUMENT, who + ": ROI does not match ri_size");
-    if (!pp->mask[i] || !pp->kq2[i] || (pp->acyclic && !pp->ramp[i]))
+    if (!pp->mask[i] || !pp->kq2[i] || (pp->acyclic && !pp->ramp[i]) || (H.np == 3 && !pp->rad[i]))
       raise(ODT_ERR_INVALID_ARGUMENT, who + ": NULL table");
   }
   if (pp->bornmax < 0) raise(ODT_ERR_INVALID_ARGUMENT, who + ": bornmax < 0");
@@ -506,6 +544,7 @@ void set_potential_slot(const std::shared_ptr<Handle>& Hp, int k, const odt_pote
     const size_t n = g.sim_size[i];
     ODT_CUDA(cudaMemcpy(P.mask[i], pp->mask[i], n * sizeof(float), cudaMemcpyHostToDevice));
     ODT_CUDA(cudaMemcpy(P.kq2[i], pp->kq2[i], n * sizeof(float), cudaMemcpyHostToDevice));
+    if (H.np == 3) ODT_CUDA(cudaMemcpy(P.rad[i], pp->rad[i], n * sizeof(float), cudaMemcpyHostToDevice));
     if (pp->acyclic) {
       ODT_CUDA(cudaMemcpy(P.ramp[i], pp->ramp[i], n * sizeof(float2), cudaMemcpyHostToDevice));
     } else {
@@ -518,6 +557,7 @@ void set_potential_slot(const std::shared_ptr<Handle>& Hp, int k, const odt_pote
     P.pp.mask[i] = nullptr;
     P.pp.ramp[i] = nullptr;
     P.pp.kq2[i] = nullptr;
+    P.pp.rad[i] = nullptr;
   }
   P.have = true;
 }
@@ -557,6 +597,8 @@ odt_status odt_create(const odt_geometry* geom, const odt_cfloat* refocus,
     }
     if (g.max_batch < 0 || g.mem_budget < 0)
       raise(ODT_ERR_INVALID_ARGUMENT, "odt_create: negative max_batch / mem_budget");
+    if (g.pol != 0 && g.pol != 1 && g.pol != 3)
+      raise(ODT_ERR_INVALID_ARGUMENT, "odt_create: pol must be 1 (scalar) or 3 (dyadic)");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
       cudaGetLastError();
@@ -568,6 +610,9 @@ odt_status odt_create(const odt_geometry* geom, const odt_cfloat* refocus,
     auto H = std::make_shared<Handle>();
     H->g = g;
     H->budget = (size_t)g.mem_budget;
+    H->np = g.pol == 3 ? 3 : 1;
+    H->npol = g.pol == 3 ? 2 : 1;
+    ODT_CUDA(cudaDeviceGetAttribute(&H->max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, g.device));
     if (const char* k = std::getenv("ODT_KERNELS")) H->use_pipe = std::string(k) != "generic";
     ODT_CUDA(cudaStreamCreateWithFlags(&H->own_stream, cudaStreamNonBlocking));
     H->fx = make_dev_fft(*H, g.sim_size[0], kKindBornX, "sim_size(1)");
@@ -612,6 +657,26 @@ odt_status odt_set_adjoint_potential(odt_handle h, const odt_potential_params* p
   return guarded([&] { set_potential_slot(lookup(h), 1, pp, V, "odt_set_adjoint_potential"); });
 }
 
+odt_status odt_set_polarisation(odt_handle h, const float* radial, const float* perp,
+                                const float* tangent, const uint8_t* kmask) {
+  return guarded([&] {
+    auto H = lookup(h);
+    if (H->np != 3) raise(ODT_ERR_INVALID_ARGUMENT, "odt_set_polarisation: not a dyadic (pol = 3) handle");
+    if (!radial || !perp || !tangent || !kmask)
+      raise(ODT_ERR_INVALID_ARGUMENT, "odt_set_polarisation: NULL table");
+    DeviceGuard dg(H->g.device);
+    const long long n = H->nf();
+    std::vector<float> tab((size_t)8 * n);
+    std::copy(radial, radial + 2 * n, tab.begin());
+    std::copy(perp, perp + 2 * n, tab.begin() + 2 * n);
+    std::copy(tangent, tangent + 3 * n, tab.begin() + 4 * n);
+    for (long long i = 0; i < n; ++i) tab[7 * n + i] = kmask[i] ? 1.f : 0.f;
+    if (!H->pol_tab) H->pol_tab = H->dalloc<float>(tab.size(), false);
+    ODT_CUDA(cudaMemcpy(H->pol_tab, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice));
+    H->have_pol = true;
+  });
+}
+
 odt_status odt_solve(odt_handle h, const odt_solve_args* args) {
   return guarded([&] {
     auto H = lookup(h);
@@ -626,6 +691,8 @@ odt_status odt_solve(odt_handle h, const odt_solve_args* args) {
     const bool want_t = A.trans != nullptr, want_r = A.ref != nullptr;
     if (want_t && !H->ktrans) raise(ODT_ERR_INVALID_ARGUMENT, "odt_solve: created without kernel_trans");
     if (want_r && !H->kref) raise(ODT_ERR_INVALID_ARGUMENT, "odt_solve: created without kernel_ref");
+    if (H->np == 3 && !H->have_pol)
+      raise(ODT_ERR_NOT_READY, "odt_solve: a dyadic handle needs odt_set_polarisation first");
     DeviceGuard dg(H->g.device);
     const bool dev = A.memory == ODT_MEM_DEVICE;
     if (dev) {
@@ -639,7 +706,8 @@ odt_status odt_solve(odt_handle h, const odt_solve_args* args) {
     ensure_batch(*H, want_batch);
     const cudaMemcpyKind kin = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     const cudaMemcpyKind kout = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-    const long long nF = H->nf(), nR = H->nri();
+    // per illumination: npol planes of [F_x, F_y] in and out, np components of [ri] in 3D
+    const long long nF = H->nf() * H->npol, nR = H->nri() * H->np;
     ODT_CUDA(cudaMemsetAsync(H->d_count, 0, sizeof(unsigned int), s));
     for (int b0 = 0; b0 < A.n_ill; b0 += H->batch) {
       const int nb = std::min(H->batch, A.n_ill - b0);
@@ -651,10 +719,10 @@ odt_status odt_solve(odt_handle h, const odt_solve_args* args) {
         ODT_CUDA(cudaMemcpyAsync(A.field3d + (size_t)b0 * nR, H->fout,
                                  (size_t)nb * nR * sizeof(float2), kout, s));
       if (want_t)
-        ODT_CUDA(cudaMemcpyAsync(A.trans + (size_t)b0 * nF, H->out_t,
+        ODT_CUDA(cudaMemcpyAsync(A.trans + (size_t)b0 * nF, H->res_t,
                                  (size_t)nb * nF * sizeof(float2), kout, s));
       if (want_r)
-        ODT_CUDA(cudaMemcpyAsync(A.ref + (size_t)b0 * nF, H->out_r,
+        ODT_CUDA(cudaMemcpyAsync(A.ref + (size_t)b0 * nF, H->res_r,
                                  (size_t)nb * nF * sizeof(float2), kout, s));
       if (!dev) ODT_CUDA(cudaStreamSynchronize(s));
       H->collect(s);
@@ -674,6 +742,8 @@ odt_status odt_gradient(odt_handle h, const odt_gradient_args* args) {
     auto H = lookup(h);
     if (!args) raise(ODT_ERR_INVALID_ARGUMENT, "odt_gradient: NULL args");
     const odt_gradient_args& A = *args;
+    if (H->np == 3)
+      raise(ODT_ERR_UNSUPPORTED, "odt_gradient: the dyadic (vector) gradient is not supported");
     if (!H->pot[0].have || !H->pot[1].have)
       raise(ODT_ERR_NOT_READY, "odt_gradient: set the forward and the adjoint potential first");
     if (A.n_ill < 1 || !A.fields_in || !A.fields_meas || !A.grad || !A.err)

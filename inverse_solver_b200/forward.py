@@ -19,8 +19,8 @@ import numpy as np
 
 from . import _lib
 from .optics import (C64, F32, OpticalTool, basic_optical_parameter, centered_fft2,
-                     centered_fftn, mround, potential2ri, ri2potential, truncated_green_plus,
-                     update_struct)
+                     centered_fftn, mround, polarisation_basis, potential2ri, ri2potential,
+                     truncated_green_plus, update_struct)
 
 
 def _f32(x):
@@ -54,10 +54,9 @@ class CBSHostSetup:
     def __init__(self, params):
         """Constructor (FORWARD_SOLVER_CONVERGENT_BORN.m:48-133)."""
         p = self.parameters = copy.deepcopy(params)
-        if p.get("vector_simulation", True):
-            raise NotImplementedError(
-                "vector_simulation=true (dyadic Green's function) is not supported by this "
-                "library yet; pass vector_simulation=false")
+        # pole_num (:293-296): 3 field components with the dyadic Green's function
+        self.vector = bool(p.get("vector_simulation", True))
+        self.pole_num = 3 if self.vector else 1
         for key, val in (("used_gpu", 0), ("max_batch", 0), ("mem_budget", 0)):
             p.setdefault(key, val)
         self.utility = u = OpticalTool(p)
@@ -102,6 +101,8 @@ class CBSHostSetup:
         self.conv_size = (list(self.field_size) if self.cyclic_boundary_xy
                           else [self.field_size[0] + ri[0], self.field_size[1] + ri[1]])
         self.pupil_in, self.pupil_out = self._pupils()
+        if self.vector:
+            self.polarisation = polarisation_basis(self.field_size, p)
 
     @staticmethod
     def _crop_shift(a, rc):
@@ -169,6 +170,11 @@ class CBSHostSetup:
         else:
             sc = list(ub.fourier_coor)
         kq2 = [np.fft.ifftshift(c * c).astype(F32) for c in sc]
+        # dyadic Green's function: rads = shifted coordinate / k0_nm (:316-319),
+        # ifftshifted (:385), and the absorptive correction (:322)
+        rads = [np.fft.ifftshift((np.asarray(c, dtype=F32) / ub.k0_nm).astype(F32)) for c in sc]
+        a2 = F32((2 * math.pi * ub.k0_nm) ** 2)
+        absorb = C64(a2 / C64(a2 + 1j * self.eps_imag))
         step = F32(abs(2 * (2 * math.pi * ub.k0_nm) / self.eps_imag))
         nrm = float(np.linalg.norm(np.asarray(V.shape, dtype=np.float64) * np.asarray(p["resolution"], dtype=np.float64)))
         bopt = int(math.ceil(float(F32(F32(nrm / step) / 2 + 1)))) * 2
@@ -197,11 +203,16 @@ class CBSHostSetup:
         pp.roi[:] = [int(r) for r in self.ROI]
         pp.bornmax = int(self.Bornmax)
         pp.acyclic = 1 if p["acyclic"] else 0
-        keep = [_f32(m) for m in masks] + [_c64(r) for r in ramps] + [_f32(k) for k in kq2]
+        keep = ([_f32(m) for m in masks] + [_c64(r) for r in ramps] + [_f32(k) for k in kq2]
+                + [_f32(r) for r in rads])
         for j in range(3):
             pp.mask[j] = _lib.ptr(keep[j])
             pp.ramp[j] = _lib.ptr(keep[3 + j])
             pp.kq2[j] = _lib.ptr(keep[6 + j])
+            pp.rad[j] = _lib.ptr(keep[9 + j])
+        pp.absorb[:] = [float(absorb.real), float(absorb.imag)]
+        self.rads1d = rads
+        self.green_absorbtion_correction = absorb
         self.V = V
         self.attenuation_mask1d = masks
         self.ramp1d = ramps
@@ -214,8 +225,9 @@ class CBSHostSetup:
 
 
 class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
-    """Convergent Born series forward solver (scalar Green's function) whose
-    per-illumination work runs in libodt on the GPU."""
+    """Convergent Born series forward solver (scalar Green's function, or the
+    dyadic one with vector_simulation) whose per-illumination work runs in
+    libodt on the GPU."""
 
     def __init__(self, params):
         """Constructor + CudaBorn action 0 (FORWARD_SOLVER_CONVERGENT_BORN_CUDA.m:18-41)."""
@@ -238,12 +250,17 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
         g.device = int(p["used_gpu"])
         g.max_batch = int(p["max_batch"])
         g.mem_budget = int(p["mem_budget"])
+        g.pol = self.pole_num
         self._keep = [_c64(self.refocusing_util), _c64(self.kernel_trans), _c64(self.kernel_ref),
                       _f32(self.pupil_in), _f32(self.pupil_out)]
         h = C.c_uint32(0)
         _lib.check(self.lib.odt_create(C.byref(g), *[_lib.ptr(a) for a in self._keep], C.byref(h)))
         self._handle = h.value
         self._keep = None
+        if self.vector:
+            rad, perp, tan, km = self.polarisation
+            keep = [_f32(rad), _f32(perp), _f32(tan), np.asfortranarray(km.astype(np.uint8))]
+            _lib.check(self.lib.odt_set_polarisation(self._handle, *[_lib.ptr(k) for k in keep]))
 
     def set_RI(self, RI):
         """set_RI (FORWARD_SOLVER_CONVERGENT_BORN.m:180-198) + CudaBorn action 1
@@ -278,6 +295,8 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
             x = x[:, :, :, None]
         if y.ndim == 3:
             y = y[:, :, :, None]
+        if self.vector:
+            raise NotImplementedError("the gradient is available for the scalar solver only")
         if x.shape != y.shape or x.shape[2] != 1:
             raise ValueError("input and output fields must be [F_x, F_y, 1, n] alike")
         xin, yin = _c64(x), _c64(y)
@@ -298,8 +317,8 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
         p = self.parameters
         F = self.field_size
         R = self.expected_RI_size
-        shp_t = (F[0], F[1], 1, n_ill)
-        shp_3 = (R[0], R[1], R[2], 1, n_ill)
+        shp_t = (F[0], F[1], 2 if self.vector else 1, n_ill)
+        shp_3 = (R[0], R[1], R[2], self.pole_num, n_ill)
         mk = (lambda s: np.empty(s, dtype=C64, order="F"))
         return (mk(shp_t) if p["return_transmission"] else None,
                 mk(shp_t) if p["return_reflection"] else None,
@@ -307,15 +326,21 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
 
     def solve(self, input_field):
         """solve (FORWARD_SOLVER_CONVERGENT_BORN.m:397-520): input_field is the
-        spatial field [F_x, F_y, 1, n_ill]; returns (fields_trans, fields_ref,
-        fields_3D), each None when its return_* flag is false."""
+        spatial field [F_x, F_y, npol, n_ill] (npol = 1, or 2 with
+        vector_simulation); returns (fields_trans, fields_ref, fields_3D),
+        each None when its return_* flag is false ([F_x, F_y, npol, n_ill],
+        and [x, y, z, pole_num, n_ill] for the 3D field)."""
         x = np.asarray(input_field)
         if x.ndim == 2:
             x = x[:, :, None, None]
         elif x.ndim == 3:
             x = x[:, :, :, None]
-        if x.shape[2] > 1:
+        if x.shape[2] > 1 and not self.vector:                         # :404-414
             raise ValueError("the source is 2D but parameter indicate a vectorial simulation")
+        if x.shape[2] == 1 and self.vector:
+            raise ValueError("the source is 3D but parameter indicate a non-vectorial simulation")
+        if x.shape[2] > 2:
+            raise ValueError("Input field must be either a scalar or a 2D vector")
         if list(x.shape[:2]) != list(self.field_size):
             raise ValueError("input field must be %d x %d" % tuple(self.field_size))
         n_ill = x.shape[3]
@@ -343,7 +368,7 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
         if stream is None:
             stream = torch.cuda.current_stream()
         sh = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
-        nF = self.field_size[0] * self.field_size[1]
+        nF = self.field_size[0] * self.field_size[1] * (2 if self.vector else 1)
         n_ill = fields_in.numel() // nF
         for t in (fields_in, trans, ref, field3d):
             if t is not None and (not t.is_cuda or not t.is_contiguous() or t.dtype != torch.complex64):

@@ -94,6 +94,42 @@ class OpticalTool:
         self.cos_theta = self.k3 / self.k0_nm
 
 
+def polarisation_basis(field_size, params):
+    """polarisation_utility (FORWARD_SOLVER.m:131-180) in single precision:
+    per pixel of the centred [N, N] field spectrum the pupil-plane radial and
+    perpendicular unit vectors, the unit tangent of the Ewald sphere and the
+    mask of propagating waves.  Returns (radial [N,N,2], perp [N,N,2],
+    tangent [N,N,3], kmask [N,N] bool).  Square fields only: the reference
+    builds its second coordinate with the first size as the range end."""
+    n1, n2 = int(field_size[0]), int(field_size[1])
+    if n1 != n2:
+        raise ValueError("the dyadic solver needs a square field (polarisation_utility)")
+    k = 2 * math.pi * float(params["RI_bg"]) / float(params["wavelength"])
+    res = [float(r) for r in params["resolution"]]
+    kx = (2 * math.pi * (1.0 / res[0] / n1) / k
+          * np.arange(-(n1 // 2), n1 - n1 // 2, dtype=np.float64)).astype(F32)[:, None]
+    ky = (2 * math.pi * (1.0 / res[1] / n2) / k
+          * np.arange(-(n2 // 2), n1 - n2 // 2, dtype=np.float64)).astype(F32)[None, :]
+    kxy2 = kx * kx + ky * ky
+    kz = np.sqrt(np.maximum(F32(1) - kxy2, F32(0)))
+    kmask = kz != 0
+    rho = np.sqrt(kxy2)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        ux, uy = kx / rho, ky / rho
+    ux = np.where(rho == 0, F32(1), ux).astype(F32)
+    uy = np.where(rho == 0, F32(0), uy).astype(F32)
+    radial = np.stack([ux, uy], axis=2)
+    perp = np.stack([uy, -ux], axis=2)
+    rn = np.sqrt(kxy2 + kz * kz)
+    s3 = [np.broadcast_to(kx / rn, rn.shape), np.broadcast_to(ky / rn, rn.shape), kz / rn]
+    proj = s3[0] * ux + s3[1] * uy
+    t = [(ux - proj * s3[0]).astype(F32), (uy - proj * s3[1]).astype(F32), (F32(0) - proj * s3[2]).astype(F32)]
+    tn = np.sqrt((t[0] * t[0] + t[1] * t[1]) + t[2] * t[2])
+    tn[~kmask] = 1
+    tangent = np.stack([c / tn for c in t], axis=2).astype(F32)
+    return radial.astype(F32), perp.astype(F32), tangent, kmask
+
+
 def ri2potential(RI, wavelength, base_RI):
     """RI2potential (sub_code/RI2potential.m:1-5)."""
     k = 2 * math.pi * base_RI * (1.0 / wavelength)

@@ -348,17 +348,56 @@ def truncated_green_plus(params, refocus_version, P: Prec):
     return green_out
 
 
+def polarisation_utility(ZP, params, P: Prec):
+    """``FORWARD_SOLVER.m:131-180``: per k-pixel radial / perpendicular unit
+    vectors of the pupil plane, the unit tangent of the Ewald sphere and the
+    propagating-wave mask.  Returns (Radial_2D [N1,N2,2], Perp_2D [N1,N2,2],
+    ewald_TanVec [N1,N2,3], K_mask [N1,N2]).  The reference builds K_2 with
+    ZP(1) as the end of its range (:139), so the field must be square."""
+    N1, N2 = int(ZP[0]), int(ZP[1])
+    if N1 != N2:
+        raise ValueError("the polarisation basis needs a square field")
+    lam = float(params["wavelength"])
+    dx = [float(v) for v in params["resolution"]]
+    k0 = 1.0 / lam
+    k = 2 * math.pi * float(params["RI_bg"]) * k0
+    kres = [1.0 / dx[0] / N1, 1.0 / dx[1] / N2]
+    K1 = P.R(2 * math.pi * kres[0] / k * np.arange(-(N1 // 2), N1 - N1 // 2, dtype=np.float64))[:, None]
+    K2 = P.R(2 * math.pi * kres[1] / k * np.arange(-(N2 // 2), N1 - N2 // 2, dtype=np.float64))[None, :]
+    s3 = P.R(1) - (K1 ** 2 + K2 ** 2)
+    K3 = np.sqrt(np.maximum(s3, 0)).astype(P.r)        # real(sqrt(.)) of a negative is 0
+    K_mask = ~(K3 == 0)
+    nr = np.sqrt(K1 ** 2 + K2 ** 2)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        t1 = K1 / nr
+        t2 = K2 / nr
+    t1 = np.where(nr == 0, P.R(1), t1)
+    t2 = np.where(nr == 0, P.R(0), t2)
+    R2 = np.stack([t1, t2], axis=2).astype(P.r)
+    P2 = np.stack([t2, -t1], axis=2).astype(P.r)
+    ns = np.sqrt((K1 ** 2 + K2 ** 2) + K3 ** 2)
+    R3 = np.stack([np.broadcast_to(K1 / ns, ns.shape), np.broadcast_to(K2 / ns, ns.shape), K3 / ns], axis=2).astype(P.r)
+    proj = R3[:, :, 0] * R2[:, :, 0] + R3[:, :, 1] * R2[:, :, 1]
+    E = np.zeros((N1, N1, 3), dtype=P.r)
+    E[:, :, 0:2] = R2
+    E = (E - proj[:, :, None] * R3).astype(P.r)
+    en = np.sqrt((E[:, :, 0] ** 2 + E[:, :, 1] ** 2) + E[:, :, 2] ** 2)
+    en[~K_mask] = 1
+    E = (E / en[:, :, None]).astype(P.r)
+    return R2, P2, E, K_mask
+
+
 # ---------------------------------------------------------- the solver
 class ForwardSolverCBS:
-    """Restatement of ``Codes/FORWARD_SOLVER_CONVERGENT_BORN.m`` (scalar
-    Green's function; ``vector_simulation`` must be false)."""
+    """Restatement of ``Codes/FORWARD_SOLVER_CONVERGENT_BORN.m``: the scalar
+    Green's function, and with ``vector_simulation`` the dyadic one
+    (``pole_num = 3``, isotropic RI)."""
 
     def __init__(self, params, single=True):
         """Constructor ``:48-133``."""
         self.P = P = Prec(single)
         self.parameters = p = copy.deepcopy(params)
-        if p.get("vector_simulation", False):
-            raise NotImplementedError("dyadic (vector) CBS is not restated")
+        self.vector = bool(p.get("vector_simulation", False))
         self.utility = derive_optical_tool(p, P)
         p["RI_xy_size"] = list(p["RI_xy_size"])
         if p["RI_xy_size"][0] == 0:
@@ -508,7 +547,7 @@ class ForwardSolverCBS:
         pb = copy.deepcopy(p)
         pb["size"] = list(self.RI.shape)
         ub = self.utility_border = derive_optical_tool(pb, P)
-        self.pole_num = 1
+        self.pole_num = 3 if self.vector else 1                      # :293-296
         fc, fr = ub["fourier_coor"], ub["fourier_res"]
         if p["acyclic"] and self.cyclic_boundary_xy:
             sc = [fc[0], fc[1], fc[2] + fr[2] / 4]
@@ -518,6 +557,11 @@ class ForwardSolverCBS:
             sc = list(fc)
         self.shifted_coordinate = sc
         k0nm = ub["k0_nm"]
+        # rads(:,:,:,i) = shifted_coordinate{i} / k0_nm (:316-319); the
+        # absorptive correction of the dyadic Green's function (:322)
+        self.rads1d = [P.S(P.S(sc[i]) / k0nm) for i in range(3)]
+        a2 = P.S((2 * math.pi * k0nm) ** 2)
+        self.green_absorbtion_correction = P.S(a2 / P.S(a2 + 1j * self.eps_imag))
         step = P.S(abs(2 * (2 * math.pi * k0nm) / self.eps_imag))     # :326
         nrm = float(np.linalg.norm(np.asarray(self.RI.shape[:3], dtype=np.float64) * np.asarray(p["resolution"], dtype=np.float64)))
         Bopt = math.ceil(float(P.S(P.S(nrm / step) / 2 + 1))) * 2      # :327
@@ -555,10 +599,18 @@ class ForwardSolverCBS:
             self.phase_ramp = np.ones((1, 1, 1), dtype=P.c)
             self.ramp1d = None
         self.Greenp = np.fft.ifftshift(self.Greenp)                  # :384
+        if self.pole_num == 3:                                        # :385
+            n = self.V.shape
+            r = np.zeros(tuple(n) + (3,), dtype=P.r)
+            r[..., 0] = self.rads1d[0][:, None, None]
+            r[..., 1] = self.rads1d[1][None, :, None]
+            r[..., 2] = self.rads1d[2][None, None, :]
+            self.rads = np.fft.ifftshift(r, axes=(0, 1, 2))
 
     # --- solve :397-520
     def transform_field_3D(self, f):
-        """``FORWARD_SOLVER.m:38-68`` (scalar)."""
+        """``FORWARD_SOLVER.m:38-68``: pupil (NA, Abbe sine) and, for two
+        polarisations, the 2 -> 3 component change of basis."""
         u = self.utility
         NA = u["NA_circle"]
         f = f * NA.reshape(NA.shape + (1,) * (f.ndim - 2))
@@ -566,18 +618,45 @@ class ForwardSolverCBS:
             filt = self.P.R(NA)
             filt[NA] = filt[NA] / np.sqrt(u["cos_theta"][NA])
             f = f * filt.reshape(filt.shape + (1,) * (f.ndim - 2))
-        return f
+        if f.ndim < 3 or f.shape[2] == 1:
+            return f
+        if f.shape[2] != 2:
+            raise ValueError("Far field has two polarisation")
+        R2, P2, E, K = polarisation_utility(f.shape[:2], self.parameters, self.P)
+        f = f * K[:, :, None, None]
+        b1 = f[:, :, 0] * R2[:, :, 0, None] + f[:, :, 1] * R2[:, :, 1, None]
+        b2 = f[:, :, 0] * P2[:, :, 0, None] + f[:, :, 1] * P2[:, :, 1, None]
+        out = np.zeros((f.shape[0], f.shape[1], 3, f.shape[3]), dtype=self.P.c)
+        out = out + b1[:, :, None, :] * E[:, :, :, None]
+        out[:, :, 0:2] = out[:, :, 0:2] + b2[:, :, None, :] * P2[:, :, :, None]
+        return out
 
-    def transform_field_2D(self, f):
-        """``FORWARD_SOLVER.m:69-97`` (scalar; the reflection variant
-        ``:98-128`` is identical for one polarisation)."""
+    def transform_field_2D(self, f, reflection=False):
+        """``FORWARD_SOLVER.m:69-128``: pupil (NA, Abbe sine) and, for three
+        components, the 3 -> 2 polarisation change of basis (the reflection
+        variant flips the axial component of the tangent vector, :113)."""
         u = self.utility
         NA = u["NA_circle"]
         sh = NA.shape + (1,) * (f.ndim - 2)
         f = f * NA.reshape(sh)
         if self.parameters["use_abbe_sine"]:
             f = f * np.sqrt(u["cos_theta"]).reshape(sh) * NA.reshape(sh)
-        return f
+        if f.ndim < 3 or f.shape[2] == 1:
+            return f
+        if f.shape[2] != 3:
+            raise ValueError("Near field has three polarisation")
+        R2, P2, E, K = polarisation_utility(f.shape[:2], self.parameters, self.P)
+        if reflection:
+            E = E.copy()
+            E[:, :, 2] = -E[:, :, 2]
+        f = f * K.reshape(K.shape + (1,) * (f.ndim - 2))
+        x = f if f.ndim == 4 else f[..., None]
+        b1 = (x[:, :, 0] * E[:, :, 0, None] + x[:, :, 1] * E[:, :, 1, None]) + x[:, :, 2] * E[:, :, 2, None]
+        b2 = x[:, :, 0] * P2[:, :, 0, None] + x[:, :, 1] * P2[:, :, 1, None]
+        out = np.zeros((x.shape[0], x.shape[1], 2, x.shape[3]), dtype=self.P.c)
+        out = out + b1[:, :, None, :] * R2[:, :, :, None]
+        out = out + b2[:, :, None, :] * P2[:, :, :, None]
+        return out if f.ndim == 4 else out[..., 0]
 
     def solve(self, input_field):
         P, p = self.P, self.parameters
@@ -586,35 +665,43 @@ class ForwardSolverCBS:
             inp = inp[:, :, None, None]
         elif inp.ndim == 3:
             inp = inp[:, :, :, None]
-        if inp.shape[2] != 1:
+        if inp.shape[2] > 1 and not self.vector:                      # :404-414
             raise ValueError("the source is 2D but parameter indicate a vectorial simulation")
+        if inp.shape[2] == 1 and self.vector:
+            raise ValueError("the source is 3D but parameter indicate a non-vectorial simulation")
+        if inp.shape[2] > 2:
+            raise ValueError("Input field must be either a scalar or a 2D vector")
         inp = fftc2(inp)
         inp = self.transform_field_3D(inp)
         R = self.ROI
         nx, ny, nz = R[1] - R[0] + 1, R[3] - R[2] + 1, R[5] - R[4] + 1
         nill = inp.shape[3]
-        ft = np.ones((nx, ny, 1, nill), dtype=P.c) if p["return_transmission"] else None
-        fr = np.ones((nx, ny, 1, nill), dtype=P.c) if p["return_reflection"] else None
-        f3 = np.ones((nx, ny, nz, 1, nill), dtype=P.c) if p["return_3D"] else None
+        npol = inp.shape[2]
+        out_pol = 2 if self.pole_num == 3 else 1
+        ft = np.ones((nx, ny, out_pol, nill), dtype=P.c) if p["return_transmission"] else None
+        fr = np.ones((nx, ny, out_pol, nill), dtype=P.c) if p["return_reflection"] else None
+        f3 = np.ones((nx, ny, nz, npol, nill), dtype=P.c) if p["return_3D"] else None
         for k in range(nill):
-            Field = self.solve_raw(inp[:, :, :, k])
+            src = inp[:, :, :, k] if self.vector else inp[:, :, 0, k]
+            Field = self.solve_raw(src)
+            F4 = Field if self.vector else Field[..., None]
             if p["return_3D"]:
-                f3[:, :, :, 0, k] = Field
+                f3[:, :, :, :, k] = F4
             if p["return_transmission"] or p["return_reflection"]:
                 pot = ri2potential(self.RI[R[0] - 1:R[1], R[2] - 1:R[3], R[4] - 1:R[5]], p["wavelength"], p["RI_bg"], P)
-                em = Field * pot * self.utility_border["dV"]
+                em = F4 * pot[..., None] * self.utility_border["dV"]
                 em = self.padd_RI2conv(em)
                 em = fftc2(em)
             if p["return_transmission"]:
-                t = self.crop_conv2field(fftc2(np.sum(em * self.kernel_trans, axis=2), inverse=True))
-                t = fftc2(t) + inp[:, :, 0, k]
+                t = self.crop_conv2field(fftc2(np.sum(em * self.kernel_trans[..., None], axis=2), inverse=True))
+                t = fftc2(t) + inp[:, :, :, k]
                 t = self.transform_field_2D(t)
-                ft[:, :, 0, k] = fftc2(t, inverse=True)
+                ft[:, :, :, k] = fftc2(t, inverse=True)
             if p["return_reflection"]:
-                r = self.crop_conv2field(fftc2(np.sum(em * self.kernel_ref, axis=2), inverse=True))
+                r = self.crop_conv2field(fftc2(np.sum(em * self.kernel_ref[..., None], axis=2), inverse=True))
                 r = fftc2(r)
-                r = self.transform_field_2D(r)
-                fr[:, :, 0, k] = fftc2(r, inverse=True)
+                r = self.transform_field_2D(r, reflection=True)
+                fr[:, :, :, k] = fftc2(r, inverse=True)
         return ft, fr, f3
 
     def refocus_source(self, source):
@@ -622,7 +709,10 @@ class ForwardSolverCBS:
         s = fftc2(source, inverse=True)
         s = self.padd_field2conv(s)
         s = fftc2(s)
-        s = s[:, :, None] * self.refocusing_util
+        if s.ndim == 3:   # components: [C, C, 1, 3] .* refocusing_util
+            s = s[:, :, None, :] * self.refocusing_util[:, :, :, None]
+        else:
+            s = s[:, :, None] * self.refocusing_util
         s = fftc2(s, inverse=True)
         return self.crop_conv2RI(s)
 
@@ -630,10 +720,11 @@ class ForwardSolverCBS:
         """``:521-654``: the Born loop, restated literally.  ``n_iter``
         truncates the loop (used only to time a bounded CPU sample)."""
         P = self.P
-        if source.ndim == 3:
+        vec = self.pole_num == 3
+        if source.ndim == 3 and not vec:
             source = source[:, :, 0]
         V = self.V
-        shp = V.shape
+        shp = V.shape + ((3,) if vec else ())
         psi = np.zeros(shp, dtype=P.c)
         Field = np.zeros(shp, dtype=P.c)
         Field_n = np.zeros(shp, dtype=P.c)
@@ -641,9 +732,12 @@ class ForwardSolverCBS:
         incident = source
         R = self.ROI
         roi = (slice(R[0] - 1, R[1]), slice(R[2] - 1, R[3]), slice(R[4] - 1, R[5]))
-        source = (V[roi] + 1j * self.eps_imag) * source               # :566
+        Vx = V[..., None] if vec else V
+        source = ((V[roi] + 1j * self.eps_imag)[..., None] if vec else (V[roi] + 1j * self.eps_imag)) * source  # :566
         Greenp = self.Greenp
         ramp = self.phase_ramp
+        rads = self.rads if vec else None
+        corr = self.green_absorbtion_correction
         acyc = self.parameters["acyclic"]
         c = 1j / self.eps_imag
         nB = self.Bornmax if n_iter is None else min(n_iter, self.Bornmax)
@@ -651,19 +745,32 @@ class ForwardSolverCBS:
         for jj in range(1, nB + 1):
             if acyc:
                 Greenp = fft_flip(Greenp, [1, 1, 1], False)
+                if vec:
+                    rads = fft_flip(rads, [1, 1, 1], False)
                 ramp = np.conj(ramp)
             psi[...] = 0
             if jj in (1, 2):
                 Field_n[...] = 0
                 psi[roi] = c * source / 2
             else:
-                psi = c * Field_n * V
-            PSI = Greenp * sfft.fftn(psi * ramp, workers=_WORKERS)
-            PSI = sfft.ifftn(PSI, workers=_WORKERS) * np.conj(ramp)
+                psi = c * Field_n * Vx
+            if vec:   # dyadic absorptive Green's function (:597-601)
+                PSI = np.zeros(shp, dtype=P.c)
+                for j2 in range(3):
+                    coeff = sfft.fftn(psi[..., j2] * ramp, workers=_WORKERS)
+                    eye = np.zeros(3, dtype=P.r)
+                    eye[j2] = 1
+                    d = eye - (corr * rads) * rads[..., j2:j2 + 1]
+                    PSI = PSI + (Greenp[..., None] * d) * coeff[..., None]
+                for j1 in range(3):
+                    PSI[..., j1] = sfft.ifftn(PSI[..., j1], workers=_WORKERS) * np.conj(ramp)
+            else:
+                PSI = Greenp * sfft.fftn(psi * ramp, workers=_WORKERS)
+                PSI = sfft.ifftn(PSI, workers=_WORKERS) * np.conj(ramp)
             if jj not in (1, 2):
                 Field_n = Field_n - psi
-            Field_n = Field_n + V * PSI
-            Field_n = Field_n * self.attenuation_mask
+            Field_n = Field_n + Vx * PSI
+            Field_n = Field_n * (self.attenuation_mask[..., None] if vec else self.attenuation_mask)
             if jj == 2:
                 temp = Field
             Field = Field + Field_n

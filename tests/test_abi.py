@@ -23,7 +23,7 @@ def test_library_exports_every_declared_symbol():
     for n in names:
         assert hasattr(lib, n), n
         assert n in _lib.SIGNATURES, n
-    assert lib.odt_abi_version() == 1
+    assert lib.odt_abi_version() == 2
 
 
 def test_bad_handle_and_null_arguments():

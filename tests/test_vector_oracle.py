@@ -1,0 +1,102 @@
+"""Dyadic (vector) branch without a GPU: the polarisation basis of
+polarisation_utility (FORWARD_SOLVER.m:131-180) and its 2 <-> 3 component
+round trip, the library's host tables against the oracle's, and the oracle's
+vector solve (single against double precision; weak-scatterer limit against
+the scalar solve)."""
+import numpy as np
+
+import cases
+from inverse_solver_b200.forward import CBSHostSetup
+from inverse_solver_b200.optics import polarisation_basis
+from oracle import cbs
+
+SIZE = [28, 28, 20]
+
+
+def vparams(**kw):
+    p = cases.params(SIZE, [2, 2, 1.5], **kw)
+    p["vector_simulation"] = True
+    return p
+
+
+def test_basis_is_orthonormal_and_tangent():
+    p = vparams()
+    R2, P2, E, K = cbs.polarisation_utility(SIZE[:2], p, cbs.Prec(True))
+    assert np.allclose(np.sum(R2 * R2, 2), 1, atol=1e-6)
+    assert np.allclose(np.sum(P2 * P2, 2), 1, atol=1e-6)
+    assert np.allclose(np.sum(R2 * P2, 2), 0, atol=1e-6)
+    assert K.sum() > 0 and not K.all()
+    e = E[K]
+    assert np.allclose(np.sum(e * e, 1), 1, atol=1e-5)
+    # the tangent is orthogonal to the perpendicular vector (P2 has no z part)
+    assert np.allclose(np.sum(E[:, :, :2] * P2, 2)[K], 0, atol=1e-5)
+
+
+def test_polarisation_round_trip_is_identity_on_propagating_pixels():
+    """transform_field_2D(transform_field_3D(f)) without the pupil factors:
+    the 2 -> 3 -> 2 basis change returns f wherever K_mask holds."""
+    p = vparams(use_abbe_sine=False)
+    p["NA"] = 1.3
+    o = cbs.ForwardSolverCBS(p, single=False)
+    rng = np.random.default_rng(0)
+    f = rng.standard_normal((28, 28, 2, 3)) + 1j * rng.standard_normal((28, 28, 2, 3))
+    NA = o.utility["NA_circle"]
+    _, _, _, K = cbs.polarisation_utility(SIZE[:2], p, cbs.Prec(False))
+    g = o.transform_field_2D(o.transform_field_3D(f))
+    m = (NA & K)[:, :, None, None]
+    assert np.allclose(g * m, f * m, atol=1e-12)
+
+
+def test_library_basis_equals_oracle_bitwise():
+    p = vparams()
+    ref = cbs.polarisation_utility(SIZE[:2], p, cbs.Prec(True))
+    got = polarisation_basis(SIZE[:2], p)
+    for a, b in zip(got, ref):
+        assert np.array_equal(a, b)
+
+
+def test_library_dyadic_tables_equal_oracle():
+    p = vparams()
+    RI = cases.sphere_phantom(SIZE, [0.1] * 3, cases.NM, seed=5, n_spheres=2, radius_um=(0.4, 0.8))
+    h = CBSHostSetup(p)
+    h.prepare_potential(RI)
+    o = cbs.ForwardSolverCBS(p, single=True)
+    o.set_RI(RI)
+    for a, b in zip(h.rads1d, o.rads1d):
+        assert np.array_equal(a, np.fft.ifftshift(b))
+    assert h.green_absorbtion_correction == o.green_absorbtion_correction
+    r = o.rads
+    assert np.array_equal(r[:, 0, 0, 0], h.rads1d[0])
+    assert np.array_equal(r[0, :, 0, 1], h.rads1d[1])
+    assert np.array_equal(r[0, 0, :, 2], h.rads1d[2])
+
+
+def _vector_inputs(n=2):
+    f = cases.circle_fields(cases.params(SIZE, [2, 2, 1.5]), n)
+    fv = np.zeros((SIZE[0], SIZE[1], 2, n), np.complex64)
+    fv[:, :, 0, 0] = f[:, :, 0, 0]                     # x-polarised
+    fv[:, :, 0, 1] = f[:, :, 0, 1] * np.float32(0.6)   # mixed polarisation
+    fv[:, :, 1, 1] = f[:, :, 0, 1] * np.float32(0.8)
+    return fv
+
+
+def test_vector_oracle_single_vs_double_and_scalar_limit():
+    p = vparams(return_reflection=True, return_3D=True)
+    RI = cases.sphere_phantom(SIZE, [0.1] * 3, cases.NM, seed=5, n_spheres=2, radius_um=(0.4, 0.8))
+    fv = _vector_inputs()
+    o32 = cbs.ForwardSolverCBS(p, single=True)
+    o32.set_RI(RI)
+    t, r, f3 = o32.solve(fv)
+    o64 = cbs.ForwardSolverCBS(p, single=False)
+    o64.set_RI(RI)
+    t64, r64, f364 = o64.solve(fv)
+    assert t.shape == (28, 28, 2, 2) and f3.shape == (28, 28, 20, 3, 2)
+    assert cbs.rel_l2(t, t64) < 1e-5 and cbs.rel_l2(f3, f364) < 1e-5 and cbs.rel_l2(r, r64) < 1e-4
+    # x-polarised input: the x component follows the scalar solve to within the
+    # (small) vector coupling of this weak phantom; little cross-polarisation
+    ps = cases.params(SIZE, [2, 2, 1.5], return_3D=True)
+    os_ = cbs.ForwardSolverCBS(ps, single=True)
+    os_.set_RI(RI)
+    ts, _, _ = os_.solve(fv[:, :, 0:1, 0:1])
+    assert cbs.rel_l2(t[:, :, 0, 0], ts[:, :, 0, 0]) < 0.05
+    assert np.linalg.norm(t[:, :, 1, 0]) < 0.05 * np.linalg.norm(t[:, :, 0, 0])
