@@ -142,6 +142,20 @@ struct Handle {
   // in the environment at odt_create selects the generic tile kernels)
   bool use_pipe = true;
 
+  // CUDA graphs of a batch's whole solve (run_chunk), keyed by batch size,
+  // outputs and potential slot; captured the second time a key is seen (the
+  // first run is eager, so every kernel attribute is set before a capture)
+  // and dropped whenever a buffer or a potential they captured changes.
+  // ODT_GRAPHS=0 in the environment at odt_create turns them off.
+  bool use_graphs = true;
+  std::map<long long, cudaGraphExec_t> graphs;
+  std::map<long long, int> graph_seen;
+  void drop_graphs() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    graphs.clear();
+    graph_seen.clear();
+  }
+
   // profiling
   bool profiling = false;
   std::vector<cudaEvent_t> ev;
@@ -192,6 +206,7 @@ struct Handle {
   }
 
   ~Handle() {
+    drop_graphs();
     for (void* p : batch_allocs) cudaFree(p);
     for (void* p : allocs) cudaFree(p);
     for (cudaEvent_t e : ev) cudaEventDestroy(e);
@@ -304,6 +319,7 @@ bool is_device_ptr(const void* p) {
 void ensure_batch(Handle& H, int nb) {
   if (H.batch >= nb) return;
   ODT_CUDA(cudaDeviceSynchronize());  // buffers may still be in use by queued work
+  H.drop_graphs();
   H.free_batch();
   const size_t nbp = (size_t)nb * H.np;  // field planes of nb illuminations
   H.work = H.dalloc<float2>((size_t)H.work_elems() * nbp, true);
@@ -502,6 +518,45 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
 }
 
 
+// run_chunk through the handle's graph cache: eager the first time a key is
+// seen, captured (thread-local capture mode) the second time, replayed after.
+// Not on the legacy / per-thread default streams (they cannot be captured)
+// nor while per-kernel profiling is on.
+void run_chunk_graph(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int slot,
+                     float2* fout) {
+  if (!H.use_graphs || H.profiling || s == nullptr || s == cudaStreamLegacy || s == cudaStreamPerThread) {
+    run_chunk(H, nb, s, want_t, want_r, slot, fout);
+    return;
+  }
+  const long long key = (long long)nb | ((long long)want_t << 32) | ((long long)want_r << 33) |
+                        ((long long)slot << 34) | ((long long)(fout == H.fout_adj) << 35);
+  auto it = H.graphs.find(key);
+  if (it == H.graphs.end()) {
+    if (H.graph_seen[key]++ == 0) {
+      run_chunk(H, nb, s, want_t, want_r, slot, fout);
+      return;
+    }
+    ODT_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+      run_chunk(H, nb, s, want_t, want_r, slot, fout);
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(s, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      throw;
+    }
+    cudaGraph_t g = nullptr;
+    ODT_CUDA(cudaStreamEndCapture(s, &g));
+    cudaGraphExec_t ge = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    ODT_CUDA(e);
+    it = H.graphs.emplace(key, ge).first;
+  }
+  ODT_CUDA(cudaGraphLaunch(it->second, s));
+}
+
 void alloc_slot(Handle& H, int k) {
   Handle::PotSlot& P = H.pot[k];
   if (P.allocated) return;
@@ -535,6 +590,8 @@ void set_potential_slot(const std::shared_ptr<Handle>& Hp, int k, const odt_pote
   if (!std::isfinite(pp->green_scale) || !std::isfinite(pp->green_offset) || !std::isfinite(pp->dV))
     raise(ODT_ERR_INVALID_ARGUMENT, who + ": non-finite scalar");
   DeviceGuard dg(g.device);
+  ODT_CUDA(cudaDeviceSynchronize());  // a queued graph may still read the old tables
+  H.drop_graphs();
   alloc_slot(H, k);
   Handle::PotSlot& P = H.pot[k];
   const size_t nv = (size_t)H.nvox();
@@ -614,6 +671,7 @@ odt_status odt_create(const odt_geometry* geom, const odt_cfloat* refocus,
     H->npol = g.pol == 3 ? 2 : 1;
     ODT_CUDA(cudaDeviceGetAttribute(&H->max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, g.device));
     if (const char* k = std::getenv("ODT_KERNELS")) H->use_pipe = std::string(k) != "generic";
+    if (const char* k = std::getenv("ODT_GRAPHS")) H->use_graphs = std::string(k) != "0";
     ODT_CUDA(cudaStreamCreateWithFlags(&H->own_stream, cudaStreamNonBlocking));
     H->fx = make_dev_fft(*H, g.sim_size[0], kKindBornX, "sim_size(1)");
     H->fy = make_dev_fft(*H, g.sim_size[1], kKindCols, "sim_size(2)");
@@ -671,6 +729,8 @@ odt_status odt_set_polarisation(odt_handle h, const float* radial, const float* 
     std::copy(perp, perp + 2 * n, tab.begin() + 2 * n);
     std::copy(tangent, tangent + 3 * n, tab.begin() + 4 * n);
     for (long long i = 0; i < n; ++i) tab[7 * n + i] = kmask[i] ? 1.f : 0.f;
+    ODT_CUDA(cudaDeviceSynchronize());
+    H->drop_graphs();
     if (!H->pol_tab) H->pol_tab = H->dalloc<float>(tab.size(), false);
     ODT_CUDA(cudaMemcpy(H->pol_tab, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice));
     H->have_pol = true;
@@ -713,7 +773,7 @@ odt_status odt_solve(odt_handle h, const odt_solve_args* args) {
       const int nb = std::min(H->batch, A.n_ill - b0);
       ODT_CUDA(cudaMemcpyAsync(H->in2d, A.fields_in + (size_t)b0 * nF,
                                (size_t)nb * nF * sizeof(float2), kin, s));
-      run_chunk(*H, nb, s, want_t, want_r, 0, H->fout);
+      run_chunk_graph(*H, nb, s, want_t, want_r, 0, H->fout);
       ODT_CUDA(launch_count_nonfinite(H->fout, nR * nb, H->d_count, s));
       if (A.field3d)
         ODT_CUDA(cudaMemcpyAsync(A.field3d + (size_t)b0 * nR, H->fout,
@@ -782,9 +842,9 @@ odt_status odt_gradient(odt_handle h, const odt_gradient_args* args) {
                                (size_t)nb * nF * sizeof(float2), kin, s));
       ODT_CUDA(cudaMemcpyAsync(H->out_r, A.fields_meas + (size_t)b0 * nF,
                                (size_t)nb * nF * sizeof(float2), kin, s));
-      run_chunk(*H, nb, s, true, false, 0, H->fout);              // E_3D, trans
+      run_chunk_graph(*H, nb, s, true, false, 0, H->fout);        // E_3D, trans
       ODT_CUDA(launch_residual(H->out_t, H->out_r, H->in2d, nF * nb, H->d_err, s));
-      run_chunk(*H, nb, s, false, false, 1, H->fout_adj);         // adjoint 3D field
+      run_chunk_graph(*H, nb, s, false, false, 1, H->fout_adj);   // adjoint 3D field
       ODT_CUDA(launch_grad_accumulate(H->fout, H->fout_adj, H->grad_acc, H->g.ri_size[0],
                                       H->g.ri_size[1], H->g.ri_size[2], nb, s));
       H->collect(s);
