@@ -139,6 +139,39 @@ def cpu_baseline(p, RI, fields, n_iter):
                       f"on the {list(o.V.shape)} padded grid ({dt:.1f} s)"}
 
 
+def plain_single_solve(p, RI, fields, n_ill=3):
+    """The library's plain path on the same workload: one illumination per
+    solve (batch of 1), the generic (non-pipelined) tile kernels, no graph
+    replay; synchronous host calls, timed on the host clock after one warm-up
+    solve.  Returns voxel-iterations/s."""
+    import os as _os
+
+    from inverse_solver_b200 import FORWARD_SOLVER_CONVERGENT_BORN
+
+    saved = {k: _os.environ.get(k) for k in ("ODT_KERNELS", "ODT_GRAPHS")}
+    _os.environ["ODT_KERNELS"] = "generic"
+    _os.environ["ODT_GRAPHS"] = "0"
+    try:
+        q = dict(p, max_batch=1)
+        s = FORWARD_SOLVER_CONVERGENT_BORN(q)
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                _os.environ.pop(k, None)
+            else:
+                _os.environ[k] = v
+    s.set_RI(RI)
+    one = np.ascontiguousarray(fields[:, :, :, :1])
+    s.solve(one)
+    t0 = time.perf_counter()
+    for k in range(n_ill):
+        s.solve(np.ascontiguousarray(fields[:, :, :, k:k + 1]))
+    dt = time.perf_counter() - t0
+    v = s.voxel_iterations(n_ill) / dt
+    s.delete()
+    return v
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -285,6 +318,12 @@ def run_ours(args, rank, world, local_rank):
     }
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(p, RI, fields, args.ref_iters)
+    if world == 1 and not args.no_plain:
+        pv = plain_single_solve(p, RI, fields)
+        out["plain_single_solve"] = {
+            "value": pv, "unit": UNIT, "speedup_of_value": value / pv,
+            "what": "same workload, one illumination per solve, generic tile kernels, no graph "
+                    "replay, host calls (3 illuminations timed)"}
     s.delete()
     print(json.dumps(out))
 
@@ -302,6 +341,8 @@ def main():
     ap.add_argument("--ref-iters", type=int, default=16,
                     help="Born iterations in the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="skip the plain single-solve comparison")
     ap.add_argument("--n-ill", type=int, default=N_ILL,
                     help="illuminations per step (profiling runs use fewer)")
     ap.add_argument("--profile-run", action="store_true",

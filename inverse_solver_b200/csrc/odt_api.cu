@@ -61,6 +61,12 @@ struct ApiError {
 
 [[noreturn]] void raise(odt_status st, const std::string& msg) { throw ApiError{st, msg}; }
 
+// A stream capture (run_chunk_graph) must not overlap with device-wide work
+// of other threads -- cudaDeviceSynchronize, and allocation / release calls
+// that may synchronise the device -- so handles used from several threads
+// (the request loop) take this lock around both.
+std::recursive_mutex g_device_mu;
+
 // RAII guard restoring the caller's current device (CudaBorn does the same,
 // main.cpp:50-53).
 struct DeviceGuard {
@@ -187,6 +193,7 @@ struct Handle {
       raise(ODT_ERR_OUT_OF_MEMORY, "memory budget exceeded (" + std::to_string(bytes + nb) +
                                        " > " + std::to_string(budget) + " bytes)");
     void* p = nullptr;
+    std::lock_guard<std::recursive_mutex> lk(g_device_mu);
     cudaError_t e = cudaMalloc(&p, nb ? nb : 1);
     if (e == cudaErrorMemoryAllocation) {
       cudaGetLastError();
@@ -199,6 +206,7 @@ struct Handle {
   }
 
   void free_batch() {
+    std::lock_guard<std::recursive_mutex> lk(g_device_mu);
     for (void* p : batch_allocs) cudaFree(p);
     batch_allocs.clear();
     batch_bytes = 0;
@@ -206,6 +214,7 @@ struct Handle {
   }
 
   ~Handle() {
+    std::lock_guard<std::recursive_mutex> lk(g_device_mu);
     drop_graphs();
     for (void* p : batch_allocs) cudaFree(p);
     for (void* p : allocs) cudaFree(p);
@@ -318,6 +327,7 @@ bool is_device_ptr(const void* p) {
 
 void ensure_batch(Handle& H, int nb) {
   if (H.batch >= nb) return;
+  std::lock_guard<std::recursive_mutex> lk(g_device_mu);
   ODT_CUDA(cudaDeviceSynchronize());  // buffers may still be in use by queued work
   H.drop_graphs();
   H.free_batch();
@@ -536,6 +546,7 @@ void run_chunk_graph(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r
       run_chunk(H, nb, s, want_t, want_r, slot, fout);
       return;
     }
+    std::lock_guard<std::recursive_mutex> lk(g_device_mu);
     ODT_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     try {
       run_chunk(H, nb, s, want_t, want_r, slot, fout);
@@ -590,6 +601,7 @@ void set_potential_slot(const std::shared_ptr<Handle>& Hp, int k, const odt_pote
   if (!std::isfinite(pp->green_scale) || !std::isfinite(pp->green_offset) || !std::isfinite(pp->dV))
     raise(ODT_ERR_INVALID_ARGUMENT, who + ": non-finite scalar");
   DeviceGuard dg(g.device);
+  std::lock_guard<std::recursive_mutex> lk(g_device_mu);
   ODT_CUDA(cudaDeviceSynchronize());  // a queued graph may still read the old tables
   H.drop_graphs();
   alloc_slot(H, k);
@@ -729,6 +741,7 @@ odt_status odt_set_polarisation(odt_handle h, const float* radial, const float* 
     std::copy(perp, perp + 2 * n, tab.begin() + 2 * n);
     std::copy(tangent, tangent + 3 * n, tab.begin() + 4 * n);
     for (long long i = 0; i < n; ++i) tab[7 * n + i] = kmask[i] ? 1.f : 0.f;
+    std::lock_guard<std::recursive_mutex> lk(g_device_mu);
     ODT_CUDA(cudaDeviceSynchronize());
     H->drop_graphs();
     if (!H->pol_tab) H->pol_tab = H->dalloc<float>(tab.size(), false);
@@ -822,6 +835,7 @@ odt_status odt_gradient(odt_handle h, const odt_gradient_args* args) {
     if (H->grad_batch != H->batch) {
       for (void** p : {(void**)&H->fout_adj, (void**)&H->grad_acc, (void**)&H->d_err}) {
         if (*p) {
+          std::lock_guard<std::recursive_mutex> lk(g_device_mu);
           cudaFree(*p);
           auto& L = H->allocs;
           L.erase(std::remove(L.begin(), L.end(), *p), L.end());

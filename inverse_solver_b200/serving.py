@@ -320,7 +320,8 @@ def run_stream(reqs, rate_per_s, seed, budget_bytes=None, slots=4):
     """Poisson arrivals at ``rate_per_s``: submit each request at its arrival
     time, wait for all; returns (results, stats)."""
     rng = np.random.default_rng(seed)
-    gaps = rng.exponential(1.0 / rate_per_s, size=len(reqs))
+    gaps = (np.zeros(len(reqs)) if not np.isfinite(rate_per_s)
+            else rng.exponential(1.0 / rate_per_s, size=len(reqs)))
     srv = SolveServer(budget_bytes=budget_bytes, slots=slots)
     t0 = time.perf_counter()
     futs = []
@@ -348,10 +349,28 @@ def main():
     ap.add_argument("--slots", type=int, default=4)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--recon-every", type=int, default=6)
+    ap.add_argument("--uneven", action="store_true",
+                    help="batched uneven solves: all requests submitted at once, forward only, "
+                         "grids 64^3 / 96x96x64 / 128^3 / 192x192x96, 1-64 illuminations")
     a = ap.parse_args()
-    reqs = make_mix(a.requests, a.seed, recon_every=a.recon_every)
+    if a.uneven:
+        reqs = make_mix(a.requests, a.seed, sizes=((64, 64, 64), (96, 96, 64), (128, 128, 128),
+                                                   (192, 192, 96)), max_ill=64, recon_every=0)
+        a.rate = float("inf")
+    else:
+        reqs = make_mix(a.requests, a.seed, recon_every=a.recon_every)
     serial = one_at_a_time(reqs)
     _, st = run_stream(reqs, a.rate, a.seed + 1, slots=a.slots)
+    vox = 0
+    for r in reqs:
+        if isinstance(r, ForwardRequest):
+            from .forward import CBSHostSetup
+
+            h = CBSHostSetup(r.params)
+            h.prepare_potential(r.RI)
+            vox += h.voxel_iterations(r.fields.shape[3])
+    if vox:
+        st["forward_voxel_iter_per_s"] = vox * st["throughput_per_s"] / len(reqs)
     st.update(one_at_a_time_s=serial, serial_throughput_per_s=len(reqs) / serial,
               rate_per_s=a.rate, slots=a.slots, seed=a.seed, n_requests=len(reqs))
     print(json.dumps(st))
