@@ -217,6 +217,23 @@ class CroppedHankel:
         return (self.bwd @ (vals / self.K[:self.pos, None])) * self.Rv[:, None]
 
 
+_HANKEL_CACHE = {}
+
+
+def _cropped_hankel(samples, cropping):
+    """The order-0 unit-radius transform of truncated_green_plus; the
+    refocusing kernel and the Green's function of one geometry use the same
+    one, so it is built once (its Bessel matrices are most of the set-up
+    time).  Keeps the last few."""
+    key = (int(samples), float(cropping))
+    hk = _HANKEL_CACHE.get(key)
+    if hk is None:
+        if len(_HANKEL_CACHE) >= 4:
+            _HANKEL_CACHE.pop(next(iter(_HANKEL_CACHE)))
+        hk = _HANKEL_CACHE[key] = CroppedHankel(1, samples, 0, cropping)
+    return hk
+
+
 def _nearest_bins(value, grid):
     """Bracketing sample indices and linear weight of `value` in the sorted
     `grid` (truncated_green_plus.m:111-129), 1-based like the reference."""
@@ -258,7 +275,7 @@ def truncated_green_plus(params, refocus_version=False):
     samples = params["oversample_xy"] * ovf
     if samples < math.sqrt(S1 ** 2 + S2 ** 2) * 5:
         raise ValueError("truncated_green_plus: grid too large for the Hankel sampling")
-    hk = CroppedHankel(1, samples, 0, (math.sqrt(S1 ** 2 + S2 ** 2) * ovf) / (2 * samples))
+    hk = _cropped_hankel(samples, (math.sqrt(S1 ** 2 + S2 ** 2) * ovf) / (2 * samples))
     H = hk.r / hk.r.max()
     H = H * (u.coorxy.max() * ovf)
     Hk3 = u.k0_nm ** 2 - H ** 2
