@@ -74,3 +74,17 @@ def test_pipe_matches_generic_on_benchmark_grid():
     assert sim == [152, 152, 152] and bm >= 30
     assert worst(t1, t2) < 1e-6
     assert worst(f1, f2) < 1e-6
+
+
+def test_pipe_passes_cyclic_boundary_matches_oracle():
+    """acyclic = false (no phase ramp, no Green's-function flips) through the
+    pipelined x-, y- and z-passes: padded grid (120, 88, 40)."""
+    size = [96, 64, 16]
+    p = cases.params(size, [6, 6, 6], return_3D=True, acyclic=False)
+    RI = cases.sphere_phantom(size, [0.1] * 3, cases.NM, seed=9, n_spheres=3, radius_um=(0.3, 0.8))
+    fields = cases.circle_fields(p, 2)
+    (t, _, f), (sim, bm) = _solve(p, RI, fields)
+    o = cbs.ForwardSolverCBS(p, single=True)
+    o.set_RI(RI)
+    ot, _, of = o.solve(fields)
+    assert worst(f, of) < 1e-5 and worst(t, ot) < 1e-5
