@@ -4,7 +4,8 @@
 // FORWARD_SOLVER_CONVERGENT_BORN.m:588-605, :616-642), restructured for the
 // B200 memory system:
 //
-//   * persistent CTAs (two per SM) walk the tiles of 16 x-lines; a tile of
+//   * persistent CTAs (two per SM) walk the tiles of 16 x-lines (8 lines and
+//     three CTAs per SM for n = 200, 216); a tile of
 //     consecutive lines is one contiguous block of T, Field_n and Field, so
 //     one thread moves it into shared memory with bulk asynchronous copies
 //     (the TMA engine) completing on an mbarrier;
@@ -32,9 +33,8 @@
 namespace odt {
 namespace {
 
-constexpr int kW = 16;                 // x-lines per tile
-constexpr int kR1 = 8;
-constexpr int kThreads = kW * kR1;     // one radix-R2 butterfly per thread
+constexpr int kR1 = 8;                 // a tile of W x-lines takes W * 8 threads:
+                                       // one radix-R2 butterfly per thread
 
 struct PipeLine {      // per-line constants of a tile
   long long g;         // element offset of x = 0 in T / Field_n / Field
@@ -46,7 +46,7 @@ struct PipeLine {      // per-line constants of a tile
 
 constexpr size_t a16(size_t b) { return (b + 15) & ~(size_t)15; }
 
-template <int N>
+template <int N, int kW>
 struct PipeSmem {
   static constexpr int kLdB = (N + N / 8 + 1) + ((8 - ((N + N / 8 + 1) & 15)) & 15);
   static constexpr size_t kBars = 0;                                   // 3 mbarriers
@@ -63,13 +63,17 @@ struct PipeSmem {
   static constexpr size_t kTotal = kB + sizeof(float2) * kLdB * kW;
 };
 
-template <int R2>
-__global__ void __launch_bounds__(kThreads, 2)
+// W = 16 x-lines per tile (two CTAs per SM) where the shared memory allows,
+// else 8 (n = 200, 216: three CTAs per SM)
+template <int R2, int W>
+__global__ void __launch_bounds__(W * 8, W == 16 ? 2 : 3)
     born_x_pipe_kernel(const BornArgs a, const int jj, const float2* __restrict__ twg, const int ntiles,
                        int* __restrict__ fault) {
 #if defined(__CUDA_ARCH__)
   constexpr int N = kR1 * R2;
-  using L = PipeSmem<N>;
+  constexpr int kW = W;
+  constexpr int kThreads = W * kR1;
+  using L = PipeSmem<N, W>;
   extern __shared__ __align__(128) unsigned char sm[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + L::kBars);  // [0], [1]: T stages, [2]: Fn/F
   float2* tw = reinterpret_cast<float2*>(sm + L::kTw);
@@ -271,15 +275,23 @@ __global__ void __launch_bounds__(kThreads, 2)
 #endif
 }
 
+constexpr size_t kSmemCap = 113 * 1024;   // two CTAs per SM
+
+template <int R2>
+constexpr int tile_lines() {
+  return PipeSmem<kR1 * R2, 16>::kTotal <= kSmemCap ? 16 : 8;
+}
+
 template <int R2>
 cudaError_t launch_r2(const BornArgs& a, int jj, const DevFft& fx, int* fault, cudaStream_t s) {
-  using L = PipeSmem<kR1 * R2>;
+  constexpr int W = tile_lines<R2>();
+  using L = PipeSmem<kR1 * R2, W>;
   static int configured = -1;   // per process: attribute set once per device
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (configured != dev) {
-    e = cudaFuncSetAttribute(born_x_pipe_kernel<R2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(born_x_pipe_kernel<R2, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)L::kTotal);
     if (e != cudaSuccess) return e;
     configured = dev;
@@ -287,11 +299,23 @@ cudaError_t launch_r2(const BornArgs& a, int jj, const DevFft& fx, int* fault, c
   int nsm = 0;
   e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
-  const int nty = (a.py + kW - 1) / kW;
+  const int per_sm = W == 16 ? 2 : 3;
+  const int nty = (a.py + W - 1) / W;
   const long long ntiles = (long long)nty * a.pz * a.nbatch;
-  const int grid = (int)(ntiles < 2LL * nsm ? ntiles : 2LL * nsm);
-  born_x_pipe_kernel<R2><<<grid, kThreads, L::kTotal, s>>>(a, jj, fx.tw, (int)ntiles, fault);
+  const int grid = (int)(ntiles < (long long)per_sm * nsm ? ntiles : (long long)per_sm * nsm);
+  born_x_pipe_kernel<R2, W><<<grid, W * kR1, L::kTotal, s>>>(a, jj, fx.tw, (int)ntiles, fault);
   return cudaGetLastError();
+}
+
+int lines_of(int r2) {
+  switch (r2) {
+    case 11: return tile_lines<11>();
+    case 15: return tile_lines<15>();
+    case 19: return tile_lines<19>();
+    case 25: return tile_lines<25>();
+    case 27: return tile_lines<27>();
+    default: return 0;
+  }
 }
 
 }  // namespace
@@ -299,8 +323,9 @@ cudaError_t launch_r2(const BornArgs& a, int jj, const DevFft& fx, int* fault, c
 bool born_x_pipe_supported(const BornArgs& a, const DevFft& fx) {
   if (fx.plan.n != a.px || a.px % kR1 != 0) return false;
   const int r2 = a.px / kR1;
-  if (r2 != 11 && r2 != 15 && r2 != 19) return false;
-  const long long ntiles = (long long)((a.py + kW - 1) / kW) * a.pz * a.nbatch;
+  const int W = lines_of(r2);
+  if (W == 0) return false;
+  const long long ntiles = (long long)((a.py + W - 1) / W) * a.pz * a.nbatch;
   return ntiles < (1LL << 31);
 }
 
@@ -309,6 +334,8 @@ cudaError_t launch_born_x_pipe(const BornArgs& a, int jj, const DevFft& fx, int*
     case 11: return launch_r2<11>(a, jj, fx, fault, s);
     case 15: return launch_r2<15>(a, jj, fx, fault, s);
     case 19: return launch_r2<19>(a, jj, fx, fault, s);
+    case 25: return launch_r2<25>(a, jj, fx, fault, s);
+    case 27: return launch_r2<27>(a, jj, fx, fault, s);
     default: return cudaErrorNotSupported;
   }
 }

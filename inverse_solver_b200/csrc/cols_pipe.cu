@@ -306,6 +306,8 @@ cudaError_t dispatch(const BornArgs& a, int jj, const DevFft& f, int* fault, cud
     case 11: return launch_kind<11, KIND>(a, jj, f, fault, s);
     case 15: return launch_kind<15, KIND>(a, jj, f, fault, s);
     case 19: return launch_kind<19, KIND>(a, jj, f, fault, s);
+    case 25: return launch_kind<25, KIND>(a, jj, f, fault, s);
+    case 27: return launch_kind<27, KIND>(a, jj, f, fault, s);
     default: return cudaErrorNotSupported;
   }
 }
@@ -316,7 +318,7 @@ bool cols_pipe_supported(const BornArgs& a, const DevFft& f, bool zpass) {
   const int n = f.plan.n;
   if (n != (zpass ? a.pz : a.py) || n % kR1 != 0) return false;
   const int r2 = n / kR1;
-  if (r2 != 11 && r2 != 15 && r2 != 19) return false;
+  if (r2 != 11 && r2 != 15 && r2 != 19 && r2 != 25 && r2 != 27) return false;
   if (a.px % 2 != 0 || !encoder()) return false;   // row strides must be multiples of 16 bytes
   const long long nout = zpass ? (long long)a.py * a.nbatch : (long long)a.pz * a.nbatch;
   return nout * ((a.px + kW - 1) / kW) < (1LL << 31);

@@ -88,3 +88,20 @@ def test_pipe_passes_cyclic_boundary_matches_oracle():
     o.set_RI(RI)
     ot, _, of = o.solve(fields)
     assert worst(f, of) < 1e-5 and worst(t, ot) < 1e-5
+
+
+@pytest.mark.parametrize("size", [[176, 24, 16], [24, 192, 16], [24, 24, 192], [192, 24, 16]])
+def test_pipe_radix_25_27_match_oracle(size):
+    """Padded lengths 200 = 8 x 25 and 216 = 8 x 27 on each axis in turn:
+    (200, 48, 40), (48, 216, 40), (48, 48, 216), (216, 48, 40); the x-pass
+    uses tiles of 8 lines there."""
+    p = cases.params(size, [6, 6, 6], return_3D=True)
+    RI = cases.sphere_phantom(size, [0.1] * 3, cases.NM, seed=sum(size), n_spheres=2,
+                              radius_um=(0.3, 0.8))
+    fields = cases.circle_fields(p, 2)
+    (t, _, f), (sim, bm) = _solve(p, RI, fields)
+    assert sim == [v + 24 for v in size] and bm >= 4
+    o = cbs.ForwardSolverCBS(p, single=True)
+    o.set_RI(RI)
+    ot, _, of = o.solve(fields)
+    assert worst(f, of) < 1e-5 and worst(t, ot) < 1e-5
