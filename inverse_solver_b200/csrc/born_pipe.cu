@@ -151,6 +151,20 @@ __global__ void __launch_bounds__(W * 8, W == 16 ? 2 : 3)
     }
     int b, y0, z, nl;
     decode(tile, b, y0, z, nl);
+    // V of this thread's first mid-pass butterfly, loaded now so that its
+    // latency hides behind the wait for T and the first FFT pass; each later
+    // round's V is loaded before the previous round's arithmetic
+    auto v_base = [&](int idx) {
+      const int c = idx / R2;
+      const int yy = c < nl ? y0 + c : y0;
+      return (yy + a.py * z) * N + (idx - c * R2);
+    };
+    float2 Vn[kR1];
+    if (tid < kW * R2) {
+      const int vb = v_base(tid);
+#pragma unroll
+      for (int r = 0; r < kR1; ++r) Vn[r] = a.V[vb + R2 * r];
+    }
     if (tid < kW) {
       PipeLine P;
       P.valid = tid < nl;
@@ -200,7 +214,12 @@ __global__ void __launch_bounds__(W * 8, W == 16 ? 2 : 3)
       const PipeLine& Ln = lines[c];
       float2 Vv[kR1];
 #pragma unroll
-      for (int r = 0; r < kR1; ++r) Vv[r] = a.V[Ln.v + j + R2 * r];
+      for (int r = 0; r < kR1; ++r) Vv[r] = Vn[r];
+      if (idx + kThreads < kW * R2) {
+        const int vb = v_base(idx + kThreads);
+#pragma unroll
+        for (int r = 0; r < kR1; ++r) Vn[r] = a.V[vb + R2 * r];
+      }
       float2 v[kR1];
 #pragma unroll
       for (int r = 0; r < kR1; ++r) v[r] = T0[c * N + j + R2 * r];
