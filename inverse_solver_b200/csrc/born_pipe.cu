@@ -298,22 +298,26 @@ constexpr size_t kSmemCap = 113 * 1024;   // two CTAs per SM
 
 template <int R2>
 constexpr int tile_lines() {
+#if defined(ODT_X_LINES)  // build-time override of the tile height (8 or 16) for measurements
+  return ODT_X_LINES;
+#else
   return PipeSmem<kR1 * R2, 16>::kTotal <= kSmemCap ? 16 : 8;
+#endif
 }
 
 template <int R2>
 cudaError_t launch_r2(const BornArgs& a, int jj, const DevFft& fx, int* fault, cudaStream_t s) {
   constexpr int W = tile_lines<R2>();
   using L = PipeSmem<kR1 * R2, W>;
-  static int configured = -1;   // per process: attribute set once per device
+  static DeviceFlags configured;   // attribute raised once per device
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if (configured != dev) {
+  if (!configured.test(dev)) {
     e = cudaFuncSetAttribute(born_x_pipe_kernel<R2, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)L::kTotal);
     if (e != cudaSuccess) return e;
-    configured = dev;
+    configured.set(dev);
   }
   int nsm = 0;
   e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);

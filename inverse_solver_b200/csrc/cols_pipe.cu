@@ -277,15 +277,15 @@ template <int R2, int KIND>
 cudaError_t launch_kind(const BornArgs& a, int jj, const DevFft& f, int* fault, cudaStream_t s) {
   using L = ColSmem<kR1 * R2>;
   constexpr size_t smem = KIND == 2 ? L::kTotalZ : L::kTotalY;
-  static int configured = -1;
+  static DeviceFlags configured;   // attribute raised once per device
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if (configured != dev) {
+  if (!configured.test(dev)) {
     e = cudaFuncSetAttribute(cols_pipe_kernel<R2, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
     if (e != cudaSuccess) return e;
-    configured = dev;
+    configured.set(dev);
   }
   CUtensorMap map;
   if (!make_map(a, KIND == 2, &map)) return cudaErrorInvalidValue;

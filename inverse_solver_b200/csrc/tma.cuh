@@ -10,6 +10,8 @@
 
 #include <stdint.h>
 
+#include <atomic>
+
 namespace odt {
 
 #if defined(__CUDA_ARCH__)
@@ -71,6 +73,16 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 }
 
 #endif  // __CUDA_ARCH__
+
+// Host side: one flag per (kernel instantiation, device) saying that the
+// kernel's dynamic shared-memory limit has been raised on that device.
+struct DeviceFlags {
+  std::atomic<unsigned long long> bits{0};
+  bool test(int dev) const { return dev < 64 && ((bits.load() >> dev) & 1ull); }
+  void set(int dev) {
+    if (dev < 64) bits.fetch_or(1ull << dev);
+  }
+};
 
 // fault codes written by the pipelined kernels (first one wins)
 enum PipeFault { kFaultNone = 0, kFaultTimeout = 1, kFaultAlign = 2 };
