@@ -37,9 +37,11 @@ SEED = 0
 # algorithmic HBM bytes per voxel and launch of each Born kernel kind
 # (complex64 = 8 B): born_x reads T, Field_n, Field, V and writes T, Field_n,
 # Field; born_y / born_z read and write T once.  "_pipe" = the pipelined
-# (TMA-fed, persistent) variants of the same passes.
+# (TMA-fed, persistent) variants of the same passes; "born_x_pipe_edge" = the
+# pipelined x-pass of iterations 2, 3 and the final pass (56 B nominal).
 ALG_BYTES_PER_VOXEL = {"born_x": 56, "born_y": 16, "born_z": 16,
-                       "born_x_pipe": 56, "born_y_pipe": 16, "born_z_pipe": 16}
+                       "born_x_pipe": 56, "born_y_pipe": 16, "born_z_pipe": 16,
+                       "born_x_pipe_edge": 56}
 
 
 def workload_params():

@@ -1,7 +1,9 @@
 // Pipelined x-pass of the Born iteration for x-lengths n = 8 * R2 (R2 odd):
-// the same arithmetic as born_x_body in mode Mid (inverse x-FFT, update of
-// iteration jj-1 for jj-1 >= 3, source term of iteration jj, forward x-FFT;
-// FORWARD_SOLVER_CONVERGENT_BORN.m:588-605, :616-642), restructured for the
+// the same arithmetic as born_x_body in modes Mid (inverse x-FFT, update of
+// iteration jj-1, source term of iteration jj, forward x-FFT;
+// FORWARD_SOLVER_CONVERGENT_BORN.m:588-605, :616-642; jj >= 2) and Last
+// (update of the final iteration, Field(ROI) + incident field, :646-647),
+// restructured for the
 // B200 memory system:
 //
 //   * persistent CTAs (two per SM) walk the tiles of 16 x-lines (8 lines and
@@ -38,8 +40,10 @@ constexpr int kR1 = 8;                 // a tile of W x-lines takes W * 8 thread
 
 struct PipeLine {      // per-line constants of a tile
   long long g;         // element offset of x = 0 in T / Field_n / Field
+  long long einc;      // Einc / Fout offset of x = 0 (when roi != 0)
   int v;               // element offset of x = 0 in V
   int valid;
+  int roi;             // y and z inside the ROI
   float my, mz;
   float2 ry, rz;
 };
@@ -64,8 +68,15 @@ struct PipeSmem {
 };
 
 // W = 16 x-lines per tile (two CTAs per SM) where the shared memory allows,
-// else 8 (n = 200, 216: three CTAs per SM)
-template <int R2, int W>
+// else 8 (n = 200, 216: three CTAs per SM).  KIND (compile time, so the
+// steady-state kernel carries none of the other cases' work):
+//   kSteady: jj >= 4 (update of iteration jj-1 >= 3, source V .* Field_n)
+//   kEarly:  jj = 2, 3 (first updates, incident-field source for jj = 2)
+//   kFinal:  the final pass (update of the last iteration, Field(ROI) +
+//            incident field into Fout, :646-647; no source, no forward FFT)
+enum PipeKind { kSteady = 0, kEarly = 1, kFinal = 2 };
+
+template <int R2, int W, int KIND>
 __global__ void __launch_bounds__(W * 8, W == 16 ? 2 : 3)
     born_x_pipe_kernel(const BornArgs a, const int jj, const float2* __restrict__ twg, const int ntiles,
                        int* __restrict__ fault) {
@@ -138,7 +149,8 @@ __global__ void __launch_bounds__(W * 8, W == 16 ? 2 : 3)
     issue_F(tile);
   }
   uint32_t phT0 = 0, phT1 = 0, phF = 0;
-  const int e = jj - 1;  // iteration whose update completes here (>= 3)
+  const int e = jj - 1;  // iteration whose update completes here (>= 1)
+  const long long est = (long long)a.rx * a.ry * a.rz;
   const float2 cc = make_float2(0.f, a.c_im);
   const float2 z2 = make_float2(0.f, 0.f);
 
@@ -165,12 +177,35 @@ __global__ void __launch_bounds__(W * 8, W == 16 ? 2 : 3)
 #pragma unroll
       for (int r = 0; r < kR1; ++r) Vn[r] = a.V[vb + R2 * r];
     }
+    // the incident field (iteration 2's source, the final pass's Fout) is
+    // prefetched the same way; zero outside the ROI
+    constexpr bool kHasE = KIND != kSteady;
+    const bool need_e = KIND == kFinal || (KIND == kEarly && jj <= 2);
+    auto e_load = [&](int idx, float2* En) {
+      const int c = idx / R2, j = idx - c * R2;
+      const int yy = c < nl ? y0 + c : y0;
+      const bool roi = need_e && (unsigned)(yy - a.ry0) < (unsigned)a.ry && (unsigned)(z - a.rz0) < (unsigned)a.rz;
+      const long long base = (long long)b * est + (long long)(yy - a.ry0) * a.rx +
+                             (long long)(z - a.rz0) * a.rx * a.ry - a.rx0;
+#pragma unroll
+      for (int r = 0; r < kR1; ++r) {
+        const int x = j + R2 * r;
+        En[r] = roi && (unsigned)(x - a.rx0) < (unsigned)a.rx ? a.Einc[base + x] : z2;
+      }
+    };
+    float2 En[kHasE ? kR1 : 1];
+    if constexpr (kHasE) {
+      if (tid < kW * R2) e_load(tid, En);
+    }
     if (tid < kW) {
       PipeLine P;
       P.valid = tid < nl;
       const int yy = P.valid ? y0 + tid : y0;
       P.g = tile_off(b, yy, z);
       P.v = (yy + a.py * z) * N;
+      P.roi = (unsigned)(yy - a.ry0) < (unsigned)a.ry && (unsigned)(z - a.rz0) < (unsigned)a.rz;
+      P.einc = (long long)b * est + (long long)(yy - a.ry0) * a.rx +
+               (long long)(z - a.rz0) * a.rx * a.ry - a.rx0;
       P.my = a.mask[1][yy];
       P.mz = a.mask[2][z];
       P.ry = a.ramp[1][yy];
@@ -215,10 +250,16 @@ __global__ void __launch_bounds__(W * 8, W == 16 ? 2 : 3)
       float2 Vv[kR1];
 #pragma unroll
       for (int r = 0; r < kR1; ++r) Vv[r] = Vn[r];
+      float2 Ev[kHasE ? kR1 : 1];
+      if constexpr (kHasE) {
+#pragma unroll
+        for (int r = 0; r < kR1; ++r) Ev[r] = En[r];
+      }
       if (idx + kThreads < kW * R2) {
         const int vb = v_base(idx + kThreads);
 #pragma unroll
         for (int r = 0; r < kR1; ++r) Vn[r] = a.V[vb + R2 * r];
+        if constexpr (kHasE) e_load(idx + kThreads, En);
       }
       float2 v[kR1];
 #pragma unroll
@@ -235,30 +276,54 @@ __global__ void __launch_bounds__(W * 8, W == 16 ? 2 : 3)
         const int x = j + R2 * r;
         const float2 V = Vv[r];
         const float2 r0 = a.acyclic ? cmul(cmul(r0t[x], Ln.ry), Ln.rz) : make_float2(1.f, 0.f);
+        const bool in_roi = KIND != kSteady && Ln.roi && (unsigned)(x - a.rx0) < (unsigned)a.rx;
+        float2 Ei = z2;
+        if constexpr (kHasE) Ei = Ev[r];
         float2 P = v[r];
         if (a.acyclic) P = cmul(P, (e & 1) ? r0 : cconj(r0));
         const float m = (m0t[x] * Ln.my) * Ln.mz;
         const float2 vP = cmul(V, P);
-        const float2 fo = sFn[c * N + x];
-        const float2 fp = sF[c * N + x];
-        const float2 psi = cmul(cmul(cc, fo), V);
-        const float2 fn = cscale(cadd(csub(fo, psi), vP), m);
         float2 ftot, fn_new;
-        if (e == 3) {  // Field = (Field_n1 + Field_n2) + Field_n3; Field_n = Field_n3 + Field_n1
-          ftot = cadd(cadd(fp, fo), fn);
-          fn_new = cadd(fn, fp);
+        if (KIND != kSteady && e <= 2) {   // Field_n = (0 + V.*PSI) .* mask
+          fn_new = cscale(vP, m);
+          // Field = 0 + Field_n after iteration 1; after iteration 2 Field
+          // keeps Field_n(1) until the e == 3 update
+          ftot = e == 1 ? fn_new : cadd(sF[c * N + x], fn_new);
+          if (KIND != kFinal && Ln.valid) {
+            a.Fn[Ln.g + x] = fn_new;
+            if (e == 1) a.F[Ln.g + x] = fn_new;
+          }
         } else {
-          ftot = cadd(fp, fn);
-          fn_new = fn;
+          const float2 fo = sFn[c * N + x];
+          const float2 fp = sF[c * N + x];
+          const float2 psi = cmul(cmul(cc, fo), V);
+          const float2 fn = cscale(cadd(csub(fo, psi), vP), m);
+          if (e == 3) {  // Field = (Field_n1 + Field_n2) + Field_n3; Field_n = Field_n3 + Field_n1
+            ftot = cadd(cadd(fp, fo), fn);
+            fn_new = cadd(fn, fp);
+          } else {
+            ftot = cadd(fp, fn);
+            fn_new = fn;
+          }
+          if (KIND != kFinal && Ln.valid) {
+            a.F[Ln.g + x] = ftot;
+            a.Fn[Ln.g + x] = fn_new;
+          }
         }
-        if (Ln.valid) {
-          a.F[Ln.g + x] = ftot;
-          a.Fn[Ln.g + x] = fn_new;
+        if (KIND == kFinal) {
+          if (Ln.valid && in_roi) a.Fout[Ln.einc + x] = cadd(ftot, Ei);
+          continue;
         }
-        float2 src = cmul(cmul(cc, fn_new), V);
+        float2 src;
+        if (KIND == kEarly && jj <= 2) {  // (1i/eps) .* ((V(ROI) + 1i*eps) .* E_inc) / 2 inside the ROI
+          src = in_roi ? cscale(cmul(cc, cmul(make_float2(V.x, V.y + a.eps), Ei)), 0.5f) : z2;
+        } else {        // (1i/eps) .* Field_n .* V
+          src = cmul(cmul(cc, fn_new), V);
+        }
         if (a.acyclic) src = cmul(src, (jj & 1) ? cconj(r0) : r0);
         v[r] = Ln.valid ? src : z2;
       }
+      if (KIND == kFinal) continue;
       Butterfly<kR1, false>::run(v, tw, N);
 #pragma unroll
       for (int r = 0; r < kR1; ++r) {
@@ -271,6 +336,7 @@ __global__ void __launch_bounds__(W * 8, W == 16 ? 2 : 3)
       fence_proxy_async();
       issue_F(next);
     }
+    if (KIND == kFinal) continue;   // nothing to transform back: Fout is written
     // ---- forward radix-R2 pass (ns = 8) -> T
     {
       const int c = tid >> 3, j = tid & 7;
@@ -305,7 +371,7 @@ constexpr int tile_lines() {
 #endif
 }
 
-template <int R2>
+template <int R2, int KIND>
 cudaError_t launch_r2(const BornArgs& a, int jj, const DevFft& fx, int* fault, cudaStream_t s) {
   constexpr int W = tile_lines<R2>();
   using L = PipeSmem<kR1 * R2, W>;
@@ -314,7 +380,7 @@ cudaError_t launch_r2(const BornArgs& a, int jj, const DevFft& fx, int* fault, c
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (!configured.test(dev)) {
-    e = cudaFuncSetAttribute(born_x_pipe_kernel<R2, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(born_x_pipe_kernel<R2, W, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)L::kTotal);
     if (e != cudaSuccess) return e;
     configured.set(dev);
@@ -326,7 +392,7 @@ cudaError_t launch_r2(const BornArgs& a, int jj, const DevFft& fx, int* fault, c
   const int nty = (a.py + W - 1) / W;
   const long long ntiles = (long long)nty * a.pz * a.nbatch;
   const int grid = (int)(ntiles < (long long)per_sm * nsm ? ntiles : (long long)per_sm * nsm);
-  born_x_pipe_kernel<R2, W><<<grid, W * kR1, L::kTotal, s>>>(a, jj, fx.tw, (int)ntiles, fault);
+  born_x_pipe_kernel<R2, W, KIND><<<grid, W * kR1, L::kTotal, s>>>(a, jj, fx.tw, (int)ntiles, fault);
   return cudaGetLastError();
 }
 
@@ -352,13 +418,22 @@ bool born_x_pipe_supported(const BornArgs& a, const DevFft& fx) {
   return ntiles < (1LL << 31);
 }
 
-cudaError_t launch_born_x_pipe(const BornArgs& a, int jj, const DevFft& fx, int* fault, cudaStream_t s) {
+cudaError_t launch_born_x_pipe(const BornArgs& a, int mode, int jj, const DevFft& fx, int* fault,
+                               cudaStream_t s) {
+  if (jj < 2 || (mode != kBornMid && mode != kBornLast)) return cudaErrorInvalidValue;
+  const int kind = mode == kBornLast ? kFinal : (jj <= 3 ? kEarly : kSteady);
   switch (a.px / kR1) {
-    case 11: return launch_r2<11>(a, jj, fx, fault, s);
-    case 15: return launch_r2<15>(a, jj, fx, fault, s);
-    case 19: return launch_r2<19>(a, jj, fx, fault, s);
-    case 25: return launch_r2<25>(a, jj, fx, fault, s);
-    case 27: return launch_r2<27>(a, jj, fx, fault, s);
+#define ODT_PIPE_CASE(R)                                                     \
+  case R:                                                                    \
+    return kind == kFinal   ? launch_r2<R, kFinal>(a, jj, fx, fault, s)      \
+           : kind == kEarly ? launch_r2<R, kEarly>(a, jj, fx, fault, s)      \
+                            : launch_r2<R, kSteady>(a, jj, fx, fault, s);
+    ODT_PIPE_CASE(11)
+    ODT_PIPE_CASE(15)
+    ODT_PIPE_CASE(19)
+    ODT_PIPE_CASE(25)
+    ODT_PIPE_CASE(27)
+#undef ODT_PIPE_CASE
     default: return cudaErrorNotSupported;
   }
 }

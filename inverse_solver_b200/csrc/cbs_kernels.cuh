@@ -68,11 +68,12 @@ cudaError_t launch_born_z_dyadic(const BornArgs& a, const DyadArgs& d, int jj, c
 // x-pass of iteration jj: inverse x-FFT + update of iteration jj-1 (Mid/Last)
 // and source term + forward x-FFT of iteration jj (First/Mid).
 cudaError_t launch_born_x(const BornArgs& a, int mode, int jj, const DevFft& fx, cudaStream_t s);
-// Pipelined x-pass (persistent CTAs, bulk asynchronous copies) for mode Mid
-// with jj >= 4 and x-lengths 8 * {11, 15, 19, 25, 27}; same results as launch_born_x.
-// A wait that times out sets *fault (device int) and ends the kernel.
+// Pipelined x-pass (persistent CTAs, bulk asynchronous copies) for modes Mid
+// (jj >= 2) and Last and x-lengths 8 * {11, 15, 19, 25, 27}; same results as
+// launch_born_x.  A wait that times out sets *fault (device int) and ends
+// the kernel.
 bool born_x_pipe_supported(const BornArgs& a, const DevFft& fx);
-cudaError_t launch_born_x_pipe(const BornArgs& a, int jj, const DevFft& fx, int* fault,
+cudaError_t launch_born_x_pipe(const BornArgs& a, int mode, int jj, const DevFft& fx, int* fault,
                                cudaStream_t s);
 // Pipelined column passes (persistent CTAs, tiled TMA copies) for lengths
 // 8 * {11, 15, 19, 25, 27} along y / z: the y-FFT of the Born loop in place on a.T,

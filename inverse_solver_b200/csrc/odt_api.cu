@@ -81,9 +81,11 @@ struct DeviceGuard {
 };
 
 const char* const kKindNames[] = {"born_x", "born_y", "born_z", "io_fft", "io_elementwise",
-                                  "born_x_pipe", "born_y_pipe", "born_z_pipe"};
+                                  "born_x_pipe", "born_y_pipe", "born_z_pipe", "born_x_pipe_edge"};
+// born_x_pipe_edge: the pipelined x-pass of iterations 2, 3 and of the final
+// pass (incident-field source / output), timed apart from the steady state
 enum Kind { kKBornX = 0, kKBornY, kKBornZ, kKIoFft, kKIoElem, kKBornXPipe, kKBornYPipe, kKBornZPipe,
-            kNumKinds };
+            kKBornXPipeEdge, kNumKinds };
 
 struct Handle {
   odt_geometry g{};
@@ -459,9 +461,9 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
     dy.absorb = make_float2(P.pp.absorb.re, P.pp.absorb.im);
   }
   for (int jj = 1; jj <= B; ++jj) {
-    if (pipe_x && jj >= 4) {
-      H.mark_begin(kKBornXPipe, s);
-      ODT_CUDA(launch_born_x_pipe(a, jj, H.fx, H.d_fault, s));
+    if (pipe_x && jj >= 2) {
+      H.mark_begin(jj <= 3 ? kKBornXPipeEdge : kKBornXPipe, s);
+      ODT_CUDA(launch_born_x_pipe(a, kBornMid, jj, H.fx, H.d_fault, s));
     } else {
       H.mark_begin(kKBornX, s);
       ODT_CUDA(launch_born_x(a, jj == 1 ? kBornFirst : kBornMid, jj, H.fx, s));
@@ -488,8 +490,13 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
       ODT_CUDA(launch_fft_cols(a.T, a.T, a.px, (long long)a.pz * nbp, 0, 0, 1.0f, true, H.fy, s));
     H.mark_end(s);
   }
-  H.mark_begin(kKBornX, s);
-  ODT_CUDA(launch_born_x(a, kBornLast, B + 1, H.fx, s));
+  if (pipe_x && B + 1 >= 2) {
+    H.mark_begin(kKBornXPipeEdge, s);
+    ODT_CUDA(launch_born_x_pipe(a, kBornLast, B + 1, H.fx, H.d_fault, s));
+  } else {
+    H.mark_begin(kKBornX, s);
+    ODT_CUDA(launch_born_x(a, kBornLast, B + 1, H.fx, s));
+  }
   H.mark_end(s);
 
   // ---- output projection (:445-511)

@@ -1,7 +1,8 @@
-"""GPU parity of the pipelined Born passes (csrc/born_pipe.cu, the x-pass;
+"""GPU parity of the pipelined Born passes (csrc/born_pipe.cu, the x-pass of
+iterations 2 onward and the final pass;
 csrc/cols_pipe.cu, the y-FFTs and the z-pass: persistent CTAs, bulk / tiled
 asynchronous copies, compile-time 8 x R2 plans), which the library selects
-for grid lengths 88, 120 and 152.
+for grid lengths 88, 120, 152, 200 and 216.
 
   * against the single-precision oracle on grids that put each of 88, 120
     and 152 on each axis (relative L2 per illumination 1e-5 for the
@@ -105,3 +106,20 @@ def test_pipe_radix_25_27_match_oracle(size):
     o.set_RI(RI)
     ot, _, of = o.solve(fields)
     assert worst(f, of) < 1e-5 and worst(t, ot) < 1e-5
+
+
+@pytest.mark.parametrize("iters", [1, 2, 3, 5])
+def test_pipe_short_series_match_oracle(iters):
+    """The pipelined x-pass in iterations 2 and 3 (incident-field source,
+    the half-series bookkeeping) and in the final pass (Field(ROI) +
+    incident field), for short series on a padded (88, 48, 40) grid."""
+    size = [64, 24, 16]
+    p = cases.params(size, [6, 6, 6], return_reflection=True, return_3D=True, iterations_number=iters)
+    RI = cases.sphere_phantom(size, [0.1] * 3, cases.NM, seed=77, n_spheres=2, radius_um=(0.3, 0.8))
+    fields = cases.circle_fields(p, 2)
+    (t, r, f), (sim, bm) = _solve(p, RI, fields)
+    assert bm == iters
+    o = cbs.ForwardSolverCBS(p, single=True)
+    o.set_RI(RI)
+    ot, orr, of = o.solve(fields)
+    assert worst(f, of) < 1e-5 and worst(t, ot) < 1e-5 and worst(r, orr) < 3e-5
