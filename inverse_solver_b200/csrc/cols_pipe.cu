@@ -72,6 +72,14 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, i
       "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_addr(bar))
       : "memory");
 }
+// Reciprocal to within the hardware approximation (PTX rcp.approx.ftz.f32,
+// at most 1 ulp from the rounded quotient); its argument here is
+// q^2 + eps^2 >= eps^2, far from zero, subnormals and infinity.
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 #endif
 
 // KIND 0: forward y-FFT, 1: inverse y-FFT, 2: z-pass with Green's multiply.
@@ -200,9 +208,9 @@ __global__ void __launch_bounds__(kThreads, 3)
         for (int r = 0; r < kR1; ++r) {
           float q = qxy + kz[j + R2 * r];
           q = a.g_scale * q - a.g_off;
-          const float rden = __frcp_rn(q * q + a.eps * a.eps);
-          const float2 G = make_float2(q * rden, a.eps * rden);  // 1 / (q - i eps)
-          v[r] = cscale(cmul(G, v[r]), a.inv_n);
+          const float rden = rcp_approx(q * q + a.eps * a.eps) * a.inv_n;
+          const float2 G = make_float2(q * rden, a.eps * rden);  // (1 / (q - i eps)) / N
+          v[r] = cmul(G, v[r]);
         }
         Butterfly<kR1, true>::run(v, tw, N);
 #pragma unroll
@@ -227,8 +235,12 @@ __global__ void __launch_bounds__(kThreads, 3)
 #pragma unroll
         for (int r = 0; r < R2; ++r) out[(jr + kR1 * r) * rstride] = v[r];
       }
+    } else {
+      // the next iteration's copy refills the stage just read; the z-pass
+      // reads its stage only before the barrier above, and its next writes
+      // to sB follow the barriers of the next radix-R2 pass
+      __syncthreads();
     }
-    __syncthreads();
   }
 #endif
 }
