@@ -122,6 +122,37 @@ cudaError_t launch_emitter(const BornArgs& a, float2* conv, int c0, int c1, int 
 // tk[X, Y, b] = sum_z conv * Kt ; rk likewise with Kr (either output may be null)
 cudaError_t launch_zreduce(const float2* conv, const float2* Kt, const float2* Kr, float2* tk,
                            float2* rk, int c0, int c1, int rz, long long nb, cudaStream_t s);
+// Fused input / output stages (io_fused.cu): conv plane cx x cy, RI grid
+// rx x ry x rz, window offset (ox, oy) of the RI / field grid in the conv
+// plane, nbp planes per z.
+struct IoGeom {
+  int cx, cy;
+  int rx, ry, rz;
+  int ox, oy;
+  long long nbp;
+};
+// Einc[x, y, z, b] = ifft2c(sk[., ., b] .* refocus[., ., z])[x + ox, y + oy]
+// (the expand -> centred inverse 2D FFT -> crop chain); mid holds
+// rx * cy * rz * nbp elements
+cudaError_t launch_refocus_in(const float2* sk, const float2* refocus, float2* mid, float2* einc,
+                              const IoGeom& g, const DevFft& fx, const DevFft& fy, cudaStream_t s);
+// tk / rk = the emitter -> centred forward 2D FFT -> z-reduce chain (either
+// output may be null); mid (cap elements) holds cx * ry * rz * nbp elements
+// and, where it has room, the per-chunk partial sums of the z-reduction
+cudaError_t launch_project_out(const BornArgs& a, float2* mid, long long cap, const float2* Kt, const float2* Kr,
+                               float2* tk, float2* rk, const IoGeom& g, float dV, const DevFft& fx,
+                               const DevFft& fy, cudaStream_t s);
+// whether the fused kernels' tiles fit the device (shared memory, prefetch)
+bool io_fused_fits(const IoGeom& g, const DevFft& fx, const DevFft& fy, int nacc, int max_smem);
+template <int C>
+cudaError_t io_in_launch(const float2* sk, const float2* refocus, float2* mid, float2* einc, const IoGeom& g,
+                         const DevFft& fx, const DevFft& fy, cudaStream_t s);
+template <int C>
+cudaError_t io_out_lines_launch(const BornArgs& a, float2* mid, const IoGeom& g, float dV, const DevFft& fx,
+                                cudaStream_t s);
+template <int C>
+cudaError_t io_out_cols_launch(const float2* mid, const float2* Kt, const float2* Kr, float2* tk, float2* rk,
+                               float2* part, int zs, const IoGeom& g, const DevFft& fy, cudaStream_t s);
 // out[i] = (x[i] + add[i]) * filt[i % plane]   (add may be null)
 cudaError_t launch_combine(const float2* x, const float2* add, const float* filt, float2* out,
                            long long plane, long long total, cudaStream_t s);

@@ -413,13 +413,25 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
   ODT_CUDA(launch_pad2d(src2, H.c2a, Fx, Fy, Cx, Cy, ocx, ocy, nbp, s));
   H.mark_end(s);
   fftc2(H, H.c2a, H.fcx, H.fcy, nbp, false, s);
-  H.mark_begin(kKIoElem, s);
-  ODT_CUDA(launch_refocus_expand(H.c2a, H.refocus, conv, Cx, Cy, Rz, nbp, s));
-  H.mark_end(s);
-  fftc2(H, conv, H.fcx, H.fcy, (long long)Rz * nbp, true, s);
-  H.mark_begin(kKIoElem, s);
-  ODT_CUDA(launch_crop_volume(conv, H.einc, Cx, Cy, Rx, Ry, Rz, ocx, ocy, nbp, s));
-  H.mark_end(s);
+  // fused refocus / inverse 2D FFT / crop (io_fused.cu) where its tiles fit;
+  // the unfused chain is kept for ODT_KERNELS=generic
+  const int nacc = (want_t ? 1 : 0) + (want_r ? 1 : 0);
+  const IoGeom gin{Cx, Cy, Rx, Ry, Rz, ocx, ocy, nbp}, gout{Cx, Cy, Rx, Ry, Rz, orx, ory, nbp};
+  const bool io_fused = H.use_pipe && io_fused_fits(gin, H.fcx, H.fcy, nacc, H.max_smem) &&
+                        io_fused_fits(gout, H.fcx, H.fcy, nacc, H.max_smem);
+  if (io_fused) {
+    H.mark_begin(kKIoFft, s);
+    ODT_CUDA(launch_refocus_in(H.c2a, H.refocus, conv, H.einc, gin, H.fcx, H.fcy, s));
+    H.mark_end(s);
+  } else {
+    H.mark_begin(kKIoElem, s);
+    ODT_CUDA(launch_refocus_expand(H.c2a, H.refocus, conv, Cx, Cy, Rz, nbp, s));
+    H.mark_end(s);
+    fftc2(H, conv, H.fcx, H.fcy, (long long)Rz * nbp, true, s);
+    H.mark_begin(kKIoElem, s);
+    ODT_CUDA(launch_crop_volume(conv, H.einc, Cx, Cy, Rx, Ry, Rz, ocx, ocy, nbp, s));
+    H.mark_end(s);
+  }
 
   // ---- Born series (:577-647)
   BornArgs a{};
@@ -501,14 +513,22 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
 
   // ---- output projection (:445-511)
   if (want_t || want_r) {
-    H.mark_begin(kKIoElem, s);
-    ODT_CUDA(launch_emitter(a, conv, Cx, Cy, orx, ory, P.pp.dV, s));
-    H.mark_end(s);
-    fftc2(H, conv, H.fcx, H.fcy, (long long)Rz * nbp, false, s);
-    H.mark_begin(kKIoElem, s);
-    ODT_CUDA(launch_zreduce(conv, want_t ? H.ktrans : nullptr, want_r ? H.kref : nullptr,
-                            want_t ? H.c2a : nullptr, want_r ? H.c2b : nullptr, Cx, Cy, Rz, nbp, s));
-    H.mark_end(s);
+    if (io_fused) {
+      H.mark_begin(kKIoFft, s);
+      ODT_CUDA(launch_project_out(a, conv, H.work_elems() * nbp, want_t ? H.ktrans : nullptr,
+                                  want_r ? H.kref : nullptr, want_t ? H.c2a : nullptr, want_r ? H.c2b : nullptr,
+                                  gout, P.pp.dV, H.fcx, H.fcy, s));
+      H.mark_end(s);
+    } else {
+      H.mark_begin(kKIoElem, s);
+      ODT_CUDA(launch_emitter(a, conv, Cx, Cy, orx, ory, P.pp.dV, s));
+      H.mark_end(s);
+      fftc2(H, conv, H.fcx, H.fcy, (long long)Rz * nbp, false, s);
+      H.mark_begin(kKIoElem, s);
+      ODT_CUDA(launch_zreduce(conv, want_t ? H.ktrans : nullptr, want_r ? H.kref : nullptr,
+                              want_t ? H.c2a : nullptr, want_r ? H.c2b : nullptr, Cx, Cy, Rz, nbp, s));
+      H.mark_end(s);
+    }
     for (int w = 0; w < 2; ++w) {
       if ((w == 0 && !want_t) || (w == 1 && !want_r)) continue;
       float2* c2 = w == 0 ? H.c2a : H.c2b;
