@@ -65,6 +65,37 @@ ODT_HD int unrot_n(int X, int shift, int n) {  // the row r with rot_n(r, shift,
   return r < 0 ? r + n : r;
 }
 
+// Transforms of the power-of-two lengths 128, 256 and 512 run with the plan
+// fixed at compile time (radices 8, 8, 2 / 8, 8, 4 / 8, 8, 8: the run-time
+// planner's order for these lengths), so the pass loop's strides, radix
+// switch and index arithmetic fold to constants; NF = 0 keeps the run-time
+// plan for every other length.
+template <int N>
+struct Pow2Plan {
+  static constexpr int P = 3;
+  __host__ __device__ static constexpr int rad(int i) { return i < 2 ? 8 : (N == 128 ? 2 : (N == 256 ? 4 : 8)); }
+};
+
+template <int N, bool INV, int I, int NS, class Map, class G1, class G2, class S>
+__device__ __forceinline__ void pow2_passes(const Thr& th, const Map& m, const float2* tw, const G1& src,
+                                            const G2& dst, S cur, S oth) {
+  constexpr int P = Pow2Plan<N>::P;
+  constexpr int R = INV ? Pow2Plan<N>::rad(P - 1 - I) : Pow2Plan<N>::rad(I);
+  if constexpr (I == 0) tile_pass<R, INV>(th, m, N, NS, tw, src, cur);
+  else if constexpr (I == P - 1) tile_pass<R, INV>(th, m, N, NS, tw, oth, dst);
+  else tile_pass<R, INV>(th, m, N, NS, tw, oth, cur);
+  __syncthreads();
+  if constexpr (I + 1 < P) pow2_passes<N, INV, I + 1, NS * R>(th, m, tw, src, dst, oth, cur);
+}
+
+// the tile FFT of the fused kernels: fixed plan for NF != 0, else run-time plan
+template <int CLS, int NF, bool INV, class Map, class S, class G1, class G2>
+__device__ __forceinline__ void io_fft(const Thr& th, const FftPlan& plan, const Map& m, const float2* tw,
+                                       const G1& src, const G2& dst, S cur, S oth) {
+  if constexpr (NF != 0) pow2_passes<NF, INV, 0, 1>(th, m, tw, src, dst, cur, oth);
+  else tile_fft_io<CLS, INV>(th, plan, m, tw, src, dst, cur, oth);
+}
+
 // stores x = X - lo in [0, len) of line c at out[c * len + x]; X = (row + n/2) % n
 struct CropLineDst {
   float2* out;
@@ -115,13 +146,13 @@ size_t cols_smem(int n, int nacc) {
          (size_t)nacc * sizeof(float2) * n * kIoW;
 }
 
-template <int CLS>
+template <int CLS, int NF>
 __global__ void __launch_bounds__(kIoThreads)
 refocus_lines_kernel(const float2* __restrict__ sk, const float2* __restrict__ ref, float2* __restrict__ mid,
                      IoGeom g, FftPlan plan, const float2* __restrict__ twg) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const Thr th = thr();
-  const int n = plan.n;  // == cx
+  const int n = NF ? NF : plan.n;  // == cx
   const int ld = smem_line_ld(n);
   float2* tw = reinterpret_cast<float2*>(smraw);
   float2* bufA = reinterpret_cast<float2*>(smraw + align16(sizeof(float2) * n));
@@ -159,16 +190,16 @@ refocus_lines_kernel(const float2* __restrict__ sk, const float2* __restrict__ r
   }
   __syncthreads();
   const CropLineDst dst{mid + L0 * g.rx, nl, n, n / 2, g.ox, g.rx};
-  tile_fft_io<CLS, true>(th, plan, LineMap{kIoW}, tw, S, dst, SmemLine{bufB, ld}, S);
+  io_fft<CLS, NF, true>(th, plan, LineMap{kIoW}, tw, S, dst, SmemLine{bufB, ld}, S);
 }
 
-template <int CLS>
+template <int CLS, int NF>
 __global__ void __launch_bounds__(kIoThreads)
 refocus_cols_kernel(const float2* __restrict__ mid, float2* __restrict__ einc, IoGeom g, float scale,
                     FftPlan plan, const float2* __restrict__ twg) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const Thr th = thr();
-  const int n = plan.n;  // == cy
+  const int n = NF ? NF : plan.n;  // == cy
   float2* tw = reinterpret_cast<float2*>(smraw);
   float2* bufA = reinterpret_cast<float2*>(smraw + align16(sizeof(float2) * n));
   float2* bufB = bufA + (size_t)n * (kIoW + 1);
@@ -200,16 +231,16 @@ refocus_cols_kernel(const float2* __restrict__ mid, float2* __restrict__ einc, I
   __syncthreads();
   const CropColDst dst{einc + x0 + (long long)g.rx * g.ry * (z + g.rz * b), ncol, n, n / 2, g.oy, g.ry, g.rx,
                        scale};
-  tile_fft_io<CLS, true>(th, plan, ColMap{kIoLgW}, tw, S, dst, SmemCol{bufB, kIoW + 1}, S);
+  io_fft<CLS, NF, true>(th, plan, ColMap{kIoLgW}, tw, S, dst, SmemCol{bufB, kIoW + 1}, S);
 }
 
-template <int CLS>
+template <int CLS, int NF>
 __global__ void __launch_bounds__(kIoThreads)
 emit_lines_kernel(const BornArgs a, float2* __restrict__ mid, IoGeom g, float dV, FftPlan plan,
                   const float2* __restrict__ twg) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const Thr th = thr();
-  const int n = plan.n;  // == cx
+  const int n = NF ? NF : plan.n;  // == cx
   const int ld = smem_line_ld(n);
   float2* tw = reinterpret_cast<float2*>(smraw);
   float2* bufA = reinterpret_cast<float2*>(smraw + align16(sizeof(float2) * n));
@@ -251,7 +282,7 @@ emit_lines_kernel(const BornArgs a, float2* __restrict__ mid, IoGeom g, float dV
   }
   __syncthreads();
   const GlobalShift dst{nullptr, mid + L0 * n, 1, n, nl, n, n / 2, 1.f};
-  tile_fft_io<CLS, false>(th, plan, LineMap{kIoW}, tw, S, dst, SmemLine{bufB, ld}, S);
+  io_fft<CLS, NF, false>(th, plan, LineMap{kIoW}, tw, S, dst, SmemLine{bufB, ld}, S);
 }
 
 // CTA -> (b fastest, then 8 kx columns, then a chunk of zs z-planes): the CTAs
@@ -259,7 +290,7 @@ emit_lines_kernel(const BornArgs a, float2* __restrict__ mid, IoGeom g, float dV
 // one chunk the sums go straight to tk / rk, else to part[chunk][t|r][...].
 // The window's rows of the next plane are loaded into registers while the
 // current plane is transformed (ry * 8 <= kPf * threads).
-template <int CLS>
+template <int CLS, int NF>
 __global__ void __launch_bounds__(kIoThreads)
 emit_cols_reduce_kernel(const float2* __restrict__ mid, const float2* __restrict__ Kt,
                         const float2* __restrict__ Kr, float2* __restrict__ tk, float2* __restrict__ rk,
@@ -267,7 +298,7 @@ emit_cols_reduce_kernel(const float2* __restrict__ mid, const float2* __restrict
                         const float2* __restrict__ twg) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const Thr th = thr();
-  const int n = plan.n;  // == cy
+  const int n = NF ? NF : plan.n;  // == cy
   float2* tw = reinterpret_cast<float2*>(smraw);
   float2* bufA = reinterpret_cast<float2*>(smraw + align16(sizeof(float2) * n));
   float2* bufB = bufA + (size_t)n * (kIoW + 1);
@@ -325,7 +356,7 @@ emit_cols_reduce_kernel(const float2* __restrict__ mid, const float2* __restrict
     }
     const ReduceDst dst{accT, accR, Kt ? Kt + plane * z + x0 : nullptr, Kr ? Kr + plane * z + x0 : nullptr, ncol,
                         n, n / 2, g.cx};
-    tile_fft_io<CLS, false>(th, plan, ColMap{kIoLgW}, tw, S, dst, SmemCol{bufB, kIoW + 1}, S);
+    io_fft<CLS, NF, false>(th, plan, ColMap{kIoLgW}, tw, S, dst, SmemCol{bufB, kIoW + 1}, S);
   }
   __syncthreads();
   const long long tot = plane * g.nbp;
@@ -339,6 +370,22 @@ emit_cols_reduce_kernel(const float2* __restrict__ mid, const float2* __restrict
     if (Kr) outR[p] = accR[i];
   }
 }
+
+// NF for a transform length: the fixed-plan lengths (class-0 units only), else 0
+#define ODT_NF_DISPATCH(n, ...)                                          \
+  if (ODT_CLS == 0 && (n) == 256) {                                      \
+    constexpr int NF = ODT_CLS == 0 ? 256 : 0;                           \
+    __VA_ARGS__;                                                         \
+  } else if (ODT_CLS == 0 && (n) == 128) {                               \
+    constexpr int NF = ODT_CLS == 0 ? 128 : 0;                           \
+    __VA_ARGS__;                                                         \
+  } else if (ODT_CLS == 0 && (n) == 512) {                               \
+    constexpr int NF = ODT_CLS == 0 ? 512 : 0;                           \
+    __VA_ARGS__;                                                         \
+  } else {                                                               \
+    constexpr int NF = 0;                                                \
+    __VA_ARGS__;                                                         \
+  }
 
 template <typename K>
 cudaError_t raise_smem(K kernel, size_t bytes) {
@@ -354,19 +401,23 @@ cudaError_t io_in_launch<ODT_CLS>(const float2* sk, const float2* refocus, float
   cudaError_t e;
   {
     const size_t sm = lines_smem(fx.plan.n);
-    if ((e = raise_smem(refocus_lines_kernel<ODT_CLS>, sm)) != cudaSuccess) return e;
     const long long nlines = g.nbp * g.cy * g.rz;
     const unsigned blocks = (unsigned)((nlines + kIoW - 1) / kIoW);
-    refocus_lines_kernel<ODT_CLS><<<blocks, kIoThreads, sm, s>>>(sk, refocus, mid, g, fx.plan, fx.tw);
+    ODT_NF_DISPATCH(fx.plan.n, {
+      if ((e = raise_smem(refocus_lines_kernel<ODT_CLS, NF>, sm)) != cudaSuccess) return e;
+      refocus_lines_kernel<ODT_CLS, NF><<<blocks, kIoThreads, sm, s>>>(sk, refocus, mid, g, fx.plan, fx.tw);
+    })
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   {
     const size_t sm = cols_smem(fy.plan.n, 0);
-    if ((e = raise_smem(refocus_cols_kernel<ODT_CLS>, sm)) != cudaSuccess) return e;
     const long long ntx = (g.rx + kIoW - 1) / kIoW;
     const unsigned blocks = (unsigned)(ntx * g.nbp * g.rz);
     const float scale = 1.0f / ((float)g.cx * (float)g.cy);
-    refocus_cols_kernel<ODT_CLS><<<blocks, kIoThreads, sm, s>>>(mid, einc, g, scale, fy.plan, fy.tw);
+    ODT_NF_DISPATCH(fy.plan.n, {
+      if ((e = raise_smem(refocus_cols_kernel<ODT_CLS, NF>, sm)) != cudaSuccess) return e;
+      refocus_cols_kernel<ODT_CLS, NF><<<blocks, kIoThreads, sm, s>>>(mid, einc, g, scale, fy.plan, fy.tw);
+    })
   }
   return cudaGetLastError();
 }
@@ -375,11 +426,13 @@ template <>
 cudaError_t io_out_lines_launch<ODT_CLS>(const BornArgs& a, float2* mid, const IoGeom& g, float dV,
                                          const DevFft& fx, cudaStream_t s) {
   const size_t sm = lines_smem(fx.plan.n);
-  cudaError_t e = raise_smem(emit_lines_kernel<ODT_CLS>, sm);
-  if (e != cudaSuccess) return e;
   const long long nlines = g.nbp * g.ry * g.rz;
   const unsigned blocks = (unsigned)((nlines + kIoW - 1) / kIoW);
-  emit_lines_kernel<ODT_CLS><<<blocks, kIoThreads, sm, s>>>(a, mid, g, dV, fx.plan, fx.tw);
+  cudaError_t e;
+  ODT_NF_DISPATCH(fx.plan.n, {
+    if ((e = raise_smem(emit_lines_kernel<ODT_CLS, NF>, sm)) != cudaSuccess) return e;
+    emit_lines_kernel<ODT_CLS, NF><<<blocks, kIoThreads, sm, s>>>(a, mid, g, dV, fx.plan, fx.tw);
+  })
   return cudaGetLastError();
 }
 
@@ -389,13 +442,15 @@ cudaError_t io_out_cols_launch<ODT_CLS>(const float2* mid, const float2* Kt, con
                                         cudaStream_t s) {
   const int nacc = (Kt ? 1 : 0) + (Kr ? 1 : 0);
   const size_t sm = cols_smem(fy.plan.n, nacc);
-  cudaError_t e = raise_smem(emit_cols_reduce_kernel<ODT_CLS>, sm);
-  if (e != cudaSuccess) return e;
   const long long ntx = (g.cx + kIoW - 1) / kIoW;
   const long long nchunk = (g.rz + zs - 1) / zs;
   const unsigned blocks = (unsigned)(ntx * g.nbp * nchunk);
-  emit_cols_reduce_kernel<ODT_CLS><<<blocks, kIoThreads, sm, s>>>(mid, Kt, Kr, tk, rk, part, g, zs, fy.plan,
-                                                                  fy.tw);
+  cudaError_t e;
+  ODT_NF_DISPATCH(fy.plan.n, {
+    if ((e = raise_smem(emit_cols_reduce_kernel<ODT_CLS, NF>, sm)) != cudaSuccess) return e;
+    emit_cols_reduce_kernel<ODT_CLS, NF><<<blocks, kIoThreads, sm, s>>>(mid, Kt, Kr, tk, rk, part, g, zs,
+                                                                        fy.plan, fy.tw);
+  })
   return cudaGetLastError();
 }
 
