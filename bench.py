@@ -330,6 +330,66 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(out))
 
 
+def run_fista(args):
+    """Inverse-solver workload (BACKWARD_SOLVER_MULTI, config-3 shape): time
+    per FISTA outer iteration (forward + adjoint CBS solves of every
+    illumination, TV prox with 100 inner iterations, momentum update) with
+    the device-resident loop and with the host-array loop.  RI 192x192x129
+    (odd z, as the reference requires), seeded multi-sphere phantom, 49
+    ring illuminations, measured fields from a forward solve of the phantom,
+    start from the phantom pulled halfway to the background."""
+    import time
+
+    import torch
+
+    from inverse_solver_b200 import FORWARD_SOLVER_CONVERGENT_BORN
+    from inverse_solver_b200.backward import BACKWARD_SOLVER_MULTI
+    from inverse_solver_b200.inputs import ring_illumination, sphere_phantom
+
+    grid = [192, 192, 129]
+    nm = 1.3355
+    fp = FORWARD_SOLVER_CONVERGENT_BORN.get_default_parameters(dict(
+        size=grid, wavelength=0.532, NA=1.2, RI_bg=nm, resolution=[0.1] * 3, vector_simulation=False,
+        return_transmission=True, return_reflection=True, return_3D=True))
+    RI = sphere_phantom(grid, [0.1] * 3, nm, seed=SEED)
+    fields = np.ascontiguousarray(ring_illumination(fp)[:, :, :, :args.n_ill])
+    fw = FORWARD_SOLVER_CONVERGENT_BORN(fp)
+    fw.set_RI(RI)
+    meas, _, _ = fw.solve(fields)
+    fw.delete()
+    start = (RI * 0.5 + nm * 0.5).astype(np.float32)
+
+    class Start:
+        def solve(self, input_field, output_field):
+            return start
+
+    out = {"metric": "FISTA outer iteration time", "unit": "s", "higher_is_better": False,
+           "config": {"workload": "BACKWARD_SOLVER_MULTI: 192x192x129 RI grid, 0.1 um voxels, seeded "
+                                  "multi-sphere phantom, %d ring illuminations, inner_itt 100, "
+                                  "tv_param 7.5e-3" % fields.shape[3], "grid": grid,
+                      "n_ill": int(fields.shape[3])}}
+    for device_loop in (True, False):
+        bp = BACKWARD_SOLVER_MULTI.get_default_parameters(dict(
+            RI_bg=nm, wavelength=0.532, NA=1.2, resolution=[0.1] * 3, size=grid,
+            forward_solver=FORWARD_SOLVER_CONVERGENT_BORN, forward_solver_parameters=fp,
+            init_solver=Start(), step=0.01, tv_param=7.5e-3, inner_itt=100, use_non_negativity=True,
+            nmin=nm, nmax=1.5, device_loop=device_loop))
+        times = []
+        for iters in (1, 1 + args.steps):
+            bp["itter_max"] = iters
+            b = BACKWARD_SOLVER_MULTI(bp)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            b.solve(fields, meas)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+            b.delete()
+        out["device_loop" if device_loop else "host_loop"] = (times[1] - times[0]) / args.steps
+    out["value"] = out["device_loop"]
+    out["steps"] = args.steps
+    print(json.dumps(out), flush=True)
+
+
 def workload_key():
     return "cbs_forward_128cube_49ill"
 
@@ -349,12 +409,17 @@ def main():
                     help="illuminations per step (profiling runs use fewer)")
     ap.add_argument("--profile-run", action="store_true",
                     help="only run --warmup solves (for ncu captures) and exit")
+    ap.add_argument("--fista", action="store_true",
+                    help="time FISTA outer iterations of the inverse solver (device vs host loop)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.fista:
+        run_fista(args)
         return
     if world > 1:
         import datetime

@@ -195,6 +195,65 @@ typedef struct odt_gradient_args {
 odt_status odt_gradient(odt_handle h, const odt_gradient_args* args);
 
 /*
+ * Device-resident outer loop of BACKWARD_SOLVER_MULTI (BACKWARD_SOLVER_MULTI.m
+ * :92-196 with set_RI, FORWARD_SOLVER_CONVERGENT_BORN.m:180-279, run on
+ * gpuArrays as the reference does with use_GPU): the RI stays in device
+ * memory between outer iterations.
+ *
+ * odt_potential_eps_device: eps_imag = single(1.01 * max|RI2potential(RI)|)
+ *   (condition_RI, :199-222) of a device RI array [ri_x, ri_y, ri_z]
+ *   (float or complex64); synchronous, the result is a host float.
+ * odt_set_potential_device: the padded potential built on the device from the
+ *   same RI (create_boundary_RI's zero-potential padding and RI2potential /
+ *   potential2RI round trips, :223-279, then V - i eps_imag) into the forward
+ *   slot, or with adjoint = 1 from conj(flip(RI, 3)) into the adjoint slot
+ *   (BACKWARD_SOLVER_MULTI.m:48); `pp` carries the scalars and 1D tables as
+ *   for odt_set_potential (its eps_imag is the one to subtract).  The device
+ *   values agree with a host-built potential to a few units in the last
+ *   place.
+ */
+typedef struct odt_ri_device_args {
+  const void* ri;          /* device [ri_x, ri_y, ri_z], float or complex64   */
+  int32_t is_complex;
+  int32_t adjoint;         /* 1: conj(flip(RI, 3)) into the adjoint slot      */
+  double wavelength;       /* params.wavelength                                */
+  double ri_bg;            /* params.RI_bg                                     */
+  void* stream;            /* cudaStream_t ordering the reads of `ri`          */
+} odt_ri_device_args;
+
+odt_status odt_potential_eps_device(odt_handle h, const odt_ri_device_args* args, float* eps_imag);
+odt_status odt_set_potential_device(odt_handle h, const odt_potential_params* pp,
+                                    const odt_ri_device_args* args);
+
+/*
+ * FISTA element-wise steps on device arrays of n elements
+ * (BACKWARD_SOLVER_MULTI.m:150-160):
+ *   odt_fista_prox_input: prox_in = u - step * grad (its real part when
+ *     prox_complex = 0: the reference's TV prox keeps the real part when
+ *     Vimag_max = 0);
+ *   odt_fista_update: s = prox_out; u = s + coef (s - x); x = s;
+ *     ri = ri_bg * sqrt(u + 1).
+ * Ordered on `stream`; asynchronous.
+ */
+typedef struct odt_fista_args {
+  int64_t n;
+  const odt_cfloat* grad;  /* odt_gradient's output                             */
+  odt_cfloat* u;           /* FISTA iterate u_n, complex64                      */
+  odt_cfloat* x;           /* previous prox result x_n, complex64              */
+  odt_cfloat* ri;          /* RI of the next gradient, complex64              */
+  void* prox_in;           /* float (prox_complex = 0) or complex64            */
+  const void* prox_out;
+  int32_t prox_complex;
+  double step;             /* 1 / alpha                                        */
+  double coef;             /* (t_n - 1) / t_{n+1}                              */
+  double ri_bg;
+  void* stream;
+} odt_fista_args;
+
+odt_status odt_fista_prox_input(const odt_fista_args* args);
+odt_status odt_fista_update(const odt_fista_args* args);
+
+/*
  * Isotropic-TV proximal operator by dual FISTA (sub_code/TV_FISTA_inner_v2.m
  * :1-53, called from BACKWARD_SOLVER_MULTI.m:152): `inner_itt` iterations on
  * a [size] array with periodic differences; projections onto

@@ -110,6 +110,34 @@ class GradientArgs(C.Structure):
     ]
 
 
+class RIDeviceArgs(C.Structure):
+    _fields_ = [
+        ("ri", C.c_void_p),
+        ("is_complex", C.c_int32),
+        ("adjoint", C.c_int32),
+        ("wavelength", C.c_double),
+        ("ri_bg", C.c_double),
+        ("stream", C.c_void_p),
+    ]
+
+
+class FistaArgs(C.Structure):
+    _fields_ = [
+        ("n", C.c_int64),
+        ("grad", C.c_void_p),
+        ("u", C.c_void_p),
+        ("x", C.c_void_p),
+        ("ri", C.c_void_p),
+        ("prox_in", C.c_void_p),
+        ("prox_out", C.c_void_p),
+        ("prox_complex", C.c_int32),
+        ("step", C.c_double),
+        ("coef", C.c_double),
+        ("ri_bg", C.c_double),
+        ("stream", C.c_void_p),
+    ]
+
+
 class TVArgs(C.Structure):
     _fields_ = [
         ("size", C.c_int32 * 3),
@@ -195,6 +223,10 @@ SIGNATURES = {
     "odt_set_adjoint_potential": (C.c_int, [C.c_uint32, C.POINTER(PotentialParams), C.c_void_p]),
     "odt_gradient": (C.c_int, [C.c_uint32, C.POINTER(GradientArgs)]),
     "odt_tv_prox": (C.c_int, [C.POINTER(TVArgs)]),
+    "odt_potential_eps_device": (C.c_int, [C.c_uint32, C.POINTER(RIDeviceArgs), C.POINTER(C.c_float)]),
+    "odt_set_potential_device": (C.c_int, [C.c_uint32, C.POINTER(PotentialParams), C.POINTER(RIDeviceArgs)]),
+    "odt_fista_prox_input": (C.c_int, [C.POINTER(FistaArgs)]),
+    "odt_fista_update": (C.c_int, [C.POINTER(FistaArgs)]),
     "odt_rytov": (C.c_int, [C.POINTER(RytovArgs)]),
     "odt_unwrap_goldstein": (C.c_int, [C.POINTER(UnwrapArgs)]),
     "odt_last_error": (C.c_char_p, []),

@@ -122,6 +122,18 @@ cudaError_t launch_emitter(const BornArgs& a, float2* conv, int c0, int c1, int 
 // tk[X, Y, b] = sum_z conv * Kt ; rk likewise with Kr (either output may be null)
 cudaError_t launch_zreduce(const float2* conv, const float2* Kt, const float2* Kr, float2* tk,
                            float2* rk, int c0, int c1, int rz, long long nb, cudaStream_t s);
+// Device-resident outer loop (potential_dev.cu): max |RI2potential(RI)| as
+// float bits into d_out; the padded potential V (forward or adjoint); the
+// FISTA prox input and momentum update.
+cudaError_t launch_potential_absmax(const void* ri, int is_complex, long long n, double wavelength, double ri_bg,
+                                    unsigned int* d_out, cudaStream_t s);
+cudaError_t launch_build_potential(const void* ri, int is_complex, int adjoint, const int sim[3], const int roi0[3],
+                                   const int ri_size[3], double wavelength, double ri_bg, float eps, float2* V,
+                                   cudaStream_t s);
+cudaError_t launch_fista_prox_input(const float2* u, const float2* grad, float step, int complex_out, void* out,
+                                    long long n, cudaStream_t s);
+cudaError_t launch_fista_update(const void* sv, int s_complex, float coef, float nb, float2* u, float2* x, float2* ri,
+                                long long n, cudaStream_t s);
 // Fused input / output stages (io_fused.cu): conv plane cx x cy, RI grid
 // rx x ry x rz, window offset (ox, oy) of the RI / field grid in the conv
 // plane, nbp planes per z.

@@ -609,11 +609,13 @@ void alloc_slot(Handle& H, int k) {
   P.allocated = true;
 }
 
+// V from the host (odt_set_potential) or built on the device from an RI
+// array in device memory (odt_set_potential_device: dev != NULL)
 void set_potential_slot(const std::shared_ptr<Handle>& Hp, int k, const odt_potential_params* pp,
-                        const odt_cfloat* V, const char* fn) {
+                        const odt_cfloat* V, const char* fn, const odt_ri_device_args* dev = nullptr) {
   Handle& H = *Hp;
   const std::string who(fn);
-  if (!pp || !V) raise(ODT_ERR_INVALID_ARGUMENT, who + ": NULL argument");
+  if (!pp || (!V && !dev)) raise(ODT_ERR_INVALID_ARGUMENT, who + ": NULL argument");
   const odt_geometry& g = H.g;
   for (int i = 0; i < 3; ++i) {
     const int lo = pp->roi[2 * i], hi = pp->roi[2 * i + 1];
@@ -634,7 +636,16 @@ void set_potential_slot(const std::shared_ptr<Handle>& Hp, int k, const odt_pote
   alloc_slot(H, k);
   Handle::PotSlot& P = H.pot[k];
   const size_t nv = (size_t)H.nvox();
-  ODT_CUDA(cudaMemcpy(P.V, V, nv * sizeof(float2), cudaMemcpyHostToDevice));
+  if (dev) {
+    int roi0[3];
+    for (int i = 0; i < 3; ++i) roi0[i] = pp->roi[2 * i] - 1;
+    cudaStream_t s = (cudaStream_t)dev->stream;
+    ODT_CUDA(launch_build_potential(dev->ri, dev->is_complex, dev->adjoint, g.sim_size, roi0, g.ri_size,
+                                    dev->wavelength, dev->ri_bg, pp->eps_imag, P.V, s));
+    ODT_CUDA(cudaStreamSynchronize(s));
+  } else {
+    ODT_CUDA(cudaMemcpy(P.V, V, nv * sizeof(float2), cudaMemcpyHostToDevice));
+  }
   std::vector<float2> one;
   for (int i = 0; i < 3; ++i) {
     const size_t n = g.sim_size[i];
@@ -752,6 +763,78 @@ odt_status odt_set_potential(odt_handle h, const odt_potential_params* pp, const
 odt_status odt_set_adjoint_potential(odt_handle h, const odt_potential_params* pp,
                                      const odt_cfloat* V) {
   return guarded([&] { set_potential_slot(lookup(h), 1, pp, V, "odt_set_adjoint_potential"); });
+}
+
+namespace {
+void check_ri_device_args(const Handle& H, const odt_ri_device_args* a, const char* fn) {
+  const std::string who(fn);
+  if (!a || !a->ri) raise(ODT_ERR_INVALID_ARGUMENT, who + ": NULL argument");
+  if (!is_device_ptr(a->ri)) raise(ODT_ERR_INVALID_ARGUMENT, who + ": ri is not a device pointer");
+  if (!(a->wavelength > 0.0) || !(a->ri_bg > 0.0) || !std::isfinite(a->wavelength) || !std::isfinite(a->ri_bg))
+    raise(ODT_ERR_INVALID_ARGUMENT, who + ": wavelength and ri_bg must be positive");
+  if (H.np != 1) raise(ODT_ERR_UNSUPPORTED, who + ": scalar handles only");
+}
+}  // namespace
+
+odt_status odt_potential_eps_device(odt_handle h, const odt_ri_device_args* a, float* eps_imag) {
+  return guarded([&] {
+    auto H = lookup(h);
+    check_ri_device_args(*H, a, "odt_potential_eps_device");
+    if (!eps_imag) raise(ODT_ERR_INVALID_ARGUMENT, "odt_potential_eps_device: NULL eps_imag");
+    DeviceGuard dg(H->g.device);
+    cudaStream_t s = (cudaStream_t)a->stream;
+    unsigned int* d = nullptr;
+    {
+      std::lock_guard<std::recursive_mutex> lk(g_device_mu);
+      ODT_CUDA(cudaMallocAsync((void**)&d, sizeof(unsigned int), s));
+    }
+    const long long n = (long long)H->g.ri_size[0] * H->g.ri_size[1] * H->g.ri_size[2];
+    unsigned int bits = 0;
+    cudaError_t e = launch_potential_absmax(a->ri, a->is_complex, n, a->wavelength, a->ri_bg, d, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&bits, d, sizeof(bits), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFreeAsync(d, s);
+    ODT_CUDA(e);
+    float m;
+    std::memcpy(&m, &bits, sizeof(m));
+    *eps_imag = m * 1.01f;   // single(max|V|) * 1.01 in single, as condition_RI (:205)
+  });
+}
+
+odt_status odt_set_potential_device(odt_handle h, const odt_potential_params* pp, const odt_ri_device_args* a) {
+  return guarded([&] {
+    auto H = lookup(h);
+    check_ri_device_args(*H, a, "odt_set_potential_device");
+    set_potential_slot(H, a->adjoint ? 1 : 0, pp, nullptr, "odt_set_potential_device", a);
+  });
+}
+
+namespace {
+void check_fista_args(const odt_fista_args* a, const char* fn) {
+  const std::string who(fn);
+  if (!a || a->n <= 0 || !a->u || !a->x || !a->ri || !a->prox_in || !a->prox_out || !a->grad)
+    raise(ODT_ERR_INVALID_ARGUMENT, who + ": NULL argument or n <= 0");
+  for (const void* p : {(const void*)a->u, (const void*)a->x, (const void*)a->ri, (const void*)a->prox_in,
+                        a->prox_out, (const void*)a->grad})
+    if (!is_device_ptr(p)) raise(ODT_ERR_INVALID_ARGUMENT, who + ": arrays must be device pointers");
+}
+}  // namespace
+
+odt_status odt_fista_prox_input(const odt_fista_args* a) {
+  return guarded([&] {
+    check_fista_args(a, "odt_fista_prox_input");
+    ODT_CUDA(launch_fista_prox_input(reinterpret_cast<const float2*>(a->u), reinterpret_cast<const float2*>(a->grad),
+                                     (float)a->step, a->prox_complex, a->prox_in, a->n, (cudaStream_t)a->stream));
+  });
+}
+
+odt_status odt_fista_update(const odt_fista_args* a) {
+  return guarded([&] {
+    check_fista_args(a, "odt_fista_update");
+    ODT_CUDA(launch_fista_update(a->prox_out, a->prox_complex, (float)a->coef, (float)a->ri_bg,
+                                 reinterpret_cast<float2*>(a->u), reinterpret_cast<float2*>(a->x),
+                                 reinterpret_cast<float2*>(a->ri), a->n, (cudaStream_t)a->stream));
+  });
 }
 
 odt_status odt_set_polarisation(odt_handle h, const float* radial, const float* perp,

@@ -93,6 +93,11 @@ class BACKWARD_SOLVER_MULTI_MULTI_GPU(BACKWARD_SOLVER_MULTI):
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
 
+    def _use_device_loop(self):
+        """The data-parallel solver runs the host-array outer loop (its
+        gradient exchange works on host arrays)."""
+        return False
+
     def local_gradient(self, RI, input_field, output_field):
         """Gradient and error of one share (get_gradiant_static); None for an
         empty share."""

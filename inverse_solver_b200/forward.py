@@ -143,9 +143,27 @@ class CBSHostSetup:
         RIp = potential2ri(RIp, lam, nm)
         self.ROI = [btp[0] + 1, btp[0] + old[0], btp[1] + 1, btp[1] + old[1], btp[2] + 1, btp[2] + old[2]]
         V_temp = ri2potential(RIp, lam, nm)
+        self.RI = potential2ri(V_temp, lam, nm)
+        V = (ri2potential(self.RI, lam, nm) - 1j * self.eps_imag).astype(C64)
+        pp, keep = self.potential_params(self.eps_imag)
+        self.V = V
+        return pp, keep + [_c64(V)]
+
+    def potential_params(self, eps_imag):
+        """The RI-independent part of create_boundary_RI and init
+        (FORWARD_SOLVER_CONVERGENT_BORN.m:251-396) for a given eps_imag:
+        attenuation masks, ramps, Green's coordinates, Bornmax and the
+        scalars, as the PotentialParams struct plus the arrays it points
+        into (keep them alive until the call returns)."""
+        p = self.parameters
+        self.eps_imag = F32(eps_imag)
+        btp = [int(b) for b in self.boundary_thickness_pixel]
+        old = list(self.expected_RI_size)
+        self.ROI = [btp[0] + 1, btp[0] + old[0], btp[1] + 1, btp[1] + old[1], btp[2] + 1, btp[2] + old[2]]
+        shape = tuple(old[j] + 2 * btp[j] for j in range(3))
         masks = []
         for j in range(3):
-            n = V_temp.shape[j]
+            n = shape[j]
             x = (np.abs(np.arange(1, n + 1) - math.floor(n / 2 + 1) + 0.5) - 0.5).astype(F32)
             x = np.roll(x, -(n // 2)) / (btp[j] - 0.5)
             v0 = x.copy()
@@ -157,11 +175,9 @@ class CBSHostSetup:
             if btp[j] == 0:
                 v0[:] = 0
             masks.append((1 - v0 * 1).astype(F32))
-        self.RI = potential2ri(V_temp, lam, nm)
-        V = (ri2potential(self.RI, lam, nm) - 1j * self.eps_imag).astype(C64)
         # init :280-396
         pb = copy.deepcopy(p)
-        pb["size"] = list(V.shape)
+        pb["size"] = list(shape)
         ub = self.utility_border = OpticalTool(pb)
         if p["acyclic"] and self.cyclic_boundary_xy:
             sc = [ub.fourier_coor[0], ub.fourier_coor[1], ub.fourier_coor[2] + ub.fourier_res[2] / 4]
@@ -176,14 +192,14 @@ class CBSHostSetup:
         a2 = F32((2 * math.pi * ub.k0_nm) ** 2)
         absorb = C64(a2 / C64(a2 + 1j * self.eps_imag))
         step = F32(abs(2 * (2 * math.pi * ub.k0_nm) / self.eps_imag))
-        nrm = float(np.linalg.norm(np.asarray(V.shape, dtype=np.float64) * np.asarray(p["resolution"], dtype=np.float64)))
+        nrm = float(np.linalg.norm(np.asarray(shape, dtype=np.float64) * np.asarray(p["resolution"], dtype=np.float64)))
         bopt = int(math.ceil(float(F32(F32(nrm / step) / 2 + 1)))) * 2
         it = p["iterations_number"]
         self.Bornmax = 0 if it == 0 else (bopt * abs(int(it)) if it < 0 else int(it))
         ramps = []
         if p["acyclic"]:
             for j in range(3):
-                n = V.shape[j]
+                n = shape[j]
                 if self.boundary_thickness_pixel[0] == 0 and self.boundary_thickness_pixel[1] == 0:
                     if j < 2:
                         ramps.append(np.ones(n, dtype=C64))
@@ -194,7 +210,7 @@ class CBSHostSetup:
                     x = np.exp(-1j * math.pi * (np.arange(1, n + 1) - 1) / n / 2).astype(C64)
                     ramps.append(x / x[n // 2])
         else:
-            ramps = [np.ones(V.shape[j], dtype=C64) for j in range(3)]
+            ramps = [np.ones(shape[j], dtype=C64) for j in range(3)]
         pp = _lib.PotentialParams()
         pp.eps_imag = float(self.eps_imag)
         pp.green_scale = float(F32(4 * math.pi ** 2))
@@ -213,11 +229,10 @@ class CBSHostSetup:
         pp.absorb[:] = [float(absorb.real), float(absorb.imag)]
         self.rads1d = rads
         self.green_absorbtion_correction = absorb
-        self.V = V
         self.attenuation_mask1d = masks
         self.ramp1d = ramps
         self.kq2 = kq2
-        return pp, keep + [_c64(V)]
+        return pp, keep
 
     def voxel_iterations(self, n_ill):
         """Born voxel-iterations of one solve of n_ill illuminations."""
@@ -284,6 +299,71 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
         finally:
             for k, v in saved.items():
                 setattr(self, k, v)
+
+    def _ri_device_args(self, ri, adjoint, stream):
+        import torch
+
+        n = int(np.prod(self.expected_RI_size))
+        if not (isinstance(ri, torch.Tensor) and ri.is_cuda and ri.is_contiguous() and ri.numel() == n):
+            raise ValueError("set_RI_device: RI must be a contiguous CUDA tensor of %d elements "
+                             "(the column-major [RI_x, RI_y, RI_z] grid)" % n)
+        if ri.dtype not in (torch.complex64, torch.float32):
+            raise ValueError("set_RI_device: RI must be complex64 or float32")
+        a = _lib.RIDeviceArgs()
+        a.ri = ri.data_ptr()
+        a.is_complex = 1 if ri.dtype == torch.complex64 else 0
+        a.adjoint = 1 if adjoint else 0
+        a.wavelength = float(self.parameters["wavelength"])
+        a.ri_bg = float(self.parameters["RI_bg"])
+        a.stream = torch.cuda.current_stream(ri.device).cuda_stream if stream is None else stream
+        return a
+
+    def set_RI_device(self, ri, adjoint=False, stream=None):
+        """set_RI (or, with adjoint=True, set_RI_adjoint) for an RI array that
+        is already in device memory: a contiguous CUDA tensor holding the
+        column-major [RI_x, RI_y, RI_z] grid (complex64 or float32).  eps_imag
+        and the padded potential are computed on the GPU
+        (odt_potential_eps_device, odt_set_potential_device); only the
+        RI-independent tables come from the host.  Used by the device-resident
+        outer loop of BACKWARD_SOLVER_MULTI."""
+        a = self._ri_device_args(ri, adjoint, stream)
+        eps = C.c_float(0)
+        _lib.check(self.lib.odt_potential_eps_device(self._handle, C.byref(a), C.byref(eps)))
+        saved = {k: getattr(self, k) for k in self._STATE if hasattr(self, k)} if adjoint else {}
+        try:
+            pp, keep = self.potential_params(eps.value)
+            _lib.check(self.lib.odt_set_potential_device(self._handle, C.byref(pp), C.byref(a)))
+            if adjoint:
+                self.adjoint_Bornmax = self.Bornmax
+        finally:
+            for k, v in saved.items():
+                setattr(self, k, v)
+
+    def gradient_device(self, fields_in, fields_meas, grad, stream=None):
+        """gradient() on device arrays: fields_in / fields_meas contiguous CUDA
+        complex64 tensors of F_x*F_y*n_ill elements (column-major
+        [F_x, F_y, n_ill]), grad a CUDA complex64 tensor of the RI grid's size;
+        returns err."""
+        import torch
+
+        if self.vector:
+            raise NotImplementedError("the gradient is available for the scalar solver only")
+        nF = int(self.field_size[0] * self.field_size[1])
+        n_ill = fields_in.numel() // nF
+        if fields_in.numel() != nF * n_ill or fields_meas.numel() != fields_in.numel() or n_ill < 1:
+            raise ValueError("input and output fields must be [F_x, F_y, n] alike")
+        err = C.c_double(0)
+        a = _lib.GradientArgs()
+        a.fields_in, a.fields_meas = fields_in.data_ptr(), fields_meas.data_ptr()
+        a.n_ill = n_ill
+        a.grad = grad.data_ptr()
+        a.err = C.addressof(err)
+        a.memory = _lib.ODT_MEM_DEVICE
+        s = torch.cuda.current_stream(grad.device) if stream is None else stream
+        a.stream = s.cuda_stream
+        _lib.check(self.lib.odt_gradient(self._handle, C.byref(a)))
+        s.synchronize()
+        return err.value
 
     def gradient(self, input_field, output_field):
         """Fused forward + adjoint gradient of get_gradiant_static
