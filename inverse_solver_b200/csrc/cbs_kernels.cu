@@ -218,13 +218,13 @@ size_t fft_smem_bytes(int n, int W, int kind) {
   }
 }
 
-// radix classes 0-2 have device kernels (radices <= 19); make_dev_fft
-// rejects plans of class 3
+// radix classes 0-3 (radices <= 8, <= 15, <= 19, <= 31) each have device kernels
 #define ODT_CLS_DISPATCH(cls, F, ...)                 \
   switch (cls) {                                      \
     case 0: return F<0>(__VA_ARGS__);                 \
     case 1: return F<1>(__VA_ARGS__);                 \
-    default: return F<2>(__VA_ARGS__);                \
+    case 2: return F<2>(__VA_ARGS__);                 \
+    default: return F<3>(__VA_ARGS__);                \
   }
 
 cudaError_t launch_born_x(const BornArgs& a, int mode, int jj, const DevFft& fx, cudaStream_t s) {

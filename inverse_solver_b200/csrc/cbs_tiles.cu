@@ -3,12 +3,12 @@
 // and column FFTs).
 //
 // This file is compiled once per (kernel kind, radix class) pair
-// (-DODT_KIND=0..3 -DODT_CLS=0..2, see the Makefile) so the heavily unrolled
+// (-DODT_KIND=0..3 -DODT_CLS=0..3, see the Makefile) so the heavily unrolled
 // radix code builds in parallel; cbs_kernels.cu dispatches.
 #include "tile_bodies.cuh"
 
 #ifndef ODT_KIND
-#error "compile with -DODT_KIND=<0..3> -DODT_CLS=<0..2>"
+#error "compile with -DODT_KIND=<0..3> -DODT_CLS=<0..3>"
 #endif
 
 namespace odt {
@@ -17,22 +17,28 @@ namespace {
 
 __device__ __forceinline__ Thr thr() { return Thr{(int)threadIdx.x, (int)blockDim.x}; }
 
+// launch bound of the tile kernels: 256 threads (128-register budget), 128
+// for radix class 3 (butterflies of up to 31 points held in registers); the
+// launches use 128 threads in every class
+template <int CLS>
+constexpr int kMaxThreads = CLS == 3 ? 128 : 256;
+
 template <int CLS, int MODE>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(kMaxThreads<CLS>, 2)
 born_x_kernel(BornArgs a, int jj, FftPlan plan, const float2* __restrict__ twg, int W) {
   extern __shared__ __align__(16) unsigned char smraw[];
   born_x_body<CLS, MODE>(a, jj, plan, twg, W, smraw, blockIdx.x, thr());
 }
 
 template <int CLS>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(kMaxThreads<CLS>, 2)
 born_z_kernel(BornArgs a, int jj, FftPlan plan, const float2* __restrict__ twg, int lgW) {
   extern __shared__ __align__(16) unsigned char smraw[];
   born_z_body<CLS>(a, jj, plan, twg, lgW, smraw, blockIdx.x, thr());
 }
 
 template <int CLS, bool INV>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(kMaxThreads<CLS>, 2)
 fft_lines_kernel(const float2* in, float2* out, long long nlines, int in_shift, int out_shift,
                  float scale, FftPlan plan, const float2* __restrict__ twg, int W) {
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -41,7 +47,7 @@ fft_lines_kernel(const float2* in, float2* out, long long nlines, int in_shift, 
 }
 
 template <int CLS, bool INV, bool SHIFT>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(kMaxThreads<CLS>, 2)
 fft_cols_kernel(const float2* in, float2* out, long long n0, int in_shift, int out_shift,
                 float scale, FftPlan plan, const float2* __restrict__ twg, int lgW) {
   extern __shared__ __align__(16) unsigned char smraw[];

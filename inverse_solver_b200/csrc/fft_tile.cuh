@@ -254,6 +254,20 @@ ODT_HD void tile_mid(const Thr& th, const Map& m, int n, const float2* tw, const
           case 19: { constexpr int RR = (CLS == 2) ? 19 : 2; CALL; } break;         \
           default: break;                                                          \
         }                                                                          \
+      } else if (CLS == 3) {                                                         \
+        switch (R) {                                                               \
+          case 7: { constexpr int RR = (CLS == 3) ? 7 : 2; CALL; } break;           \
+          case 9: { constexpr int RR = (CLS == 3) ? 9 : 2; CALL; } break;           \
+          case 11: { constexpr int RR = (CLS == 3) ? 11 : 2; CALL; } break;         \
+          case 13: { constexpr int RR = (CLS == 3) ? 13 : 2; CALL; } break;         \
+          case 15: { constexpr int RR = (CLS == 3) ? 15 : 2; CALL; } break;         \
+          case 17: { constexpr int RR = (CLS == 3) ? 17 : 2; CALL; } break;         \
+          case 19: { constexpr int RR = (CLS == 3) ? 19 : 2; CALL; } break;         \
+          case 23: { constexpr int RR = (CLS == 3) ? 23 : 2; CALL; } break;          \
+          case 29: { constexpr int RR = (CLS == 3) ? 29 : 2; CALL; } break;          \
+          case 31: { constexpr int RR = (CLS == 3) ? 31 : 2; CALL; } break;          \
+          default: break;                                                          \
+        }                                                                          \
       }                                                                            \
       break;                                                                       \
   }

@@ -37,12 +37,12 @@
 // a few loads per butterfly.  Tiles are 8 lines / columns wide (about 38 KB
 // of shared memory, five CTAs per SM).
 //
-// Compiled once per radix class (-DODT_CLS=0..2, see the Makefile); the
+// Compiled once per radix class (-DODT_CLS=0..3, see the Makefile); the
 // class-independent dispatchers are compiled with class 0.
 #include "tile_bodies.cuh"
 
 #ifndef ODT_CLS
-#error "compile with -DODT_CLS=<0..2>"
+#error "compile with -DODT_CLS=<0..3>"
 #endif
 
 namespace odt {
@@ -486,7 +486,8 @@ cudaError_t launch_refocus_in(const float2* sk, const float2* refocus, float2* m
   switch (fx.plan.rclass > fy.plan.rclass ? fx.plan.rclass : fy.plan.rclass) {
     case 0: return io_in_launch<0>(sk, refocus, mid, einc, g, fx, fy, s);
     case 1: return io_in_launch<1>(sk, refocus, mid, einc, g, fx, fy, s);
-    default: return io_in_launch<2>(sk, refocus, mid, einc, g, fx, fy, s);
+    case 2: return io_in_launch<2>(sk, refocus, mid, einc, g, fx, fy, s);
+    default: return io_in_launch<3>(sk, refocus, mid, einc, g, fx, fy, s);
   }
 }
 
@@ -497,7 +498,8 @@ cudaError_t launch_project_out(const BornArgs& a, float2* mid, long long cap, co
   switch (fx.plan.rclass) {
     case 0: e = io_out_lines_launch<0>(a, mid, g, dV, fx, s); break;
     case 1: e = io_out_lines_launch<1>(a, mid, g, dV, fx, s); break;
-    default: e = io_out_lines_launch<2>(a, mid, g, dV, fx, s); break;
+    case 2: e = io_out_lines_launch<2>(a, mid, g, dV, fx, s); break;
+    default: e = io_out_lines_launch<3>(a, mid, g, dV, fx, s); break;
   }
   if (e != cudaSuccess) return e;
   // z in chunks of 16 planes (partial sums after the mid buffer) where the
@@ -515,7 +517,8 @@ cudaError_t launch_project_out(const BornArgs& a, float2* mid, long long cap, co
   switch (fy.plan.rclass) {
     case 0: e = io_out_cols_launch<0>(mid, Kt, Kr, tk, rk, part, zs, g, fy, s); break;
     case 1: e = io_out_cols_launch<1>(mid, Kt, Kr, tk, rk, part, zs, g, fy, s); break;
-    default: e = io_out_cols_launch<2>(mid, Kt, Kr, tk, rk, part, zs, g, fy, s); break;
+    case 2: e = io_out_cols_launch<2>(mid, Kt, Kr, tk, rk, part, zs, g, fy, s); break;
+    default: e = io_out_cols_launch<3>(mid, Kt, Kr, tk, rk, part, zs, g, fy, s); break;
   }
   if (e != cudaSuccess || !part) return e;
   long long blocks = (tot + 255) / 256;

@@ -298,9 +298,6 @@ DevFft make_dev_fft(Handle& H, int n, int kind, const char* what) {
   const int order = kind == kKindBornX ? kSmallFirst : kLargeFirst;
   if (!make_plan(n, &f.plan, &why, order))
     raise(ODT_ERR_UNSUPPORTED, std::string(what) + ": " + why);
-  if (f.plan.rclass > 2)
-    raise(ODT_ERR_UNSUPPORTED, std::string(what) + ": length " + std::to_string(n) +
-                                   " has a prime factor > 19 (device kernels take radices <= 19)");
   f.lgW = n <= 512 ? 4 : 3;
   f.W = 1 << f.lgW;
   f.nthr = 128;

@@ -236,8 +236,8 @@ struct Buffers {
 };
 
 bool dev_fft(Buffers& B, int n, int kind, DevFft* f, std::string* why) {
-  if (!make_plan(n, &f->plan, why, kLargeFirst) || f->plan.rclass > 2) {
-    if (why->empty()) *why = "length " + std::to_string(n) + " has a prime factor > 19";
+  if (!make_plan(n, &f->plan, why, kLargeFirst)) {
+    if (why->empty()) *why = "length " + std::to_string(n) + " has a prime factor > 31";
     return false;
   }
   f->lgW = n <= 512 ? 4 : 3;

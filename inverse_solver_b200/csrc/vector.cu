@@ -193,6 +193,7 @@ cudaError_t launch_born_z_dyadic(const BornArgs& a, const DyadArgs& d, int jj, c
     ODT_DYAD_CASE(0)
     ODT_DYAD_CASE(1)
     ODT_DYAD_CASE(2)
+    ODT_DYAD_CASE(3)
 #undef ODT_DYAD_CASE
     default:
       return cudaErrorNotSupported;
