@@ -390,6 +390,45 @@ def run_fista(args):
     print(json.dumps(out), flush=True)
 
 
+def run_bpm(args):
+    """Beam-propagation workload (FORWARD_SOLVER_BPM): voxel-steps/s (field
+    plane x slices x illuminations per second) of whole solves through the
+    host API (inputs and outputs in host memory), RI 128^3 at 0.1 um
+    (seeded multi-sphere phantom), 49 ring illuminations, cosine correction
+    on, transmitted field only; beside it the single-precision oracle on
+    the host cores for 2 illuminations."""
+    from inverse_solver_b200 import FORWARD_SOLVER_BPM
+    from inverse_solver_b200.inputs import ring_illumination, sphere_phantom
+    from oracle import bpm as obpm
+
+    nm = 1.3355
+    p = FORWARD_SOLVER_BPM.get_default_parameters(dict(size=list(GRID), wavelength=0.532, NA=1.2, RI_bg=nm,
+                                                       resolution=[0.1] * 3, vector_simulation=False))
+    RI = sphere_phantom(GRID, [0.1] * 3, nm, seed=SEED)
+    fields = np.ascontiguousarray(ring_illumination(p)[:, :, :, :args.n_ill])
+    s = FORWARD_SOLVER_BPM(p)
+    s.set_RI(RI)
+    for _ in range(args.warmup):
+        s.solve(fields)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s.solve(fields)
+    dt = (time.perf_counter() - t0) / args.steps
+    units = int(np.prod(GRID)) * fields.shape[3]
+    o = obpm.ForwardSolverBPM(p, single=True)
+    o.set_RI(RI)
+    t0 = time.perf_counter()
+    o.solve(fields[:, :, :, :2])
+    dtc = time.perf_counter() - t0
+    print(json.dumps({
+        "metric": "BPM voxel-steps/s", "value": units / dt, "unit": "voxel-steps/s", "higher_is_better": True,
+        "ms_per_solve": dt * 1e3, "steps": args.steps, "warmup": args.warmup,
+        "config": {"workload": "FORWARD_SOLVER_BPM: 128^3 RI grid, 0.1 um voxels, seeded multi-sphere "
+                               "phantom, %d ring illuminations, cos_correction, host API" % fields.shape[3]},
+        "cpu_baseline": {"value": int(np.prod(GRID)) * 2 / dtc, "unit": "voxel-steps/s",
+                         "cores": os.cpu_count(), "kind": "port", "sample": "2 illuminations"}}), flush=True)
+
+
 def workload_key():
     return "cbs_forward_128cube_49ill"
 
@@ -409,6 +448,8 @@ def main():
                     help="illuminations per step (profiling runs use fewer)")
     ap.add_argument("--profile-run", action="store_true",
                     help="only run --warmup solves (for ncu captures) and exit")
+    ap.add_argument("--bpm", action="store_true",
+                    help="time the beam-propagation forward solver")
     ap.add_argument("--fista", action="store_true",
                     help="time FISTA outer iterations of the inverse solver (device vs host loop)")
     args = ap.parse_args()
@@ -420,6 +461,9 @@ def main():
         return
     if args.fista:
         run_fista(args)
+        return
+    if args.bpm:
+        run_bpm(args)
         return
     if world > 1:
         import datetime

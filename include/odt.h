@@ -254,6 +254,40 @@ odt_status odt_fista_prox_input(const odt_fista_args* args);
 odt_status odt_fista_update(const odt_fista_args* args);
 
 /*
+ * Beam-propagation forward solver (FORWARD_SOLVER_BPM.m:44-117), scalar
+ * fields, all illuminations marched through the slices together.  The
+ * tables are set_RI's (:23-44) and DERIVE_OPTICAL_TOOL's single-precision
+ * arrays as the host computed them:
+ *   field_multiplier [F_x, F_y, Nz]  1i 2 pi k0 (RI - RI_bg) res_z      (:33)
+ *   refocus_kernel   [F_x, F_y]      ifftshift(exp(refocusing_kernel res_z) .* NA_circle) (:35)
+ *   filter_out       [F_x, F_y]      ifftshift(NA_circle), real (:34); needed for field3d
+ *   pre / post       [F_x, F_y]      exp(refocusing_kernel res_z (-floor(Nz/2)-1)) and
+ *                                    exp(refocusing_kernel res_z (-(Nz-floor(Nz/2)-1))),
+ *                                    centred (:94, :112)
+ *   cos_theta        [F_x, F_y]      centred; NULL = cos_correction off (:58-63)
+ * Outputs: trans [F_x, F_y, n_ill]; field3d [F_x, F_y, Nz, n_ill] or NULL.
+ * Scratch comes from the stream-ordered allocator.  Synchronous for host
+ * pointers; ordered on `stream` for device pointers.
+ */
+typedef struct odt_bpm_args {
+  int32_t size[3];                    /* [F_x, F_y, Nz]                        */
+  const odt_cfloat* field_multiplier;
+  const odt_cfloat* refocus_kernel;
+  const float* filter_out;
+  const odt_cfloat* pre;
+  const odt_cfloat* post;
+  const float* cos_theta;
+  const odt_cfloat* fields_in;        /* [F_x, F_y, n_ill] spatial fields       */
+  int32_t n_ill;
+  odt_cfloat* trans;
+  odt_cfloat* field3d;
+  int32_t memory;                     /* ODT_MEM_HOST or ODT_MEM_DEVICE         */
+  void* stream;
+} odt_bpm_args;
+
+odt_status odt_bpm_solve(const odt_bpm_args* args);
+
+/*
  * Isotropic-TV proximal operator by dual FISTA (sub_code/TV_FISTA_inner_v2.m
  * :1-53, called from BACKWARD_SOLVER_MULTI.m:152): `inner_itt` iterations on
  * a [size] array with periodic differences; projections onto

@@ -138,6 +138,24 @@ class FistaArgs(C.Structure):
     ]
 
 
+class BPMArgs(C.Structure):
+    _fields_ = [
+        ("size", C.c_int32 * 3),
+        ("field_multiplier", C.c_void_p),
+        ("refocus_kernel", C.c_void_p),
+        ("filter_out", C.c_void_p),
+        ("pre", C.c_void_p),
+        ("post", C.c_void_p),
+        ("cos_theta", C.c_void_p),
+        ("fields_in", C.c_void_p),
+        ("n_ill", C.c_int32),
+        ("trans", C.c_void_p),
+        ("field3d", C.c_void_p),
+        ("memory", C.c_int32),
+        ("stream", C.c_void_p),
+    ]
+
+
 class TVArgs(C.Structure):
     _fields_ = [
         ("size", C.c_int32 * 3),
@@ -227,6 +245,7 @@ SIGNATURES = {
     "odt_set_potential_device": (C.c_int, [C.c_uint32, C.POINTER(PotentialParams), C.POINTER(RIDeviceArgs)]),
     "odt_fista_prox_input": (C.c_int, [C.POINTER(FistaArgs)]),
     "odt_fista_update": (C.c_int, [C.POINTER(FistaArgs)]),
+    "odt_bpm_solve": (C.c_int, [C.POINTER(BPMArgs)]),
     "odt_rytov": (C.c_int, [C.POINTER(RytovArgs)]),
     "odt_unwrap_goldstein": (C.c_int, [C.POINTER(UnwrapArgs)]),
     "odt_last_error": (C.c_char_p, []),

@@ -1,0 +1,105 @@
+"""Beam-propagation forward solver (Codes/FORWARD_SOLVER_BPM.m) on the B200
+library: the host computes set_RI's tables in MATLAB single semantics
+(:23-44) and the refocusing phases of solve (:93-95, :110-114); the slice
+loop, the 2D FFTs, the cosine correction (:58-63) and the optional 3D field
+run on the GPU (odt_bpm_solve)."""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from .optics import C64, F32, OpticalTool, basic_optical_parameter, update_struct
+
+
+def _f32(x):
+    return np.asfortranarray(np.asarray(x, dtype=F32))
+
+
+def _c64(x):
+    return np.asfortranarray(np.asarray(x, dtype=C64))
+
+
+class FORWARD_SOLVER_BPM:
+    """Codes/FORWARD_SOLVER_BPM.m: scalar beam propagation, one slice per z
+    of the RI grid (whose xy size is the field size)."""
+
+    @staticmethod
+    def get_default_parameters(init_params=None):
+        """FORWARD_SOLVER.m:9-20 + FORWARD_SOLVER_BPM.m:9-19."""
+        p = basic_optical_parameter()
+        p.update(return_transmission=True, return_reflection=False, return_3D=False, use_GPU=True)
+        p.update(iterations_number=-1, use_GPU=True, cos_correction=True)
+        return update_struct(p, init_params) if init_params else p
+
+    def __init__(self, params):
+        """FORWARD_SOLVER_BPM.m:21-23 (DERIVE_OPTICAL_TOOL of the parameters)."""
+        self.parameters = dict(params)
+        self.utility = OpticalTool(self.parameters)
+        self.lib = _lib.load()
+        self.RI = None
+
+    def set_RI(self, RI):
+        """:23-44 in single precision."""
+        p, u = self.parameters, self.utility
+        RI = np.asarray(RI)
+        RI = RI.astype(C64 if np.iscomplexobj(RI) else F32)
+        if RI.ndim != 3 or list(RI.shape[:2]) != [int(p["size"][0]), int(p["size"][1])]:
+            raise ValueError("the RI must be [size(1), size(2), Nz]")
+        self.RI = RI
+        c = 1j * 2 * math.pi * u.k0
+        self.field_multiplier = ((c * (RI - p["RI_bg"])).astype(C64) * p["resolution"][2]).astype(C64)
+        self.filter_out = np.fft.ifftshift(u.NA_circle).astype(F32)
+        rk = np.asarray(u.refocusing_kernel, dtype=C64)
+        self.refocus_kernel = np.fft.ifftshift((np.exp((rk * p["resolution"][2]).astype(C64)) * u.NA_circle)
+                                               .astype(C64))
+
+    def _phases(self):
+        p, u = self.parameters, self.utility
+        nz = self.field_multiplier.shape[2]
+        rk = (np.asarray(u.refocusing_kernel, dtype=C64) * p["resolution"][2]).astype(C64)
+        pre = np.exp((rk * (-math.floor(nz / 2) - 1)).astype(C64)).astype(C64)
+        post = np.exp((rk * (-(nz - math.floor(nz / 2) - 1))).astype(C64)).astype(C64)
+        return pre, post
+
+    def solve(self, input_field):
+        """:45-117 -> (fields_trans, fields_ref, fields_3D); fields_ref is
+        the reference's untouched ones(...) array when return_reflection."""
+        if self.RI is None:
+            raise RuntimeError("call set_RI first")
+        p = self.parameters
+        f = np.asarray(input_field)
+        if f.ndim == 3:
+            f = f[:, :, :, None]
+        if f.shape[2] > 1:
+            if f.shape[2] != 2:
+                raise ValueError("must give far field polarisation with 2 pols only")
+            raise ValueError("Look at the old version for polarised version but it is useless")
+        n1, n2, nz = self.field_multiplier.shape
+        if list(f.shape[:2]) != [n1, n2]:
+            raise ValueError("input fields must be [size(1), size(2), 1, n]")
+        nill = f.shape[3]
+        fin = _c64(f[:, :, 0, :])
+        trans = np.empty((n1, n2, nill), dtype=C64, order="F")
+        f3 = np.empty((n1, n2, nz, nill), dtype=C64, order="F") if p["return_3D"] else None
+        pre, post = self._phases()
+        keep = [_c64(self.field_multiplier), _c64(self.refocus_kernel), _f32(self.filter_out), _c64(pre),
+                _c64(post), _f32(self.utility.cos_theta)]
+        a = _lib.BPMArgs()
+        a.size[:] = [n1, n2, nz]
+        a.field_multiplier, a.refocus_kernel, a.filter_out = (_lib.ptr(k) for k in keep[:3])
+        a.pre, a.post = _lib.ptr(keep[3]), _lib.ptr(keep[4])
+        a.cos_theta = _lib.ptr(keep[5]) if p["cos_correction"] else None
+        a.fields_in = _lib.ptr(fin)
+        a.n_ill = nill
+        a.trans = _lib.ptr(trans)
+        a.field3d = _lib.ptr(f3) if f3 is not None else None
+        a.memory = _lib.ODT_MEM_HOST
+        a.stream = None
+        _lib.check(self.lib.odt_bpm_solve(C.byref(a)))
+        fields_trans = trans[:, :, None, :]
+        fields_ref = np.ones(fields_trans.shape, dtype=C64) if p["return_reflection"] else None
+        fields_3D = f3[:, :, :, None, :] if f3 is not None else None
+        return fields_trans, fields_ref, fields_3D

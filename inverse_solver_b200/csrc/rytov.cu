@@ -23,6 +23,7 @@
 #include "../../include/odt.h"
 #include "cbs_kernels.cuh"
 #include "fft_plan.h"
+#include "scratch.cuh"
 
 namespace odt {
 const char* set_last_error(const std::string& msg);
@@ -220,40 +221,6 @@ odt_status fail(odt_status st, const std::string& m) {
   return st;
 }
 
-struct Buffers {
-  std::vector<void*> ptrs;
-  cudaStream_t s;
-  ~Buffers() {
-    for (void* p : ptrs) cudaFreeAsync(p, s);
-  }
-  template <typename T>
-  T* get(size_t n) {
-    void* p = nullptr;
-    if (cudaMallocAsync(&p, n * sizeof(T) + 16, s) != cudaSuccess) return nullptr;
-    ptrs.push_back(p);
-    return static_cast<T*>(p);
-  }
-};
-
-bool dev_fft(Buffers& B, int n, int kind, DevFft* f, std::string* why) {
-  if (!make_plan(n, &f->plan, why, kLargeFirst)) {
-    if (why->empty()) *why = "length " + std::to_string(n) + " has a prime factor > 31";
-    return false;
-  }
-  f->lgW = n <= 512 ? 4 : 3;
-  f->W = 1 << f->lgW;
-  f->nthr = 128;
-  (void)kind;
-  std::vector<float2> tw = make_twiddles(n);
-  float2* d = B.get<float2>(n);
-  if (!d || cudaMemcpyAsync(d, tw.data(), n * sizeof(float2), cudaMemcpyHostToDevice, B.s) != cudaSuccess) {
-    *why = "twiddle upload failed";
-    return false;
-  }
-  f->tw = d;
-  return true;
-}
-
 #define RY_CHECK(call)                                                              \
   do {                                                                              \
     cudaError_t e_ = (call);                                                        \
@@ -275,7 +242,7 @@ extern "C" odt_status odt_rytov(const odt_rytov_args* a) {
     return fail(ODT_ERR_INVALID_ARGUMENT, "odt_rytov: bad memory flag");
   const bool dev = a->memory == ODT_MEM_DEVICE;
   cudaStream_t s = dev ? (cudaStream_t)a->stream : (cudaStream_t)0;
-  Buffers B;
+  Scratch B;
   B.s = s;
   const long long n12 = (long long)n1 * n2, n3d = n12 * n3, nf = n12 * nill;
   const cudaMemcpyKind kin = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
@@ -308,8 +275,7 @@ extern "C" odt_status odt_rytov(const odt_rytov_args* a) {
   fill_int_kernel<<<grid_for(n12 * nill), kThreads, 0, s>>>(kzmap, n12 * nill, -1);
   DevFft f1{}, f2{}, f3{};
   std::string why;
-  if (!dev_fft(B, n1, kKindLines, &f1, &why) || !dev_fft(B, n2, kKindCols, &f2, &why) ||
-      !dev_fft(B, n3, kKindCols, &f3, &why))
+  if (!scratch_fft(B, n1, &f1, &why) || !scratch_fft(B, n2, &f2, &why) || !scratch_fft(B, n3, &f3, &why))
     return fail(ODT_ERR_UNSUPPORTED, "odt_rytov: " + why);
   auto fftc2 = [&](float2* x, long long nsl, bool inv) -> cudaError_t {
     cudaError_t e = launch_fft_lines(x, x, (long long)n2 * nsl, n1 / 2, n1 / 2, 1.f, inv, f1, s);
