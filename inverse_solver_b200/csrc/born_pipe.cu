@@ -166,23 +166,41 @@ __global__ void __launch_bounds__(W * 8, W == 16 ? 2 : 3)
     // V of this thread's first mid-pass butterfly, loaded now so that its
     // latency hides behind the wait for T and the first FFT pass; each later
     // round's V is loaded before the previous round's arithmetic
-    auto v_base = [&](int idx) {
-      const int c = idx / R2;
+    //
+    // Mid-pass work items: a half-warp takes two lines x 8 consecutive
+    // butterflies, slot s -> line 2 (s/16 / kJB) + (s%16)/8, butterfly
+    // 8 (s/16 % kJB) + s%8.  The line pitch N = 8 (mod 16) elements puts the
+    // other line 8 banks away, so every shared-memory access of the pass
+    // (T, Field_n, Field, the second buffer) hits 16 distinct 8-byte banks
+    // per half-warp; slots with j >= R2 idle.  (kW / 2) kJB 16 slots take as
+    // many rounds of kThreads as the kW R2 butterflies would.
+    constexpr int kJB = (R2 + 7) / 8;
+    constexpr int kSlots = (kW / 2) * kJB * 16;
+    auto item = [&](int sl, int& c, int& j) {
+      const int hw = sl >> 4, l = sl & 15;
+      const int pair = hw / kJB;
+      c = 2 * pair + (l >> 3);
+      j = 8 * (hw - pair * kJB) + (l & 7);
+      return j < R2;
+    };
+    auto v_base = [&](int c, int j) {
       const int yy = c < nl ? y0 + c : y0;
-      return (yy + a.py * z) * N + (idx - c * R2);
+      return (yy + a.py * z) * N + j;
     };
     float2 Vn[kR1];
-    if (tid < kW * R2) {
-      const int vb = v_base(tid);
+    {
+      int c0, j0;
+      if (tid < kSlots && item(tid, c0, j0)) {
+        const int vb = v_base(c0, j0);
 #pragma unroll
-      for (int r = 0; r < kR1; ++r) Vn[r] = a.V[vb + R2 * r];
+        for (int r = 0; r < kR1; ++r) Vn[r] = a.V[vb + R2 * r];
+      }
     }
     // the incident field (iteration 2's source, the final pass's Fout) is
     // prefetched the same way; zero outside the ROI
     constexpr bool kHasE = KIND != kSteady;
     const bool need_e = KIND == kFinal || (KIND == kEarly && jj <= 2);
-    auto e_load = [&](int idx, float2* En) {
-      const int c = idx / R2, j = idx - c * R2;
+    auto e_load = [&](int c, int j, float2* En) {
       const int yy = c < nl ? y0 + c : y0;
       const bool roi = need_e && (unsigned)(yy - a.ry0) < (unsigned)a.ry && (unsigned)(z - a.rz0) < (unsigned)a.rz;
       const long long base = (long long)b * est + (long long)(yy - a.ry0) * a.rx +
@@ -195,7 +213,8 @@ __global__ void __launch_bounds__(W * 8, W == 16 ? 2 : 3)
     };
     float2 En[kHasE ? kR1 : 1];
     if constexpr (kHasE) {
-      if (tid < kW * R2) e_load(tid, En);
+      int c0, j0;
+      if (tid < kSlots && item(tid, c0, j0)) e_load(c0, j0, En);
     }
     if (tid < kW) {
       PipeLine P;
@@ -244,9 +263,9 @@ __global__ void __launch_bounds__(W * 8, W == 16 ? 2 : 3)
       return;
     }
     // ---- inverse radix-8 (ns = R2) -> update + source -> forward radix-8
-    for (int idx = tid; idx < kW * R2; idx += kThreads) {
-      const int c = idx / R2, j = idx - c * R2;
-      const PipeLine& Ln = lines[c];
+    for (int sl = tid; sl < kSlots; sl += kThreads) {
+      int c, j;
+      const bool live = item(sl, c, j);
       float2 Vv[kR1];
 #pragma unroll
       for (int r = 0; r < kR1; ++r) Vv[r] = Vn[r];
@@ -255,12 +274,17 @@ __global__ void __launch_bounds__(W * 8, W == 16 ? 2 : 3)
 #pragma unroll
         for (int r = 0; r < kR1; ++r) Ev[r] = En[r];
       }
-      if (idx + kThreads < kW * R2) {
-        const int vb = v_base(idx + kThreads);
+      {
+        int cn, jn;
+        if (sl + kThreads < kSlots && item(sl + kThreads, cn, jn)) {
+          const int vb = v_base(cn, jn);
 #pragma unroll
-        for (int r = 0; r < kR1; ++r) Vn[r] = a.V[vb + R2 * r];
-        if constexpr (kHasE) e_load(idx + kThreads, En);
+          for (int r = 0; r < kR1; ++r) Vn[r] = a.V[vb + R2 * r];
+          if constexpr (kHasE) e_load(cn, jn, En);
+        }
       }
+      if (!live) continue;
+      const PipeLine& Ln = lines[c];
       float2 v[kR1];
 #pragma unroll
       for (int r = 0; r < kR1; ++r) v[r] = T0[c * N + j + R2 * r];
