@@ -154,6 +154,10 @@ class BACKWARD_SOLVER_MULTI:
             self.RI_inter = RI
         return RI
 
+    def _device_gradient(self, fs, fields_in, fields_meas, grad, n_sel):
+        """Gradient of the selected illuminations into `grad` (device), err."""
+        return fs.gradient_device(fields_in, fields_meas, grad)
+
     def _solve_device(self, input_field, output_field):
         """:92-196 with the iterates in device memory (see the module docstring)."""
         import torch
@@ -215,7 +219,7 @@ class BACKWARD_SOLVER_MULTI:
                 f2 = fmeas.view(nill, nF).index_select(0, idx).reshape(-1)
             fs.set_RI_device(ri)
             fs.set_RI_device(ri, adjoint=True)
-            err = fs.gradient_device(f1, f2, grad)
+            err = self._device_gradient(fs, f1, f2, grad, len(sl))
             self.err_list.append(err)
             t_n = t_np
             _lib.check(lib.odt_fista_prox_input(C.byref(fa)))

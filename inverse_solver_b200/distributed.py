@@ -94,9 +94,33 @@ class BACKWARD_SOLVER_MULTI_MULTI_GPU(BACKWARD_SOLVER_MULTI):
         self.world = dist.get_world_size(group)
 
     def _use_device_loop(self):
-        """The data-parallel solver runs the host-array outer loop (its
-        gradient exchange works on host arrays)."""
-        return False
+        """Device-resident outer loop with the NCCL backend (the gradient is
+        all-reduced in device memory); the host-array loop with gloo."""
+        import torch.distributed as dist
+
+        return super()._use_device_loop() and dist.get_backend(self.group) == "nccl"
+
+    def _device_gradient(self, fs, fields_in, fields_meas, grad, n_sel):
+        """:66-116 on device arrays: this rank's share of the selected
+        illuminations, its gradient weighted by the share size, one sum
+        all-reduce of the gradient and one of the weighted error."""
+        import torch
+        import torch.distributed as dist
+
+        nF = fields_in.numel() // n_sel
+        a, b = shard_ranges(n_sel, self.world)[self.rank]
+        cnt = b - a
+        e = 0.0
+        if cnt > 0:
+            e = fs.gradient_device(fields_in[a * nF:b * nF], fields_meas[a * nF:b * nF], grad)
+            grad.mul_(float(cnt))
+        else:
+            grad.zero_()
+        dist.all_reduce(grad, op=dist.ReduceOp.SUM, group=self.group)
+        grad.div_(float(n_sel))
+        et = torch.tensor([e * cnt], dtype=torch.float64, device=grad.device)
+        dist.all_reduce(et, op=dist.ReduceOp.SUM, group=self.group)
+        return float(et.item()) / n_sel
 
     def local_gradient(self, RI, input_field, output_field):
         """Gradient and error of one share (get_gradiant_static); None for an
