@@ -429,6 +429,27 @@ def run_bpm(args):
                          "cores": os.cpu_count(), "kind": "port", "sample": "2 illuminations"}}), flush=True)
 
 
+def run_setup(args):
+    """Solver construction time (Green's / refocusing kernels, pupils, device
+    plans) for the benchmark geometry (128^3 RI grid, 256^2 conv plane), with
+    the plane part of truncated_green_plus on the GPU and on the host; the
+    second construction of each is timed (the Hankel matrices of the radial
+    part are cached per geometry within a process)."""
+    from inverse_solver_b200 import FORWARD_SOLVER_CONVERGENT_BORN
+
+    p = workload_params()
+    out = {"metric": "solver construction time", "unit": "s", "higher_is_better": False,
+           "config": {"workload": "FORWARD_SOLVER_CONVERGENT_BORN constructor, 128^3 RI grid, 0.1 um voxels"}}
+    for dev in (True, False):
+        q = dict(p, green_on_device=dev)
+        FORWARD_SOLVER_CONVERGENT_BORN(q).delete()
+        t0 = time.perf_counter()
+        FORWARD_SOLVER_CONVERGENT_BORN(q).delete()
+        out["green_on_device" if dev else "green_on_host"] = time.perf_counter() - t0
+    out["value"] = out["green_on_device"]
+    print(json.dumps(out), flush=True)
+
+
 def workload_key():
     return "cbs_forward_128cube_49ill"
 
@@ -448,6 +469,8 @@ def main():
                     help="illuminations per step (profiling runs use fewer)")
     ap.add_argument("--profile-run", action="store_true",
                     help="only run --warmup solves (for ncu captures) and exit")
+    ap.add_argument("--setup", action="store_true",
+                    help="time the solver constructor (Green's kernels on the GPU vs the host)")
     ap.add_argument("--bpm", action="store_true",
                     help="time the beam-propagation forward solver")
     ap.add_argument("--fista", action="store_true",
@@ -464,6 +487,9 @@ def main():
         return
     if args.bpm:
         run_bpm(args)
+        return
+    if args.setup:
+        run_setup(args)
         return
     if world > 1:
         import datetime

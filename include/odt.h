@@ -254,6 +254,37 @@ odt_status odt_fista_prox_input(const odt_fista_args* args);
 odt_status odt_fista_update(const odt_fista_args* args);
 
 /*
+ * The plane part of truncated_green_plus (sub_code/truncated_green_plus.m
+ * :67-110) on the GPU: the band-limited radial profile [n_r, Nz] of the
+ * xy-truncated Green's function (or refocusing kernel) interpolated onto the
+ * oversized grid [S1, S2] per z with the host's bin_search_nearest maps
+ * (:111-129), then the reference's centred inverse 2D FFT / crop to
+ * out_size(1:2) / centred forward 2D FFT and the same along z, each chain
+ * applied as the linear map the caller passes: m1 [out_size(1), S1],
+ * m2 [out_size(2), S2], mz [out_size(3), Nz] (C_out * rows of C_S^-1, with C_n
+ * the centred DFT matrix), so that out(:,:,k) = sum_z mz(k,z) m1 G_z m2^T
+ * (three single-precision complex GEMMs; any lengths).  All arrays are host
+ * memory; synchronous.  Scratch comes from the stream-ordered allocator.
+ */
+typedef struct odt_green_args {
+  const odt_cfloat* radial;   /* [n_r, creation[2]]                           */
+  int32_t n_r;
+  const int32_t* near1;       /* [S1 * S2] 1-based bracketing profile samples  */
+  const int32_t* near2;
+  const float* w;             /* [S1 * S2] weight of near1                     */
+  int32_t creation[3];        /* S1, S2, Nz of the oversized grid              */
+  int32_t out_size[3];
+  float scale;                /* Nz / (res_x * res_y)                          */
+  const odt_cfloat* m1;       /* [out_size[0], S1]                             */
+  const odt_cfloat* m2;       /* [out_size[1], S2]                             */
+  const odt_cfloat* mz;       /* [out_size[2], Nz]                             */
+  odt_cfloat* out;            /* [out_size]                                    */
+  int32_t device;             /* CUDA device (-1: the current one)             */
+} odt_green_args;
+
+odt_status odt_green_planes(const odt_green_args* args);
+
+/*
  * Beam-propagation forward solver (FORWARD_SOLVER_BPM.m:44-117), scalar
  * fields, all illuminations marched through the slices together.  The
  * tables are set_RI's (:23-44) and DERIVE_OPTICAL_TOOL's single-precision

@@ -138,6 +138,24 @@ class FistaArgs(C.Structure):
     ]
 
 
+class GreenArgs(C.Structure):
+    _fields_ = [
+        ("radial", C.c_void_p),
+        ("n_r", C.c_int32),
+        ("near1", C.c_void_p),
+        ("near2", C.c_void_p),
+        ("w", C.c_void_p),
+        ("creation", C.c_int32 * 3),
+        ("out_size", C.c_int32 * 3),
+        ("scale", C.c_float),
+        ("m1", C.c_void_p),
+        ("m2", C.c_void_p),
+        ("mz", C.c_void_p),
+        ("out", C.c_void_p),
+        ("device", C.c_int32),
+    ]
+
+
 class BPMArgs(C.Structure):
     _fields_ = [
         ("size", C.c_int32 * 3),
@@ -246,6 +264,7 @@ SIGNATURES = {
     "odt_fista_prox_input": (C.c_int, [C.POINTER(FistaArgs)]),
     "odt_fista_update": (C.c_int, [C.POINTER(FistaArgs)]),
     "odt_bpm_solve": (C.c_int, [C.POINTER(BPMArgs)]),
+    "odt_green_planes": (C.c_int, [C.POINTER(GreenArgs)]),
     "odt_rytov": (C.c_int, [C.POINTER(RytovArgs)]),
     "odt_unwrap_goldstein": (C.c_int, [C.POINTER(UnwrapArgs)]),
     "odt_last_error": (C.c_char_p, []),

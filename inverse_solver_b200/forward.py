@@ -20,7 +20,7 @@ import numpy as np
 from . import _lib
 from .optics import (C64, F32, OpticalTool, basic_optical_parameter, centered_fft2,
                      centered_fftn, mround, polarisation_basis, potential2ri, ri2potential,
-                     truncated_green_plus, update_struct)
+                     green_plane_maps, truncated_green_plus, truncated_green_radial, update_struct)
 
 
 def _f32(x):
@@ -84,10 +84,10 @@ class CBSHostSetup:
             ptg = copy.deepcopy(p)
             ptg["size"] = [p["size"][0] + self.expected_RI_size[0] + rc[0],
                            p["size"][1] + self.expected_RI_size[1] + rc[1], p["size"][2]]
-            ru = self._crop_shift(truncated_green_plus(ptg, True), rc)
+            ru = self._crop_shift(self._truncated_green(ptg, True), rc)
             ru = centered_fft2(centered_fftn(ru, inverse=True))
             ru = ru * (u.image_res[0] * u.image_res[1])
-            fsg = self._crop_shift(truncated_green_plus(ptg, False), rc)
+            fsg = self._crop_shift(self._truncated_green(ptg, False), rc)
             fsg = centered_fftn(fsg, inverse=True)
         self.refocusing_util = ru.astype(C64)
         self.kernel_trans = centered_fft2(np.conj(fsg)).astype(C64)   # :114
@@ -103,6 +103,10 @@ class CBSHostSetup:
         self.pupil_in, self.pupil_out = self._pupils()
         if self.vector:
             self.polarisation = polarisation_basis(self.field_size, p)
+
+    def _truncated_green(self, params, refocus_version):
+        """truncated_green_plus on the host (MATLAB single semantics)."""
+        return truncated_green_plus(params, refocus_version)
 
     @staticmethod
     def _crop_shift(a, rc):
@@ -250,6 +254,35 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
         self.lib = _lib.load()
         super().__init__(params)
         self._create_handle()
+
+    def _truncated_green(self, params, refocus_version):
+        """truncated_green_plus with its plane part (interpolation onto the
+        oversized grid, the centred 2D and z FFTs and crops: most of the
+        set-up time) on the GPU (odt_green_planes); the radial profile and the
+        interpolation maps come from the host.  The result equals the host
+        path's to single-precision rounding (the FFTs are the library's).
+        Parameter ``green_on_device=False`` keeps the host path."""
+        if not self.parameters.get("green_on_device", True):
+            return super()._truncated_green(params, refocus_version)
+        r = truncated_green_radial(params, refocus_version)
+        keep = [np.asfortranarray(np.asarray(r["green"], dtype=C64)),
+                np.asfortranarray(np.asarray(r["near"], dtype=np.int32)),
+                np.asfortranarray(np.asarray(r["near2"], dtype=np.int32)),
+                np.asfortranarray(np.asarray(r["w"], dtype=F32))]
+        keep += [np.asfortranarray(m) for m in green_plane_maps(r)]
+        out = np.empty(r["out_px"], dtype=C64, order="F")
+        a = _lib.GreenArgs()
+        a.radial = _lib.ptr(keep[0])
+        a.n_r = keep[0].shape[0]
+        a.near1, a.near2, a.w = _lib.ptr(keep[1]), _lib.ptr(keep[2]), _lib.ptr(keep[3])
+        a.creation[:] = r["creation"]
+        a.out_size[:] = r["out_px"]
+        a.scale = float(r["scale"])
+        a.m1, a.m2, a.mz = _lib.ptr(keep[4]), _lib.ptr(keep[5]), _lib.ptr(keep[6])
+        a.out = _lib.ptr(out)
+        a.device = int(self.parameters.get("used_gpu", 0))
+        _lib.check(self.lib.odt_green_planes(C.byref(a)))
+        return out
 
     def _create_handle(self):
         p = self.parameters

@@ -254,10 +254,12 @@ def _nearest_bins(value, grid):
     return near, near2, w
 
 
-def truncated_green_plus(params, refocus_version=False):
-    """xy-truncated free-space Green's function (or refocusing kernel) on the
-    [size(1), size(2), size(3)] grid, Fourier in xy and z
-    (sub_code/truncated_green_plus.m:1-110)."""
+def truncated_green_radial(params, refocus_version=False):
+    """The radial part of truncated_green_plus (sub_code/truncated_green_plus.m
+    :1-66 and bin_search_nearest :111-129): the band-limited radial profile
+    [samples, Nz] and the interpolation maps of the oversized xy grid.
+    Returns a dict (green, near, near2, w, creation [S1, S2, Nz], out_px,
+    scale)."""
     req = basic_optical_parameter()
     req.update(use_GPU=True, oversize_z=10, oversample_xy=20000, oversample_xy_fourier=2,
                simultanous_process=30)
@@ -295,21 +297,61 @@ def truncated_green_plus(params, refocus_version=False):
     band = (nk < 0.9) + (nk < 1) * (nk > 0.9) * (1 - nk) * 10
     green = hk.backward(img * band.astype(F32)[:, None])
     near, near2, w = _nearest_bins(u.coorxy, H)
+    return dict(green=green, near=near, near2=near2, w=w, creation=[S1, S2, Nz], out_px=out_px,
+                scale=Nz / (u.image_res[0] * u.image_res[1]), simultanous_process=params["simultanous_process"])
+
+
+def centred_dft_matrix(n, inverse=False):
+    """C[k, j] with C @ x = fftshift(fft(ifftshift(x))) (ifft with 1/n for
+    inverse), in double."""
+    c = n // 2
+    k = np.arange(n) - c
+    e = np.exp((2j if inverse else -2j) * math.pi * np.outer(k, k) / n)
+    return e / n if inverse else e
+
+
+def green_plane_maps(r):
+    """The linear maps of truncated_green_plus's plane part (:67-110) for the
+    GPU path: centred inverse DFT of the oversized length, crop to the output
+    length, centred forward DFT, per axis, as [out, S] complex64 matrices."""
+    S1, S2, Nz = r["creation"]
+    o = r["out_px"]
+    offs = [S1 // 2 - o[0] // 2, S2 // 2 - o[1] // 2, Nz // 2 - o[2] // 2]
+    maps = []
+    for n, m, r0 in zip((S1, S2, Nz), o, offs):
+        maps.append((centred_dft_matrix(m) @ centred_dft_matrix(n, inverse=True)[r0:r0 + m, :]).astype(C64))
+    return maps
+
+
+def truncated_green_planes(r):
+    """The plane part of truncated_green_plus (:67-110) on the host: the
+    radial profile interpolated onto the oversized xy grid per z, centred
+    inverse 2D FFT, crop to the output xy size, centred forward 2D FFT, then
+    the centred inverse z-FFT, crop to the output z size and forward z-FFT."""
+    green, near, near2, w = r["green"], r["near"], r["near2"], r["w"]
+    S1, S2, Nz = r["creation"]
+    out_px = r["out_px"]
     out = np.zeros((out_px[0], out_px[1], Nz), dtype=C64)
-    slices = list(range(1, Nz + 1, params["simultanous_process"]))
+    slices = list(range(1, Nz + 1, r["simultanous_process"]))
     if len(slices) == 1 or slices[-1] != Nz:
         slices.append(Nz)
-    scale = Nz / (u.image_res[0] * u.image_res[1])
     r0 = S1 // 2 - out_px[0] // 2
     r1 = S2 // 2 - out_px[1] // 2
     for a, b in zip(slices[:-1], slices[1:]):
         zi = np.arange(a - 1, b)
         g = green[:, zi]
         gs = g[near - 1, :] * w[:, :, None] + g[near2 - 1, :] * (1 - w)[:, :, None]
-        gs = centered_fft2(gs * scale, inverse=True)
+        gs = centered_fft2(gs * r["scale"], inverse=True)
         gs = centered_fft2(gs[r0:r0 + out_px[0], r1:r1 + out_px[1], :])
         out[:, :, zi] = gs
     out = centered_fft_axis(out, 2, inverse=True)
     z0 = Nz // 2 - out_px[2] // 2
     out = out[:, :, z0:z0 + out_px[2]]
     return centered_fft_axis(out, 2)
+
+
+def truncated_green_plus(params, refocus_version=False):
+    """xy-truncated free-space Green's function (or refocusing kernel) on the
+    [size(1), size(2), size(3)] grid, Fourier in xy and z
+    (sub_code/truncated_green_plus.m:1-110)."""
+    return truncated_green_planes(truncated_green_radial(params, refocus_version))
