@@ -158,6 +158,26 @@ odt_status odt_set_polarisation(odt_handle h, const float* radial, const float* 
 odt_status odt_set_potential(odt_handle h, const odt_potential_params* pp,
                              const odt_cfloat* V);
 
+/*
+ * Asynchronous solves for a host that serves requests (no counterpart in
+ * the reference, whose MEX calls are synchronous): odt_submit queues an
+ * odt_solve with these arguments on the handle's worker thread (created on
+ * the first submit) and returns a ticket at once; the buffers the arguments
+ * point to must stay valid and untouched until the ticket completes.  Jobs
+ * of one handle run in submission order, concurrently with the calling
+ * thread and with other handles' jobs.  odt_poll sets *done and, once the
+ * job has finished, *status to the solve's own status (its message becomes
+ * the polling thread's odt_last_error) and releases the ticket; odt_wait
+ * blocks until then.  odt_destroy lets queued jobs finish first.
+ * odt_budget: the bytes the handle holds on the device and its budget
+ * (odt_geometry.mem_budget; 0 = none).
+ */
+typedef uint64_t odt_ticket;
+odt_status odt_submit(odt_handle h, const odt_solve_args* args, odt_ticket* ticket);
+odt_status odt_poll(odt_handle h, odt_ticket ticket, int32_t* done, odt_status* status);
+odt_status odt_wait(odt_handle h, odt_ticket ticket, odt_status* status);
+odt_status odt_budget(odt_handle h, int64_t* held_bytes, int64_t* budget_bytes);
+
 /* Solve n_ill illuminations (CudaBorn action 4, main.cpp:175-210, plus the
  * MATLAB pre/post-processing of FORWARD_SOLVER_CONVERGENT_BORN.solve,
  * :397-520): fft2 + pupil_in, refocus into the volume, Born series, emitter

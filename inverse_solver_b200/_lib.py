@@ -265,6 +265,10 @@ SIGNATURES = {
     "odt_fista_update": (C.c_int, [C.POINTER(FistaArgs)]),
     "odt_bpm_solve": (C.c_int, [C.POINTER(BPMArgs)]),
     "odt_green_planes": (C.c_int, [C.POINTER(GreenArgs)]),
+    "odt_submit": (C.c_int, [C.c_uint32, C.POINTER(SolveArgs), C.POINTER(C.c_uint64)]),
+    "odt_poll": (C.c_int, [C.c_uint32, C.c_uint64, C.POINTER(C.c_int32), C.POINTER(C.c_int)]),
+    "odt_wait": (C.c_int, [C.c_uint32, C.c_uint64, C.POINTER(C.c_int)]),
+    "odt_budget": (C.c_int, [C.c_uint32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "odt_rytov": (C.c_int, [C.POINTER(RytovArgs)]),
     "odt_unwrap_goldstein": (C.c_int, [C.POINTER(UnwrapArgs)]),
     "odt_last_error": (C.c_char_p, []),

@@ -10,6 +10,8 @@
 //                       Einc and Fout [ri], and small 2D planes.
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
+#include <deque>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -18,6 +20,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/odt.h"
@@ -983,7 +986,158 @@ odt_status odt_gradient(odt_handle h, const odt_gradient_args* args) {
   });
 }
 
+}  // extern "C"
+
+namespace {
+// Asynchronous solves: one worker thread and a FIFO of jobs per handle that
+// has had one submitted.  A job is a copy of the caller's odt_solve_args;
+// the worker runs odt_solve on it and keeps the status and message until a
+// poll or wait reports them.
+struct Job {
+  odt_solve_args args;
+  bool done = false;
+  odt_status status = ODT_OK;
+  std::string message;
+};
+
+struct JobQueue {
+  std::mutex mu;
+  std::condition_variable cv;       // work arrived / stop
+  std::condition_variable done_cv;  // a job finished
+  std::deque<odt_ticket> pending;
+  std::map<odt_ticket, std::shared_ptr<Job>> jobs;
+  odt_ticket next = 1;
+  bool stop = false;
+  std::thread worker;
+};
+
+std::mutex g_qmu;
+std::map<odt_handle, std::shared_ptr<JobQueue>> g_queues;
+
+void run_jobs(odt_handle h, JobQueue* q) {
+  for (;;) {
+    std::shared_ptr<Job> job;
+    {
+      std::unique_lock<std::mutex> lk(q->mu);
+      q->cv.wait(lk, [&] { return q->stop || !q->pending.empty(); });
+      if (q->pending.empty()) return;   // stop requested and nothing left
+      job = q->jobs[q->pending.front()];
+      q->pending.pop_front();
+    }
+    const odt_status st = odt_solve(h, &job->args);
+    std::lock_guard<std::mutex> lk(q->mu);
+    job->status = st;
+    job->message = st == ODT_OK ? std::string() : std::string(odt_last_error());
+    job->done = true;
+    q->done_cv.notify_all();
+  }
+}
+
+std::shared_ptr<JobQueue> queue_of(odt_handle h, bool create) {
+  std::lock_guard<std::mutex> lk(g_qmu);
+  auto it = g_queues.find(h);
+  if (it != g_queues.end()) return it->second;
+  if (!create) return nullptr;
+  auto q = std::make_shared<JobQueue>();
+  q->worker = std::thread(run_jobs, h, q.get());
+  g_queues[h] = q;
+  return q;
+}
+
+// stop the handle's worker after the jobs it holds (called by odt_destroy)
+void drain_queue(odt_handle h) {
+  std::shared_ptr<JobQueue> q;
+  {
+    std::lock_guard<std::mutex> lk(g_qmu);
+    auto it = g_queues.find(h);
+    if (it == g_queues.end()) return;
+    q = it->second;
+    g_queues.erase(it);
+  }
+  {
+    std::lock_guard<std::mutex> lk(q->mu);
+    q->stop = true;
+  }
+  q->cv.notify_all();
+  if (q->worker.joinable()) q->worker.join();
+}
+
+// report a finished job to the calling thread and release it
+odt_status take_job(JobQueue& q, odt_ticket t, odt_status* status) {
+  auto it = q.jobs.find(t);
+  const std::shared_ptr<Job> job = it->second;
+  q.jobs.erase(it);
+  if (status) *status = job->status;
+  if (job->status != ODT_OK) set_last_error(job->message);
+  return ODT_OK;
+}
+}  // namespace
+
+extern "C" {
+
+odt_status odt_submit(odt_handle h, const odt_solve_args* args, odt_ticket* ticket) {
+  return guarded([&] {
+    lookup(h);
+    if (!args || !ticket) raise(ODT_ERR_INVALID_ARGUMENT, "odt_submit: NULL argument");
+    auto q = queue_of(h, true);
+    std::lock_guard<std::mutex> lk(q->mu);
+    auto job = std::make_shared<Job>();
+    job->args = *args;
+    const odt_ticket t = q->next++;
+    q->jobs[t] = job;
+    q->pending.push_back(t);
+    *ticket = t;
+    q->cv.notify_one();
+  });
+}
+
+odt_status odt_poll(odt_handle h, odt_ticket ticket, int32_t* done, odt_status* status) {
+  odt_status st = ODT_OK;
+  const odt_status g = guarded([&] {
+    lookup(h);
+    if (!done) raise(ODT_ERR_INVALID_ARGUMENT, "odt_poll: NULL done");
+    auto q = queue_of(h, false);
+    if (!q) raise(ODT_ERR_INVALID_ARGUMENT, "odt_poll: unknown ticket " + std::to_string(ticket));
+    std::lock_guard<std::mutex> lk(q->mu);
+    auto it = q->jobs.find(ticket);
+    if (it == q->jobs.end()) raise(ODT_ERR_INVALID_ARGUMENT, "odt_poll: unknown ticket " + std::to_string(ticket));
+    *done = it->second->done ? 1 : 0;
+    if (*done) st = take_job(*q, ticket, status);
+  });
+  return g != ODT_OK ? g : st;
+}
+
+odt_status odt_wait(odt_handle h, odt_ticket ticket, odt_status* status) {
+  odt_status st = ODT_OK;
+  const odt_status g = guarded([&] {
+    lookup(h);
+    auto q = queue_of(h, false);
+    if (!q) raise(ODT_ERR_INVALID_ARGUMENT, "odt_wait: unknown ticket " + std::to_string(ticket));
+    std::unique_lock<std::mutex> lk(q->mu);
+    if (q->jobs.find(ticket) == q->jobs.end())
+      raise(ODT_ERR_INVALID_ARGUMENT, "odt_wait: unknown ticket " + std::to_string(ticket));
+    // a poll in another thread may release the ticket meanwhile
+    q->done_cv.wait(lk, [&] {
+      auto it = q->jobs.find(ticket);
+      return it == q->jobs.end() || it->second->done;
+    });
+    if (q->jobs.find(ticket) == q->jobs.end())
+      raise(ODT_ERR_INVALID_ARGUMENT, "odt_wait: ticket " + std::to_string(ticket) + " released by another call");
+    st = take_job(*q, ticket, status);
+  });
+  return g != ODT_OK ? g : st;
+}
+
+odt_status odt_budget(odt_handle h, int64_t* held_bytes, int64_t* budget_bytes) {
+  return guarded([&] {
+    auto H = lookup(h);
+    if (held_bytes) *held_bytes = (int64_t)(H->static_bytes + H->batch_bytes);
+    if (budget_bytes) *budget_bytes = (int64_t)H->budget;
+  });
+}
+
 odt_status odt_destroy(odt_handle h) {
+  drain_queue(h);   // queued solves finish first
   return guarded([&] {
     std::shared_ptr<Handle> H;
     {

@@ -251,6 +251,7 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
     def __init__(self, params):
         """Constructor + CudaBorn action 0 (FORWARD_SOLVER_CONVERGENT_BORN_CUDA.m:18-41)."""
         self._handle = 0
+        self._jobs = {}
         self.lib = _lib.load()
         super().__init__(params)
         self._create_handle()
@@ -456,6 +457,11 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
             raise ValueError("Input field must be either a scalar or a 2D vector")
         if list(x.shape[:2]) != list(self.field_size):
             raise ValueError("input field must be %d x %d" % tuple(self.field_size))
+        a, keep, out = self._host_args(x)
+        _lib.check(self.lib.odt_solve(self._handle, C.byref(a)))
+        return out
+
+    def _host_args(self, x):
         n_ill = x.shape[3]
         xin = _c64(x)
         ft, fr, f3 = self._outputs(n_ill)
@@ -467,8 +473,48 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
         a.field3d = _lib.ptr(f3)
         a.memory = _lib.ODT_MEM_HOST
         a.stream = None
-        _lib.check(self.lib.odt_solve(self._handle, C.byref(a)))
-        return ft, fr, f3
+        return a, xin, (ft, fr, f3)
+
+    # ------------------------------------------------- asynchronous solves
+    def submit(self, input_field):
+        """odt_submit: queue the solve of input_field (as for solve) on the
+        handle's worker thread and return a ticket for poll / wait; the
+        buffers are held until the ticket is collected."""
+        x = np.asarray(input_field)
+        if x.ndim == 3:
+            x = x[:, :, :, None]
+        if x.ndim != 4 or list(x.shape[:2]) != list(self.field_size):
+            raise ValueError("input field must be [F_x, F_y, npol, n_ill]")
+        a, keep, out = self._host_args(x)
+        t = C.c_uint64(0)
+        _lib.check(self.lib.odt_submit(self._handle, C.byref(a), C.byref(t)))
+        self._jobs[t.value] = (a, keep, out)
+        return t.value
+
+    def poll(self, ticket):
+        """odt_poll: None while the solve runs, then its outputs (raises
+        OdtError if it failed)."""
+        done, st = C.c_int32(0), C.c_int(0)
+        _lib.check(self.lib.odt_poll(self._handle, C.c_uint64(ticket), C.byref(done), C.byref(st)))
+        if not done.value:
+            return None
+        _, _, out = self._jobs.pop(ticket)
+        _lib.check(st.value)
+        return out
+
+    def wait(self, ticket):
+        """odt_wait: block until the ticket's solve finishes; its outputs."""
+        st = C.c_int(0)
+        _lib.check(self.lib.odt_wait(self._handle, C.c_uint64(ticket), C.byref(st)))
+        _, _, out = self._jobs.pop(ticket)
+        _lib.check(st.value)
+        return out
+
+    def budget(self):
+        """odt_budget: (bytes held on the device, budget in bytes or 0)."""
+        held, bud = C.c_int64(0), C.c_int64(0)
+        _lib.check(self.lib.odt_budget(self._handle, C.byref(held), C.byref(bud)))
+        return held.value, bud.value
 
     def solve_device(self, fields_in, trans=None, ref=None, field3d=None, stream=None):
         """Device-resident solve: arguments are CUDA tensors (torch) whose memory
