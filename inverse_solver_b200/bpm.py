@@ -2,7 +2,8 @@
 library: the host computes set_RI's tables in MATLAB single semantics
 (:23-44) and the refocusing phases of solve (:93-95, :110-114); the slice
 loop, the 2D FFTs, the cosine correction (:58-63) and the optional 3D field
-run on the GPU (odt_bpm_solve)."""
+run on the GPU (odt_bpm_solve).  The tables are uploaded once per set_RI and
+each solve moves only its fields."""
 from __future__ import annotations
 
 import ctypes as C
@@ -12,14 +13,6 @@ import numpy as np
 
 from . import _lib
 from .optics import C64, F32, OpticalTool, basic_optical_parameter, update_struct
-
-
-def _f32(x):
-    return np.asfortranarray(np.asarray(x, dtype=F32))
-
-
-def _c64(x):
-    return np.asfortranarray(np.asarray(x, dtype=C64))
 
 
 class FORWARD_SOLVER_BPM:
@@ -55,6 +48,24 @@ class FORWARD_SOLVER_BPM:
         rk = np.asarray(u.refocusing_kernel, dtype=C64)
         self.refocus_kernel = np.fft.ifftshift((np.exp((rk * p["resolution"][2]).astype(C64)) * u.NA_circle)
                                                .astype(C64))
+        self._dev = None   # device copies of the tables, made by the first solve
+
+    def _device_tables(self):
+        """The RI-dependent tables and the slice-independent phases in device
+        memory (column-major), uploaded once per set_RI."""
+        import torch
+
+        if self._dev is None:
+            dev = torch.device("cuda", int(self.parameters.get("used_gpu", 0)))
+
+            def up(a, dt):
+                return torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=dt).ravel(order="F"))).to(dev)
+
+            pre, post = self._phases()
+            self._dev = dict(fm=up(self.field_multiplier, C64), rk=up(self.refocus_kernel, C64),
+                             fo=up(self.filter_out, F32), pre=up(pre, C64), post=up(post, C64),
+                             ct=up(self.utility.cos_theta, F32), device=dev)
+        return self._dev
 
     def _phases(self):
         p, u = self.parameters, self.utility
@@ -80,25 +91,30 @@ class FORWARD_SOLVER_BPM:
         n1, n2, nz = self.field_multiplier.shape
         if list(f.shape[:2]) != [n1, n2]:
             raise ValueError("input fields must be [size(1), size(2), 1, n]")
+        import torch
+
         nill = f.shape[3]
-        fin = _c64(f[:, :, 0, :])
-        trans = np.empty((n1, n2, nill), dtype=C64, order="F")
-        f3 = np.empty((n1, n2, nz, nill), dtype=C64, order="F") if p["return_3D"] else None
-        pre, post = self._phases()
-        keep = [_c64(self.field_multiplier), _c64(self.refocus_kernel), _f32(self.filter_out), _c64(pre),
-                _c64(post), _f32(self.utility.cos_theta)]
+        d = self._device_tables()
+        dev = d["device"]
+        fin = torch.from_numpy(np.ascontiguousarray(np.asarray(f[:, :, 0, :], dtype=C64).transpose(2, 1, 0))).to(dev)
+        trans_d = torch.empty_like(fin)
+        f3_d = torch.empty((nill, nz, n2, n1), dtype=torch.complex64, device=dev) if p["return_3D"] else None
         a = _lib.BPMArgs()
         a.size[:] = [n1, n2, nz]
-        a.field_multiplier, a.refocus_kernel, a.filter_out = (_lib.ptr(k) for k in keep[:3])
-        a.pre, a.post = _lib.ptr(keep[3]), _lib.ptr(keep[4])
-        a.cos_theta = _lib.ptr(keep[5]) if p["cos_correction"] else None
-        a.fields_in = _lib.ptr(fin)
+        a.field_multiplier, a.refocus_kernel = d["fm"].data_ptr(), d["rk"].data_ptr()
+        a.filter_out = d["fo"].data_ptr()
+        a.pre, a.post = d["pre"].data_ptr(), d["post"].data_ptr()
+        a.cos_theta = d["ct"].data_ptr() if p["cos_correction"] else None
+        a.fields_in = fin.data_ptr()
         a.n_ill = nill
-        a.trans = _lib.ptr(trans)
-        a.field3d = _lib.ptr(f3) if f3 is not None else None
-        a.memory = _lib.ODT_MEM_HOST
-        a.stream = None
+        a.trans = trans_d.data_ptr()
+        a.field3d = f3_d.data_ptr() if f3_d is not None else None
+        a.memory = _lib.ODT_MEM_DEVICE
+        s = torch.cuda.current_stream(dev)
+        a.stream = s.cuda_stream
         _lib.check(self.lib.odt_bpm_solve(C.byref(a)))
+        trans = trans_d.cpu().numpy().transpose(2, 1, 0)
+        f3 = f3_d.cpu().numpy().transpose(3, 2, 1, 0) if f3_d is not None else None
         fields_trans = trans[:, :, None, :]
         fields_ref = np.ones(fields_trans.shape, dtype=C64) if p["return_reflection"] else None
         fields_3D = f3[:, :, :, None, :] if f3 is not None else None
