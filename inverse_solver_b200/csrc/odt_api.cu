@@ -1011,8 +1011,17 @@ struct JobQueue {
   std::thread worker;
 };
 
-std::mutex g_qmu;
-std::map<odt_handle, std::shared_ptr<JobQueue>> g_queues;
+// The registry is never destroyed: a host that exits without odt_destroy
+// leaves an idle worker blocked on its condition variable, which the process
+// exit ends; destroying a joinable std::thread at exit would abort instead.
+struct QueueRegistry {
+  std::mutex mu;
+  std::map<odt_handle, std::shared_ptr<JobQueue>> queues;
+};
+QueueRegistry& registry() {
+  static QueueRegistry* r = new QueueRegistry();
+  return *r;
+}
 
 void run_jobs(odt_handle h, JobQueue* q) {
   for (;;) {
@@ -1034,13 +1043,14 @@ void run_jobs(odt_handle h, JobQueue* q) {
 }
 
 std::shared_ptr<JobQueue> queue_of(odt_handle h, bool create) {
-  std::lock_guard<std::mutex> lk(g_qmu);
-  auto it = g_queues.find(h);
-  if (it != g_queues.end()) return it->second;
+  QueueRegistry& R = registry();
+  std::lock_guard<std::mutex> lk(R.mu);
+  auto it = R.queues.find(h);
+  if (it != R.queues.end()) return it->second;
   if (!create) return nullptr;
   auto q = std::make_shared<JobQueue>();
   q->worker = std::thread(run_jobs, h, q.get());
-  g_queues[h] = q;
+  R.queues[h] = q;
   return q;
 }
 
@@ -1048,11 +1058,12 @@ std::shared_ptr<JobQueue> queue_of(odt_handle h, bool create) {
 void drain_queue(odt_handle h) {
   std::shared_ptr<JobQueue> q;
   {
-    std::lock_guard<std::mutex> lk(g_qmu);
-    auto it = g_queues.find(h);
-    if (it == g_queues.end()) return;
+    QueueRegistry& R = registry();
+    std::lock_guard<std::mutex> lk(R.mu);
+    auto it = R.queues.find(h);
+    if (it == R.queues.end()) return;
     q = it->second;
-    g_queues.erase(it);
+    R.queues.erase(it);
   }
   {
     std::lock_guard<std::mutex> lk(q->mu);
