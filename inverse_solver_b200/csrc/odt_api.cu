@@ -1048,10 +1048,27 @@ std::shared_ptr<JobQueue> queue_of(odt_handle h, bool create) {
   auto it = R.queues.find(h);
   if (it != R.queues.end()) return it->second;
   if (!create) return nullptr;
+  // registered after the handle table exists, so it runs before that table
+  // is destroyed at exit
+  static const bool at_exit = (std::atexit(drain_all_queues), true);
+  (void)at_exit;
   auto q = std::make_shared<JobQueue>();
   q->worker = std::thread(run_jobs, h, q.get());
   R.queues[h] = q;
   return q;
+}
+
+void drain_queue(odt_handle h);
+
+// at exit, before the handles are destroyed: let every queue finish its jobs
+void drain_all_queues() {
+  std::vector<odt_handle> hs;
+  {
+    QueueRegistry& R = registry();
+    std::lock_guard<std::mutex> lk(R.mu);
+    for (const auto& kv : R.queues) hs.push_back(kv.first);
+  }
+  for (odt_handle h : hs) drain_queue(h);
 }
 
 // stop the handle's worker after the jobs it holds (called by odt_destroy)
