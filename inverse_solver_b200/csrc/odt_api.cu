@@ -1042,6 +1042,8 @@ void run_jobs(odt_handle h, JobQueue* q) {
   }
 }
 
+void drain_all_queues();
+
 std::shared_ptr<JobQueue> queue_of(odt_handle h, bool create) {
   QueueRegistry& R = registry();
   std::lock_guard<std::mutex> lk(R.mu);
