@@ -450,6 +450,51 @@ def run_setup(args):
     print(json.dumps(out), flush=True)
 
 
+def run_retrieval(args):
+    """Field retrieval workload (FIELD_EXPERIMENTAL_RETRIEVAL.get_fields):
+    holograms per second for background / sample stacks of 49 synthetic
+    off-axis holograms of 1024 x 1024 pixels (camera pixel 0.0625 um, output
+    pixel 0.1 um: 640 x 640 spectra, 636 x 636 fields), the whole call
+    through the host API (hologram upload, GPU transforms and unwrapping,
+    host per-image steps, field download); beside it the oracle with its
+    Goldstein restatement on the host for 2 holograms."""
+    import sys as _sys
+
+    _sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import cases
+
+    from inverse_solver_b200.retrieval import FIELD_EXPERIMENTAL_RETRIEVAL
+    from oracle import goldstein, retrieval
+
+    N, n = 1024, args.n_ill
+    bg, sp, _ = cases.off_axis_holograms(N, n, seed=SEED)
+    p = FIELD_EXPERIMENTAL_RETRIEVAL.get_default_parameters(dict(
+        size=[N, N, 64], resolution=[0.1, 0.1, 0.1], resolution_image=[0.0625, 0.0625], NA=1.2,
+        wavelength=0.532, RI_bg=1.3355))
+    r = FIELD_EXPERIMENTAL_RETRIEVAL(p)
+    for _ in range(args.warmup):
+        r.get_fields(bg, sp)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r.get_fields(bg, sp)
+    dt = (time.perf_counter() - t0) / args.steps
+
+    def unwrap(ph):
+        out = goldstein.unwrapp2(ph)
+        return np.asarray(out[0] if isinstance(out, tuple) else out, dtype=np.float32)
+
+    t0 = time.perf_counter()
+    retrieval.get_fields(p, bg[:, :, :2], sp[:, :, :2], unwrap=unwrap)
+    dtc = time.perf_counter() - t0
+    print(json.dumps({
+        "metric": "holograms/s", "value": n / dt, "unit": "holograms/s", "higher_is_better": True,
+        "ms_per_stack": dt * 1e3, "steps": args.steps, "warmup": args.warmup,
+        "config": {"workload": "FIELD_EXPERIMENTAL_RETRIEVAL.get_fields: %d background / sample off-axis "
+                               "holograms of %d x %d, 0.0625 um camera pixel, 0.1 um output" % (n, N, N)},
+        "cpu_baseline": {"value": 2 / dtc, "unit": "holograms/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": "2 holograms"}}), flush=True)
+
+
 def workload_key():
     return "cbs_forward_128cube_49ill"
 
@@ -469,6 +514,8 @@ def main():
                     help="illuminations per step (profiling runs use fewer)")
     ap.add_argument("--profile-run", action="store_true",
                     help="only run --warmup solves (for ncu captures) and exit")
+    ap.add_argument("--retrieval", action="store_true",
+                    help="time the field retrieval from off-axis holograms")
     ap.add_argument("--setup", action="store_true",
                     help="time the solver constructor (Green's kernels on the GPU vs the host)")
     ap.add_argument("--bpm", action="store_true",
@@ -490,6 +537,9 @@ def main():
         return
     if args.setup:
         run_setup(args)
+        return
+    if args.retrieval:
+        run_retrieval(args)
         return
     if world > 1:
         import datetime

@@ -305,6 +305,52 @@ typedef struct odt_green_args {
 odt_status odt_green_planes(const odt_green_args* args);
 
 /*
+ * Field retrieval from off-axis holograms, the transform part of get_fields
+ * (FIELD_EXPERIMENTAL_RETRIEVAL.m:110-178): centred 2D FFT of each background
+ * and sample hologram; the sideband = the first maximum of |F_bg(:,:,1)|
+ * outside the deleted bands (rows round(N cutout):N, and columns
+ * round(N cutout):N or, with other_corner, 1:round(N (1 - cutout))),
+ * returned 1-based in sideband[2]; the spectra re-centred on it, cropped
+ * (crop > 0: source rows / columns crop .. crop+M-1) or zero-padded
+ * (crop < 0) to out_size M, times na_circle [M, M] (uint8, centred); for
+ * each image the first maximum of |F_bg| and |F_bg| at its four neighbours
+ * (peaks [7, n]: i1, i2 1-based, the peak, (i1-1,i2), (i1+1,i2), (i1,i2-1),
+ * (i1,i2+1); 0 outside); and the centred inverse 2D FFTs cropped by two
+ * pixels on every side into bg_field / sp_field [M-4, M-4, n].  sideband is
+ * a host pointer in both memory modes.  Synchronous.
+ */
+typedef struct odt_hologram_args {
+  int32_t size[3];          /* [N, N, n] hologram stacks                      */
+  const float* bg;
+  const float* sp;
+  double cutout_portion;
+  int32_t other_corner;
+  int32_t out_size;         /* M                                              */
+  int32_t crop;             /* crop size (> 0) or minus the padding (< 0)     */
+  const uint8_t* na_circle; /* [M, M]                                         */
+  odt_cfloat* bg_field;     /* [M-4, M-4, n]                                  */
+  odt_cfloat* sp_field;
+  float* peaks;             /* [7, n]                                         */
+  int32_t* sideband;        /* [2], host                                      */
+  int32_t memory;
+  void* stream;
+} odt_hologram_args;
+
+odt_status odt_hologram_fields(const odt_hologram_args* args);
+
+/* refocus (FIELD_EXPERIMENTAL_RETRIEVAL.m:392-394): out = centred inverse 2D
+ * FFT of (centred 2D FFT of each field plane .* kernel), kernel =
+ * exp(z .* refocusing_kernel) [size(1), size(2)]; host arrays, synchronous. */
+typedef struct odt_refocus_args {
+  int32_t size[3];          /* [N1, N2, n]                                    */
+  const odt_cfloat* field;
+  const odt_cfloat* kernel;
+  odt_cfloat* out;
+} odt_refocus_args;
+
+odt_status odt_refocus_2d(const odt_refocus_args* args);
+
+/*
  * Beam-propagation forward solver (FORWARD_SOLVER_BPM.m:44-117), scalar
  * fields, all illuminations marched through the slices together.  The
  * tables are set_RI's (:23-44) and DERIVE_OPTICAL_TOOL's single-precision

@@ -138,6 +138,34 @@ class FistaArgs(C.Structure):
     ]
 
 
+class HologramArgs(C.Structure):
+    _fields_ = [
+        ("size", C.c_int32 * 3),
+        ("bg", C.c_void_p),
+        ("sp", C.c_void_p),
+        ("cutout_portion", C.c_double),
+        ("other_corner", C.c_int32),
+        ("out_size", C.c_int32),
+        ("crop", C.c_int32),
+        ("na_circle", C.c_void_p),
+        ("bg_field", C.c_void_p),
+        ("sp_field", C.c_void_p),
+        ("peaks", C.c_void_p),
+        ("sideband", C.c_void_p),
+        ("memory", C.c_int32),
+        ("stream", C.c_void_p),
+    ]
+
+
+class RefocusArgs(C.Structure):
+    _fields_ = [
+        ("size", C.c_int32 * 3),
+        ("field", C.c_void_p),
+        ("kernel", C.c_void_p),
+        ("out", C.c_void_p),
+    ]
+
+
 class GreenArgs(C.Structure):
     _fields_ = [
         ("radial", C.c_void_p),
@@ -265,6 +293,8 @@ SIGNATURES = {
     "odt_fista_update": (C.c_int, [C.POINTER(FistaArgs)]),
     "odt_bpm_solve": (C.c_int, [C.POINTER(BPMArgs)]),
     "odt_green_planes": (C.c_int, [C.POINTER(GreenArgs)]),
+    "odt_hologram_fields": (C.c_int, [C.POINTER(HologramArgs)]),
+    "odt_refocus_2d": (C.c_int, [C.POINTER(RefocusArgs)]),
     "odt_submit": (C.c_int, [C.c_uint32, C.POINTER(SolveArgs), C.POINTER(C.c_uint64)]),
     "odt_poll": (C.c_int, [C.c_uint32, C.c_uint64, C.POINTER(C.c_int32), C.POINTER(C.c_int)]),
     "odt_wait": (C.c_int, [C.c_uint32, C.c_uint64, C.POINTER(C.c_int)]),

@@ -1,0 +1,197 @@
+"""Field retrieval from off-axis holograms (Codes/FIELD_EXPERIMENTAL_RETRIEVAL.m)
+on the B200 library: the transforms of get_fields (centred FFTs of the
+background and sample holograms, the sideband search and re-centring, the
+resolution crop / pad, the NA circle, the inverse transforms) run on the GPU
+(odt_hologram_fields), phase unwrapping on the GPU (unwrapp2_gpu); the
+per-image scalar steps (sub-pixel peak positions, normalisation, the border
+plane fit of PhiShiftMS) are host code in MATLAB single semantics.  The
+interactive branches of the reference (the "rectangle" ROI picker,
+PhiShiftMS's hand-drawn masks) are not mirrored: ROI is numeric or absent.
+"""
+from __future__ import annotations
+
+import copy
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from .optics import C64, F32, OpticalTool, basic_optical_parameter, mround, update_struct
+
+
+def load_tiff(fname, num_images=None):
+    """loadTIFF (FIELD_EXPERIMENTAL_RETRIEVAL.m:451-466): the pages of a TIFF
+    file as a single-precision stack [rows, cols, pages] (squeezed to 2D for
+    one page)."""
+    from PIL import Image
+
+    img = Image.open(fname)
+    n = getattr(img, "n_frames", 1) if num_images is None else int(num_images)
+    pages = []
+    for k in range(n):
+        img.seek(k)
+        pages.append(np.asarray(img, dtype=F32))
+    out = np.stack(pages, axis=2)
+    return out[:, :, 0] if n == 1 else out
+
+
+def _subpixel(pk, M):
+    """peak_subpixel_positioner.m:1-67 on the peak data of one image (i1, i2
+    1-based, |F| at the peak and at its neighbours along each axis): the
+    position relative to the centre floor(M/2)+1 plus the neighbour-ratio
+    refinement, in single precision."""
+    i1, i2, v0, a1, b1, a2, b2 = (F32(x) for x in pk)
+    centre = M // 2 + 1
+
+    def refine(lo, hi):
+        nb, sgn = (lo, -1) if lo >= hi else (hi, 1)   # max([lo, hi]): the first on ties
+        d = np.array([nb / (nb + v0), nb / (nb - v0)], dtype=F32)
+        d[np.abs(d) > 1] = 0
+        return F32(sgn * d.max())
+
+    return F32(F32(i1 - centre) + refine(a1, b1)), F32(F32(i2 - centre) + refine(a2, b2))
+
+
+def _omit_outliers(v):
+    lst = v[v != 0].astype(np.float64)
+    p25, p75 = np.percentile(lst, [25, 75], method="hazen")        # MATLAB prctile
+    lo, hi = p25 - 1.5 * (p75 - p25), p75 + 1.5 * (p75 - p25)
+    out = v.copy()
+    out[(out < lo) | (out > hi)] = 0
+    return out
+
+
+def phi_shift_ms(p2, bsize=8):
+    """PhiShiftMS(p2, 1, 1) (sub_code/PhiShiftMS.m, D2_LSAms with n = 1 and
+    omit_outliers): a + b x + c y fitted by least squares to the border of
+    width bsize - 1 (outliers and exact zeros left out) and subtracted.  A'A
+    in double, A'p and the solve in single, as MATLAB evaluates them."""
+    imY, imX = p2.shape
+    mask = np.ones((imY, imX), F32)
+    mask[bsize - 1:imY - bsize + 1, bsize - 1:imX - bsize + 1] = 0
+    XX, YY = np.meshgrid(np.arange(1, imX + 1, dtype=np.float64), np.arange(1, imY + 1, dtype=np.float64))
+    v = _omit_outliers((p2 * mask).astype(F32).ravel(order="F"))
+    keep = v != 0
+    A = np.stack([XX.ravel(order="F")[keep], YY.ravel(order="F")[keep], np.ones(int(keep.sum()))], axis=1)
+    coef = np.linalg.solve((A.T @ A).astype(F32), (A.astype(F32).T @ v[keep]).astype(F32)).astype(F32)
+    g = (p2 - coef[2]).astype(F32)
+    g = (g - coef[0] * XX.astype(F32)).astype(F32)
+    return (g - coef[1] * YY.astype(F32)).astype(F32)
+
+
+class FIELD_EXPERIMENTAL_RETRIEVAL:
+    """Codes/FIELD_EXPERIMENTAL_RETRIEVAL.m: complex fields from off-axis
+    background / sample hologram pairs."""
+
+    @staticmethod
+    def get_default_parameters(init_params=None):
+        """:8-22."""
+        p = basic_optical_parameter()
+        p.update(resolution_image=[0.1, 0.1], use_abbe_correction=True, cutout_portion=1 / 3,
+                 other_corner=False, conjugate_field=False, use_GPU=True)
+        return update_struct(p, init_params) if init_params else p
+
+    def __init__(self, params):
+        self.parameters = copy.deepcopy(params)
+        self.utility = None
+        self.lib = _lib.load()
+
+    def get_fields(self, bg_file, sp_file, ROI=None):
+        """:27-229 (numeric ROI [r0 r1 c0 c1], 1-based inclusive, or None):
+        returns (input_field, output_field, updated_optical_parameters, k0s,
+        is_overexposed, ROI); the holograms are TIFF file names or arrays
+        [N, N(, n)]."""
+        from .unwrap import unwrapp2_gpu
+
+        p = self.parameters
+        bg = load_tiff(bg_file) if isinstance(bg_file, str) else np.asarray(bg_file, dtype=F32)
+        sp = load_tiff(sp_file) if isinstance(sp_file, str) else np.asarray(sp_file, dtype=F32)
+        if bg.shape != sp.shape:
+            raise ValueError("Background and sample field must be of same size")
+        if bg.shape[0] != bg.shape[1]:
+            raise ValueError("the image must be a square")
+        if p["resolution_image"][0] != p["resolution_image"][1]:
+            raise ValueError("please enter an isotropic resolution for the image")
+        if p["resolution"][0] != p["resolution"][1]:
+            raise ValueError("please enter an isotropic resolution for the output image")
+        if ROI is not None:
+            if isinstance(ROI, str):
+                raise ValueError("the interactive ROI picker is not available; give [r0 r1 c0 c1]")
+            bg = bg[ROI[0] - 1:ROI[1], ROI[2] - 1:ROI[3]]
+            sp = sp[ROI[0] - 1:ROI[1], ROI[2] - 1:ROI[3]]
+        if bg.ndim == 2:
+            bg, sp = bg[:, :, None], sp[:, :, None]
+        if bg.shape[0] != bg.shape[1]:
+            raise ValueError("the image must be a square")
+        over = np.maximum(bg, sp).max(axis=(0, 1)) > 254
+        N, nimg = bg.shape[0], bg.shape[2]
+        # resolution matching (:131-145)
+        ratio = p["resolution"][0] / p["resolution_image"][0]
+        if ratio >= 1:
+            d = int(mround(0.5 * (N - N / ratio)))
+            M = N - 2 * d
+        else:
+            pad = -int(mround(0.5 * (N - N / ratio)))
+            d, M = -pad, N + 2 * pad
+        p["resolution"] = list(p["resolution"])
+        p["resolution"][0] = p["resolution_image"][0] * N / M
+        p["resolution"][1] = p["resolution_image"][1] * N / M
+        p["size"] = list(p["size"])
+        p["size"][0], p["size"][1] = M, M
+        na = np.asfortranarray(OpticalTool(p).NA_circle.astype(np.uint8))
+        hb = np.asfortranarray(bg, dtype=F32)
+        hs = np.asfortranarray(sp, dtype=F32)
+        bgf = np.empty((M - 4, M - 4, nimg), dtype=C64, order="F")
+        spf = np.empty_like(bgf)
+        peaks = np.empty((7, nimg), dtype=F32, order="F")
+        side = np.zeros(2, dtype=np.int32)
+        a = _lib.HologramArgs()
+        a.size[:] = [N, N, nimg]
+        a.bg, a.sp = _lib.ptr(hb), _lib.ptr(hs)
+        a.cutout_portion = float(p["cutout_portion"])
+        a.other_corner = 1 if p["other_corner"] else 0
+        a.out_size, a.crop = M, d
+        a.na_circle = _lib.ptr(na)
+        a.bg_field, a.sp_field = _lib.ptr(bgf), _lib.ptr(spf)
+        a.peaks, a.sideband = _lib.ptr(peaks), _lib.ptr(side)
+        a.memory = _lib.ODT_MEM_HOST
+        a.stream = None
+        _lib.check(self.lib.odt_hologram_fields(C.byref(a)))
+        k0s = np.zeros((2, nimg), dtype=F32)
+        for jj in range(nimg):
+            k0s[0, jj], k0s[1, jj] = _subpixel(peaks[:, jj], M)
+        # normalisation, phase, unwrapping, ramp removal (:179-204)
+        p["size"][0], p["size"][1] = M - 4, M - 4
+        amean = (np.abs(bgf).sum(axis=(0, 1)) / ((M - 4) * (M - 4))).astype(F32)
+        bgf = (bgf / amean).astype(C64)
+        spf = (spf / amean).astype(C64)
+        if p["conjugate_field"]:
+            bgf, spf = np.conj(bgf), np.conj(spf)
+        q = (spf / bgf).astype(C64)
+        phase = np.asarray(unwrapp2_gpu(np.ascontiguousarray(np.angle(q).astype(F32))), dtype=F32)
+        amp = np.abs(q).astype(F32)
+        for jj in range(nimg):
+            phase[:, :, jj] = phi_shift_ms(phase[:, :, jj])
+        spf = (amp * bgf * np.exp(1j * phase).astype(C64)).astype(C64)
+        self.utility = OpticalTool(p)
+        base = basic_optical_parameter()
+        updated = {k: copy.deepcopy(p[k]) for k in base}
+        return bgf[:, :, None, :], spf[:, :, None, :], updated, k0s, over, ROI
+
+    def refocus(self, field_trans, z):
+        """:392-394 on the GPU (odt_refocus_2d), with the utility of the last
+        get_fields (or of the parameters)."""
+        u = self.utility if self.utility is not None else OpticalTool(self.parameters)
+        f = np.asarray(field_trans, dtype=C64)
+        shape = f.shape
+        f = np.asfortranarray(f.reshape(shape[0], shape[1], -1, order="F"))
+        k = np.asfortranarray(np.exp(z * np.asarray(u.refocusing_kernel)).astype(C64))
+        if k.shape != shape[:2]:
+            raise ValueError("field and optical grid sizes differ")
+        out = np.empty_like(f, order="F")
+        a = _lib.RefocusArgs()
+        a.size[:] = [shape[0], shape[1], f.shape[2]]
+        a.field, a.kernel, a.out = _lib.ptr(f), _lib.ptr(k), _lib.ptr(out)
+        _lib.check(self.lib.odt_refocus_2d(C.byref(a)))
+        return out.reshape(shape, order="F")

@@ -71,3 +71,25 @@ def wrapped_phase(shape, seed, noise=0.6, amp=25.0):
         phi = amp * np.exp(-((x - c[0]) ** 2 + (y - c[1]) ** 2) / 0.2) + rng.normal(0, noise, (N1, N2))
         out[:, :, z] = np.angle(np.exp(1j * phi)).astype(np.float32)
     return out
+
+
+def off_axis_holograms(N=128, n=3, seed=0, carrier=(-0.23, -0.27), noise=0.0, phase_amp=2.5):
+    """Synthetic off-axis hologram stacks [N, N, n] (single): |R + U|^2 with
+    a tilted reference R (carrier in cycles per pixel, placing the sideband
+    in the search window of the retrieval) and object waves U: small random
+    tilts for the background, the same waves times amp * exp(i phi) (a
+    Gaussian phase bump of `phase_amp` rad and a 20 % absorption dip) for the
+    sample; scaled to an 8-bit-like range.  Returns (bg, sp, phi)."""
+    rng = np.random.default_rng(seed)
+    y, x = np.meshgrid(np.arange(N), np.arange(N), indexing="ij")
+    R = np.exp(2j * np.pi * (carrier[0] * y + carrier[1] * x))
+    r2 = ((y - N / 2) ** 2 + (x - N / 2) ** 2) / (N / 6) ** 2
+    phi = phase_amp * np.exp(-r2)
+    amp = 1 - 0.2 * np.exp(-r2)
+    bg, sp = [], []
+    for _ in range(n):
+        t = rng.uniform(-0.02, 0.02, 2)
+        U = 0.8 * np.exp(2j * np.pi * (t[0] * y + t[1] * x))
+        bg.append(np.abs(R + U) ** 2 * 60 + noise * rng.standard_normal((N, N)))
+        sp.append(np.abs(R + U * amp * np.exp(1j * phi)) ** 2 * 60 + noise * rng.standard_normal((N, N)))
+    return np.stack(bg, 2).astype(np.float32), np.stack(sp, 2).astype(np.float32), phi
