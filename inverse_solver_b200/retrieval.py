@@ -62,22 +62,39 @@ def _omit_outliers(v):
     return out
 
 
+_BORDER = {}
+
+
+def _border(imY, imX, bsize):
+    """Column-major indices of the border of width bsize - 1 (PhiShiftMS's
+    mask) with their x / y coordinates, and the full coordinate grids, per
+    image shape."""
+    key = (imY, imX, bsize)
+    if key not in _BORDER:
+        mask = np.ones((imY, imX), bool)
+        mask[bsize - 1:imY - bsize + 1, bsize - 1:imX - bsize + 1] = False
+        idx = np.flatnonzero(mask.ravel(order="F"))
+        XX, YY = np.meshgrid(np.arange(1, imX + 1, dtype=np.float64), np.arange(1, imY + 1, dtype=np.float64))
+        _BORDER[key] = (idx, XX.ravel(order="F")[idx], YY.ravel(order="F")[idx], XX.astype(F32),
+                        YY.astype(F32))
+    return _BORDER[key]
+
+
 def phi_shift_ms(p2, bsize=8):
     """PhiShiftMS(p2, 1, 1) (sub_code/PhiShiftMS.m, D2_LSAms with n = 1 and
     omit_outliers): a + b x + c y fitted by least squares to the border of
     width bsize - 1 (outliers and exact zeros left out) and subtracted.  A'A
-    in double, A'p and the solve in single, as MATLAB evaluates them."""
+    in double, A'p and the solve in single, as MATLAB evaluates them; only
+    the border pixels are visited, in the reference's column-major order."""
     imY, imX = p2.shape
-    mask = np.ones((imY, imX), F32)
-    mask[bsize - 1:imY - bsize + 1, bsize - 1:imX - bsize + 1] = 0
-    XX, YY = np.meshgrid(np.arange(1, imX + 1, dtype=np.float64), np.arange(1, imY + 1, dtype=np.float64))
-    v = _omit_outliers((p2 * mask).astype(F32).ravel(order="F"))
+    idx, bx, by, XX, YY = _border(imY, imX, bsize)
+    v = _omit_outliers(np.asarray(p2, dtype=F32).ravel(order="F")[idx])
     keep = v != 0
-    A = np.stack([XX.ravel(order="F")[keep], YY.ravel(order="F")[keep], np.ones(int(keep.sum()))], axis=1)
+    A = np.stack([bx[keep], by[keep], np.ones(int(keep.sum()))], axis=1)
     coef = np.linalg.solve((A.T @ A).astype(F32), (A.astype(F32).T @ v[keep]).astype(F32)).astype(F32)
     g = (p2 - coef[2]).astype(F32)
-    g = (g - coef[0] * XX.astype(F32)).astype(F32)
-    return (g - coef[1] * YY.astype(F32)).astype(F32)
+    g = (g - coef[0] * XX).astype(F32)
+    return (g - coef[1] * YY).astype(F32)
 
 
 class FIELD_EXPERIMENTAL_RETRIEVAL:
