@@ -338,6 +338,37 @@ typedef struct odt_hologram_args {
 
 odt_status odt_hologram_fields(const odt_hologram_args* args);
 
+/* The per-pixel steps of get_fields after the transforms (:179-201), on
+ * device arrays of n planes [size[0], size[1]], ordered on `stream`:
+ * odt_hologram_phase: amean = sum |bg| / plane per image, bg and sp divided
+ *   by it (and conjugated with conjugate = 1), phase = angle(sp ./ bg) and
+ *   amp = abs(sp ./ bg) (float);
+ * odt_hologram_combine: sp = amp .* bg .* exp(1i (phase - c0 - c1 x - c2 y))
+ *   with coef [3, n] = (c0, c1, c2) per image (PhiShiftMS's ramp, x / y the
+ *   1-based column / row). */
+typedef struct odt_hologram_phase_args {
+  int32_t size[3];
+  odt_cfloat* bg;
+  odt_cfloat* sp;
+  int32_t conjugate;
+  float* phase;
+  float* amp;
+  void* stream;
+} odt_hologram_phase_args;
+
+typedef struct odt_hologram_combine_args {
+  int32_t size[3];
+  const odt_cfloat* bg;
+  const float* amp;
+  const float* phase;
+  const float* coef;
+  odt_cfloat* sp;
+  void* stream;
+} odt_hologram_combine_args;
+
+odt_status odt_hologram_phase(const odt_hologram_phase_args* args);
+odt_status odt_hologram_combine(const odt_hologram_combine_args* args);
+
 /* refocus (FIELD_EXPERIMENTAL_RETRIEVAL.m:392-394): out = centred inverse 2D
  * FFT of (centred 2D FFT of each field plane .* kernel), kernel =
  * exp(z .* refocusing_kernel) [size(1), size(2)]; host arrays, synchronous. */

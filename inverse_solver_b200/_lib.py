@@ -157,6 +157,30 @@ class HologramArgs(C.Structure):
     ]
 
 
+class HologramPhaseArgs(C.Structure):
+    _fields_ = [
+        ("size", C.c_int32 * 3),
+        ("bg", C.c_void_p),
+        ("sp", C.c_void_p),
+        ("conjugate", C.c_int32),
+        ("phase", C.c_void_p),
+        ("amp", C.c_void_p),
+        ("stream", C.c_void_p),
+    ]
+
+
+class HologramCombineArgs(C.Structure):
+    _fields_ = [
+        ("size", C.c_int32 * 3),
+        ("bg", C.c_void_p),
+        ("amp", C.c_void_p),
+        ("phase", C.c_void_p),
+        ("coef", C.c_void_p),
+        ("sp", C.c_void_p),
+        ("stream", C.c_void_p),
+    ]
+
+
 class RefocusArgs(C.Structure):
     _fields_ = [
         ("size", C.c_int32 * 3),
@@ -295,6 +319,8 @@ SIGNATURES = {
     "odt_green_planes": (C.c_int, [C.POINTER(GreenArgs)]),
     "odt_hologram_fields": (C.c_int, [C.POINTER(HologramArgs)]),
     "odt_refocus_2d": (C.c_int, [C.POINTER(RefocusArgs)]),
+    "odt_hologram_phase": (C.c_int, [C.POINTER(HologramPhaseArgs)]),
+    "odt_hologram_combine": (C.c_int, [C.POINTER(HologramCombineArgs)]),
     "odt_submit": (C.c_int, [C.c_uint32, C.POINTER(SolveArgs), C.POINTER(C.c_uint64)]),
     "odt_poll": (C.c_int, [C.c_uint32, C.c_uint64, C.POINTER(C.c_int32), C.POINTER(C.c_int)]),
     "odt_wait": (C.c_int, [C.c_uint32, C.c_uint64, C.POINTER(C.c_int)]),

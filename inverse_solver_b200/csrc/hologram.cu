@@ -9,9 +9,11 @@
 //     peak_subpixel_positioner)
 //   field = fftshift(ifft2(ifftshift(F)))(3:end-2, 3:end-2)
 //
-// and the centred 2D refocus of refocus (:392-394).  The per-image scalar
-// steps that follow (sub-pixel positions, normalisation, phase unwrapping
-// on the GPU, border plane fit) are the host mirror's.
+// the per-pixel steps after them (:179-201: normalisation, the phase and
+// amplitude of sp / bg, and the recombination with the ramp-free phase), and
+// the centred 2D refocus of refocus (:392-394).  Phase unwrapping has its
+// own kernels; the per-image scalar steps (sub-pixel positions, the border
+// plane fit of PhiShiftMS) are the host mirror's.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -293,6 +295,126 @@ extern "C" odt_status odt_hologram_fields(const odt_hologram_args* a) {
     cudaGetLastError();
     return hfail(ODT_ERR_CUDA, std::string("odt_hologram_fields: ") + cudaGetErrorString(e));
   }
+  return ODT_OK;
+}
+
+namespace {
+// The arithmetic below follows numpy's complex64 loops operation by
+// operation (no contraction into FMAs), so that the fields agree with the
+// host restatement to a few ulp:
+//   x / r (r real)  -> x * (1 / r) per component (r is promoted to r + 0i);
+//   y / x           -> Smith's division with the reciprocal of the scale;
+//   r * x (r real)  -> r * x per component; x * y the textbook product.
+__device__ __forceinline__ float2 cdiv_np(float2 y, float2 x) {
+  const float br = x.x, bi = x.y;
+  float re, im;
+  if (fabsf(br) >= fabsf(bi)) {
+    if (br == 0.f && bi == 0.f) {
+      re = y.x / fabsf(br);
+      im = y.y / fabsf(br);
+    } else {
+      const float rat = bi / br, scl = 1.0f / __fadd_rn(br, __fmul_rn(bi, rat));
+      re = __fmul_rn(__fadd_rn(y.x, __fmul_rn(y.y, rat)), scl);
+      im = __fmul_rn(__fsub_rn(y.y, __fmul_rn(y.x, rat)), scl);
+    }
+  } else {
+    const float rat = br / bi, scl = 1.0f / __fadd_rn(bi, __fmul_rn(br, rat));
+    re = __fmul_rn(__fadd_rn(__fmul_rn(y.x, rat), y.y), scl);
+    im = __fmul_rn(__fsub_rn(__fmul_rn(y.y, rat), y.x), scl);
+  }
+  return make_float2(re, im);
+}
+
+// one CTA per image: amean = sum |bg| / plane (summed in double); bg and sp
+// divided by amean (conjugated if asked); phase = angle(sp / bg) and
+// amp = |sp / bg|
+__global__ void __launch_bounds__(1024) norm_phase_kernel(float2* __restrict__ bg, float2* __restrict__ sp,
+                                                          long long plane, int conj, float* __restrict__ phase,
+                                                          float* __restrict__ amp) {
+  __shared__ double red[32];
+  __shared__ float amean;
+  float2* b = bg + plane * blockIdx.x;
+  float2* q = sp + plane * blockIdx.x;
+  double s = 0.0;
+  for (long long i = threadIdx.x; i < plane; i += blockDim.x) s += (double)cabs_f(b[i]);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = threadIdx.x < (blockDim.x + 31) / 32 ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) amean = (float)t / (float)plane;
+  }
+  __syncthreads();
+  const float r = 1.0f / amean;
+  float* ph = phase + plane * blockIdx.x;
+  float* am = amp + plane * blockIdx.x;
+  for (long long i = threadIdx.x; i < plane; i += blockDim.x) {
+    float2 x = make_float2(__fmul_rn(b[i].x, r), __fmul_rn(b[i].y, r));
+    float2 y = make_float2(__fmul_rn(q[i].x, r), __fmul_rn(q[i].y, r));
+    if (conj) {
+      x.y = -x.y;
+      y.y = -y.y;
+    }
+    b[i] = x;
+    q[i] = y;
+    const float2 z = cdiv_np(y, x);
+    ph[i] = atan2f(z.y, z.x);
+    am[i] = cabs_f(z);
+  }
+}
+
+// sp = (amp * bg) * exp(1i g), g = ((phase - c0) - c1 x) - c2 y with x, y
+// the 1-based column / row of the [n1, n2] plane (coef [3, n]: height, x
+// and y slopes per image)
+__global__ void combine_kernel(const float2* __restrict__ bg, const float* __restrict__ amp,
+                               const float* __restrict__ phase, const float* __restrict__ coef, int n1, int n2,
+                               long long total, float2* __restrict__ sp) {
+  const long long plane = (long long)n1 * n2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long k = i / plane, p = i - k * plane;
+    const float y = (float)(p % n1 + 1), x = (float)(p / n1 + 1);
+    const float* c = coef + 3 * k;
+    const float g = __fsub_rn(__fsub_rn(__fsub_rn(phase[i], c[0]), __fmul_rn(c[1], x)), __fmul_rn(c[2], y));
+    float sn, cs;
+    sincosf(g, &sn, &cs);
+    const float2 b = bg[i];
+    const float tr = __fmul_rn(amp[i], b.x), ti = __fmul_rn(amp[i], b.y);
+    sp[i] = make_float2(__fsub_rn(__fmul_rn(tr, cs), __fmul_rn(ti, sn)), __fadd_rn(__fmul_rn(tr, sn), __fmul_rn(ti, cs)));
+  }
+}
+}  // namespace
+
+extern "C" odt_status odt_hologram_phase(const odt_hologram_phase_args* a) {
+  if (!a || !a->bg || !a->sp || !a->phase || !a->amp)
+    return hfail(ODT_ERR_INVALID_ARGUMENT, "odt_hologram_phase: NULL argument");
+  if (a->size[0] < 1 || a->size[1] < 1 || a->size[2] < 1)
+    return hfail(ODT_ERR_INVALID_ARGUMENT, "odt_hologram_phase: bad sizes");
+  for (const void* p : {(const void*)a->bg, (const void*)a->sp, (const void*)a->phase, (const void*)a->amp})
+    if (!is_dev(p)) return hfail(ODT_ERR_INVALID_ARGUMENT, "odt_hologram_phase: arrays must be device pointers");
+  const long long plane = (long long)a->size[0] * a->size[1];
+  norm_phase_kernel<<<a->size[2], 1024, 0, (cudaStream_t)a->stream>>>(
+      reinterpret_cast<float2*>(a->bg), reinterpret_cast<float2*>(a->sp), plane, a->conjugate, a->phase, a->amp);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return hfail(ODT_ERR_CUDA, std::string("odt_hologram_phase: ") + cudaGetErrorString(e));
+  return ODT_OK;
+}
+
+extern "C" odt_status odt_hologram_combine(const odt_hologram_combine_args* a) {
+  if (!a || !a->bg || !a->amp || !a->phase || !a->coef || !a->sp)
+    return hfail(ODT_ERR_INVALID_ARGUMENT, "odt_hologram_combine: NULL argument");
+  if (a->size[0] < 1 || a->size[1] < 1 || a->size[2] < 1)
+    return hfail(ODT_ERR_INVALID_ARGUMENT, "odt_hologram_combine: bad sizes");
+  for (const void* p : {(const void*)a->bg, (const void*)a->amp, (const void*)a->phase, (const void*)a->coef,
+                        (const void*)a->sp})
+    if (!is_dev(p)) return hfail(ODT_ERR_INVALID_ARGUMENT, "odt_hologram_combine: arrays must be device pointers");
+  const long long total = (long long)a->size[0] * a->size[1] * a->size[2];
+  combine_kernel<<<grid_for(total), kThreads, 0, (cudaStream_t)a->stream>>>(
+      reinterpret_cast<const float2*>(a->bg), a->amp, a->phase, a->coef, a->size[0], a->size[1], total,
+      reinterpret_cast<float2*>(a->sp));
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return hfail(ODT_ERR_CUDA, std::string("odt_hologram_combine: ") + cudaGetErrorString(e));
   return ODT_OK;
 }
 

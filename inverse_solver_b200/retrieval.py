@@ -1,10 +1,14 @@
 """Field retrieval from off-axis holograms (Codes/FIELD_EXPERIMENTAL_RETRIEVAL.m)
-on the B200 library: the transforms of get_fields (centred FFTs of the
-background and sample holograms, the sideband search and re-centring, the
-resolution crop / pad, the NA circle, the inverse transforms) run on the GPU
-(odt_hologram_fields), phase unwrapping on the GPU (unwrapp2_gpu); the
-per-image scalar steps (sub-pixel peak positions, normalisation, the border
-plane fit of PhiShiftMS) are host code in MATLAB single semantics.  The
+on the B200 library.  get_fields keeps the hologram stacks on the GPU from
+upload to result: the transforms (centred FFTs of the background and sample
+holograms, the sideband search and re-centring, the resolution crop / pad,
+the NA circle, the inverse transforms: odt_hologram_fields), the
+normalisation and the phase / amplitude of sp ./ bg (odt_hologram_phase),
+Goldstein unwrapping (unwrap_goldstein_device) and the recombination with
+the ramp-free phase (odt_hologram_combine).  Only the per-image scalar steps
+run on the host, in MATLAB single semantics: the sub-pixel peak positions
+and the border plane fit of PhiShiftMS, for which the unwrapped phase on the
+border band (a few percent of the pixels) comes back from the device.  The
 interactive branches of the reference (the "rectangle" ROI picker,
 PhiShiftMS's hand-drawn masks) are not mirrored: ROI is numeric or absent.
 """
@@ -80,21 +84,39 @@ def _border(imY, imX, bsize):
     return _BORDER[key]
 
 
+def _plane_coef(vb, bx, by):
+    """D2_LSAms (n = 1) on the border values vb (column-major order, with
+    their x / y coordinates): outliers and exact zeros left out, A'A in
+    double, A'p and the solve in single, as MATLAB evaluates them; returns
+    (x slope, y slope, height) in single."""
+    v = _omit_outliers(vb)
+    keep = v != 0
+    A = np.stack([bx[keep], by[keep], np.ones(int(keep.sum()))], axis=1)
+    return np.linalg.solve((A.T @ A).astype(F32), (A.astype(F32).T @ v[keep]).astype(F32)).astype(F32)
+
+
 def phi_shift_ms(p2, bsize=8):
     """PhiShiftMS(p2, 1, 1) (sub_code/PhiShiftMS.m, D2_LSAms with n = 1 and
     omit_outliers): a + b x + c y fitted by least squares to the border of
-    width bsize - 1 (outliers and exact zeros left out) and subtracted.  A'A
-    in double, A'p and the solve in single, as MATLAB evaluates them; only
-    the border pixels are visited, in the reference's column-major order."""
+    width bsize - 1 and subtracted; only the border pixels are visited, in
+    the reference's column-major order."""
     imY, imX = p2.shape
     idx, bx, by, XX, YY = _border(imY, imX, bsize)
-    v = _omit_outliers(np.asarray(p2, dtype=F32).ravel(order="F")[idx])
-    keep = v != 0
-    A = np.stack([bx[keep], by[keep], np.ones(int(keep.sum()))], axis=1)
-    coef = np.linalg.solve((A.T @ A).astype(F32), (A.astype(F32).T @ v[keep]).astype(F32)).astype(F32)
+    coef = _plane_coef(np.asarray(p2, dtype=F32).ravel(order="F")[idx], bx, by)
     g = (p2 - coef[2]).astype(F32)
     g = (g - coef[0] * XX).astype(F32)
     return (g - coef[1] * YY).astype(F32)
+
+
+def _col_major(a, device):
+    """A CUDA tensor whose storage is the column-major layout of the numpy
+    array a (its shape reversed)."""
+    import torch
+
+    if a.flags.f_contiguous:
+        return torch.from_numpy(a.T).to(device)
+    t = torch.from_numpy(np.ascontiguousarray(a)).to(device)
+    return t.permute(*reversed(range(t.dim()))).contiguous()
 
 
 class FIELD_EXPERIMENTAL_RETRIEVAL:
@@ -141,7 +163,6 @@ class FIELD_EXPERIMENTAL_RETRIEVAL:
             bg, sp = bg[:, :, None], sp[:, :, None]
         if bg.shape[0] != bg.shape[1]:
             raise ValueError("the image must be a square")
-        over = np.maximum(bg, sp).max(axis=(0, 1)) > 254
         N, nimg = bg.shape[0], bg.shape[2]
         # resolution matching (:131-145)
         ratio = p["resolution"][0] / p["resolution_image"][0]
@@ -156,45 +177,66 @@ class FIELD_EXPERIMENTAL_RETRIEVAL:
         p["resolution"][1] = p["resolution_image"][1] * N / M
         p["size"] = list(p["size"])
         p["size"][0], p["size"][1] = M, M
+        import torch
+
+        dev = torch.device("cuda", torch.cuda.current_device())
+        stream = torch.cuda.current_stream(dev)
         na = np.asfortranarray(OpticalTool(p).NA_circle.astype(np.uint8))
-        hb = np.asfortranarray(bg, dtype=F32)
-        hs = np.asfortranarray(sp, dtype=F32)
-        bgf = np.empty((M - 4, M - 4, nimg), dtype=C64, order="F")
-        spf = np.empty_like(bgf)
-        peaks = np.empty((7, nimg), dtype=F32, order="F")
+        hb, hs = _col_major(np.asarray(bg, dtype=F32), dev), _col_major(np.asarray(sp, dtype=F32), dev)
+        over = (torch.maximum(hb, hs).amax(dim=(1, 2)) > 254).cpu().numpy()
+        bgf = torch.empty((nimg, M - 4, M - 4), dtype=torch.complex64, device=dev)   # column-major [M-4, M-4, n]
+        spf = torch.empty_like(bgf)
+        peaks = torch.empty((nimg, 7), dtype=torch.float32, device=dev)
+        nat = torch.from_numpy(na.T).to(dev)
         side = np.zeros(2, dtype=np.int32)
         a = _lib.HologramArgs()
         a.size[:] = [N, N, nimg]
-        a.bg, a.sp = _lib.ptr(hb), _lib.ptr(hs)
+        a.bg, a.sp = hb.data_ptr(), hs.data_ptr()
         a.cutout_portion = float(p["cutout_portion"])
         a.other_corner = 1 if p["other_corner"] else 0
         a.out_size, a.crop = M, d
-        a.na_circle = _lib.ptr(na)
-        a.bg_field, a.sp_field = _lib.ptr(bgf), _lib.ptr(spf)
-        a.peaks, a.sideband = _lib.ptr(peaks), _lib.ptr(side)
-        a.memory = _lib.ODT_MEM_HOST
-        a.stream = None
+        a.na_circle = nat.data_ptr()
+        a.bg_field, a.sp_field = bgf.data_ptr(), spf.data_ptr()
+        a.peaks, a.sideband = peaks.data_ptr(), _lib.ptr(side)
+        a.memory = _lib.ODT_MEM_DEVICE
+        a.stream = stream.cuda_stream
         _lib.check(self.lib.odt_hologram_fields(C.byref(a)))
+        del hb, hs
+        pk = peaks.cpu().numpy().T
         k0s = np.zeros((2, nimg), dtype=F32)
         for jj in range(nimg):
-            k0s[0, jj], k0s[1, jj] = _subpixel(peaks[:, jj], M)
+            k0s[0, jj], k0s[1, jj] = _subpixel(pk[:, jj], M)
         # normalisation, phase, unwrapping, ramp removal (:179-204)
-        p["size"][0], p["size"][1] = M - 4, M - 4
-        amean = (np.abs(bgf).sum(axis=(0, 1)) / ((M - 4) * (M - 4))).astype(F32)
-        bgf = (bgf / amean).astype(C64)
-        spf = (spf / amean).astype(C64)
-        if p["conjugate_field"]:
-            bgf, spf = np.conj(bgf), np.conj(spf)
-        q = (spf / bgf).astype(C64)
-        phase = np.asarray(unwrapp2_gpu(np.ascontiguousarray(np.angle(q).astype(F32))), dtype=F32)
-        amp = np.abs(q).astype(F32)
+        L = M - 4
+        p["size"][0], p["size"][1] = L, L
+        phase = torch.empty((nimg, L, L), dtype=torch.float32, device=dev)
+        amp = torch.empty_like(phase)
+        g = _lib.HologramPhaseArgs()
+        g.size[:] = [L, L, nimg]
+        g.bg, g.sp = bgf.data_ptr(), spf.data_ptr()
+        g.conjugate = 1 if p["conjugate_field"] else 0
+        g.phase, g.amp = phase.data_ptr(), amp.data_ptr()
+        g.stream = stream.cuda_stream
+        _lib.check(self.lib.odt_hologram_phase(C.byref(g)))
+        phase = unwrapp2_gpu(phase.permute(2, 1, 0)).permute(2, 1, 0)   # column-major again, no copy
+        idx, bx, by, _, _ = _border(L, L, 8)
+        vb = phase.reshape(nimg, L * L)[:, torch.from_numpy(idx).to(dev)].cpu().numpy()
+        coef = np.empty((nimg, 3), dtype=F32)
         for jj in range(nimg):
-            phase[:, :, jj] = phi_shift_ms(phase[:, :, jj])
-        spf = (amp * bgf * np.exp(1j * phase).astype(C64)).astype(C64)
+            cx, cy, c0 = _plane_coef(vb[jj], bx, by)
+            coef[jj] = (c0, cx, cy)
+        coef_d = torch.from_numpy(coef).to(dev)
+        c = _lib.HologramCombineArgs()
+        c.size[:] = [L, L, nimg]
+        c.bg, c.amp, c.phase, c.coef = bgf.data_ptr(), amp.data_ptr(), phase.data_ptr(), coef_d.data_ptr()
+        c.sp = spf.data_ptr()
+        c.stream = stream.cuda_stream
+        _lib.check(self.lib.odt_hologram_combine(C.byref(c)))
+        bgh, sph = bgf.cpu().numpy().T, spf.cpu().numpy().T      # Fortran-ordered [L, L, n] views
         self.utility = OpticalTool(p)
         base = basic_optical_parameter()
         updated = {k: copy.deepcopy(p[k]) for k in base}
-        return bgf[:, :, None, :], spf[:, :, None, :], updated, k0s, over, ROI
+        return bgh[:, :, None, :], sph[:, :, None, :], updated, k0s, over, ROI
 
     def refocus(self, field_trans, z):
         """:392-394 on the GPU (odt_refocus_2d), with the utility of the last
