@@ -369,6 +369,68 @@ typedef struct odt_hologram_combine_args {
 odt_status odt_hologram_phase(const odt_hologram_phase_args* args);
 odt_status odt_hologram_combine(const odt_hologram_combine_args* args);
 
+/* get_aberration_pattern (FIELD_EXPERIMENTAL_RETRIEVAL.m:216-352): the
+ * stitched, phase-matched and low-passed pupil of the fields [N1, N2, n]
+ * (n >= 2), the aberration pattern [N1, N2] and the corrected fields
+ * ifft2c(fft2c(field) .* exp(-1i angle(pattern))).  k0s [2, n] are the
+ * sub-pixel sideband positions of get_fields; pupil_mask is the reference's
+ * fMask (coorxy < max(coorxy) * overlap_factor), na_circle and
+ * refocusing_kernel the optical tool's; dist_list the defocus candidates.
+ * The fields, the pattern and the corrected fields live where `memory`
+ * says; the tables, k0s, dist_list and *chosen (the 0-based index of the
+ * selected distance; may be NULL) on the host.  Synchronous on `stream`. */
+typedef struct odt_aberration_args {
+  int32_t size[3];
+  const odt_cfloat* input_field;
+  const odt_cfloat* output_field;
+  const float* k0s;
+  const uint8_t* pupil_mask;
+  const uint8_t* na_circle;
+  const odt_cfloat* refocusing_kernel;
+  const double* dist_list;
+  int32_t n_dist;
+  odt_cfloat* pattern;
+  odt_cfloat* input_out;
+  odt_cfloat* output_out;
+  int32_t* chosen;
+  int32_t memory;
+  void* stream;
+} odt_aberration_args;
+
+odt_status odt_aberration_pattern(const odt_aberration_args* args);
+
+/* Centred 2D FFT, in place, of every [N1, N2] plane of data [N1, N2, n]:
+ * fftshift(fft2(ifftshift(x))), or with inverse = 1 the inverse transform
+ * (normalised by N1 N2), as correct_aberration (:356-370) applies it.
+ * Synchronous on `stream`. */
+typedef struct odt_fft2c_args {
+  int32_t size[3];
+  odt_cfloat* data;
+  int32_t inverse;
+  int32_t memory;
+  void* stream;
+} odt_fft2c_args;
+
+odt_status odt_fft2c(const odt_fft2c_args* args);
+
+/* remove_dirty_fields (FIELD_EXPERIMENTAL_RETRIEVAL.m:399-452) up to its
+ * decision, for scalar fields bg, sp [N1, N2, n]: with the Goldstein-
+ * unwrapped phase and the amplitude of sp ./ bg, per image the standard
+ * deviation of the gradient energy of amp_k - amp_1 (gradient_std [n]) and
+ * the number of phase values above 1.5 max(phase_1) or below
+ * 1.5 min(phase_1) (outside_count [n]); both outputs on the host. */
+typedef struct odt_field_quality_args {
+  int32_t size[3];
+  const odt_cfloat* bg;
+  const odt_cfloat* sp;
+  float* gradient_std;
+  int64_t* outside_count;
+  int32_t memory;
+  void* stream;
+} odt_field_quality_args;
+
+odt_status odt_field_quality(const odt_field_quality_args* args);
+
 /* refocus (FIELD_EXPERIMENTAL_RETRIEVAL.m:392-394): out = centred inverse 2D
  * FFT of (centred 2D FFT of each field plane .* kernel), kernel =
  * exp(z .* refocusing_kernel) [size(1), size(2)]; host arrays, synchronous. */

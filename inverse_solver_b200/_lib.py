@@ -181,6 +181,48 @@ class HologramCombineArgs(C.Structure):
     ]
 
 
+class AberrationArgs(C.Structure):
+    _fields_ = [
+        ("size", C.c_int32 * 3),
+        ("input_field", C.c_void_p),
+        ("output_field", C.c_void_p),
+        ("k0s", C.c_void_p),
+        ("pupil_mask", C.c_void_p),
+        ("na_circle", C.c_void_p),
+        ("refocusing_kernel", C.c_void_p),
+        ("dist_list", C.c_void_p),
+        ("n_dist", C.c_int32),
+        ("pattern", C.c_void_p),
+        ("input_out", C.c_void_p),
+        ("output_out", C.c_void_p),
+        ("chosen", C.c_void_p),
+        ("memory", C.c_int32),
+        ("stream", C.c_void_p),
+    ]
+
+
+class Fft2cArgs(C.Structure):
+    _fields_ = [
+        ("size", C.c_int32 * 3),
+        ("data", C.c_void_p),
+        ("inverse", C.c_int32),
+        ("memory", C.c_int32),
+        ("stream", C.c_void_p),
+    ]
+
+
+class FieldQualityArgs(C.Structure):
+    _fields_ = [
+        ("size", C.c_int32 * 3),
+        ("bg", C.c_void_p),
+        ("sp", C.c_void_p),
+        ("gradient_std", C.c_void_p),
+        ("outside_count", C.c_void_p),
+        ("memory", C.c_int32),
+        ("stream", C.c_void_p),
+    ]
+
+
 class RefocusArgs(C.Structure):
     _fields_ = [
         ("size", C.c_int32 * 3),
@@ -321,6 +363,9 @@ SIGNATURES = {
     "odt_refocus_2d": (C.c_int, [C.POINTER(RefocusArgs)]),
     "odt_hologram_phase": (C.c_int, [C.POINTER(HologramPhaseArgs)]),
     "odt_hologram_combine": (C.c_int, [C.POINTER(HologramCombineArgs)]),
+    "odt_aberration_pattern": (C.c_int, [C.POINTER(AberrationArgs)]),
+    "odt_field_quality": (C.c_int, [C.POINTER(FieldQualityArgs)]),
+    "odt_fft2c": (C.c_int, [C.POINTER(Fft2cArgs)]),
     "odt_submit": (C.c_int, [C.c_uint32, C.POINTER(SolveArgs), C.POINTER(C.c_uint64)]),
     "odt_poll": (C.c_int, [C.c_uint32, C.c_uint64, C.POINTER(C.c_int32), C.POINTER(C.c_int)]),
     "odt_wait": (C.c_int, [C.c_uint32, C.c_uint64, C.POINTER(C.c_int)]),

@@ -21,6 +21,8 @@
 
 #include "../../include/odt.h"
 #include "cbs_kernels.cuh"
+#include "np_complex.cuh"
+#include "fft_any.cuh"
 #include "scratch.cuh"
 
 namespace odt {
@@ -39,7 +41,6 @@ int grid_for(long long n) {
   return (int)(b < 1 ? 1 : b);
 }
 
-__device__ __forceinline__ float cabs_f(float2 v) { return (float)sqrt((double)v.x * v.x + (double)v.y * v.y); }
 
 __global__ void to_complex_kernel(const float* __restrict__ a, float2* __restrict__ out, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -197,13 +198,6 @@ bool is_dev(const void* p) {
   return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
 }
 
-// centred 2D FFT of every [n1, n2] plane of x (in place)
-cudaError_t fftc2(float2* x, int n1, int n2, long long nsl, bool inv, const DevFft& f1, const DevFft& f2,
-                  cudaStream_t s) {
-  cudaError_t e = launch_fft_lines(x, x, (long long)n2 * nsl, n1 / 2, n1 / 2, 1.f, inv, f1, s);
-  if (e != cudaSuccess) return e;
-  return launch_fft_cols(x, x, n1, nsl, n2 / 2, n2 / 2, inv ? 1.0f / ((float)n1 * (float)n2) : 1.f, inv, f2, s);
-}
 
 }  // namespace
 
@@ -237,9 +231,9 @@ extern "C" odt_status odt_hologram_fields(const odt_hologram_args* a) {
   int* sb = B.get<int>(2);
   if (!Fb || !Fs || !Gb || !Gs || !sb || (!dev && (!hb || !hs || !na || !ob || !os || !pk)))
     return hfail(ODT_ERR_OUT_OF_MEMORY, "odt_hologram_fields: device allocation failed");
-  DevFft fN{}, fM{};
+  AnyFft fN{}, fM{};
   std::string why;
-  if (!scratch_fft(B, N, &fN, &why) || !scratch_fft(B, M, &fM, &why))
+  if (!scratch_fft_any(B, N, &fN, &why) || !scratch_fft_any(B, M, &fM, &why))
     return hfail(ODT_ERR_UNSUPPORTED, "odt_hologram_fields: " + why);
   auto run = [&]() -> cudaError_t {
     cudaError_t e;
@@ -257,8 +251,8 @@ extern "C" odt_status odt_hologram_fields(const odt_hologram_args* a) {
     }
     to_complex_kernel<<<grid_for(nin), kThreads, 0, s>>>(db, Fb, nin);
     to_complex_kernel<<<grid_for(nin), kThreads, 0, s>>>(ds, Fs, nin);
-    if ((e = cudaGetLastError()) || (e = fftc2(Fb, N, N, nimg, false, fN, fN, s)) ||
-        (e = fftc2(Fs, N, N, nimg, false, fN, fN, s)))
+    if ((e = cudaGetLastError()) || (e = fftc2_any(B, Fb, N, N, nimg, false, fN, fN, s)) ||
+        (e = fftc2_any(B, Fs, N, N, nimg, false, fN, fN, s)))
       return e;
     // deleted bands (1-based): rows round(N cp):N; columns round(N cp):N, or
     // 1:round(N (1 - cp)) with other_corner
@@ -273,8 +267,8 @@ extern "C" odt_status odt_hologram_fields(const odt_hologram_args* a) {
     centre_crop_kernel<<<grid_for(nmid), kThreads, 0, s>>>(Fb, N, M, d, sb, dna, nimg, Gb);
     centre_crop_kernel<<<grid_for(nmid), kThreads, 0, s>>>(Fs, N, M, d, sb, dna, nimg, Gs);
     peak_kernel<<<nimg, 256, 0, s>>>(Gb, M, dev ? a->peaks : pk);
-    if ((e = cudaGetLastError()) || (e = fftc2(Gb, M, M, nimg, true, fM, fM, s)) ||
-        (e = fftc2(Gs, M, M, nimg, true, fM, fM, s)))
+    if ((e = cudaGetLastError()) || (e = fftc2_any(B, Gb, M, M, nimg, true, fM, fM, s)) ||
+        (e = fftc2_any(B, Gs, M, M, nimg, true, fM, fM, s)))
       return e;
     float2* outb = dev ? reinterpret_cast<float2*>(a->bg_field) : ob;
     float2* outs = dev ? reinterpret_cast<float2*>(a->sp_field) : os;
@@ -299,32 +293,9 @@ extern "C" odt_status odt_hologram_fields(const odt_hologram_args* a) {
 }
 
 namespace {
-// The arithmetic below follows numpy's complex64 loops operation by
-// operation (no contraction into FMAs), so that the fields agree with the
-// host restatement to a few ulp:
-//   x / r (r real)  -> x * (1 / r) per component (r is promoted to r + 0i);
-//   y / x           -> Smith's division with the reciprocal of the scale;
-//   r * x (r real)  -> r * x per component; x * y the textbook product.
-__device__ __forceinline__ float2 cdiv_np(float2 y, float2 x) {
-  const float br = x.x, bi = x.y;
-  float re, im;
-  if (fabsf(br) >= fabsf(bi)) {
-    if (br == 0.f && bi == 0.f) {
-      re = y.x / fabsf(br);
-      im = y.y / fabsf(br);
-    } else {
-      const float rat = bi / br, scl = 1.0f / __fadd_rn(br, __fmul_rn(bi, rat));
-      re = __fmul_rn(__fadd_rn(y.x, __fmul_rn(y.y, rat)), scl);
-      im = __fmul_rn(__fsub_rn(y.y, __fmul_rn(y.x, rat)), scl);
-    }
-  } else {
-    const float rat = br / bi, scl = 1.0f / __fadd_rn(bi, __fmul_rn(br, rat));
-    re = __fmul_rn(__fadd_rn(__fmul_rn(y.x, rat), y.y), scl);
-    im = __fmul_rn(__fsub_rn(__fmul_rn(y.y, rat), y.x), scl);
-  }
-  return make_float2(re, im);
-}
-
+// The arithmetic below follows numpy's complex64 loops (np_complex.cuh):
+// x / r (r real) is x * (1 / r) per component (r is promoted to r + 0i),
+// r * x (r real) is r * x per component.
 // one CTA per image: amean = sum |bg| / plane (summed in double); bg and sp
 // divided by amean (conjugated if asked); phase = angle(sp / bg) and
 // amp = |sp / bg|
@@ -429,18 +400,18 @@ extern "C" odt_status odt_refocus_2d(const odt_refocus_args* a) {
   float2* x = B.get<float2>(tot);
   float2* k = B.get<float2>(plane);
   if (!x || !k) return hfail(ODT_ERR_OUT_OF_MEMORY, "odt_refocus_2d: device allocation failed");
-  DevFft f1{}, f2{};
+  AnyFft f1{}, f2{};
   std::string why;
-  if (!scratch_fft(B, n1, &f1, &why) || !scratch_fft(B, n2, &f2, &why))
+  if (!scratch_fft_any(B, n1, &f1, &why) || !scratch_fft_any(B, n2, &f2, &why))
     return hfail(ODT_ERR_UNSUPPORTED, "odt_refocus_2d: " + why);
   auto run = [&]() -> cudaError_t {
     cudaError_t e;
     if ((e = cudaMemcpyAsync(x, a->field, tot * sizeof(float2), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(k, a->kernel, plane * sizeof(float2), cudaMemcpyHostToDevice, s)) ||
-        (e = fftc2(x, n1, n2, n, false, f1, f2, s)))
+        (e = fftc2_any(B, x, n1, n2, n, false, f1, f2, s)))
       return e;
     cmul_plane_kernel<<<grid_for(tot), kThreads, 0, s>>>(x, k, plane, tot);
-    if ((e = cudaGetLastError()) || (e = fftc2(x, n1, n2, n, true, f1, f2, s)) ||
+    if ((e = cudaGetLastError()) || (e = fftc2_any(B, x, n1, n2, n, true, f1, f2, s)) ||
         (e = cudaMemcpyAsync(a->out, x, tot * sizeof(float2), cudaMemcpyDeviceToHost, s)))
       return e;
     return cudaStreamSynchronize(s);

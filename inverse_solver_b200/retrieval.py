@@ -108,6 +108,33 @@ def phi_shift_ms(p2, bsize=8):
     return (g - coef[1] * YY).astype(F32)
 
 
+ISOUTLIER_SCALE = 1.4826022185056018   # -1 / (sqrt(2) erfcinv(3/2)): MAD -> standard deviation
+
+
+def _isoutlier(x):
+    """MATLAB isoutlier(x), default 'median' method: more than three scaled
+    median absolute deviations from the median."""
+    x = np.asarray(x, dtype=np.float64)
+    med = np.median(x)
+    mad = ISOUTLIER_SCALE * np.median(np.abs(x - med))
+    return (x < med - 3 * mad) | (x > med + 3 * mad)
+
+
+def _stack(field):
+    """A field array [N1, N2(, 1), n] as a Fortran-ordered complex64 stack
+    [N1, N2, n]."""
+    f = np.asarray(field, dtype=C64)
+    return np.asfortranarray(f.reshape(f.shape[0], f.shape[1], -1, order="F"))
+
+
+def _rmul(x, m):
+    """MATLAB's real-times-complex product: both parts scaled by m."""
+    out = np.empty(x.shape, dtype=C64)
+    out.real = x.real * m
+    out.imag = x.imag * m
+    return out
+
+
 def _col_major(a, device):
     """A CUDA tensor whose storage is the column-major layout of the numpy
     array a (its shape reversed)."""
@@ -237,6 +264,143 @@ class FIELD_EXPERIMENTAL_RETRIEVAL:
         base = basic_optical_parameter()
         updated = {k: copy.deepcopy(p[k]) for k in base}
         return bgh[:, :, None, :], sph[:, :, None, :], updated, k0s, over, ROI
+
+    def _utility(self):
+        return self.utility if self.utility is not None else OpticalTool(self.parameters)
+
+    def _fft2c(self, x, inverse=False):
+        f = np.asfortranarray(np.asarray(x, dtype=C64)).copy(order="F")
+        a = _lib.Fft2cArgs()
+        a.size[:] = [f.shape[0], f.shape[1], 1 if f.ndim == 2 else f.shape[2]]
+        a.data = _lib.ptr(f)
+        a.inverse = 1 if inverse else 0
+        a.memory = _lib.ODT_MEM_HOST
+        a.stream = None
+        _lib.check(self.lib.odt_fft2c(C.byref(a)))
+        return f
+
+    def get_aberration_pattern(self, input_field, output_field, correct_params):
+        """:216-352 on the GPU (odt_aberration_pattern) with the optical tool
+        of the last get_fields (or of the parameters).  correct_params holds
+        overlap_factor, k0s [2, n] (get_fields' sub-pixel positions) and
+        distList.  Returns (input_field_f, output_field_f, aberration_params
+        = {pattern, distance, utility})."""
+        u = self._utility()
+        fin, fout = _stack(input_field), _stack(output_field)
+        N1, N2, n = fin.shape
+        if fout.shape != fin.shape:
+            raise ValueError("input and output fields differ in size")
+        if (N1, N2) != tuple(u.NA_circle.shape):
+            raise ValueError("field and optical grid sizes differ")
+        coorxy = np.asarray(u.coorxy, dtype=F32)
+        fmask = np.asfortranarray(coorxy < coorxy.max() * F32(correct_params["overlap_factor"])).astype(np.uint8)
+        na = np.asfortranarray(u.NA_circle.astype(np.uint8))
+        rk = np.asfortranarray(np.asarray(u.refocusing_kernel, dtype=C64))
+        k0s = np.asfortranarray(np.asarray(correct_params["k0s"], dtype=F32).reshape(2, -1))
+        if k0s.shape[1] != n:
+            raise ValueError("k0s must hold one position per field")
+        dl = np.ascontiguousarray(np.atleast_1d(np.asarray(correct_params["distList"], dtype=np.float64)))
+        pattern = np.empty((N1, N2), dtype=C64, order="F")
+        oi, oo = np.empty_like(fin, order="F"), np.empty_like(fin, order="F")
+        chosen = C.c_int32(0)
+        a = _lib.AberrationArgs()
+        a.size[:] = [N1, N2, n]
+        a.input_field, a.output_field = _lib.ptr(fin), _lib.ptr(fout)
+        a.k0s, a.pupil_mask, a.na_circle = _lib.ptr(k0s), _lib.ptr(fmask), _lib.ptr(na)
+        a.refocusing_kernel = _lib.ptr(rk)
+        a.dist_list, a.n_dist = _lib.ptr(dl), len(dl)
+        a.pattern, a.input_out, a.output_out = _lib.ptr(pattern), _lib.ptr(oi), _lib.ptr(oo)
+        a.chosen = C.cast(C.byref(chosen), C.c_void_p)
+        a.memory = _lib.ODT_MEM_HOST
+        a.stream = None
+        _lib.check(self.lib.odt_aberration_pattern(C.byref(a)))
+        shape = np.shape(input_field)
+        return (oi.reshape(shape, order="F"), oo.reshape(shape, order="F"),
+                {"pattern": pattern, "distance": float(dl[chosen.value]), "utility": u})
+
+    def correct_aberration(self, input_field, field_trans, aberration_params):
+        """:354-390: the pattern of get_aberration_pattern brought to these
+        fields' Fourier resolution and field of view (the reference's steps,
+        transforms on the GPU), masked by the NA circle of the pattern's
+        coordinates, then both stacks filtered by exp(-1i angle(pattern)) on
+        the GPU (odt_refocus_2d)."""
+        u = self._utility()
+        pattern = np.asarray(aberration_params["pattern"], dtype=C64)
+        ua = aberration_params["utility"]
+        N = np.shape(input_field)[0]
+        target = int(mround(N * ua.fourier_res[0] / u.fourier_res[0] / 2) * 2)
+
+        def half(a, b):
+            d = float(np.floor(a - b)) / 2
+            if d != int(d):
+                raise ValueError("odd size difference in correct_aberration")
+            return int(d)
+
+        if target > N:
+            p = self._fft2c(pattern)
+            c = half(target, p.shape[0])
+            p0 = np.zeros((target, target), dtype=C64)
+            p0[c:target - c, c:target - c] = p
+            pattern = self._fft2c(p0, inverse=True)
+        elif target < N:
+            p = self._fft2c(pattern)
+            c = half(p.shape[0], target)
+            pattern = self._fft2c(p[c:p.shape[0] - c, c:p.shape[1] - c], inverse=True)
+        if pattern.shape[0] > N:
+            c = half(pattern.shape[0], N)
+            pattern = self._fft2c(pattern[c:pattern.shape[0] - c, c:pattern.shape[1] - c], inverse=True)
+        elif pattern.shape[0] < N:
+            c = half(target, pattern.shape[0])
+            p0 = np.zeros((target, target), dtype=C64)
+            p0[c:target - c, c:target - c] = pattern
+            pattern = p0
+        f1 = (np.asarray(ua.fourier_coor[0], dtype=F32) * F32(pattern.shape[0])) / F32(target)
+        f2 = (np.asarray(ua.fourier_coor[1], dtype=F32) * F32(pattern.shape[1])) / F32(target)
+        na = np.sqrt(f1[:, None] ** 2 + f2[None, :] ** 2) < u.kmax
+        if na.shape != pattern.shape:
+            raise ValueError("aberration pattern and optical grid sizes differ")
+        filt = np.asfortranarray(np.exp(-1j * np.angle(_rmul(pattern, na.astype(F32))).astype(F32)).astype(C64))
+        return self._filter(input_field, filt), self._filter(field_trans, filt)
+
+    def _filter(self, field, kernel):
+        f = _stack(field)
+        if f.shape[:2] != kernel.shape:
+            raise ValueError("field and pattern sizes differ")
+        out = np.empty_like(f, order="F")
+        a = _lib.RefocusArgs()
+        a.size[:] = list(f.shape)
+        a.field, a.kernel, a.out = _lib.ptr(f), _lib.ptr(kernel), _lib.ptr(out)
+        _lib.check(self.lib.odt_refocus_2d(C.byref(a)))
+        return out.reshape(np.shape(field), order="F")
+
+    def remove_dirty_fields(self, input_field, output_field, prctile=95, manual_on=False):
+        """:399-452 for scalar fields: per image the standard deviation of the
+        gradient energy of |sp/bg|_k - |sp/bg|_1 and the fraction of the
+        (GPU-unwrapped) phase outside 1.5 x [min, max] of the first image's
+        (odt_field_quality); keeps the first field and those that are neither
+        isoutlier nor above the fraction prctile / 100.  The manual review
+        (manual_on) is interactive and not available."""
+        if manual_on:
+            raise ValueError("the manual review of remove_dirty_fields is interactive and not available")
+        if np.ndim(input_field) == 4 and np.shape(input_field)[2] != 1:
+            raise ValueError("remove_dirty_fields takes scalar fields (one polarisation)")
+        bg, sp = _stack(input_field), _stack(output_field)
+        if bg.shape != sp.shape:
+            raise ValueError("input and output fields differ in size")
+        N1, N2, n = bg.shape
+        sd = np.empty(n, dtype=F32)
+        cnt = np.empty(n, dtype=np.int64)
+        a = _lib.FieldQualityArgs()
+        a.size[:] = [N1, N2, n]
+        a.bg, a.sp = _lib.ptr(bg), _lib.ptr(sp)
+        a.gradient_std, a.outside_count = _lib.ptr(sd), _lib.ptr(cnt)
+        a.memory = _lib.ODT_MEM_HOST
+        a.stream = None
+        _lib.check(self.lib.odt_field_quality(C.byref(a)))
+        bad = cnt / float(N1 * N2) > prctile / 100
+        keep = np.flatnonzero(~_isoutlier(sd) & ~bad)
+        F = np.unique(np.concatenate([[0], keep])).astype(int)
+        return bg[:, :, F].reshape(N1, N2, 1, len(F), order="F"), sp[:, :, F].reshape(N1, N2, 1, len(F), order="F")
 
     def refocus(self, field_trans, z):
         """:392-394 on the GPU (odt_refocus_2d), with the utility of the last

@@ -7,7 +7,9 @@ picker and the GUI branches of PhiShiftMS are interactive and out of scope)
 with its helpers sub_code/CPU_placement_finder_prepare.m:1-19,
 sub_code/peak_subpixel_positioner.m:1-67 and sub_code/PhiShiftMS.m (mask
 style 1, D2_LSAms with n = 1, omit_outliers: :1-44, :103-166), and refocus
-(:392-394).  MATLAB single semantics: single(x) * double(y) is single,
+(:392-394), get_aberration_pattern (:216-352), correct_aberration
+(:354-390) and remove_dirty_fields (:399-452; without the manual review).
+MATLAB single semantics: single(x) * double(y) is single,
 prctile is numpy's "hazen" percentile, find / max return the first hit in
 column-major order.  Parity is unpinned: the reference ships no holograms.
 """
@@ -217,3 +219,192 @@ def refocus(params, field, z):
     f = fftc2(np.asarray(field, dtype=C64)).astype(C64)
     sh = (slice(None), slice(None)) + (None,) * (f.ndim - 2)
     return fftc2((f * k[sh]).astype(C64), inverse=True).astype(C64)
+
+
+# ------------------------------------------------ aberration and dirty fields
+def _rmul(x, m):
+    """MATLAB's real-times-complex product: both parts scaled by the real m
+    (which fixes the signed zeros that angle() sees where m is 0)."""
+    x = np.asarray(x, dtype=C64)
+    out = np.empty(np.broadcast_shapes(x.shape, np.shape(m)), dtype=C64)
+    out.real = x.real * m
+    out.imag = x.imag * m
+    return out
+
+
+def _stack(field):
+    f = np.asarray(field, dtype=C64)
+    return f.reshape(f.shape[0], f.shape[1], -1, order="F")
+
+
+def _phasor(z):
+    return np.exp(1j * np.angle(z).astype(F32)).astype(C64)
+
+
+def get_aberration_pattern(u, input_field, output_field, correct_params):
+    """FIELD_EXPERIMENTAL_RETRIEVAL.m:216-352 (get_aberration_pattern) with
+    the optical tool u of the fields (derive_optical_tool) and correct_params
+    {overlap_factor, k0s [2, n], distList}; returns (input_field_f,
+    output_field_f, aberration_params = {pattern, distance, utility}).  The
+    pixel sums are taken in double (the reference sums in single; the order
+    of a single-precision sum is not defined there)."""
+    fin, fout = _stack(input_field), _stack(output_field)
+    N1, N2, n = fin.shape
+    NA = np.asarray(u["NA_circle"]).astype(F32)
+    coorxy = np.asarray(u["coorxy"], dtype=F32)
+    rk = np.asarray(u["refocusing_kernel"], dtype=C64)
+    # stitch pupil (:217-227)
+    fE = fftc2((fout / fin).astype(C64)).astype(C64)
+    fmask = (coorxy < coorxy.max() * F32(correct_params["overlap_factor"])).astype(F32)
+    fdp = _rmul(_phasor((fE * np.conj(fE[:, :, :1])).astype(C64)), fmask[:, :, None])
+    k0s = np.asarray(correct_params["k0s"], dtype=F32).reshape(2, -1)
+    sh = mround(k0s).astype(int)
+    P = np.empty_like(fdp)
+    for k in range(n):
+        P[:, :, k] = np.roll(fdp[:, :, k], (sh[0, k], sh[1, k]), axis=(0, 1))
+    P = _rmul(P, NA[:, :, None])
+    # relative phase (:235-276), images in the order of |k0s| (stable sort)
+    seq = np.argsort(np.sqrt(k0s[0] * k0s[0] + k0s[1] * k0s[1]), kind="stable")
+    S = np.zeros((N1, N2), dtype=C64)
+    for ii in range(1, n):
+        S = (S + P[:, :, seq[ii - 1]]).astype(C64)
+        cur = P[:, :, seq[ii]]
+        keep = (np.abs(S) > 0) & (np.abs(cur) > 0)
+        t = (S * np.conj(cur)).astype(C64)[keep]
+        b = np.angle(np.complex64(t.astype(np.complex128).sum())).astype(F32)
+        P[:, :, seq[ii]] = (cur * np.exp(1j * b).astype(C64)).astype(C64)
+    P2 = P[:, :, 0].copy()
+    for k in range(1, n):
+        P2 = (P2 + P[:, :, k]).astype(C64)
+    # defocus search (:284-296)
+    dl = np.atleast_1d(np.asarray(correct_params["distList"], dtype=np.float64))
+    cc = np.zeros(len(dl), dtype=F32)
+    ph2 = np.exp(-1j * np.angle(P2).astype(F32)).astype(C64)
+    for i, d in enumerate(dl):
+        t = _rmul((np.exp((rk * F32(d)).astype(C64)) * ph2).astype(C64), NA)
+        cc[i] = np.abs(np.complex64(t.astype(np.complex128).sum()))
+    cmax = int(np.argmax(cc))
+    approx = (rk * F32(dl[cmax])).astype(C64)
+    approx = (approx - approx[N1 // 2, N2 // 2]).astype(C64)
+    ea = np.exp(1j * approx).astype(C64)
+    # low-pass box from the most frequent sideband step (:307-326)
+    k2 = mround(k0s[1]).astype(F32)
+    vals, counts = np.unique(np.diff(k2), return_counts=True)
+    if len(vals) == 0:
+        raise ValueError("get_aberration_pattern needs at least two fields")
+    dist = F32(abs(vals[int(np.argmax(counts))]) * F32(2))
+    if not dist > 0:
+        raise ValueError("the most frequent step of round(k0s(2,:)) is 0 (no low-pass box)")
+    c1, c2 = N1 // 2, N2 // 2
+    r0, r1 = c1 - int(np.floor(F32(N1) / dist)), c1 + int(np.ceil(F32(N1) / dist))
+    q0, q1 = c2 - int(np.floor(F32(N2) / dist)), c2 + int(np.ceil(F32(N2) / dist))
+    if r0 < 0 or q0 < 0 or r1 > N1 - 1 or q1 > N2 - 1:
+        raise ValueError("the low-pass box leaves the image")
+    lpf = np.zeros((N1, N2), dtype=F32)
+    lpf[r0:r1 + 1, q0:q1 + 1] = 1
+    psf = fftc2((P2 * ea).astype(C64), inverse=True).astype(C64)
+    psf = _rmul(psf, lpf)
+    P3 = (fftc2(psf).astype(C64) * ea).astype(C64)
+    # pattern and corrected fields (:343-351)
+    pattern = _rmul((P3 * np.exp(-1j * np.angle(P3[c1, c2]).astype(F32))).astype(C64), NA)
+    filt = np.exp(-1j * np.angle(pattern).astype(F32)).astype(C64)
+
+    def apply(f):
+        g = fftc2((fftc2(f).astype(C64) * filt[:, :, None]).astype(C64), inverse=True).astype(C64)
+        return g.reshape(np.shape(input_field), order="F")
+
+    return apply(fin), apply(fout), {"pattern": pattern, "distance": float(dl[cmax]), "utility": u}
+
+
+def correct_aberration(u, input_field, field_trans, aberration_params):
+    """:354-390 (correct_aberration): the pattern brought to the fields'
+    Fourier resolution and field of view (the reference's steps, including
+    the inverse transform after the field-of-view crop), masked by the NA
+    circle of the pattern's coordinates, then
+    ifft2c(fft2c(field) .* exp(-1i angle(pattern))) for both stacks."""
+    pattern = np.asarray(aberration_params["pattern"], dtype=C64)
+    ua = aberration_params["utility"]
+    N = np.shape(input_field)[0]
+    target = int(mround(N * ua["fourier_res"][0] / u["fourier_res"][0] / 2) * 2)
+
+    def half(a, b):
+        d = float(np.floor(a - b)) / 2
+        if d != int(d):
+            raise ValueError("odd size difference in correct_aberration")
+        return int(d)
+
+    if target > N:
+        p = fftc2(pattern).astype(C64)
+        c = half(target, p.shape[0])
+        p0 = np.zeros((target, target), dtype=C64)
+        p0[c:target - c, c:target - c] = p
+        pattern = fftc2(p0, inverse=True).astype(C64)
+    elif target < N:
+        p = fftc2(pattern).astype(C64)
+        c = half(p.shape[0], target)
+        pattern = fftc2(p[c:p.shape[0] - c, c:p.shape[1] - c], inverse=True).astype(C64)
+    if pattern.shape[0] > N:
+        c = half(pattern.shape[0], N)
+        pattern = fftc2(pattern[c:pattern.shape[0] - c, c:pattern.shape[1] - c], inverse=True).astype(C64)
+    elif pattern.shape[0] < N:
+        c = half(target, pattern.shape[0])
+        p0 = np.zeros((target, target), dtype=C64)
+        p0[c:target - c, c:target - c] = pattern
+        pattern = p0
+    f1 = (np.asarray(ua["fourier_coor"][0], dtype=F32) * F32(pattern.shape[0])) / F32(target)
+    f2 = (np.asarray(ua["fourier_coor"][1], dtype=F32) * F32(pattern.shape[1])) / F32(target)
+    na = np.sqrt(f1[:, None] ** 2 + f2[None, :] ** 2) < u["kmax"]
+    if na.shape != pattern.shape:
+        raise ValueError("aberration pattern and optical grid sizes differ")
+    pattern = _rmul(pattern, na.astype(F32))
+    filt = np.exp(-1j * np.angle(pattern).astype(F32)).astype(C64)
+
+    def apply(f):
+        s = _stack(f)
+        g = fftc2((fftc2(s).astype(C64) * filt[:, :, None]).astype(C64), inverse=True).astype(C64)
+        return g.reshape(np.shape(f), order="F")
+
+    return apply(input_field), apply(field_trans)
+
+
+ISOUTLIER_SCALE = 1.4826022185056018   # -1 / (sqrt(2) erfcinv(3/2)): MAD -> standard deviation
+
+
+def isoutlier(x):
+    """MATLAB isoutlier(x) (default 'median' method): more than three scaled
+    median absolute deviations from the median."""
+    x = np.asarray(x, dtype=np.float64)
+    med = np.median(x)
+    mad = ISOUTLIER_SCALE * np.median(np.abs(x - med))
+    return (x < med - 3 * mad) | (x > med + 3 * mad)
+
+
+def remove_dirty_fields(input_field, output_field, prctile=95, unwrap=None):
+    """:399-452 (remove_dirty_fields) for scalar fields without the manual
+    review: per image the standard deviation of the gradient energy of
+    |sp/bg|_k - |sp/bg|_1 and the fraction of unwrapped phase outside
+    1.5 x [min, max] of the first image's; keeps the first field and those
+    that are neither isoutlier nor above the fraction prctile / 100.
+    Returns (input_field_f, output_field_f, gradient_std, outside_count)."""
+    bg, sp = _stack(input_field), _stack(output_field)
+    q = (sp / bg).astype(C64)
+    amp = np.abs(q).astype(F32)
+    ph = np.angle(q).astype(F32)
+    ph = np.asarray(unwrap(ph) if unwrap is not None else ph, dtype=F32).reshape(amp.shape, order="F")
+    p0 = ph[:, :, 0]
+    hi, lo = F32(p0.max() * F32(1.5)), F32(p0.min() * F32(1.5))
+    n = amp.shape[2]
+    sd = np.zeros(n, dtype=F32)
+    cnt = np.zeros(n, dtype=np.int64)
+    for k in range(n):
+        f1 = (amp[:, :, k] - amp[:, :, 0]).astype(F32)
+        gy, gx = np.gradient(f1)
+        g = (gx * gx + gy * gy).astype(F32)
+        sd[k] = F32(np.std(g.astype(np.float64), ddof=1))
+        cnt[k] = np.count_nonzero(ph[:, :, k] > hi) + np.count_nonzero(ph[:, :, k] < lo)
+    bad2 = cnt / float(p0.size) > prctile / 100
+    keep = np.flatnonzero(~isoutlier(sd.astype(np.float64)) & ~bad2)
+    F = np.unique(np.concatenate([[0], keep])).astype(int)
+    N1, N2 = bg.shape[:2]
+    return (bg[:, :, F].reshape(N1, N2, 1, len(F), order="F"), sp[:, :, F].reshape(N1, N2, 1, len(F), order="F"),
+            sd, cnt)

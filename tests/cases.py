@@ -93,3 +93,48 @@ def off_axis_holograms(N=128, n=3, seed=0, carrier=(-0.23, -0.27), noise=0.0, ph
         bg.append(np.abs(R + U) ** 2 * 60 + noise * rng.standard_normal((N, N)))
         sp.append(np.abs(R + U * amp * np.exp(1j * phi)) ** 2 * 60 + noise * rng.standard_normal((N, N)))
     return np.stack(bg, 2).astype(np.float32), np.stack(sp, 2).astype(np.float32), phi
+
+
+def aberrated_fields(N=96, n=7, seed=0, step=4, res=0.1, NA=1.2, wavelength=0.532, RI_bg=1.3355):
+    """Synthetic scalar field pairs [N, N, 1, n] (single complex) for the
+    aberration and dirty-field tests: tilted plane waves whose spectra sit
+    at k0s = (rows, columns) pixels from the centre (columns stepping by
+    `step`, rows random with sub-pixel offsets), with and without an
+    object (a phase / absorption bump and a broadband phase screen of
+    0.5 rad), each passed through the pupil NA .* exp(1i W)
+    (W: defocus, astigmatism and coma over the NA circle).  Returns
+    (input_field, output_field, k0s [2, n], optical parameters)."""
+    rng = np.random.default_rng(seed)
+    params = dict(size=[N, N, 1], resolution=[res, res, res], NA=NA, wavelength=wavelength, RI_bg=RI_bg)
+    fr = 1.0 / (res * N)
+    idx = np.arange(N) - N // 2
+    ky, kx = np.meshgrid(idx * fr, idx * fr, indexing="ij")
+    kmax = NA / wavelength
+    rho_y, rho_x = ky / kmax, kx / kmax
+    rho2 = rho_x ** 2 + rho_y ** 2
+    W = 0.5 * rho2 + 1.2 * (rho_x ** 2 - rho_y ** 2) + 0.8 * rho_x * rho2
+    pupil = np.where(rho2 < 1, np.exp(1j * W), 0)
+    y, x = np.meshgrid(np.arange(N), np.arange(N), indexing="ij")
+    g = np.exp(-(((y - N / 2) ** 2 + (x - N / 2) ** 2) / (N / 7) ** 2))
+    # broadband phase screen (white noise smoothed over ~1 pixel): the object
+    # spectrum fills the pupil, as a cell or a diffuser does
+    screen = np.real(np.fft.ifft2(np.fft.fft2(rng.standard_normal((N, N)))
+                                  * np.exp(-0.5 * (2 * np.pi * np.fft.fftfreq(N)[:, None]) ** 2
+                                           - 0.5 * (2 * np.pi * np.fft.fftfreq(N)[None, :]) ** 2)))
+    screen *= 0.5 / screen.std()
+    obj = (1 - 0.1 * g) * np.exp(1j * (0.6 * g + screen))
+    cols = (np.arange(n) - (n - 1) / 2) * step
+    k0s = np.stack([rng.integers(-3, 4, n) + rng.uniform(-0.3, 0.3, n), cols + rng.uniform(-0.3, 0.3, n)])
+
+    def c2(a, inverse=False):
+        a = np.fft.ifftshift(a)
+        return np.fft.fftshift(np.fft.ifft2(a) if inverse else np.fft.fft2(a))
+
+    inp, out = [], []
+    for k in range(n):
+        wave = np.exp(2j * np.pi * (k0s[0, k] * y + k0s[1, k] * x) / N)
+        inp.append(c2(c2(wave) * pupil, inverse=True))
+        out.append(c2(c2(wave * obj) * pupil, inverse=True))
+    inp = np.stack(inp, 2)[:, :, None, :].astype(np.complex64)
+    out = np.stack(out, 2)[:, :, None, :].astype(np.complex64)
+    return np.asfortranarray(inp), np.asfortranarray(out), k0s.astype(np.float32), params
