@@ -464,7 +464,7 @@ def run_retrieval(args):
     import cases
 
     from inverse_solver_b200.retrieval import FIELD_EXPERIMENTAL_RETRIEVAL
-    from oracle import goldstein, retrieval
+    from oracle import cbs, goldstein, retrieval
 
     N, n = 1024, args.n_ill
     bg, sp, _ = cases.off_axis_holograms(N, n, seed=SEED)
@@ -486,13 +486,38 @@ def run_retrieval(args):
     t0 = time.perf_counter()
     retrieval.get_fields(p, bg[:, :, :2], sp[:, :, :2], unwrap=unwrap)
     dtc = time.perf_counter() - t0
+    del bg, sp
+    # aberration correction and dirty-field rejection on fields of the size
+    # get_fields returns here (636 x 636 = 4 * 3 * 53: Bluestein transforms)
+    L = 636
+    fin, fout, k0s, fp = cases.aberrated_fields(L, n, seed=SEED)
+    ra = FIELD_EXPERIMENTAL_RETRIEVAL(FIELD_EXPERIMENTAL_RETRIEVAL.get_default_parameters(fp))
+    cp = dict(overlap_factor=0.25, distList=[-2.0, -1.0, 0.0, 1.0, 2.0], k0s=k0s)
+    side = {}
+    for name, fn in (("get_aberration_pattern", lambda: ra.get_aberration_pattern(fin, fout, cp)),
+                     ("correct_aberration", lambda: ra.correct_aberration(fin, fout, ab)),
+                     ("remove_dirty_fields", lambda: ra.remove_dirty_fields(fin, fout))):
+        for _ in range(max(1, args.warmup)):
+            res = fn()
+        if name == "get_aberration_pattern":
+            ab = res[2]
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            fn()
+        side[name] = {"fields_per_s": n * args.steps / (time.perf_counter() - t0)}
+    t0 = time.perf_counter()
+    retrieval.get_aberration_pattern(cbs.derive_optical_tool(fp, cbs.Prec(True)), fin[..., :7], fout[..., :7],
+                                     dict(cp, k0s=k0s[:, :7]))
+    side["get_aberration_pattern"]["cpu_port_fields_per_s"] = 7 / (time.perf_counter() - t0)
     print(json.dumps({
         "metric": "holograms/s", "value": n / dt, "unit": "holograms/s", "higher_is_better": True,
         "ms_per_stack": dt * 1e3, "steps": args.steps, "warmup": args.warmup,
         "config": {"workload": "FIELD_EXPERIMENTAL_RETRIEVAL.get_fields: %d background / sample off-axis "
                                "holograms of %d x %d, 0.0625 um camera pixel, 0.1 um output" % (n, N, N)},
         "cpu_baseline": {"value": 2 / dtc, "unit": "holograms/s", "cores": os.cpu_count(), "kind": "port",
-                         "sample": "2 holograms"}}), flush=True)
+                         "sample": "2 holograms"},
+        "field_steps": {"config": "%d synthetic aberrated field pairs of %d x %d through the host API "
+                                  "(host arrays in and out); CPU port on 7 pairs" % (n, L, L), **side}}), flush=True)
 
 
 def workload_key():
