@@ -195,16 +195,32 @@ odt_status odt_set_adjoint_potential(odt_handle h, const odt_potential_params* p
                                      const odt_cfloat* V);
 
 /*
+ * Potential of an RI tensor (set_RI with size(RI,4) > 1,
+ * FORWARD_SOLVER_CONVERGENT_BORN.m:180-219): V [sim_x, sim_y, sim_z, 3, 3]
+ * column-major, V(:,:,:,i,j) = RI2potential of the padded tensor component
+ * (i, j), minus 1i * eps_imag on the diagonal (:216-219); eps_imag =
+ * 1.01 * max |potential| over all nine components.  Dyadic (pol = 3) handles
+ * only; replaces the forward slot's potential until the next
+ * odt_set_potential.  The x-pass then couples the three field components
+ * voxel by voxel (:567-574, :588-594, :624-627), as does the emitter of the
+ * transmitted / reflected fields (:451-455).  odt_gradient rejects it.
+ */
+odt_status odt_set_tensor_potential(odt_handle h, const odt_potential_params* pp, const odt_cfloat* V);
+
+/*
  * Gradient of the transmitted-field misfit (BACKWARD_SOLVER_MULTI.m:30-54),
  * fused on the device: forward solve (potential of odt_set_potential) ->
  * diff = trans - fields_meas, err = sum |diff|^2 (accumulated in double) ->
  * adjoint solve of conj(diff) (potential of odt_set_adjoint_potential) ->
- * grad = -1i * mean_ill(conj(E_3D) .* flip(conj(A_3D), 3)).
+ * grad = -1i * mean(conj(E_3D) .* flip(conj(A_3D), 3), [4 5]).
+ * On a dyadic (pol = 3) handle the fields carry two polarisations per
+ * illumination and the mean runs over the three field components and the
+ * illuminations, as the reference's mean over [pole_num, n_ill] does.
  * `err` is a host pointer in both memory modes.
  */
 typedef struct odt_gradient_args {
-  const odt_cfloat* fields_in;    /* [F_x, F_y, n_ill] illuminations            */
-  const odt_cfloat* fields_meas;  /* [F_x, F_y, n_ill] measured transmissions   */
+  const odt_cfloat* fields_in;    /* [F_x, F_y, npol, n_ill] illuminations      */
+  const odt_cfloat* fields_meas;  /* [F_x, F_y, npol, n_ill] measured trans.    */
   int32_t n_ill;
   odt_cfloat* grad;               /* [ri] output                                 */
   double* err;                    /* host scalar output                          */

@@ -351,6 +351,7 @@ SIGNATURES = {
                                        C.c_int32, C.POINTER(C.c_int32)]),
     "odt_born_series_noalloc": (C.c_int, [C.POINTER(NoallocBornArgs)]),
     "odt_set_adjoint_potential": (C.c_int, [C.c_uint32, C.POINTER(PotentialParams), C.c_void_p]),
+    "odt_set_tensor_potential": (C.c_int, [C.c_uint32, C.POINTER(PotentialParams), C.c_void_p]),
     "odt_gradient": (C.c_int, [C.c_uint32, C.POINTER(GradientArgs)]),
     "odt_tv_prox": (C.c_int, [C.POINTER(TVArgs)]),
     "odt_potential_eps_device": (C.c_int, [C.c_uint32, C.POINTER(RIDeviceArgs), C.POINTER(C.c_float)]),

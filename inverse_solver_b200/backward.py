@@ -120,8 +120,7 @@ class BACKWARD_SOLVER_MULTI:
 
     def _use_device_loop(self):
         fs = self.forward_solver
-        return (self.parameters.get("device_loop", True) and fs is not None and hasattr(fs, "set_RI_device")
-                and not getattr(fs, "vector", False))
+        return self.parameters.get("device_loop", True) and fs is not None and hasattr(fs, "set_RI_device")
 
     def solve(self, input_field, output_field):
         """:92-196: FISTA outer loop."""
@@ -192,12 +191,13 @@ class BACKWARD_SOLVER_MULTI:
         yin = np.asarray(output_field)
         if xin.ndim == 3:
             xin, yin = xin[:, :, :, None], yin[:, :, :, None]
-        if xin.shape != yin.shape or xin.shape[2] != 1:
-            raise ValueError("input and output fields must be [F_x, F_y, 1, n] alike")
+        npol = 2 if getattr(fs, "vector", False) else 1
+        if xin.shape != yin.shape or xin.shape[2] != npol:
+            raise ValueError("input and output fields must be [F_x, F_y, %d, n] alike" % npol)
         nill = xin.shape[3]
-        fin = up(xin[:, :, 0, :])
-        fmeas = up(yin[:, :, 0, :])
-        nF = xin.shape[0] * xin.shape[1]
+        fin = up(xin)
+        fmeas = up(yin)
+        nF = xin.shape[0] * xin.shape[1] * npol
         s = torch.cuda.current_stream(dev)
         fa = _lib.FistaArgs()
         fa.n = n

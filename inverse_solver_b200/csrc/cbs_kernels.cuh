@@ -64,6 +64,12 @@ cudaError_t launch_pol32(const float2* in, float2* out, const PolTables& t, bool
 // z-pass with the dyadic Green's function; a.nbatch = 3 * illuminations
 cudaError_t launch_born_z_dyadic(const BornArgs& a, const DyadArgs& d, int jj, const DevFft& fz,
                                  int max_smem, cudaStream_t s);
+// RI tensor (V9 [nvox, 3, 3]): the x-pass's pointwise work of iteration jj
+// (mode First / Mid / Last as launch_born_x) on the inverse x-FFT in a.T, and
+// the output stage's emitter into conv [c0, c1, rz, a.nbatch]
+cudaError_t launch_born_tensor_point(const BornArgs& a, const float2* V9, int mode, int jj, cudaStream_t s);
+cudaError_t launch_born_tensor_emitter(const BornArgs& a, const float2* V9, float2* conv, int c0, int c1,
+                                       int o0, int o1, float dV, cudaStream_t s);
 
 // x-pass of iteration jj: inverse x-FFT + update of iteration jj-1 (Mid/Last)
 // and source term + forward x-FFT of iteration jj (First/Mid).

@@ -126,6 +126,8 @@ struct Handle {
     float2* ramp[3] = {nullptr, nullptr, nullptr};
     float* kq2[3] = {nullptr, nullptr, nullptr};
     float* rad[3] = {nullptr, nullptr, nullptr};   // dyadic handles
+    float2* V9 = nullptr;  // RI tensor potential [nvox, 3, 3] (dyadic handles)
+    bool tensor = false;   // the slot's potential is V9, not V
   } pot[2];
   float2* fout_adj = nullptr;   // adjoint 3D field of a batch (odt_gradient)
   float2* grad_acc = nullptr;   // gradient accumulator [ri]
@@ -419,6 +421,9 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
   const IoGeom gin{Cx, Cy, Rx, Ry, Rz, ocx, ocy, nbp}, gout{Cx, Cy, Rx, Ry, Rz, orx, ory, nbp};
   const bool io_fused = H.use_pipe && io_fused_fits(gin, H.fcx, H.fcy, nacc, H.max_smem) &&
                         io_fused_fits(gout, H.fcx, H.fcy, nacc, H.max_smem);
+  // an RI tensor couples the field components in the emitter: unfused output
+  const bool ten = P.tensor;
+  const bool io_out_fused = io_fused && !ten;
   if (io_fused) {
     H.mark_begin(kKIoFft, s);
     ODT_CUDA(launch_refocus_in(H.c2a, H.refocus, conv, H.einc, gin, H.fcx, H.fcy, s));
@@ -464,7 +469,7 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
   a.Einc = H.einc;
   a.Fout = fout;
   const int B = P.pp.bornmax;
-  const bool pipe_x = H.use_pipe && born_x_pipe_supported(a, H.fx);
+  const bool pipe_x = !ten && H.use_pipe && born_x_pipe_supported(a, H.fx);
   const bool pipe_y = H.use_pipe && cols_pipe_supported(a, H.fy, false);
   const bool pipe_z = !vec && H.use_pipe && cols_pipe_supported(a, H.fz, true);
   DyadArgs dy{};
@@ -472,8 +477,14 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
     for (int i = 0; i < 3; ++i) dy.rad[i] = P.rad[i];
     dy.absorb = make_float2(P.pp.absorb.re, P.pp.absorb.im);
   }
+  const long long xlines = (long long)a.py * a.pz * nbp;
   for (int jj = 1; jj <= B; ++jj) {
-    if (pipe_x && jj >= 2) {
+    if (ten) {  // plain x-FFTs around the component-coupling pointwise kernel
+      H.mark_begin(kKBornX, s);
+      if (jj >= 2) ODT_CUDA(launch_fft_lines(a.T, a.T, xlines, 0, 0, 1.0f, true, H.fx, s));
+      ODT_CUDA(launch_born_tensor_point(a, P.V9, jj == 1 ? kBornFirst : kBornMid, jj, s));
+      ODT_CUDA(launch_fft_lines(a.T, a.T, xlines, 0, 0, 1.0f, false, H.fx, s));
+    } else if (pipe_x && jj >= 2) {
       H.mark_begin(jj <= 3 ? kKBornXPipeEdge : kKBornXPipe, s);
       ODT_CUDA(launch_born_x_pipe(a, kBornMid, jj, H.fx, H.d_fault, s));
     } else {
@@ -502,7 +513,11 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
       ODT_CUDA(launch_fft_cols(a.T, a.T, a.px, (long long)a.pz * nbp, 0, 0, 1.0f, true, H.fy, s));
     H.mark_end(s);
   }
-  if (pipe_x && B + 1 >= 2) {
+  if (ten) {
+    H.mark_begin(kKBornX, s);
+    if (B >= 1) ODT_CUDA(launch_fft_lines(a.T, a.T, xlines, 0, 0, 1.0f, true, H.fx, s));
+    ODT_CUDA(launch_born_tensor_point(a, P.V9, kBornLast, B + 1, s));
+  } else if (pipe_x && B + 1 >= 2) {
     H.mark_begin(kKBornXPipeEdge, s);
     ODT_CUDA(launch_born_x_pipe(a, kBornLast, B + 1, H.fx, H.d_fault, s));
   } else {
@@ -513,7 +528,7 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
 
   // ---- output projection (:445-511)
   if (want_t || want_r) {
-    if (io_fused) {
+    if (io_out_fused) {
       H.mark_begin(kKIoFft, s);
       ODT_CUDA(launch_project_out(a, conv, H.work_elems() * nbp, want_t ? H.ktrans : nullptr,
                                   want_r ? H.kref : nullptr, want_t ? H.c2a : nullptr, want_r ? H.c2b : nullptr,
@@ -521,7 +536,10 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
       H.mark_end(s);
     } else {
       H.mark_begin(kKIoElem, s);
-      ODT_CUDA(launch_emitter(a, conv, Cx, Cy, orx, ory, P.pp.dV, s));
+      if (ten)
+        ODT_CUDA(launch_born_tensor_emitter(a, P.V9, conv, Cx, Cy, orx, ory, P.pp.dV, s));
+      else
+        ODT_CUDA(launch_emitter(a, conv, Cx, Cy, orx, ory, P.pp.dV, s));
       H.mark_end(s);
       fftc2(H, conv, H.fcx, H.fcy, (long long)Rz * nbp, false, s);
       H.mark_begin(kKIoElem, s);
@@ -612,10 +630,12 @@ void alloc_slot(Handle& H, int k) {
 // V from the host (odt_set_potential) or built on the device from an RI
 // array in device memory (odt_set_potential_device: dev != NULL)
 void set_potential_slot(const std::shared_ptr<Handle>& Hp, int k, const odt_potential_params* pp,
-                        const odt_cfloat* V, const char* fn, const odt_ri_device_args* dev = nullptr) {
+                        const odt_cfloat* V, const char* fn, const odt_ri_device_args* dev = nullptr,
+                        const odt_cfloat* V9 = nullptr) {
   Handle& H = *Hp;
   const std::string who(fn);
-  if (!pp || (!V && !dev)) raise(ODT_ERR_INVALID_ARGUMENT, who + ": NULL argument");
+  if (!pp || (!V && !dev && !V9)) raise(ODT_ERR_INVALID_ARGUMENT, who + ": NULL argument");
+  if (V9 && H.np != 3) raise(ODT_ERR_INVALID_ARGUMENT, who + ": an RI tensor needs a dyadic (pol = 3) handle");
   const odt_geometry& g = H.g;
   for (int i = 0; i < 3; ++i) {
     const int lo = pp->roi[2 * i], hi = pp->roi[2 * i + 1];
@@ -636,7 +656,10 @@ void set_potential_slot(const std::shared_ptr<Handle>& Hp, int k, const odt_pote
   alloc_slot(H, k);
   Handle::PotSlot& P = H.pot[k];
   const size_t nv = (size_t)H.nvox();
-  if (dev) {
+  if (V9) {
+    if (!P.V9) P.V9 = H.dalloc<float2>(9 * nv, false);
+    ODT_CUDA(cudaMemcpy(P.V9, V9, 9 * nv * sizeof(float2), cudaMemcpyHostToDevice));
+  } else if (dev) {
     int roi0[3];
     for (int i = 0; i < 3; ++i) roi0[i] = pp->roi[2 * i] - 1;
     cudaStream_t s = (cudaStream_t)dev->stream;
@@ -660,6 +683,7 @@ void set_potential_slot(const std::shared_ptr<Handle>& Hp, int k, const odt_pote
     }
   }
   P.pp = *pp;
+  P.tensor = V9 != nullptr;
   for (int i = 0; i < 3; ++i) {  // do not keep caller pointers
     P.pp.mask[i] = nullptr;
     P.pp.ramp[i] = nullptr;
@@ -765,6 +789,13 @@ odt_status odt_set_adjoint_potential(odt_handle h, const odt_potential_params* p
   return guarded([&] { set_potential_slot(lookup(h), 1, pp, V, "odt_set_adjoint_potential"); });
 }
 
+odt_status odt_set_tensor_potential(odt_handle h, const odt_potential_params* pp, const odt_cfloat* V9) {
+  return guarded([&] {
+    if (!V9) raise(ODT_ERR_INVALID_ARGUMENT, "odt_set_tensor_potential: NULL argument");
+    set_potential_slot(lookup(h), 0, pp, nullptr, "odt_set_tensor_potential", nullptr, V9);
+  });
+}
+
 namespace {
 void check_ri_device_args(const Handle& H, const odt_ri_device_args* a, const char* fn) {
   const std::string who(fn);
@@ -772,7 +803,6 @@ void check_ri_device_args(const Handle& H, const odt_ri_device_args* a, const ch
   if (!is_device_ptr(a->ri)) raise(ODT_ERR_INVALID_ARGUMENT, who + ": ri is not a device pointer");
   if (!(a->wavelength > 0.0) || !(a->ri_bg > 0.0) || !std::isfinite(a->wavelength) || !std::isfinite(a->ri_bg))
     raise(ODT_ERR_INVALID_ARGUMENT, who + ": wavelength and ri_bg must be positive");
-  if (H.np != 1) raise(ODT_ERR_UNSUPPORTED, who + ": scalar handles only");
 }
 }  // namespace
 
@@ -925,10 +955,12 @@ odt_status odt_gradient(odt_handle h, const odt_gradient_args* args) {
     auto H = lookup(h);
     if (!args) raise(ODT_ERR_INVALID_ARGUMENT, "odt_gradient: NULL args");
     const odt_gradient_args& A = *args;
-    if (H->np == 3)
-      raise(ODT_ERR_UNSUPPORTED, "odt_gradient: the dyadic (vector) gradient is not supported");
+    if (H->np == 3 && !H->have_pol)
+      raise(ODT_ERR_NOT_READY, "odt_gradient: a dyadic handle needs odt_set_polarisation first");
     if (!H->pot[0].have || !H->pot[1].have)
       raise(ODT_ERR_NOT_READY, "odt_gradient: set the forward and the adjoint potential first");
+    if (H->pot[0].tensor)
+      raise(ODT_ERR_UNSUPPORTED, "odt_gradient: the gradient of an RI tensor is not supported");
     if (A.n_ill < 1 || !A.fields_in || !A.fields_meas || !A.grad || !A.err)
       raise(ODT_ERR_INVALID_ARGUMENT, "odt_gradient: NULL buffer or n_ill < 1");
     if (A.memory != ODT_MEM_HOST && A.memory != ODT_MEM_DEVICE)
@@ -941,7 +973,10 @@ odt_status odt_gradient(odt_handle h, const odt_gradient_args* args) {
       raise(ODT_ERR_INVALID_ARGUMENT, "odt_gradient: ODT_MEM_DEVICE with a non-device pointer");
     cudaStream_t s = dev ? (cudaStream_t)A.stream : H->own_stream;
     ensure_batch(*H, std::min<int>(A.n_ill, auto_batch(*H)));
-    const long long nF = H->nf(), nR = H->nri();
+    // per illumination: npol planes of [F_x, F_y] in, np components of [ri] in 3D;
+    // the gradient is the mean over components and illuminations (the
+    // reference's mean(..., [4 5]) over [ri, pole_num, n_ill])
+    const long long nF = H->nf() * H->npol, nR = H->nri();
     if (H->grad_batch != H->batch) {
       for (void** p : {(void**)&H->fout_adj, (void**)&H->grad_acc, (void**)&H->d_err}) {
         if (*p) {
@@ -952,7 +987,7 @@ odt_status odt_gradient(odt_handle h, const odt_gradient_args* args) {
           *p = nullptr;
         }
       }
-      H->fout_adj = H->dalloc<float2>((size_t)nR * H->batch, false);
+      H->fout_adj = H->dalloc<float2>((size_t)nR * H->np * H->batch, false);
       H->grad_acc = H->dalloc<float2>((size_t)nR, false);
       H->d_err = H->dalloc<double>(1, false);
       H->grad_batch = H->batch;
@@ -967,17 +1002,17 @@ odt_status odt_gradient(odt_handle h, const odt_gradient_args* args) {
       ODT_CUDA(cudaMemcpyAsync(H->out_r, A.fields_meas + (size_t)b0 * nF,
                                (size_t)nb * nF * sizeof(float2), kin, s));
       run_chunk_graph(*H, nb, s, true, false, 0, H->fout);        // E_3D, trans
-      ODT_CUDA(launch_residual(H->out_t, H->out_r, H->in2d, nF * nb, H->d_err, s));
+      ODT_CUDA(launch_residual(H->res_t, H->out_r, H->in2d, nF * nb, H->d_err, s));
       run_chunk_graph(*H, nb, s, false, false, 1, H->fout_adj);   // adjoint 3D field
       ODT_CUDA(launch_grad_accumulate(H->fout, H->fout_adj, H->grad_acc, H->g.ri_size[0],
-                                      H->g.ri_size[1], H->g.ri_size[2], nb, s));
+                                      H->g.ri_size[1], H->g.ri_size[2], nb * H->np, s));
       H->collect(s);
     }
     if (dev) {
       ODT_CUDA(launch_grad_finalize(H->grad_acc, reinterpret_cast<float2*>(A.grad), nR,
-                                    (float)A.n_ill, s));
+                                    (float)A.n_ill * H->np, s));
     } else {
-      ODT_CUDA(launch_grad_finalize(H->grad_acc, H->fout_adj, nR, (float)A.n_ill, s));
+      ODT_CUDA(launch_grad_finalize(H->grad_acc, H->fout_adj, nR, (float)A.n_ill * H->np, s));
       ODT_CUDA(cudaMemcpyAsync(A.grad, H->fout_adj, nR * sizeof(float2), cudaMemcpyDeviceToHost, s));
     }
     ODT_CUDA(cudaMemcpyAsync(A.err, H->d_err, sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -12,6 +12,11 @@
 //     A CTA takes 16 (x, y) columns of one illumination, z-transforms the
 //     three components into shared memory, couples them voxel by voxel and
 //     transforms each back.
+//   * an RI tensor (size(RI,4) > 1, V [sim, 3, 3]): the x-pass's pointwise
+//     work couples the components through V (:567-574, :588-594, :624-627),
+//     so it runs as its own kernel between plain x-FFTs (born_tensor_point),
+//     and the emitter of the output stage is sum_j Field_j pot_ij dV
+//     (:451-455, born_tensor_emitter).
 #include <cuda_runtime.h>
 
 #include "cbs_kernels.cuh"
@@ -154,6 +159,158 @@ __global__ void __launch_bounds__(128) born_z_dyadic_kernel(const BornArgs a, co
   }
 }
 
+// ---- RI tensor
+// Pointwise work of the x-pass (the tensor counterpart of BornXOp in
+// tile_bodies.cuh) for one voxel and one illumination, its three components
+// at batch entries 3 b + i.  T holds the inverse x-FFT of the spectral array
+// (modes Mid / Last) and receives the source term of iteration jj times the
+// phase ramp (modes First / Mid).  V9[v + nvox (i + 3 j)] = V_ij, with
+// -1i eps_imag on the diagonal.  Sums over j run in the reference's order
+// (j = 1, 2, 3, starting from the value the reference starts from).
+template <int MODE>
+__global__ void born_tensor_point_kernel(BornArgs a, const float2* __restrict__ V9, int jj, long long total) {
+  const long long nv = a.nvox;
+  const long long est = (long long)a.rx * a.ry * a.rz;
+  const float2 z2 = make_float2(0.f, 0.f);
+  const float2 cc = make_float2(0.f, a.c_im);
+  const int e = jj - 1;  // iteration whose update completes here
+  const bool upd = MODE != kBornFirst && e >= 1;
+  const bool need_fn = upd && e >= 3;
+  const bool need_f = upd && (e >= 3 || (MODE == kBornLast && e == 2));
+  const bool need_einc = MODE == kBornLast || jj <= 2;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long v = t % nv;
+    const long long b = t / nv;
+    const int x = (int)(v % a.px);
+    const long long r = v / a.px;
+    const int y = (int)(r % a.py);
+    const int z = (int)(r / a.py);
+    const bool in_roi = (unsigned)(x - a.rx0) < (unsigned)a.rx && (unsigned)(y - a.ry0) < (unsigned)a.ry &&
+                        (unsigned)(z - a.rz0) < (unsigned)a.rz;
+    const long long eo = in_roi ? (x - a.rx0) + (long long)a.rx * ((y - a.ry0) + (long long)a.ry * (z - a.rz0)) : 0;
+    float2 V[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) V[i][j] = V9[v + nv * (i + 3 * j)];
+    const float2 r0 = a.acyclic ? cmul(cmul(a.ramp[0][x], a.ramp[1][y]), a.ramp[2][z]) : make_float2(1.f, 0.f);
+    const float m = (a.mask[0][x] * a.mask[1][y]) * a.mask[2][z];
+    float2 P[3], Fo[3], Fp[3], Ei[3], fn_new[3], ftot[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const long long gi = v + nv * (3 * b + i);
+      P[i] = upd ? a.T[gi] : z2;
+      if (upd && a.acyclic) P[i] = cmul(P[i], (e & 1) ? r0 : cconj(r0));
+      Fo[i] = need_fn ? a.Fn[gi] : z2;
+      Fp[i] = need_f ? a.F[gi] : z2;
+      Ei[i] = (need_einc && in_roi) ? a.Einc[(3 * b + i) * est + eo] : z2;
+      fn_new[i] = z2;
+      ftot[i] = z2;
+    }
+    if (upd) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const long long gi = v + nv * (3 * b + i);
+        if (e <= 2) {  // Field_n = 0 + sum_j V_ij PSI_j, then the mask
+          float2 acc = cmul(V[i][0], P[0]);
+          acc = cadd(acc, cmul(V[i][1], P[1]));
+          acc = cadd(acc, cmul(V[i][2], P[2]));
+          fn_new[i] = cscale(acc, m);
+          if (MODE == kBornMid) {
+            a.Fn[gi] = fn_new[i];
+            if (e == 1) a.F[gi] = fn_new[i];
+          } else {
+            ftot[i] = (e == 1) ? fn_new[i] : cadd(Fp[i], fn_new[i]);
+          }
+        } else {
+          // psi of iteration e: sum_j (1i/eps) Field_n_j V_ij
+          float2 psi = cmul(cmul(cc, Fo[0]), V[i][0]);
+          psi = cadd(psi, cmul(cmul(cc, Fo[1]), V[i][1]));
+          psi = cadd(psi, cmul(cmul(cc, Fo[2]), V[i][2]));
+          float2 acc = csub(Fo[i], psi);
+          acc = cadd(acc, cmul(V[i][0], P[0]));
+          acc = cadd(acc, cmul(V[i][1], P[1]));
+          acc = cadd(acc, cmul(V[i][2], P[2]));
+          const float2 fn = cscale(acc, m);
+          if (e == 3) {
+            ftot[i] = cadd(cadd(Fp[i], Fo[i]), fn);
+            fn_new[i] = cadd(fn, Fp[i]);
+          } else {
+            ftot[i] = cadd(Fp[i], fn);
+            fn_new[i] = fn;
+          }
+          if (MODE == kBornMid) {
+            a.F[gi] = ftot[i];
+            a.Fn[gi] = fn_new[i];
+          }
+        }
+      }
+    }
+    if (MODE == kBornLast) {
+      if (in_roi) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) a.Fout[(3 * b + i) * est + eo] = cadd(ftot[i], Ei[i]);
+      }
+      continue;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      float2 psi = z2;
+      if (jj <= 2) {  // (1i/eps) (sum_j V_ij(ROI) E_inc_j + 1i eps E_inc_i) / 2 inside the ROI
+        if (in_roi) {
+          float2 sv = cmul(V[i][0], Ei[0]);
+          sv = cadd(sv, cmul(V[i][1], Ei[1]));
+          sv = cadd(sv, cmul(V[i][2], Ei[2]));
+          sv = cadd(sv, cmul(make_float2(0.f, a.eps), Ei[i]));
+          psi = cscale(cmul(cc, sv), 0.5f);
+        }
+      } else {  // sum_j (1i/eps) Field_n_j V_ij
+        psi = cmul(cmul(cc, fn_new[0]), V[i][0]);
+        psi = cadd(psi, cmul(cmul(cc, fn_new[1]), V[i][1]));
+        psi = cadd(psi, cmul(cmul(cc, fn_new[2]), V[i][2]));
+      }
+      if (a.acyclic) psi = cmul(psi, (jj & 1) ? cconj(r0) : r0);
+      a.T[v + nv * (3 * b + i)] = psi;
+    }
+  }
+}
+
+// emitter_i = sum_j Field_j pot_ij dV on the [c0, c1, rz] plane stack of each
+// component (entry 3 b + i), zero outside the RI window; pot = V + 1i eps on
+// the diagonal
+__global__ void born_tensor_emitter_kernel(BornArgs a, const float2* __restrict__ V9, float2* conv, int c0,
+                                           int c1, int o0, int o1, float dV, long long total) {
+  const long long est = (long long)a.rx * a.ry * a.rz;
+  const long long nv = a.nvox;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int X = (int)(t % c0);
+    long long q = t / c0;
+    const int Y = (int)(q % c1);
+    q /= c1;
+    const int z = (int)(q % a.rz);
+    const long long ent = q / a.rz;  // 3 b + i
+    const int i = (int)(ent % 3);
+    const long long b = ent / 3;
+    const int x = X - o0, y = Y - o1;
+    float2 out = make_float2(0.f, 0.f);
+    if ((unsigned)x < (unsigned)a.rx && (unsigned)y < (unsigned)a.ry) {
+      const long long eo = x + (long long)a.rx * (y + (long long)a.ry * z);
+      const long long v = (x + a.rx0) + (long long)a.px * ((y + a.ry0) + (long long)a.py * (z + a.rz0));
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        float2 pot = V9[v + nv * (i + 3 * j)];
+        if (j == i) pot.y += a.eps;
+        const float2 f = a.Fout[(3 * b + j) * est + eo];
+        const float2 term = cscale(cmul(f, pot), dV);
+        out = j == 0 ? term : cadd(out, term);
+      }
+    }
+    conv[t] = out;
+  }
+}
+
 size_t dyad_smem(int n, int W) {
   return align16(sizeof(float2) * n) + align16(sizeof(float) * 3 * W) + 5 * sizeof(float2) * (size_t)n * (W + 1);
 }
@@ -170,6 +327,24 @@ cudaError_t launch_pol32(const float2* in, float2* out, const PolTables& t, bool
                          long long nb, cudaStream_t s) {
   pol32_kernel<<<grid_for(nF * nb), kThreads, 0, s>>>(in, out, t.radial, t.perp, t.tan3, t.kmask,
                                                       reflection ? -1.f : 1.f, nF, nb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_born_tensor_point(const BornArgs& a, const float2* V9, int mode, int jj, cudaStream_t s) {
+  const long long total = a.nvox * (a.nbatch / 3);
+  switch (mode) {
+    case kBornFirst: born_tensor_point_kernel<kBornFirst><<<grid_for(total), kThreads, 0, s>>>(a, V9, jj, total); break;
+    case kBornMid: born_tensor_point_kernel<kBornMid><<<grid_for(total), kThreads, 0, s>>>(a, V9, jj, total); break;
+    case kBornLast: born_tensor_point_kernel<kBornLast><<<grid_for(total), kThreads, 0, s>>>(a, V9, jj, total); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_born_tensor_emitter(const BornArgs& a, const float2* V9, float2* conv, int c0, int c1, int o0,
+                                       int o1, float dV, cudaStream_t s) {
+  const long long total = (long long)c0 * c1 * a.rz * a.nbatch;
+  born_tensor_emitter_kernel<<<grid_for(total), kThreads, 0, s>>>(a, V9, conv, c0, c1, o0, o1, dV, total);
   return cudaGetLastError();
 }
 

@@ -151,6 +151,37 @@ class CBSHostSetup:
         V = (ri2potential(self.RI, lam, nm) - 1j * self.eps_imag).astype(C64)
         pp, keep = self.potential_params(self.eps_imag)
         self.V = V
+        self.tensor = False
+        return pp, keep + [_c64(V)]
+
+    def prepare_tensor_potential(self, RI):
+        """prepare_potential for an RI tensor [x, y, z, 3, 3]
+        (FORWARD_SOLVER_CONVERGENT_BORN.m:199-279 with size(RI,4) > 1):
+        eps_imag = 1.01 max |potential| over all nine components (the
+        reference's pagesvd runs on the 1 x 1 pages of pott(:)), every
+        component padded with zero potential and passed through the
+        RI2potential / potential2RI round trips, V(:,:,:,j,j) -= 1i eps_imag.
+        Returns the PotentialParams and the arrays it points into, V
+        ([sim, 3, 3], column-major) last."""
+        if not self.vector:
+            raise ValueError("a tensor RI needs vector_simulation (the dyadic Green's function)")
+        RI = np.asarray(RI)
+        if list(RI.shape[:3]) != list(self.expected_RI_size) or RI.shape[3:] != (3, 3):
+            raise ValueError("The refractive index tensor must be [%d %d %d 3 3]" % tuple(self.expected_RI_size))
+        RI = RI.astype(C64 if np.iscomplexobj(RI) else F32)
+        p = self.parameters
+        lam, nm = p["wavelength"], p["RI_bg"]
+        self.eps_imag = F32(np.abs(ri2potential(RI.ravel(), lam, nm)).max() * 1.01)
+        btp = [int(b) for b in self.boundary_thickness_pixel]
+        RIp = np.pad(ri2potential(RI, lam, nm), [(btp[0], btp[0]), (btp[1], btp[1]), (btp[2], btp[2]), (0, 0), (0, 0)])
+        V_temp = ri2potential(potential2ri(RIp, lam, nm), lam, nm)
+        self.RI = potential2ri(V_temp, lam, nm)
+        V = ri2potential(self.RI, lam, nm).astype(C64)
+        for j in range(3):
+            V[:, :, :, j, j] = V[:, :, :, j, j] - 1j * self.eps_imag
+        pp, keep = self.potential_params(self.eps_imag)
+        self.V = V
+        self.tensor = True
         return pp, keep + [_c64(V)]
 
     def potential_params(self, eps_imag):
@@ -313,7 +344,18 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
 
     def set_RI(self, RI):
         """set_RI (FORWARD_SOLVER_CONVERGENT_BORN.m:180-198) + CudaBorn action 1
-        (FORWARD_SOLVER_CONVERGENT_BORN_CUDA.m:42-63)."""
+        (FORWARD_SOLVER_CONVERGENT_BORN_CUDA.m:42-63).  An RI tensor
+        [x, y, z, 3, 3] (or the struct form {"scatt_pott": tensor}, :181-186)
+        goes to odt_set_tensor_potential (vector_simulation only)."""
+        if isinstance(RI, dict):
+            RI = np.asarray(RI["scatt_pott"])
+            if RI.ndim < 4 or RI.shape[3] <= 1:
+                raise ValueError("Structur form only allowed for tensor RI")
+        RI = np.asarray(RI)
+        if RI.ndim >= 4 and RI.shape[3] > 1:
+            pp, keep = self.prepare_tensor_potential(RI)
+            _lib.check(self.lib.odt_set_tensor_potential(self._handle, C.byref(pp), _lib.ptr(keep[-1])))
+            return
         pp, keep = self.prepare_potential(RI)
         _lib.check(self.lib.odt_set_potential(self._handle, C.byref(pp), _lib.ptr(keep[-1])))
 
@@ -375,17 +417,15 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
 
     def gradient_device(self, fields_in, fields_meas, grad, stream=None):
         """gradient() on device arrays: fields_in / fields_meas contiguous CUDA
-        complex64 tensors of F_x*F_y*n_ill elements (column-major
-        [F_x, F_y, n_ill]), grad a CUDA complex64 tensor of the RI grid's size;
-        returns err."""
+        complex64 tensors of F_x*F_y*npol*n_ill elements (column-major
+        [F_x, F_y, npol, n_ill]; npol = 2 with vector_simulation, else 1),
+        grad a CUDA complex64 tensor of the RI grid's size; returns err."""
         import torch
 
-        if self.vector:
-            raise NotImplementedError("the gradient is available for the scalar solver only")
-        nF = int(self.field_size[0] * self.field_size[1])
+        nF = int(self.field_size[0] * self.field_size[1]) * (2 if self.vector else 1)
         n_ill = fields_in.numel() // nF
         if fields_in.numel() != nF * n_ill or fields_meas.numel() != fields_in.numel() or n_ill < 1:
-            raise ValueError("input and output fields must be [F_x, F_y, n] alike")
+            raise ValueError("input and output fields must be [F_x, F_y, npol, n] alike")
         err = C.c_double(0)
         a = _lib.GradientArgs()
         a.fields_in, a.fields_meas = fields_in.data_ptr(), fields_meas.data_ptr()
@@ -402,17 +442,18 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
     def gradient(self, input_field, output_field):
         """Fused forward + adjoint gradient of get_gradiant_static
         (BACKWARD_SOLVER_MULTI.m:30-54) after set_RI(RI) and
-        set_RI_adjoint(RI): returns (gradient [RI size] complex64, err)."""
+        set_RI_adjoint(RI): returns (gradient [RI size] complex64, err).  With
+        vector_simulation the fields are [F_x, F_y, 2, n] and the gradient is
+        the mean over the three field components and the illuminations."""
         x = np.asarray(input_field)
         y = np.asarray(output_field)
         if x.ndim == 3:
             x = x[:, :, :, None]
         if y.ndim == 3:
             y = y[:, :, :, None]
-        if self.vector:
-            raise NotImplementedError("the gradient is available for the scalar solver only")
-        if x.shape != y.shape or x.shape[2] != 1:
-            raise ValueError("input and output fields must be [F_x, F_y, 1, n] alike")
+        npol = 2 if self.vector else 1
+        if x.shape != y.shape or x.shape[2] != npol:
+            raise ValueError("input and output fields must be [F_x, F_y, %d, n] alike" % npol)
         xin, yin = _c64(x), _c64(y)
         g = np.empty(self.expected_RI_size, dtype=C64, order="F")
         err = C.c_double(0)

@@ -391,7 +391,8 @@ def polarisation_utility(ZP, params, P: Prec):
 class ForwardSolverCBS:
     """Restatement of ``Codes/FORWARD_SOLVER_CONVERGENT_BORN.m``: the scalar
     Green's function, and with ``vector_simulation`` the dyadic one
-    (``pole_num = 3``, isotropic RI)."""
+    (``pole_num = 3``), for an isotropic RI ``[x, y, z]`` or, with the dyadic
+    Green's function, an RI tensor ``[x, y, z, 3, 3]`` (``size(RI,4) > 1``)."""
 
     def __init__(self, params, single=True):
         """Constructor ``:48-133``."""
@@ -489,22 +490,42 @@ class ForwardSolverCBS:
 
     # --- set_RI :180-198
     def set_RI(self, RI):
+        """``:180-198``; the struct form ``{"scatt_pott": RI}`` is accepted for
+        a tensor RI only (``:181-186``)."""
+        if isinstance(RI, dict):
+            RI = np.asarray(RI["scatt_pott"])
+            if RI.ndim < 4 or RI.shape[3] <= 1:
+                raise ValueError("Structur form only allowed for tensor RI")
         RI = np.asarray(RI)
         if list(RI.shape[:3]) != list(self.expected_RI_size):
             raise ValueError("The refractive index does not have the expected size")
+        self.tensor = RI.ndim >= 4 and RI.shape[3] > 1
+        if self.tensor and (RI.shape[3:] != (3, 3) or not self.vector):
+            raise ValueError("a tensor RI is [x, y, z, 3, 3] and needs vector_simulation")
+        if not self.tensor:
+            RI = RI.reshape(RI.shape[:3])
         self.RI = self.P.S(RI)
         self.condition_RI()
         self.init()
 
     def condition_RI(self):
-        """``:199-222`` (scalar potential)."""
+        """``:199-222``.  For a tensor RI the reference takes the largest
+        singular value of ``pagesvd(permute(pott(:), [4 5 1 2 3]))``: the pages
+        of the flattened column are 1 x 1, so that is max |potential| over all
+        nine components, as for the scalar case."""
         P, p = self.P, self.parameters
         pot = ri2potential(self.RI.ravel(), p["wavelength"], p["RI_bg"], P)
-        self.eps_imag = P.S(np.abs(pot).max() * 1.01)                 # :205
+        self.eps_imag = P.S(np.abs(pot).max() * 1.01)                 # :201-205
         self.ROI = self.create_boundary_RI()
         V = ri2potential(self.RI, p["wavelength"], p["RI_bg"], P)
-        self.V = V - 1j * self.eps_imag                               # :215
-        self.V = P.S(self.V)
+        if self.tensor:                                               # :216-219
+            V = P.S(V).astype(P.c)
+            for j1 in range(3):
+                V[:, :, :, j1, j1] = V[:, :, :, j1, j1] - 1j * self.eps_imag
+            self.V = V
+        else:
+            self.V = V - 1j * self.eps_imag                           # :215
+            self.V = P.S(self.V)
 
     def create_boundary_RI(self):
         """``:223-279``: zero-potential padding, ROI, attenuation mask."""
@@ -512,7 +533,8 @@ class ForwardSolverCBS:
         btp = [int(b) for b in self.boundary_thickness_pixel]  # Python ints keep single ops single
         old = self.RI.shape
         RIp = ri2potential(self.RI, p["wavelength"], p["RI_bg"], P)
-        RIp = np.pad(RIp, [(btp[0], btp[0]), (btp[1], btp[1]), (btp[2], btp[2])])
+        RIp = np.pad(RIp, [(btp[0], btp[0]), (btp[1], btp[1]), (btp[2], btp[2])]
+                     + [(0, 0)] * (RIp.ndim - 3))
         RIp = potential2ri(RIp, p["wavelength"], p["RI_bg"], P)
         ROI = [btp[0] + 1, btp[0] + old[0], btp[1] + 1, btp[1] + old[1], btp[2] + 1, btp[2] + old[2]]
         V_temp = ri2potential(RIp, p["wavelength"], p["RI_bg"], P)
@@ -545,7 +567,7 @@ class ForwardSolverCBS:
         """``:280-396``: Green's function, phase ramp, iteration count."""
         P, p = self.P, self.parameters
         pb = copy.deepcopy(p)
-        pb["size"] = list(self.RI.shape)
+        pb["size"] = list(self.RI.shape[:3])
         ub = self.utility_border = derive_optical_tool(pb, P)
         self.pole_num = 3 if self.vector else 1                      # :293-296
         fc, fr = ub["fourier_coor"], ub["fourier_res"]
@@ -600,7 +622,7 @@ class ForwardSolverCBS:
             self.ramp1d = None
         self.Greenp = np.fft.ifftshift(self.Greenp)                  # :384
         if self.pole_num == 3:                                        # :385
-            n = self.V.shape
+            n = self.V.shape[:3]
             r = np.zeros(tuple(n) + (3,), dtype=P.r)
             r[..., 0] = self.rads1d[0][:, None, None]
             r[..., 1] = self.rads1d[1][None, :, None]
@@ -689,7 +711,12 @@ class ForwardSolverCBS:
                 f3[:, :, :, :, k] = F4
             if p["return_transmission"] or p["return_reflection"]:
                 pot = ri2potential(self.RI[R[0] - 1:R[1], R[2] - 1:R[3], R[4] - 1:R[5]], p["wavelength"], p["RI_bg"], P)
-                em = F4 * pot[..., None] * self.utility_border["dV"]
+                if self.tensor:                                       # :451-455
+                    em = 0
+                    for j1 in range(3):
+                        em = em + F4[..., j1:j1 + 1] * pot[:, :, :, :, j1] * self.utility_border["dV"]
+                else:
+                    em = F4 * pot[..., None] * self.utility_border["dV"]
                 em = self.padd_RI2conv(em)
                 em = fftc2(em)
             if p["return_transmission"]:
@@ -724,7 +751,8 @@ class ForwardSolverCBS:
         if source.ndim == 3 and not vec:
             source = source[:, :, 0]
         V = self.V
-        shp = V.shape + ((3,) if vec else ())
+        ten = getattr(self, "tensor", False)
+        shp = V.shape[:3] + ((3,) if vec else ())
         psi = np.zeros(shp, dtype=P.c)
         Field = np.zeros(shp, dtype=P.c)
         Field_n = np.zeros(shp, dtype=P.c)
@@ -733,7 +761,14 @@ class ForwardSolverCBS:
         R = self.ROI
         roi = (slice(R[0] - 1, R[1]), slice(R[2] - 1, R[3]), slice(R[4] - 1, R[5]))
         Vx = V[..., None] if vec else V
-        source = ((V[roi] + 1j * self.eps_imag)[..., None] if vec else (V[roi] + 1j * self.eps_imag)) * source  # :566
+        if ten:                                                       # :567-574
+            src0 = source
+            source = np.zeros_like(src0)
+            for j1 in range(3):
+                source = source + V[roi][:, :, :, :, j1] * src0[..., j1:j1 + 1]
+            source = source + 1j * self.eps_imag * src0
+        else:
+            source = ((V[roi] + 1j * self.eps_imag)[..., None] if vec else (V[roi] + 1j * self.eps_imag)) * source  # :566
         Greenp = self.Greenp
         ramp = self.phase_ramp
         rads = self.rads if vec else None
@@ -752,6 +787,9 @@ class ForwardSolverCBS:
             if jj in (1, 2):
                 Field_n[...] = 0
                 psi[roi] = c * source / 2
+            elif ten:                                                 # :592-594
+                for j1 in range(3):
+                    psi = psi + c * Field_n[..., j1:j1 + 1] * V[:, :, :, :, j1]
             else:
                 psi = c * Field_n * Vx
             if vec:   # dyadic absorptive Green's function (:597-601)
@@ -769,7 +807,11 @@ class ForwardSolverCBS:
                 PSI = sfft.ifftn(PSI, workers=_WORKERS) * np.conj(ramp)
             if jj not in (1, 2):
                 Field_n = Field_n - psi
-            Field_n = Field_n + Vx * PSI
+            if ten:                                                   # :624-627
+                for j1 in range(3):
+                    Field_n = Field_n + V[:, :, :, :, j1] * PSI[..., j1:j1 + 1]
+            else:
+                Field_n = Field_n + Vx * PSI
             Field_n = Field_n * (self.attenuation_mask[..., None] if vec else self.attenuation_mask)
             if jj == 2:
                 temp = Field

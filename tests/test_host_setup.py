@@ -38,3 +38,26 @@ def test_cyclic_xy_setup_matches_oracle():
     p = cases.params([24, 20, 18], [0, 0, 2])
     h = _compare(p, cases.small_RI()[:24, :20, :18])
     assert h.cyclic_boundary_xy and h.conv_size == h.field_size
+
+
+def test_tensor_potential_matches_oracle():
+    """prepare_tensor_potential (set_RI with an RI tensor [x, y, z, 3, 3])
+    equals the oracle's tensor condition_RI / create_boundary_RI bit for bit:
+    V with -1i eps_imag on the diagonal, eps_imag over all nine components."""
+    p = cases.params([24, 24, 18], [1.5, 1.5, 1.5])
+    p["vector_simulation"] = True
+    RI = cases.small_RI()[:24, :24, :18]
+    T = np.empty(RI.shape + (3, 3), np.float32)
+    T[...] = np.float32(cases.NM)
+    for i in range(3):
+        T[:, :, :, i, i] = cases.NM + (RI - cases.NM) * (1 - 0.2 * i)
+    T[:, :, :, 0, 1] = T[:, :, :, 1, 0] = cases.NM + (RI - cases.NM) * 0.1
+    h = CBSHostSetup(p)
+    o = cbs.ForwardSolverCBS(p, single=True)
+    pp, keep = h.prepare_tensor_potential(T)
+    o.set_RI(T)
+    assert h.tensor and o.tensor
+    assert h.V.shape == o.V.shape == tuple(h.sim_size) + (3, 3)
+    assert np.array_equal(h.V, o.V)
+    assert np.array_equal(keep[-1], o.V) and keep[-1].flags.f_contiguous
+    assert float(h.eps_imag) == float(o.eps_imag) and h.Bornmax == o.Bornmax

@@ -130,3 +130,170 @@ def test_vector_on_pipelined_grid_matches_oracle():
     o.set_RI(RI)
     ot, _, of = o.solve(fv)
     assert worst(f3, of) < 1e-5 and worst(t, ot) < 1e-5
+
+
+def _gradient_case():
+    p = vparams(return_transmission=True, return_reflection=True, return_3D=True)
+    RI = cases.sphere_phantom(SIZE, [0.1] * 3, cases.NM, seed=8, n_spheres=2, radius_um=(0.4, 0.8))
+    fv = _inputs(3)
+    o = cbs.ForwardSolverCBS(p, single=True)
+    o.set_RI(RI)
+    meas, _, _ = o.solve(fv)
+    return p, RI, fv, meas
+
+
+def test_vector_gradient_matches_oracle():
+    """Fused dyadic gradient (odt_gradient on a pol = 3 handle) against the
+    oracle's get_gradiant_static on the vector solver: relative L2 1e-5 on
+    the gradient, relative 1e-5 on the misfit; host and device entry points
+    give the same gradient bits."""
+    import torch
+
+    from inverse_solver_b200 import FORWARD_SOLVER_CONVERGENT_BORN
+    from oracle import multi
+
+    p, RI, fv, meas = _gradient_case()
+    RI0 = (RI * 0.7 + cases.NM * 0.3).astype(np.float32)
+    s = FORWARD_SOLVER_CONVERGENT_BORN(p)
+    s.set_RI(RI0)
+    s.set_RI_adjoint(RI0)
+    g, err = s.gradient(fv, meas)
+    dev = torch.device("cuda", 0)
+
+    def up(a):
+        return torch.from_numpy(np.ascontiguousarray(np.asarray(a, np.complex64).ravel(order="F"))).to(dev)
+
+    gd = torch.empty(int(np.prod(SIZE)), dtype=torch.complex64, device=dev)
+    errd = s.gradient_device(up(fv), up(meas), gd)
+    gd = gd.cpu().numpy().reshape(SIZE, order="F")
+    s.delete()
+    o = cbs.ForwardSolverCBS(p, single=True)
+    go, erro = multi.get_gradient_static(RI0, fv, meas, o)
+    assert g.shape == go.shape == tuple(SIZE)
+    assert cbs.rel_l2(g, go) < 1e-5
+    assert abs(err - erro) / erro < 1e-5
+    # the misfit is a double-precision atomic sum: equal up to its order
+    assert np.array_equal(g, gd) and abs(err - errd) <= 1e-12 * err
+
+
+def test_vector_fista_outer_iteration_matches_oracle():
+    """One FISTA outer iteration of BACKWARD_SOLVER_MULTI.solve on the dyadic
+    solver through the device-resident loop, against the oracle's
+    solve_multi: relative L2 1e-5 on RI - RI_bg (odd z, as the reference
+    requires)."""
+    from inverse_solver_b200 import FORWARD_SOLVER_CONVERGENT_BORN
+    from inverse_solver_b200.backward import BACKWARD_SOLVER_MULTI
+    from oracle import multi
+
+    size = [28, 28, 19]
+    p = cases.params(size, [2, 2, 1.5], return_transmission=True, return_reflection=True, return_3D=True)
+    p["vector_simulation"] = True
+    RI = cases.sphere_phantom(size, [0.1] * 3, cases.NM, seed=9, n_spheres=2, radius_um=(0.4, 0.8))
+    f = cases.circle_fields(cases.params(size, [2, 2, 1.5]), 2)
+    fv = np.zeros((size[0], size[1], 2, 2), np.complex64)
+    fv[:, :, 0, 0] = f[:, :, 0, 0]
+    fv[:, :, 1, 1] = f[:, :, 0, 1]
+    o = cbs.ForwardSolverCBS(p, single=True)
+    o.set_RI(RI)
+    meas, _, _ = o.solve(fv)
+
+    class Blurred:
+        def solve(self, input_field, output_field):
+            return (RI * 0.5 + cases.NM * 0.5).astype(np.float32)
+
+    bp = BACKWARD_SOLVER_MULTI.get_default_parameters(dict(
+        RI_bg=cases.NM, wavelength=cases.LAM, NA=p["NA"], resolution=p["resolution"],
+        size=p["size"], forward_solver=FORWARD_SOLVER_CONVERGENT_BORN,
+        forward_solver_parameters=p, init_solver=Blurred(), step=0.01, tv_param=0.001,
+        inner_itt=10, itter_max=1, use_non_negativity=True, nmin=cases.NM, nmax=1.5))
+    b = BACKWARD_SOLVER_MULTI(bp)
+    assert b._use_device_loop()
+    got = b.solve(fv, meas)
+    ref, errs = multi.solve_multi(bp, Blurred().solve(None, None), fv, meas, o)
+    assert cbs.rel_l2(got - cases.NM, ref - cases.NM) < 1e-5
+    assert np.allclose(b.err_list, errs, rtol=1e-5)
+    b.delete()
+
+
+def _tensor(RI):
+    """Birefringent, coupled RI tensor [x, y, z, 3, 3]: the scalar RI scaled
+    per axis on the diagonal, a symmetric xy term, zero potential elsewhere."""
+    T = np.empty(RI.shape + (3, 3), np.float32)
+    T[...] = np.float32(cases.NM)
+    for i in range(3):
+        T[:, :, :, i, i] = cases.NM + (RI - cases.NM) * (1 - 0.25 * i)
+    T[:, :, :, 0, 1] = T[:, :, :, 1, 0] = cases.NM + (RI - cases.NM) * 0.2
+    return T
+
+
+@pytest.mark.parametrize("acyclic", [True, False])
+def test_tensor_RI_solve_matches_oracle(acyclic):
+    """RI tensor (size(RI,4) > 1) through odt_set_tensor_potential: the
+    component-coupling x-step and emitter against the oracle's tensor
+    branches; tolerances as for the isotropic dyadic solve."""
+    from inverse_solver_b200 import FORWARD_SOLVER_CONVERGENT_BORN
+
+    p = vparams(return_reflection=True, return_3D=True, acyclic=acyclic)
+    RI = cases.sphere_phantom(SIZE, [0.1] * 3, cases.NM, seed=5, n_spheres=2, radius_um=(0.4, 0.8))
+    T = _tensor(RI)
+    fv = _inputs(3)
+    s = FORWARD_SOLVER_CONVERGENT_BORN(p)
+    s.set_RI({"scatt_pott": T})
+    t, r, f3 = s.solve(fv)
+    o = cbs.ForwardSolverCBS(p, single=True)
+    o.set_RI(T)
+    assert s.Bornmax == o.Bornmax and float(s.eps_imag) == float(o.eps_imag)
+    ot, orr, of = o.solve(fv)
+    assert worst(f3, of) < 1e-5
+    assert worst(t, ot) < 1e-5
+    assert worst(r, orr) < 3e-5
+    # the scalar potential of the same handle afterwards: the isotropic solve
+    s.set_RI(RI)
+    t2, _, _ = s.solve(fv)
+    s.delete()
+    o2 = cbs.ForwardSolverCBS(p, single=True)
+    o2.set_RI(RI)
+    ot2, _, _ = o2.solve(fv)
+    assert worst(t2, ot2) < 1e-5
+    o64 = cbs.ForwardSolverCBS(p, single=False)
+    o64.set_RI(T)
+    t64, _, _ = o64.solve(fv)
+    print("tensor GPU vs FP64 oracle: trans %.2e" % worst(t, t64))
+
+
+def test_tensor_RI_on_pipelined_grid_matches_oracle():
+    """Tensor solve on a padded (88, 88, 40) grid: plain x-FFTs around the
+    coupling step, pipelined y-passes, dyadic z-pass; and odt_gradient
+    refuses a tensor potential."""
+    import ctypes as C
+
+    from inverse_solver_b200 import FORWARD_SOLVER_CONVERGENT_BORN, _lib
+
+    size = [64, 64, 16]
+    p = cases.params(size, [6, 6, 6], return_3D=True)
+    p["vector_simulation"] = True
+    RI = cases.sphere_phantom(size, [0.1] * 3, cases.NM, seed=12, n_spheres=2, radius_um=(0.3, 0.8))
+    T = _tensor(RI)
+    f = cases.circle_fields(cases.params(size, [6, 6, 6]), 2)
+    fv = np.zeros((64, 64, 2, 2), np.complex64)
+    fv[:, :, 0, 0] = f[:, :, 0, 0]
+    fv[:, :, 1, 1] = f[:, :, 0, 1]
+    s = FORWARD_SOLVER_CONVERGENT_BORN(p)
+    s.set_RI(T)
+    assert s.sim_size == [88, 88, 40]
+    t, _, f3 = s.solve(fv)
+    a = _lib.GradientArgs()
+    g = np.zeros(size, np.complex64, order="F")
+    err = C.c_double(0)
+    a.fields_in, a.fields_meas = _lib.ptr(np.asfortranarray(fv)), _lib.ptr(np.asfortranarray(fv))
+    a.n_ill = 2
+    a.grad = _lib.ptr(g)
+    a.err = C.addressof(err)
+    a.memory = _lib.ODT_MEM_HOST
+    s.set_RI_adjoint(RI)
+    assert _lib.load().odt_gradient(s._handle, C.byref(a)) != 0
+    s.delete()
+    o = cbs.ForwardSolverCBS(p, single=True)
+    o.set_RI(T)
+    ot, _, of = o.solve(fv)
+    assert worst(f3, of) < 1e-5 and worst(t, ot) < 1e-5
