@@ -75,6 +75,38 @@ class FORWARD_SOLVER_BPM:
         post = np.exp((rk * (-(nz - math.floor(nz / 2) - 1))).astype(C64)).astype(C64)
         return pre, post
 
+    def solve_device(self, fields_in, trans, stream=None):
+        """Device-resident solve: fields_in / trans contiguous complex64 CUDA
+        tensors of F_x*F_y*n_ill elements (column-major [F_x, F_y, n_ill]);
+        transmitted field only.  Work is queued on ``stream`` (default: the
+        current torch stream) and the call returns without synchronising."""
+        import torch
+
+        n1, n2, nz = self.field_multiplier.shape
+        plane = n1 * n2
+        for t in (fields_in, trans):
+            if not t.is_cuda or not t.is_contiguous() or t.dtype != torch.complex64:
+                raise ValueError("solve_device expects contiguous complex64 CUDA tensors")
+        nill = fields_in.numel() // plane
+        if nill < 1 or fields_in.numel() != nill * plane or trans.numel() != fields_in.numel():
+            raise ValueError("fields must be [F_x, F_y, n] alike")
+        d = self._device_tables()
+        a = _lib.BPMArgs()
+        a.size[:] = [n1, n2, nz]
+        a.field_multiplier, a.refocus_kernel = d["fm"].data_ptr(), d["rk"].data_ptr()
+        a.filter_out = d["fo"].data_ptr()
+        a.pre, a.post = d["pre"].data_ptr(), d["post"].data_ptr()
+        a.cos_theta = d["ct"].data_ptr() if self.parameters["cos_correction"] else None
+        a.fields_in = fields_in.data_ptr()
+        a.n_ill = nill
+        a.trans = trans.data_ptr()
+        a.field3d = None
+        a.memory = _lib.ODT_MEM_DEVICE
+        if stream is None:
+            stream = torch.cuda.current_stream(fields_in.device)
+        a.stream = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        _lib.check(self.lib.odt_bpm_solve(C.byref(a)))
+
     def solve(self, input_field):
         """:45-117 -> (fields_trans, fields_ref, fields_3D); fields_ref is
         the reference's untouched ones(...) array when return_reflection."""

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <string>
 
 #include "../../include/odt.h"
@@ -128,6 +129,161 @@ __global__ void peak_inv_cos_kernel(const float2* __restrict__ spec, const float
   }
 }
 
+// ---- fused march for 128 x 128 planes
+// One CTA per illumination keeps its 128 x 128 plane in shared memory
+// (row pitch 129 complex: column accesses are free of bank conflicts) for the
+// whole march over z.  Each 128-point transform is done by one warp with the
+// line in registers, lane l holding elements l + 32 r (r = 0..3):
+//   forward : 4-point DFT over r, twiddles W128^(l k1), then a 32-point
+//             decimation-in-frequency DFT across lanes (shuffles); element
+//             k1 + 4 brev5(l) of the result ends in lane l, register k1,
+//             i.e. at position l + 32 k1 of the line ("permuted" order);
+//   inverse : the same steps undone in reverse order (decimation in time
+//             across lanes with conjugate twiddles, conjugate twiddles, inverse
+//             4-point DFT): permuted input, natural output, unnormalised.
+// The spectrum stays in permuted order between slices, so every transform
+// reads and writes its line in place.  Per slice (z):
+//   x-pass: inverse x-FFT, * (1/N) exp(field_multiplier(:,:,z) * inv_cos),
+//           forward x-FFT (one register pass per line);
+//   y-pass: forward y-FFT, then (except after the last slice)
+//           * refocus_kernel and inverse y-FFT of the next slice's
+//           ifft2(field .* refocus_kernel) (one register pass per column).
+constexpr int kM = 128;           // plane side
+constexpr int kMP = 129;          // shared-memory row pitch (complex)
+constexpr int kMarchThreads = 512;
+
+__device__ __forceinline__ int march_perm(int p) {  // position -> frequency
+  return (p >> 5) + 4 * (int)(__brev((unsigned)(p & 31)) >> 27);
+}
+__device__ __forceinline__ int march_pos(int k) {   // frequency -> position
+  return (int)(__brev((unsigned)(k >> 2)) >> 27) + 32 * (k & 3);
+}
+
+__device__ __forceinline__ float2 shfl_c(float2 v, int m) {
+  return make_float2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+
+// natural -> permuted, W = exp(-2 pi i / 128)
+__device__ __forceinline__ void wfft128_fwd(float2 (&v)[4], const float2* tw, int l) {
+  const float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+  const float2 a2 = cadd(v[1], v[3]), a3 = csub(v[1], v[3]);
+  const float2 ma3 = make_float2(a3.y, -a3.x);  // -i * a3
+  v[0] = cadd(a0, a2);
+  v[1] = cadd(a1, ma3);
+  v[2] = csub(a0, a2);
+  v[3] = csub(a1, ma3);
+#pragma unroll
+  for (int k = 1; k < 4; ++k) v[k] = cmul(v[k], tw[l * k]);
+#pragma unroll
+  for (int h = 16; h >= 1; h >>= 1) {
+    const bool up = (l & h) == 0;
+    const float2 w = tw[(l & (h - 1)) * (64 / h)];  // W_{2h}^j
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float2 p = shfl_c(v[k], h);
+      v[k] = up ? cadd(v[k], p) : cmul(csub(p, v[k]), w);
+    }
+  }
+}
+
+// permuted -> natural, unnormalised inverse (W = exp(+2 pi i / 128))
+__device__ __forceinline__ void wfft128_inv(float2 (&v)[4], const float2* tw, int l) {
+#pragma unroll
+  for (int h = 1; h <= 16; h <<= 1) {
+    const bool up = (l & h) == 0;
+    const float2 w = cconj(tw[(l & (h - 1)) * (64 / h)]);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float2 p = shfl_c(v[k], h);
+      v[k] = up ? cadd(v[k], cmul(p, w)) : csub(p, cmul(v[k], w));
+    }
+  }
+#pragma unroll
+  for (int k = 1; k < 4; ++k) v[k] = cmul(v[k], cconj(tw[l * k]));
+  const float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+  const float2 a2 = cadd(v[1], v[3]), a3 = csub(v[1], v[3]);
+  const float2 ia3 = make_float2(-a3.y, a3.x);  // i * a3
+  v[0] = cadd(a0, a2);
+  v[1] = cadd(a1, ia3);
+  v[2] = csub(a0, a2);
+  v[3] = csub(a1, ia3);
+}
+
+// fld [128 * 128, nill]: spectrum of every illumination (natural order)
+// before the first slice's refocus multiply; on return the spectrum after
+// the last slice's fft2
+__global__ void __launch_bounds__(kMarchThreads, 1)
+bpm_march128_kernel(float2* __restrict__ fld, const float2* __restrict__ rk, const float2* __restrict__ fm,
+                    const float* __restrict__ inv_cos, const float2* __restrict__ twg, int nz, float inv_n) {
+  extern __shared__ float2 march_sm[];
+  float2* S = march_sm;
+  float2* tw = march_sm + kM * kMP;
+  const int tid = threadIdx.x, l = tid & 31, w = tid >> 5;
+  constexpr int nw = kMarchThreads / 32;
+  float2* F = fld + (long long)blockIdx.x * kM * kM;
+  const float ic = inv_cos ? inv_cos[blockIdx.x] : 1.f;
+  for (int i = tid; i < kM; i += kMarchThreads) tw[i] = twg[i];
+  for (int i = tid; i < kM * kM; i += kMarchThreads) {
+    const int kx = i & (kM - 1), ky = i >> 7;
+    S[march_pos(kx) + kMP * march_pos(ky)] = F[i];
+  }
+  __syncthreads();
+  // the first slice's refocus multiply and inverse y-FFT
+  for (int px = w; px < kM; px += nw) {
+    const int kx = march_perm(px);
+    float2 v[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) v[r] = cmul(S[px + kMP * (l + 32 * r)], rk[kx + kM * march_perm(l + 32 * r)]);
+    wfft128_inv(v, tw, l);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) S[px + kMP * (l + 32 * r)] = v[r];
+  }
+  __syncthreads();
+  for (int z = 0; z < nz; ++z) {
+    const float2* fz = fm + (long long)z * kM * kM;
+    for (int py = w; py < kM; py += nw) {
+      float2 v[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) v[r] = S[(l + 32 * r) + kMP * py];
+      wfft128_inv(v, tw, l);
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        float2 e = fz[(l + 32 * r) + kM * py];
+        if (inv_cos) e = cscale(e, ic);
+        float sn, cs;
+        sincosf(e.y, &sn, &cs);
+        const float m = expf(e.x);
+        v[r] = cmul(cscale(v[r], inv_n), make_float2(m * cs, m * sn));
+      }
+      wfft128_fwd(v, tw, l);
+#pragma unroll
+      for (int r = 0; r < 4; ++r) S[(l + 32 * r) + kMP * py] = v[r];
+    }
+    __syncthreads();
+    const bool more = z + 1 < nz;
+    for (int px = w; px < kM; px += nw) {
+      const int kx = march_perm(px);
+      float2 v[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) v[r] = S[px + kMP * (l + 32 * r)];
+      wfft128_fwd(v, tw, l);
+      if (more) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) v[r] = cmul(v[r], rk[kx + kM * march_perm(l + 32 * r)]);
+        wfft128_inv(v, tw, l);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) S[px + kMP * (l + 32 * r)] = v[r];
+      } else {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) F[kx + kM * march_perm(l + 32 * r)] = v[r];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+constexpr size_t kMarchSmem = sizeof(float2) * (kM * kMP + kM);
+
 odt_status bpm_fail(odt_status st, const std::string& m) {
   set_last_error(m);
   return st;
@@ -232,6 +388,16 @@ extern "C" odt_status odt_bpm_solve(const odt_bpm_args* a) {
   cmul_plane_kernel<<<g, kThreads, 0, s>>>(fld, pre, plane, nf);
   BPM_CHECK(fft2(fld, true, true));
   BPM_CHECK(fft2(fld, false, false));
+  // fused march (shared-memory resident planes) for 128 x 128 fields without
+  // the 3D output; ODT_KERNELS=generic keeps the per-slice launches
+  const char* kenv = std::getenv("ODT_KERNELS");
+  const bool generic = kenv && std::string(kenv) == "generic";
+  if (n1 == kM && n2 == kM && !out3d && !generic && nz > 0) {
+    BPM_CHECK(cudaFuncSetAttribute(bpm_march128_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)kMarchSmem));
+    bpm_march128_kernel<<<nill, kMarchThreads, kMarchSmem, s>>>(fld, rk, fm, inv_cos, f1.tw, nz, inv_n);
+    BPM_CHECK(cudaGetLastError());
+  } else {
   for (int z = 0; z < nz; ++z) {
     cmul_plane_kernel<<<g, kThreads, 0, s>>>(fld, rk, plane, nf);
     BPM_CHECK(fft2(fld, true, false));
@@ -242,6 +408,7 @@ extern "C" odt_status odt_bpm_solve(const odt_bpm_args* a) {
       BPM_CHECK(fft2(tmp, true, false));
       scatter_slice_kernel<<<g, kThreads, 0, s>>>(tmp, out3d, z, nz, plane, nf);
     }
+  }
   }
   BPM_CHECK(fft2(fld, true, false));
   BPM_CHECK(fft2(fld, false, true));

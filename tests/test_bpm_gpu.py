@@ -49,3 +49,30 @@ def test_bpm_homogeneous_known_answer():
     s.set_RI(np.full(p["size"], cases.NM, dtype=np.float32))
     t, _, _ = s.solve(fields)
     assert cbs.rel_l2(t, fields) < 1e-5
+
+
+@pytest.mark.parametrize("cos_correction", [True, False])
+def test_fused_march_matches_oracle_and_per_slice_path(cos_correction, monkeypatch):
+    """128 x 128 fields without the 3D output take the fused march (one CTA
+    per illumination, plane resident in shared memory, warp-level
+    transforms): against the oracle within rel-L2 1e-5, and against the
+    per-slice launches (ODT_KERNELS=generic) within 1e-5."""
+    from inverse_solver_b200 import FORWARD_SOLVER_BPM
+
+    size = [128, 128, 24]
+    p = _params(size, cos_correction=cos_correction)
+    RI = cases.sphere_phantom(size, [0.1] * 3, cases.NM, seed=41, n_spheres=4, radius_um=(0.4, 0.9))
+    fields = cases.circle_fields(p, 3)
+    s = FORWARD_SOLVER_BPM(p)
+    s.set_RI(RI)
+    t, _, _ = s.solve(fields)
+    t_again, _, _ = s.solve(fields)
+    monkeypatch.setenv("ODT_KERNELS", "generic")
+    tg, _, _ = s.solve(fields)
+    monkeypatch.delenv("ODT_KERNELS")
+    o = bpm.ForwardSolverBPM(p, single=True)
+    o.set_RI(RI)
+    ot, _, _ = o.solve(fields)
+    assert np.array_equal(t, t_again)
+    assert worst(t, ot) < 1e-5
+    assert worst(t, tg) < 1e-5
