@@ -16,6 +16,7 @@
 //
 // The cosine correction takes cos_theta at the peak of each illumination's
 // centred spectrum (:59-63: the first maximum of |.| in column-major order).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -31,6 +32,7 @@ const char* set_last_error(const std::string& msg);  // odt_api.cu
 }
 
 using namespace odt;
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -130,10 +132,12 @@ __global__ void peak_inv_cos_kernel(const float2* __restrict__ spec, const float
 }
 
 // ---- fused march for 128 x 128 planes
-// One CTA per illumination keeps its 128 x 128 plane in shared memory
-// (row pitch 129 complex: column accesses are free of bank conflicts) for the
-// whole march over z.  Each 128-point transform is done by one warp with the
-// line in registers, lane l holding elements l + 32 r (r = 0..3):
+// A cluster of two CTAs per illumination keeps the 128 x 128 plane in shared
+// memory for the whole march over z: CTA r holds rows y = 64 r .. 64 r + 63
+// (row pitch 129 complex, so column accesses are free of bank conflicts) and
+// reads the other half of each column through distributed shared memory.
+// Each 128-point transform is done by one warp with the line in registers,
+// lane l holding elements l + 32 r (r = 0..3):
 //   forward : 4-point DFT over r, twiddles W128^(l k1), then a 32-point
 //             decimation-in-frequency DFT across lanes (shuffles); element
 //             k1 + 4 brev5(l) of the result ends in lane l, register k1,
@@ -144,64 +148,87 @@ __global__ void peak_inv_cos_kernel(const float2* __restrict__ spec, const float
 // The spectrum stays in permuted order between slices, so every transform
 // reads and writes its line in place.  Per slice (z):
 //   x-pass: inverse x-FFT, * (1/N) exp(field_multiplier(:,:,z) * inv_cos),
-//           forward x-FFT (one register pass per line);
+//           forward x-FFT (one register pass per row, rows of this CTA);
 //   y-pass: forward y-FFT, then (except after the last slice)
 //           * refocus_kernel and inverse y-FFT of the next slice's
-//           ifft2(field .* refocus_kernel) (one register pass per column).
+//           ifft2(field .* refocus_kernel) (one register pass per column,
+//           columns 64 r .. 64 r + 63 for CTA r).
 constexpr int kM = 128;           // plane side
 constexpr int kMP = 129;          // shared-memory row pitch (complex)
+constexpr int kMH = kM / 2;       // rows per CTA
 constexpr int kMarchThreads = 512;
 
 __device__ __forceinline__ int march_perm(int p) {  // position -> frequency
   return (p >> 5) + 4 * (int)(__brev((unsigned)(p & 31)) >> 27);
-}
-__device__ __forceinline__ int march_pos(int k) {   // frequency -> position
-  return (int)(__brev((unsigned)(k >> 2)) >> 27) + 32 * (k & 3);
 }
 
 __device__ __forceinline__ float2 shfl_c(float2 v, int m) {
   return make_float2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
 }
 
+// per-lane twiddles: w[s] = W_{2h}^(l mod h) for h = 16 >> s, b[k-1] = W128^(l k)
+struct MarchTw {
+  float2 w[5];
+  float2 b[3];
+};
+
+__device__ __forceinline__ void march_tw(MarchTw& t, const float2* tw, int l) {
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {
+    const int h = 16 >> s;
+    t.w[s] = tw[(l & (h - 1)) * (64 / h)];
+  }
+#pragma unroll
+  for (int k = 1; k < 4; ++k) t.b[k - 1] = tw[l * k];
+}
+
 // natural -> permuted, W = exp(-2 pi i / 128)
-__device__ __forceinline__ void wfft128_fwd(float2 (&v)[4], const float2* tw, int l) {
+__device__ __forceinline__ void wfft128_fwd(float2 (&v)[4], const MarchTw& t, int l) {
   const float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
   const float2 a2 = cadd(v[1], v[3]), a3 = csub(v[1], v[3]);
   const float2 ma3 = make_float2(a3.y, -a3.x);  // -i * a3
   v[0] = cadd(a0, a2);
-  v[1] = cadd(a1, ma3);
-  v[2] = csub(a0, a2);
-  v[3] = csub(a1, ma3);
+  v[1] = cmul(cadd(a1, ma3), t.b[0]);
+  v[2] = cmul(csub(a0, a2), t.b[1]);
+  v[3] = cmul(csub(a1, ma3), t.b[2]);
 #pragma unroll
-  for (int k = 1; k < 4; ++k) v[k] = cmul(v[k], tw[l * k]);
-#pragma unroll
-  for (int h = 16; h >= 1; h >>= 1) {
-    const bool up = (l & h) == 0;
-    const float2 w = tw[(l & (h - 1)) * (64 / h)];  // W_{2h}^j
+  for (int s = 0; s < 5; ++s) {
+    const int h = 16 >> s;
+    const bool up = (l & h) == 0;  // upper lane: x_j + x_{j+h}; lower: (x_j - x_{j+h}) W
+    const float sg = up ? 1.f : -1.f;
+    const float2 w = up ? make_float2(1.f, 0.f) : t.w[s];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const float2 p = shfl_c(v[k], h);
-      v[k] = up ? cadd(v[k], p) : cmul(csub(p, v[k]), w);
+      v[k] = cmul(make_float2(fmaf(sg, v[k].x, p.x), fmaf(sg, v[k].y, p.y)), w);
     }
   }
 }
 
 // permuted -> natural, unnormalised inverse (W = exp(+2 pi i / 128))
-__device__ __forceinline__ void wfft128_inv(float2 (&v)[4], const float2* tw, int l) {
+__device__ __forceinline__ void wfft128_inv(float2 (&v)[4], const MarchTw& t, int l) {
 #pragma unroll
-  for (int h = 1; h <= 16; h <<= 1) {
+  for (int s = 4; s >= 0; --s) {
+    const int h = 16 >> s;
     const bool up = (l & h) == 0;
-    const float2 w = cconj(tw[(l & (h - 1)) * (64 / h)]);
+    // upper lane: top + bot conj(W); lower lane: top - bot conj(W), i.e.
+    // v * ca + partner * cb with (ca, cb) = (1, conj W) or (-conj W, 1)
+    const float2 cw = cconj(t.w[s]);
+    const float2 ca = up ? make_float2(1.f, 0.f) : make_float2(-cw.x, -cw.y);
+    const float2 cb = up ? cw : make_float2(1.f, 0.f);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const float2 p = shfl_c(v[k], h);
-      v[k] = up ? cadd(v[k], cmul(p, w)) : csub(p, cmul(v[k], w));
+      const float2 x = v[k];
+      v[k] = make_float2(fmaf(x.x, ca.x, fmaf(-x.y, ca.y, fmaf(p.x, cb.x, -p.y * cb.y))),
+                         fmaf(x.x, ca.y, fmaf(x.y, ca.x, fmaf(p.x, cb.y, p.y * cb.x))));
     }
   }
-#pragma unroll
-  for (int k = 1; k < 4; ++k) v[k] = cmul(v[k], cconj(tw[l * k]));
-  const float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
-  const float2 a2 = cadd(v[1], v[3]), a3 = csub(v[1], v[3]);
+  const float2 b1 = cmul(v[1], cconj(t.b[0]));
+  const float2 b2 = cmul(v[2], cconj(t.b[1]));
+  const float2 b3 = cmul(v[3], cconj(t.b[2]));
+  const float2 a0 = cadd(v[0], b2), a1 = csub(v[0], b2);
+  const float2 a2 = cadd(b1, b3), a3 = csub(b1, b3);
   const float2 ia3 = make_float2(-a3.y, a3.x);  // i * a3
   v[0] = cadd(a0, a2);
   v[1] = cadd(a1, ia3);
@@ -211,41 +238,53 @@ __device__ __forceinline__ void wfft128_inv(float2 (&v)[4], const float2* tw, in
 
 // fld [128 * 128, nill]: spectrum of every illumination (natural order)
 // before the first slice's refocus multiply; on return the spectrum after
-// the last slice's fft2
-__global__ void __launch_bounds__(kMarchThreads, 1)
+// the last slice's fft2.  Grid: 2 CTAs (one cluster) per illumination.
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kMarchThreads, 1)
 bpm_march128_kernel(float2* __restrict__ fld, const float2* __restrict__ rk, const float2* __restrict__ fm,
                     const float* __restrict__ inv_cos, const float2* __restrict__ twg, int nz, float inv_n) {
   extern __shared__ float2 march_sm[];
-  float2* S = march_sm;
-  float2* tw = march_sm + kM * kMP;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  float2* S = march_sm;                       // rows 64 rank .. 64 rank + 63
+  float2* tw = march_sm + kMH * kMP;
+  float2* const S0 = cluster.map_shared_rank(S, 0);
+  float2* const S1 = cluster.map_shared_rank(S, 1);
   const int tid = threadIdx.x, l = tid & 31, w = tid >> 5;
   constexpr int nw = kMarchThreads / 32;
-  float2* F = fld + (long long)blockIdx.x * kM * kM;
-  const float ic = inv_cos ? inv_cos[blockIdx.x] : 1.f;
+  const int ill = blockIdx.x >> 1;
+  float2* F = fld + (long long)ill * kM * kM;
+  const float ic = inv_cos ? inv_cos[ill] : 1.f;
   for (int i = tid; i < kM; i += kMarchThreads) tw[i] = twg[i];
-  for (int i = tid; i < kM * kM; i += kMarchThreads) {
-    const int kx = i & (kM - 1), ky = i >> 7;
-    S[march_pos(kx) + kMP * march_pos(ky)] = F[i];
+  for (int i = tid; i < kMH * kM; i += kMarchThreads) {
+    const int px = i & (kM - 1), jy = i >> 7;
+    S[px + kMP * jy] = F[march_perm(px) + kM * march_perm(kMH * rank + jy)];
   }
   __syncthreads();
+  MarchTw t;
+  march_tw(t, tw, l);
+  cluster.sync();
+  // column px, element y = l + 32 r: rows 0..63 live in CTA 0, 64..127 in CTA 1
+  const int ylo = l;  // row inside the owning CTA for r = 0, 2 (r = 1, 3: + 32)
   // the first slice's refocus multiply and inverse y-FFT
-  for (int px = w; px < kM; px += nw) {
+  for (int px = kMH * rank + w; px < kMH * rank + kMH; px += nw) {
     const int kx = march_perm(px);
     float2 v[4];
 #pragma unroll
-    for (int r = 0; r < 4; ++r) v[r] = cmul(S[px + kMP * (l + 32 * r)], rk[kx + kM * march_perm(l + 32 * r)]);
-    wfft128_inv(v, tw, l);
+    for (int r = 0; r < 4; ++r)
+      v[r] = cmul((r < 2 ? S0 : S1)[px + kMP * (ylo + 32 * (r & 1))], rk[kx + kM * march_perm(l + 32 * r)]);
+    wfft128_inv(v, t, l);
 #pragma unroll
-    for (int r = 0; r < 4; ++r) S[px + kMP * (l + 32 * r)] = v[r];
+    for (int r = 0; r < 4; ++r) (r < 2 ? S0 : S1)[px + kMP * (ylo + 32 * (r & 1))] = v[r];
   }
-  __syncthreads();
+  cluster.sync();
   for (int z = 0; z < nz; ++z) {
     const float2* fz = fm + (long long)z * kM * kM;
-    for (int py = w; py < kM; py += nw) {
+    for (int jy = w; jy < kMH; jy += nw) {
+      const int py = kMH * rank + jy;
       float2 v[4];
 #pragma unroll
-      for (int r = 0; r < 4; ++r) v[r] = S[(l + 32 * r) + kMP * py];
-      wfft128_inv(v, tw, l);
+      for (int r = 0; r < 4; ++r) v[r] = S[(l + 32 * r) + kMP * jy];
+      wfft128_inv(v, t, l);
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
         float2 e = fz[(l + 32 * r) + kM * py];
@@ -255,34 +294,34 @@ bpm_march128_kernel(float2* __restrict__ fld, const float2* __restrict__ rk, con
         const float m = expf(e.x);
         v[r] = cmul(cscale(v[r], inv_n), make_float2(m * cs, m * sn));
       }
-      wfft128_fwd(v, tw, l);
+      wfft128_fwd(v, t, l);
 #pragma unroll
-      for (int r = 0; r < 4; ++r) S[(l + 32 * r) + kMP * py] = v[r];
+      for (int r = 0; r < 4; ++r) S[(l + 32 * r) + kMP * jy] = v[r];
     }
-    __syncthreads();
+    cluster.sync();
     const bool more = z + 1 < nz;
-    for (int px = w; px < kM; px += nw) {
+    for (int px = kMH * rank + w; px < kMH * rank + kMH; px += nw) {
       const int kx = march_perm(px);
       float2 v[4];
 #pragma unroll
-      for (int r = 0; r < 4; ++r) v[r] = S[px + kMP * (l + 32 * r)];
-      wfft128_fwd(v, tw, l);
+      for (int r = 0; r < 4; ++r) v[r] = (r < 2 ? S0 : S1)[px + kMP * (ylo + 32 * (r & 1))];
+      wfft128_fwd(v, t, l);
       if (more) {
 #pragma unroll
         for (int r = 0; r < 4; ++r) v[r] = cmul(v[r], rk[kx + kM * march_perm(l + 32 * r)]);
-        wfft128_inv(v, tw, l);
+        wfft128_inv(v, t, l);
 #pragma unroll
-        for (int r = 0; r < 4; ++r) S[px + kMP * (l + 32 * r)] = v[r];
+        for (int r = 0; r < 4; ++r) (r < 2 ? S0 : S1)[px + kMP * (ylo + 32 * (r & 1))] = v[r];
       } else {
 #pragma unroll
         for (int r = 0; r < 4; ++r) F[kx + kM * march_perm(l + 32 * r)] = v[r];
       }
     }
-    __syncthreads();
+    cluster.sync();  // also keeps this CTA's rows alive until the partner is done
   }
 }
 
-constexpr size_t kMarchSmem = sizeof(float2) * (kM * kMP + kM);
+constexpr size_t kMarchSmem = sizeof(float2) * (kMH * kMP + kM);
 
 odt_status bpm_fail(odt_status st, const std::string& m) {
   set_last_error(m);
@@ -395,7 +434,7 @@ extern "C" odt_status odt_bpm_solve(const odt_bpm_args* a) {
   if (n1 == kM && n2 == kM && !out3d && !generic && nz > 0) {
     BPM_CHECK(cudaFuncSetAttribute(bpm_march128_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)kMarchSmem));
-    bpm_march128_kernel<<<nill, kMarchThreads, kMarchSmem, s>>>(fld, rk, fm, inv_cos, f1.tw, nz, inv_n);
+    bpm_march128_kernel<<<2 * nill, kMarchThreads, kMarchSmem, s>>>(fld, rk, fm, inv_cos, f1.tw, nz, inv_n);
     BPM_CHECK(cudaGetLastError());
   } else {
   for (int z = 0; z < nz; ++z) {

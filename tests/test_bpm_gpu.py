@@ -53,10 +53,10 @@ def test_bpm_homogeneous_known_answer():
 
 @pytest.mark.parametrize("cos_correction", [True, False])
 def test_fused_march_matches_oracle_and_per_slice_path(cos_correction, monkeypatch):
-    """128 x 128 fields without the 3D output take the fused march (one CTA
-    per illumination, plane resident in shared memory, warp-level
-    transforms): against the oracle within rel-L2 1e-5, and against the
-    per-slice launches (ODT_KERNELS=generic) within 1e-5."""
+    """128 x 128 fields without the 3D output take the fused march (a
+    cluster of two CTAs per illumination, plane resident in their shared
+    memory, warp-level transforms): against the oracle within rel-L2 1e-5,
+    and against the per-slice launches (ODT_KERNELS=generic) within 1e-5."""
     from inverse_solver_b200 import FORWARD_SOLVER_BPM
 
     size = [128, 128, 24]
