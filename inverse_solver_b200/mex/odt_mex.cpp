@@ -3,13 +3,21 @@
 //
 //   id = odt_mex(uint32(0), uint32(0), geom, refocus, kernel_trans, kernel_ref, pupil_in, pupil_out)
 //   odt_mex(uint32(1), id, pot, single(V))
-//   [trans, ref, field3d] = odt_mex(uint32(4), id, single complex input [F_x, F_y, 1, n])
+//   [trans, ref, field3d] = odt_mex(uint32(4), id, single complex input [F_x, F_y, npol, n], RI_size)
 //   odt_mex(uint32(3), id)
+// and, beyond CudaBorn's actions (vector simulations, the inverse solver):
+//   odt_mex(uint32(5), id, Radial_2D, Perp_2D, ewald_TanVec, uint8(K_mask))   polarisation basis
+//   odt_mex(uint32(6), id, pot, single(V_adjoint))                             adjoint potential
+//   [grad, err] = odt_mex(uint32(7), id, input_field, output_field, RI_size)   fused gradient
 //
 // geom: struct with simulation_size, RI_size, field_size, conv_size, used_gpu
-// (the CudaBorn names), optional max_batch.  pot: struct with eps_imag,
-// green_scale, green_offset, dV, ROI, Bornmax, acyclic, mask1/2/3, ramp1/2/3,
-// kq2_1/2/3.  Complex arrays use the interleaved layout of -R2018a.
+// (the CudaBorn names), optional max_batch and pol (3: dyadic Green's
+// function).  pot: struct with eps_imag, green_scale, green_offset, dV, ROI,
+// Bornmax, acyclic, mask1/2/3, ramp1/2/3, kq2_1/2/3, and for dyadic handles
+// rad1/2/3 and absorb (green_absorbtion_correction, complex).  V of
+// 9 * prod(simulation_size) elements ([sim, 3, 3]) is an RI tensor's
+// potential (odt_set_tensor_potential).  Complex arrays use the interleaved
+// layout of -R2018a.
 //
 // Build (needs MATLAB's mex.h, not present in this environment):
 //   mex -R2018a odt_mex.cpp -I../../include -L.. -lodt
@@ -76,6 +84,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
       ints(prhs[2], "conv_size", g.conv_size, 2);
       g.device = (int32_t)scalar(prhs[2], "used_gpu");
       g.max_batch = mxGetField(prhs[2], 0, "max_batch") ? (int32_t)scalar(prhs[2], "max_batch") : 0;
+      g.pol = mxGetField(prhs[2], 0, "pol") ? (int32_t)scalar(prhs[2], "pol") : 1;
       odt_handle h = 0;
       check(odt_create(&g, csingle(prhs[3], "refocus"), csingle(prhs[4], "kernel_trans"),
                        csingle(prhs[5], "kernel_ref"), mxGetSingles(prhs[6]), mxGetSingles(prhs[7]), &h));
@@ -83,7 +92,8 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
       *static_cast<uint32_t*>(mxGetData(plhs[0])) = h;
       break;
     }
-    case 1: {
+    case 1:
+    case 6: {
       if (nrhs < 4) mexErrMsgIdAndTxt("odt:arg", "set_potential needs pot and V");
       odt_potential_params pp{};
       pp.eps_imag = (float)scalar(prhs[2], "eps_imag");
@@ -101,7 +111,56 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
         pp.ramp[i] = static_cast<const odt_cfloat*>(array_field(prhs[2], rk[i], mxSINGLE_CLASS, true));
         pp.kq2[i] = static_cast<const float*>(array_field(prhs[2], kk[i], mxSINGLE_CLASS, false));
       }
-      check(odt_set_potential(id, &pp, csingle(prhs[3], "V")));
+      if (mxGetField(prhs[2], 0, "rad1")) {  // dyadic handle
+        const char* rd[3] = {"rad1", "rad2", "rad3"};
+        for (int i = 0; i < 3; ++i)
+          pp.rad[i] = static_cast<const float*>(array_field(prhs[2], rd[i], mxSINGLE_CLASS, false));
+        const mxArray* ab = mxGetField(prhs[2], 0, "absorb");
+        if (!ab) mexErrMsgIdAndTxt("odt:param", "missing field absorb");
+        pp.absorb.re = (float)mxGetScalar(ab);
+        pp.absorb.im = mxIsComplex(ab) ? (float)mxGetComplexDoubles(ab)[0].imag : 0.f;
+      }
+      int32_t sim[3];
+      ints(prhs[2], "simulation_size", sim, 3);
+      const size_t nsim = (size_t)sim[0] * sim[1] * sim[2];
+      const odt_cfloat* V = csingle(prhs[3], "V");
+      if (action == 6)
+        check(odt_set_adjoint_potential(id, &pp, V));
+      else if (mxGetNumberOfElements(prhs[3]) == 9 * nsim)
+        check(odt_set_tensor_potential(id, &pp, V));
+      else
+        check(odt_set_potential(id, &pp, V));
+      break;
+    }
+    case 5: {
+      if (nrhs < 6) mexErrMsgIdAndTxt("odt:arg", "polarisation needs Radial_2D, Perp_2D, ewald_TanVec, K_mask");
+      for (int i = 2; i < 5; ++i)
+        if (mxGetClassID(prhs[i]) != mxSINGLE_CLASS || mxIsComplex(prhs[i]))
+          mexErrMsgIdAndTxt("odt:arg", "the basis vectors must be real single");
+      if (mxGetClassID(prhs[5]) != mxUINT8_CLASS) mexErrMsgIdAndTxt("odt:arg", "K_mask must be uint8");
+      check(odt_set_polarisation(id, mxGetSingles(prhs[2]), mxGetSingles(prhs[3]), mxGetSingles(prhs[4]),
+                                 static_cast<const uint8_t*>(mxGetData(prhs[5]))));
+      break;
+    }
+    case 7: {
+      if (nrhs < 5) mexErrMsgIdAndTxt("odt:arg", "gradient needs input_field, output_field and RI_size");
+      const mwSize* d = mxGetDimensions(prhs[2]);
+      const mwSize nd = mxGetNumberOfDimensions(prhs[2]);
+      if (mxGetNumberOfElements(prhs[2]) != mxGetNumberOfElements(prhs[3]))
+        mexErrMsgIdAndTxt("odt:arg", "input and output fields must have the same size");
+      const double* r = mxGetPr(prhs[4]);
+      mwSize dg[3] = {(mwSize)r[0], (mwSize)r[1], (mwSize)r[2]};
+      plhs[0] = mxCreateNumericArray(3, dg, mxSINGLE_CLASS, mxCOMPLEX);
+      double err = 0;
+      odt_gradient_args a{};
+      a.fields_in = csingle(prhs[2], "input field");
+      a.fields_meas = csingle(prhs[3], "output field");
+      a.n_ill = nd >= 4 ? (int32_t)d[3] : 1;
+      a.grad = reinterpret_cast<odt_cfloat*>(mxGetComplexSingles(plhs[0]));
+      a.err = &err;
+      a.memory = ODT_MEM_HOST;
+      check(odt_gradient(id, &a));
+      if (nlhs > 1) plhs[1] = mxCreateDoubleScalar(err);
       break;
     }
     case 3:
@@ -112,9 +171,10 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
       const mwSize* d = mxGetDimensions(prhs[2]);
       const mwSize nd = mxGetNumberOfDimensions(prhs[2]);
       const int n_ill = nd >= 4 ? (int)d[3] : 1;
+      const mwSize npol = nd >= 3 ? d[2] : 1;  // 2 on dyadic handles
       int32_t ri[3] = {0, 0, 0};
       // output sizes follow the input field (field_size == RI_size(1:2))
-      mwSize dt[4] = {d[0], d[1], 1, (mwSize)n_ill};
+      mwSize dt[4] = {d[0], d[1], npol, (mwSize)n_ill};
       plhs[0] = mxCreateNumericArray(4, dt, mxSINGLE_CLASS, mxCOMPLEX);
       if (nlhs > 1) plhs[1] = mxCreateNumericArray(4, dt, mxSINGLE_CLASS, mxCOMPLEX);
       odt_solve_args a{};
@@ -126,7 +186,8 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
         if (nrhs < 4) mexErrMsgIdAndTxt("odt:arg", "pass RI_size as 4th argument to get field3d");
         const double* r = mxGetPr(prhs[3]);
         for (int i = 0; i < 3; ++i) ri[i] = (int32_t)r[i];
-        mwSize d3[5] = {(mwSize)ri[0], (mwSize)ri[1], (mwSize)ri[2], 1, (mwSize)n_ill};
+        mwSize d3[5] = {(mwSize)ri[0], (mwSize)ri[1], (mwSize)ri[2], npol == 2 ? (mwSize)3 : (mwSize)1,
+                        (mwSize)n_ill};
         plhs[2] = mxCreateNumericArray(5, d3, mxSINGLE_CLASS, mxCOMPLEX);
         a.field3d = reinterpret_cast<odt_cfloat*>(mxGetComplexSingles(plhs[2]));
       }

@@ -56,3 +56,22 @@ def test_unwrap_argument_checks():
     a.size[:] = [8, 8, 1]
     a.memory = 5
     assert lib.odt_unwrap_goldstein(C.byref(a)) == 1          # bad memory flag
+
+
+def test_mex_gateway_compiles_against_the_header():
+    """The MATLAB gateway (inverse_solver_b200/mex/odt_mex.cpp) type-checks
+    against include/odt.h, with a declarations-only stand-in for MATLAB's
+    mex.h (MATLAB is absent here, so it is not linked)."""
+    import shutil
+    import subprocess
+
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("g++ not available")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", "-Wall", "-Werror",
+                        "-I" + os.path.join(root, "tests", "native", "mex_stub"),
+                        "-I" + os.path.join(root, "include"),
+                        os.path.join(root, "inverse_solver_b200", "mex", "odt_mex.cpp")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
