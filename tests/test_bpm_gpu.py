@@ -76,3 +76,12 @@ def test_fused_march_matches_oracle_and_per_slice_path(cos_correction, monkeypat
     assert np.array_equal(t, t_again)
     assert worst(t, ot) < 1e-5
     assert worst(t, tg) < 1e-5
+    # the device-resident entry point runs the same kernels
+    import torch
+
+    dev = torch.device("cuda", 0)
+    fin = torch.from_numpy(np.ascontiguousarray(fields[:, :, 0, :].transpose(2, 1, 0))).to(dev)
+    tout = torch.empty_like(fin)
+    s.solve_device(fin, tout)
+    torch.cuda.synchronize()
+    assert np.array_equal(tout.cpu().numpy().transpose(2, 1, 0), t[:, :, 0, :])

@@ -263,8 +263,8 @@ def test_tensor_RI_solve_matches_oracle(acyclic):
 
 def test_tensor_RI_on_pipelined_grid_matches_oracle():
     """Tensor solve on a padded (88, 88, 40) grid: plain x-FFTs around the
-    coupling step, pipelined y-passes, dyadic z-pass; and odt_gradient
-    refuses a tensor potential."""
+    coupling step, pipelined y-passes, dyadic z-pass; graph replays give the
+    eager result's bits; odt_gradient refuses a tensor potential."""
     import ctypes as C
 
     from inverse_solver_b200 import FORWARD_SOLVER_CONVERGENT_BORN, _lib
@@ -282,6 +282,10 @@ def test_tensor_RI_on_pipelined_grid_matches_oracle():
     s.set_RI(T)
     assert s.sim_size == [88, 88, 40]
     t, _, f3 = s.solve(fv)
+    # second and third solves: captured into a CUDA graph, then replayed
+    for _ in range(2):
+        t2, _, f32 = s.solve(fv)
+        assert np.array_equal(t2, t) and np.array_equal(f32, f3)
     a = _lib.GradientArgs()
     g = np.zeros(size, np.complex64, order="F")
     err = C.c_double(0)
