@@ -797,7 +797,7 @@ odt_status odt_set_tensor_potential(odt_handle h, const odt_potential_params* pp
 }
 
 namespace {
-void check_ri_device_args(const Handle& H, const odt_ri_device_args* a, const char* fn) {
+void check_ri_device_args(const odt_ri_device_args* a, const char* fn) {
   const std::string who(fn);
   if (!a || !a->ri) raise(ODT_ERR_INVALID_ARGUMENT, who + ": NULL argument");
   if (!is_device_ptr(a->ri)) raise(ODT_ERR_INVALID_ARGUMENT, who + ": ri is not a device pointer");
@@ -809,7 +809,7 @@ void check_ri_device_args(const Handle& H, const odt_ri_device_args* a, const ch
 odt_status odt_potential_eps_device(odt_handle h, const odt_ri_device_args* a, float* eps_imag) {
   return guarded([&] {
     auto H = lookup(h);
-    check_ri_device_args(*H, a, "odt_potential_eps_device");
+    check_ri_device_args(a, "odt_potential_eps_device");
     if (!eps_imag) raise(ODT_ERR_INVALID_ARGUMENT, "odt_potential_eps_device: NULL eps_imag");
     DeviceGuard dg(H->g.device);
     cudaStream_t s = (cudaStream_t)a->stream;
@@ -834,7 +834,7 @@ odt_status odt_potential_eps_device(odt_handle h, const odt_ri_device_args* a, f
 odt_status odt_set_potential_device(odt_handle h, const odt_potential_params* pp, const odt_ri_device_args* a) {
   return guarded([&] {
     auto H = lookup(h);
-    check_ri_device_args(*H, a, "odt_set_potential_device");
+    check_ri_device_args(a, "odt_set_potential_device");
     set_potential_slot(H, a->adjoint ? 1 : 0, pp, nullptr, "odt_set_potential_device", a);
   });
 }

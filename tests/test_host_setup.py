@@ -61,3 +61,28 @@ def test_tensor_potential_matches_oracle():
     assert np.array_equal(h.V, o.V)
     assert np.array_equal(keep[-1], o.V) and keep[-1].flags.f_contiguous
     assert float(h.eps_imag) == float(o.eps_imag) and h.Bornmax == o.Bornmax
+
+
+def test_tensor_potential_argument_checks():
+    """A tensor RI needs the dyadic Green's function and the [x, y, z, 3, 3]
+    shape; the struct form needs a tensor (FORWARD_SOLVER_CONVERGENT_BORN.m
+    :181-186)."""
+    import pytest
+
+    RI = cases.small_RI()[:24, :24, :18]
+    T = np.full(RI.shape + (3, 3), cases.NM, np.float32)
+    for i in range(3):
+        T[:, :, :, i, i] = RI
+    scalar = CBSHostSetup(cases.params([24, 24, 18], [1.5, 1.5, 1.5]))
+    with pytest.raises(ValueError):
+        scalar.prepare_tensor_potential(T)
+    p = cases.params([24, 24, 18], [1.5, 1.5, 1.5])
+    p["vector_simulation"] = True
+    vec = CBSHostSetup(p)
+    with pytest.raises(ValueError):
+        vec.prepare_tensor_potential(T[..., :2])
+    with pytest.raises(ValueError):
+        vec.prepare_tensor_potential(T[:20])
+    vec.prepare_tensor_potential(T)
+    assert vec.tensor and np.all(vec.V[:, :, :, 0, 1] == 0)
+    assert vec.eps_imag > 0 and np.all(vec.V[:, :, :, 0, 0].imag == -vec.eps_imag)
