@@ -41,15 +41,17 @@ def _params(n_scan):
     return p
 
 
-def _inputs():
+def _inputs(npol=1):
+    """Fields [F_x, F_y, npol, n]: npol = 2 for dyadic (vector) solvers, whose
+    shares split along the illumination axis the same way."""
     rng = np.random.default_rng(1)
-    shp = (6, 5, 1, 7)
+    shp = (6, 5, npol, 7)
     a = (rng.standard_normal(shp) + 1j * rng.standard_normal(shp)).astype(np.complex64)
     b = (rng.standard_normal(shp) + 1j * rng.standard_normal(shp)).astype(np.complex64)
     return a, b
 
 
-def _worker(rank, world, port, outdir, n_scan):
+def _worker(rank, world, port, outdir, n_scan, npol):
     import torch.distributed as dist
     from datetime import timedelta
 
@@ -63,7 +65,7 @@ def _worker(rank, world, port, outdir, n_scan):
                 return (None, 0.0) if fi.shape[3] == 0 else _fake_gradient(fi, fo)
 
         s = Stub(_params(n_scan), init_solver=False)
-        a, b = _inputs()
+        a, b = _inputs(npol)
         g, e = s.get_gradiant(np.ones((6, 5, 3), np.complex64), a, b)
         g2, e2 = s.get_gradiant(np.ones((6, 5, 3), np.complex64), a, b)   # second draw of the scan list
         np.savez(os.path.join(outdir, f"r{rank}.npz"), g=g, e=e, g2=g2, e2=e2)
@@ -71,12 +73,12 @@ def _worker(rank, world, port, outdir, n_scan):
         dist.destroy_process_group()
 
 
-def _expected(world, n_scan):
+def _expected(world, n_scan, npol):
     """The reference's computation in one process."""
     from inverse_solver_b200.backward import BACKWARD_SOLVER_MULTI
 
     s = BACKWARD_SOLVER_MULTI(_params(n_scan), init_solver=False)
-    a, b = _inputs()
+    a, b = _inputs(npol)
     res = []
     for _ in range(2):
         sl = s.scan_list(a.shape[3])
@@ -98,15 +100,15 @@ def _free_port():
         return sk.getsockname()[1]
 
 
-@pytest.mark.parametrize("world,n_scan", [(2, 0), (3, 0), (2, 4)])
-def test_gloo_ranks_match_single_process(world, n_scan):
+@pytest.mark.parametrize("world,n_scan,npol", [(2, 0, 1), (3, 0, 1), (2, 4, 1), (2, 0, 2)])
+def test_gloo_ranks_match_single_process(world, n_scan, npol):
     import torch.multiprocessing as mp
 
     with tempfile.TemporaryDirectory() as d:
-        mp.start_processes(_worker, args=(world, _free_port(), d, n_scan), nprocs=world, join=True,
+        mp.start_processes(_worker, args=(world, _free_port(), d, n_scan, npol), nprocs=world, join=True,
                            start_method="spawn")
         outs = [np.load(os.path.join(d, f"r{r}.npz")) for r in range(world)]
-    (g, e), (g2, e2) = _expected(world, n_scan)
+    (g, e), (g2, e2) = _expected(world, n_scan, npol)
     for o in outs:   # every rank holds the same reduced gradient
         np.testing.assert_allclose(o["g"], g, rtol=1e-6, atol=1e-6)
         np.testing.assert_allclose(o["g2"], g2, rtol=1e-6, atol=1e-6)
