@@ -281,13 +281,16 @@ bpm_march128_kernel(float2* __restrict__ fld, const float2* __restrict__ rk, con
     const float2* fz = fm + (long long)z * kM * kM;
     for (int jy = w; jy < kMH; jy += nw) {
       const int py = kMH * rank + jy;
-      float2 v[4];
+      float2 v[4], e4[4];
 #pragma unroll
-      for (int r = 0; r < 4; ++r) v[r] = S[(l + 32 * r) + kMP * jy];
+      for (int r = 0; r < 4; ++r) {
+        v[r] = S[(l + 32 * r) + kMP * jy];
+        e4[r] = fz[(l + 32 * r) + kM * py];  // issued before the transform hides its latency
+      }
       wfft128_inv(v, t, l);
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
-        float2 e = fz[(l + 32 * r) + kM * py];
+        float2 e = e4[r];
         if (inv_cos) e = cscale(e, ic);
         float sn, cs;
         sincosf(e.y, &sn, &cs);
@@ -302,13 +305,16 @@ bpm_march128_kernel(float2* __restrict__ fld, const float2* __restrict__ rk, con
     const bool more = z + 1 < nz;
     for (int px = kMH * rank + w; px < kMH * rank + kMH; px += nw) {
       const int kx = march_perm(px);
-      float2 v[4];
+      float2 v[4], k4[4];
 #pragma unroll
-      for (int r = 0; r < 4; ++r) v[r] = (r < 2 ? S0 : S1)[px + kMP * (ylo + 32 * (r & 1))];
+      for (int r = 0; r < 4; ++r) {
+        v[r] = (r < 2 ? S0 : S1)[px + kMP * (ylo + 32 * (r & 1))];
+        k4[r] = more ? rk[kx + kM * march_perm(l + 32 * r)] : make_float2(0.f, 0.f);
+      }
       wfft128_fwd(v, t, l);
       if (more) {
 #pragma unroll
-        for (int r = 0; r < 4; ++r) v[r] = cmul(v[r], rk[kx + kM * march_perm(l + 32 * r)]);
+        for (int r = 0; r < 4; ++r) v[r] = cmul(v[r], k4[r]);
         wfft128_inv(v, t, l);
 #pragma unroll
         for (int r = 0; r < 4; ++r) (r < 2 ? S0 : S1)[px + kMP * (ylo + 32 * (r & 1))] = v[r];
