@@ -38,6 +38,12 @@ def test_bad_handle_and_null_arguments():
     with pytest.raises(_lib.OdtError) as e:
         _lib.check(lib.odt_solve(77, None))
     assert e.value.status == 2
+    # RI-tensor potential: NULL V, then an unknown handle (no device call)
+    pp = _lib.PotentialParams()
+    assert lib.odt_set_tensor_potential(77, C.byref(pp), None) == 1
+    v = (C.c_float * 18)()
+    assert lib.odt_set_tensor_potential(77, C.byref(pp), C.cast(v, C.c_void_p)) == 2
+    assert b"unknown handle" in lib.odt_last_error()
 
 
 def test_unwrap_argument_checks():
