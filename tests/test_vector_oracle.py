@@ -210,3 +210,25 @@ def test_tensor_RI_argument_checks():
     sp = cases.params(SIZE, [2, 2, 1.5])
     with pytest.raises(ValueError):
         cbs.ForwardSolverCBS(sp, single=True).set_RI(_tensor_of(RI))   # scalar Green's function
+
+
+def test_oracle_reproduces_the_vector_golden_fixture():
+    """tests/golden/vector_small.npz (make_vector_golden.py): isotropic and
+    RI-tensor dyadic solves and the vector gradient.  The oracle still gives
+    them (regression pin of the oracle), and single against double precision
+    stays within 1e-4 (the single-precision error the parity bar allows)."""
+    import os
+    import sys
+
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    sys.path.insert(0, here)
+    import make_vector_golden as mvg
+
+    g = np.load(os.path.join(here, "vector_small.npz"))
+    for single, sfx, tol in ((True, "32", 1e-6), (False, "64", 1e-12)):
+        out = mvg.compute(single)
+        for k in ("iso_trans", "iso_ref", "ten_trans", "ten_ref", "grad"):
+            assert cbs.rel_l2(out[k], g[k + sfx]) < tol, (k, sfx)
+        assert abs(float(out["err"]) - float(g["err" + sfx])) <= tol * float(g["err" + sfx])
+    for k in ("iso_trans", "ten_trans", "grad"):
+        assert cbs.rel_l2(g[k + "32"], g[k + "64"]) < 1e-4, k
