@@ -38,10 +38,19 @@ SEED = 0
 # (complex64 = 8 B): born_x reads T, Field_n, Field, V and writes T, Field_n,
 # Field; born_y / born_z read and write T once.  "_pipe" = the pipelined
 # (TMA-fed, persistent) variants of the same passes; "born_x_pipe_edge" = the
-# pipelined x-pass of iterations 2, 3 and the final pass (56 B nominal).
+# pipelined x-pass of iterations 2, 3 and the final pass (56 B nominal);
+# "born_xy" = the fused xy-pass (x-pass and both y-FFTs with the plane in
+# shared memory: the same 56 B as the x-pass), "born_xy_edge" its launches
+# for iterations 1-3 and the final pass.
 ALG_BYTES_PER_VOXEL = {"born_x": 56, "born_y": 16, "born_z": 16,
                        "born_x_pipe": 56, "born_y_pipe": 16, "born_z_pipe": 16,
-                       "born_x_pipe_edge": 56}
+                       "born_x_pipe_edge": 56, "born_xy": 56, "born_xy_edge": 56}
+# the same with T and Field_n in 16-bit block floating point (4 B per value
+# plus one exponent byte per 8 values): xy-pass 4+4 (T) + 4+4 (Field_n) + 16
+# (Field) + 8 (V) + 0.5 (exponents) = 40.5 B, z-pass 8 + 0.25 = 8.25 B; one
+# iteration 48.75 B (48 B without the exponents)
+ALG_BYTES_B16 = {"born_xy": 40.5, "born_xy_edge": 40.5, "born_z_pipe": 8.25}
+ITER_BYTES_B16 = 48.75
 
 
 def workload_params():
@@ -279,6 +288,7 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_val = world * vox_step * e2e_steps / float(te.item())
 
+    mixed = None if args.no_mixed else mixed_storage_run(args, s, fin, tout, stream, vox_step, dev, dist)
     if rank != 0:
         s.delete()
         return
@@ -318,16 +328,72 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(hin.numel() * 8),
                 "d2h_bytes_per_step": int(hout.numel() * 8)},
     }
+    if mixed is not None:
+        mk = mixed.pop("kernel_times")
+        xy_ms, xy_n = mk.get("born_xy", (0.0, 0))
+        mixed["roofline"] = {
+            "kernel": "born_xy", "bytes_per_voxel": ALG_BYTES_B16["born_xy"], "peak": peak,
+            "achieved": (ALG_BYTES_B16["born_xy"] * vox_launch / (xy_ms / xy_n / 1e3) / 1e9) if xy_n else None,
+            "iteration_frac": (ITER_BYTES_B16 * vox_step / (sum(v[0] for k, v in mk.items()
+                                                                if k in ALG_BYTES_B16) / 1e3) / 1e9) / peak,
+            "iteration_bytes_per_voxel": ITER_BYTES_B16}
+        if mixed["roofline"]["achieved"]:
+            mixed["roofline"]["frac"] = mixed["roofline"]["achieved"] / peak
+        mixed["speedup_vs_fp32_batched"] = mixed["value"] / value
+        out["mixed_b16"] = mixed
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(p, RI, fields, args.ref_iters)
     if world == 1 and not args.no_plain:
         pv = plain_single_solve(p, RI, fields)
+        if mixed is not None:
+            mixed["speedup_vs_plain_single_solve"] = mixed["value"] / pv
         out["plain_single_solve"] = {
             "value": pv, "unit": UNIT, "speedup_of_value": value / pv,
             "what": "same workload, one illumination per solve, generic tile kernels, no graph "
                     "replay, host calls (3 illuminations timed)"}
     s.delete()
     print(json.dumps(out))
+
+
+def mixed_storage_run(args, s, fin, tout, stream, vox_step, dev, dist):
+    """The same batched solve with T and Field_n in 16-bit block floating
+    point (field_storage "b16"): voxel-iter/s (CUDA events, max over ranks),
+    its per-kernel times, and the relative L2 distance of its transmitted
+    fields from the FP32 run's (the FP64 comparison is
+    tests/test_b16_storage_gpu.py)."""
+    import torch
+
+    s.set_field_storage("b16")
+    t16 = torch.empty_like(tout)
+    for _ in range(max(3, args.warmup)):
+        s.solve_device(fin, t16, stream=stream)
+    torch.cuda.synchronize()
+    s.set_profiling(True)
+    s.solve_device(fin, t16, stream=stream)
+    torch.cuda.synchronize()
+    kt = s.kernel_times()
+    s.set_profiling(False)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        s.solve_device(fin, t16, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    world = dist.get_world_size() if dist else 1
+    rel = float(torch.linalg.vector_norm(t16 - tout) / torch.linalg.vector_norm(tout))
+    s.set_field_storage("complex64")
+    return {"value": world * vox_step * args.steps / (ms / 1e3), "unit": UNIT,
+            "ms_per_step": ms / args.steps, "storage": "T and Field_n: 16-bit block floating point "
+            "(8 values per exponent, 15-bit mantissas); Field, V, inputs and outputs complex64; FP32 "
+            "arithmetic", "trans_rel_l2_vs_fp32": rel, "kernel_times": kt,
+            "kernel_ms_per_step": {k: v[0] for k, v in kt.items() if v[1]}}
 
 
 def run_fista(args):
@@ -542,6 +608,30 @@ def workload_key():
     return "cbs_forward_128cube_49ill"
 
 
+def free_port():
+    import socket
+
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as so:
+        so.bind(("127.0.0.1", 0))
+        return so.getsockname()[1]
+
+
+def rank_launch_cmd(n, argv, port):
+    """torchrun command that starts n ranks of this script on one node, each
+    with its own RANK / LOCAL_RANK / WORLD_SIZE (rendezvous on 127.0.0.1)."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+            "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + list(argv)
+
+
+def launch_ranks(n, argv):
+    """`bench.py --gpus N` started without a launcher: start N ranks (one
+    process per GPU) and return their exit status."""
+    env = dict(os.environ)
+    env.setdefault("NCCL_NVLS_ENABLE", "0")
+    return subprocess.run(["timeout", "-k", "60", "3000"] + rank_launch_cmd(n, argv, free_port()),
+                          env=env).returncode
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -553,6 +643,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the plain single-solve comparison")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the 16-bit storage (b16) measurement")
     ap.add_argument("--n-ill", type=int, default=N_ILL,
                     help="illuminations per step (profiling runs use fewer)")
     ap.add_argument("--profile-run", action="store_true",
@@ -565,10 +657,18 @@ def main():
                     help="time the beam-propagation forward solver")
     ap.add_argument("--fista", action="store_true",
                     help="time FISTA outer iterations of the inverse solver (device vs host loop)")
+    ap.add_argument("--print-rank-env", action="store_true",
+                    help="print each rank's RANK / LOCAL_RANK / WORLD_SIZE and exit (launcher check)")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(launch_ranks(args.gpus, sys.argv[1:]))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.print_rank_env:
+        print(json.dumps({"rank": rank, "local_rank": local_rank, "world": world, "gpus": args.gpus}),
+              flush=True)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

@@ -608,6 +608,26 @@ odt_status odt_destroy(odt_handle h);
 /* Number of illuminations the handle keeps resident per batch. */
 odt_status odt_get_batch(odt_handle h, int32_t* batch);
 
+/* Storage of the Born loop's spectral array T and Field_n (no counterpart in
+ * the reference, which computes in single precision throughout):
+ *   ODT_STORAGE_COMPLEX64 (default) -- complex64, the reference's precision;
+ *   ODT_STORAGE_B16 -- 16-bit block floating point: each block of 8 values
+ *     shares a power-of-two exponent and every value keeps 15-bit int16
+ *     mantissas for its real and imaginary parts.  Field (the running sum),
+ *     V and all inputs and outputs stay complex64 and every operation still
+ *     computes in FP32; only the two arrays that each iteration rewrites are
+ *     stored narrower, so an iteration moves 48 instead of 72 bytes per voxel.
+ *     The error against the FP64 result stays below 1e-4 relative L2 on the
+ *     benchmark grid (the storage rounding of the early, largest Born terms
+ *     dominates it, so every iteration uses the same format).
+ * B16 needs the fused xy-pass: a scalar potential on a grid whose x and y
+ * lengths are equal and one of 88, 96, 120, 152 (z: 8 * {11, 12, 15, 19, 25, 27});
+ * a solve on another grid fails with ODT_ERR_UNSUPPORTED.  Not to be called
+ * while a solve on the same handle runs. */
+#define ODT_STORAGE_COMPLEX64 0
+#define ODT_STORAGE_B16 1
+odt_status odt_set_field_storage(odt_handle h, int32_t storage);
+
 /* Per-kernel timing (CUDA events around every launch on the solve stream).
  * When enabled, odt_get_kernel_times fills up to `cap` entries of names
  * (static strings), accumulated milliseconds and launch counts since the
@@ -631,15 +651,20 @@ odt_status odt_get_kernel_times(odt_handle h, const char** names, double* ms,
  * and the FFT twiddles: 3 * prod(sim_size) + sum(sim_size) complex64) lives in
  * one fixed 64 MiB array that every GPU which loads the library holds until
  * the process exits.  Grids needing more (more than about 2.79 million padded
- * voxels, e.g. 152^3) are rejected with ODT_ERR_OUT_OF_MEMORY.
+ * voxels, e.g. 152^3) are rejected with ODT_ERR_OUT_OF_MEMORY.  Each padded
+ * length must factor into radices up to 31, as for odt_solve (e.g. 145 =
+ * 5 * 29 is accepted); other lengths are rejected with ODT_ERR_UNSUPPORTED.
  *
  * The first call on each device looks up the array's device address
- * (cudaGetSymbolAddress), so make that first call before any stream capture.
- * All calls share the one array and it keeps the last call's contents (each
- * call writes every scratch element before reading it, so nothing needs
- * clearing); calls that overlap on the GPU -- two host threads, or work on
- * two streams -- race on it.  The call returns after the work on `stream`
- * has finished.  Inputs are those odt_set_potential takes (V, the 1D tables,
+ * (cudaGetSymbolAddress), so make that first call before any stream capture;
+ * the address is kept for the life of the process, so do not call this entry
+ * point on a device after cudaDeviceReset.  The FFT twiddle tables are copied
+ * into the array from host memory on the first call for a grid size and
+ * reused by later calls on the same size.  All calls share the one array and
+ * it keeps the last call's contents (each call writes every scratch element
+ * before reading it, so nothing needs clearing); calls that overlap on the
+ * GPU -- two host threads, or work on two streams -- race on it.  The call
+ * returns after the work on `stream` has finished.  Inputs are those odt_set_potential takes (V, the 1D tables,
  * the scalars), plus the incident field inside the ROI; `fout` receives
  * Field(ROI) + incident field, as field3d of odt_solve does.
  */

@@ -15,6 +15,8 @@ LIB_PATH = os.path.join(_HERE, "libodt.so")
 
 ODT_MEM_HOST = 0
 ODT_MEM_DEVICE = 1
+ODT_STORAGE_COMPLEX64 = 0
+ODT_STORAGE_B16 = 1
 
 STATUS_NAMES = {
     0: "ODT_OK",
@@ -346,6 +348,7 @@ SIGNATURES = {
     "odt_destroy": (C.c_int, [C.c_uint32]),
     "odt_get_batch": (C.c_int, [C.c_uint32, C.POINTER(C.c_int32)]),
     "odt_set_profiling": (C.c_int, [C.c_uint32, C.c_int32]),
+    "odt_set_field_storage": (C.c_int, [C.c_uint32, C.c_int32]),
     "odt_get_kernel_times": (C.c_int, [C.c_uint32, C.POINTER(C.c_char_p),
                                        C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                        C.c_int32, C.POINTER(C.c_int32)]),

@@ -231,16 +231,17 @@ __global__ void __launch_bounds__(W * 8, W == 16 ? 2 : 3)
       P.rz = a.ramp[2][z];
       lines[tid] = P;
     }
-    bool ok = mbar_wait(&bar[s], s ? phT1 : phT0);
-    if (s) phT1 ^= 1; else phT0 ^= 1;
+    bool ok = mbar_wait(&bar[s], s ? phT1 : phT0, a.wait_limit);
     if (__syncthreads_or(!ok)) {
       if (tid == 0) {  // give up; let this CTA's copies in flight land first
         atomicCAS(fault, 0, kFaultTimeout);
+        mbar_wait(&bar[s], s ? phT1 : phT0);
         if (next < ntiles) mbar_wait(&bar[s ^ 1], s ? phT0 : phT1);
         mbar_wait(&bar[2], phF);
       }
       return;
     }
+    if (s) phT1 ^= 1; else phT0 ^= 1;
     float2* T0 = s ? sT1 : sT0;
     // ---- inverse radix-R2 pass (ns = 1), in place
     {
@@ -253,15 +254,16 @@ __global__ void __launch_bounds__(W * 8, W == 16 ? 2 : 3)
 #pragma unroll
       for (int r = 0; r < R2; ++r) T0[c * N + j * R2 + r] = v[r];
     }
-    ok = mbar_wait(&bar[2], phF);
-    phF ^= 1;
+    ok = mbar_wait(&bar[2], phF, a.wait_limit);
     if (__syncthreads_or(!ok)) {
       if (tid == 0) {
         atomicCAS(fault, 0, kFaultTimeout);
+        mbar_wait(&bar[2], phF);
         if (next < ntiles) mbar_wait(&bar[s ^ 1], s ? phT0 : phT1);
       }
       return;
     }
+    phF ^= 1;
     // ---- inverse radix-8 (ns = R2) -> update + source -> forward radix-8
     for (int sl = tid; sl < kSlots; sl += kThreads) {
       int c, j;

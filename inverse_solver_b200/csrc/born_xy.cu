@@ -1,0 +1,429 @@
+// Fused xy-pass of the Born iteration: the whole x-y plane of one z and one
+// illumination in shared memory, so one iteration moves 72 bytes per voxel
+// (this pass: T, Field_n, Field read and written, V read; the z-pass: T read
+// and written) instead of the 104 of separate x-, y- and y-passes.
+//
+// Per plane (FORWARD_SOLVER_CONVERGENT_BORN.m:577-647; jj = iteration):
+//   inverse y-FFT and inverse x-FFT of the spectral array T (the last two
+//   transforms of PSI = ifftn(G .* fftn(psi)) of iteration jj-1), update of
+//   iteration jj-1 (:616-642), source term of iteration jj times the phase
+//   ramp (:588-605), forward x-FFT and forward y-FFT (the first two of fftn).
+// The z-pass (cols_pipe.cu) does the z-FFT, the Green's multiply and the
+// inverse z-FFT in between.
+//
+// Transforms along an axis of length N = 8 R (R = 11, 12, 15, 19): index
+// n = R n1 + n2 (n1 < 8, n2 < R), k = k1 + 8 k2 (k1 < 8, k2 < R).
+//   forward  F1: 8-point DFT over n1 of the positions R n1 + n2 (stride R),
+//                result k1 stored at R k1 + n2;
+//            F2: times W_N^(n2 k1);
+//            F3: R-point DFT over n2 of the contiguous positions R k1 + n2,
+//                result k2 stored at R k1 + k2.
+//   inverse  the same steps in reverse order with conjugate roots.
+// Every step writes the positions it read, so the plane is transformed in
+// place and needs one buffer; the spectrum is stored in this permuted order
+// (spectral index k1 + 8 k2 at position R k1 + k2 along x and along y) and
+// the z-pass maps each column to its (kx, ky) accordingly (BornArgs.perm_xy).
+// Space-domain data is in natural order, so the pointwise work reads and
+// writes Field_n / Field / V / the incident field in their global layout.
+//
+// Seven steps per plane separated by CTA barriers:
+//   1 y-F3^-1 + F2^-1  read T from global (one R-point column group per item)
+//   2 y-F1^-1          shared memory
+//   3 x-F3^-1 + F2^-1  shared memory
+//   4 x-F1^-1, update + source, x-F1 (8 points per item; the global reads
+//                      and writes of Field_n, Field, V, E_inc)
+//   5 x-F2 + F3        shared memory
+//   6 y-F1             shared memory
+//   7 y-F2 + F3        write T to global
+// One CTA per SM (the plane takes 8 N^2 bytes: 185 KB for N = 152) with 32 R
+// threads, persistent over the planes (illumination fastest, so concurrent
+// CTAs share V's planes in L2).  The next plane's T and Field_n / Field are
+// prefetched into L2 (cp.async.bulk.prefetch) during steps 4 and 6 of the
+// current one, so their DRAM reads overlap the shared-memory steps.
+//
+// Bank conflicts: rows have a pitch of N = 8 (mod 16) complex elements for
+// odd R (N = 96: 0 mod 16, two-way conflicts in steps 3 and 5).
+// Steps 1, 2, 6, 7 put consecutive x on consecutive lanes; steps 3 and 5
+// take R consecutive elements at R k1 (lanes over k1 and rows: the stride of
+// 2R banks and the row pitch of 16 banks keep a half-warp's 8-byte accesses
+// on distinct bank pairs); step 4 takes consecutive n2 on consecutive lanes.
+#include <cuda_runtime.h>
+
+#include "b16.cuh"
+#include "cbs_kernels.cuh"
+#include "fft_core.cuh"
+#include "tma.cuh"
+
+namespace odt {
+namespace {
+
+constexpr size_t a16(size_t b) { return (b + 15) & ~(size_t)15; }
+constexpr size_t a128(size_t b) { return (b + 127) & ~(size_t)127; }
+
+template <int R>
+struct XYSmem {
+  static constexpr int N = 8 * R;
+  static constexpr size_t kTw = 0;                                    // W_N^k, k < N
+  static constexpr size_t kRampX = kTw + a16(sizeof(float2) * N);     // ramp along x
+  static constexpr size_t kRampY = kRampX + a16(sizeof(float2) * N);  // ramp along y
+  static constexpr size_t kMaskX = kRampY + a16(sizeof(float2) * N);
+  static constexpr size_t kMaskY = kMaskX + a16(sizeof(float) * N);
+  static constexpr size_t kPlane = a128(kMaskY + a16(sizeof(float) * N));
+  static constexpr size_t kTotal = kPlane + sizeof(float2) * N * N;
+};
+
+// KIND: which Born iterations a launch serves (compile time, so the steady
+// kernel carries none of the other cases' work)
+enum XYKind { kXYSteady = 0, kXYEarly = 1, kXYFinal = 2, kXYFirst = 3 };
+
+#if defined(__CUDA_ARCH__)
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+#endif
+
+// ST: storage of T and Field_n, 0 = complex64, 1 = 16-bit block floating
+// point (b16.cuh; T's blocks are 8 consecutive x of a row, Field_n's are 8
+// consecutive step-4 work items of one n1, exponent index
+// plane * N^2/8 + n1 * R^2 + item / 8)
+template <int R, int KIND, int ST>
+__global__ void __launch_bounds__(32 * R, 1)
+    born_xy_kernel(const BornArgs a, const int jj, const float2* __restrict__ twg, const int nplanes) {
+#if defined(__CUDA_ARCH__)
+  constexpr int N = 8 * R;
+  constexpr int NT = 32 * R;
+  using L = XYSmem<R>;
+  extern __shared__ __align__(128) unsigned char sm[];
+  float2* tw = reinterpret_cast<float2*>(sm + L::kTw);
+  float2* rxt = reinterpret_cast<float2*>(sm + L::kRampX);
+  float2* ryt = reinterpret_cast<float2*>(sm + L::kRampY);
+  float* mxt = reinterpret_cast<float*>(sm + L::kMaskX);
+  float* myt = reinterpret_cast<float*>(sm + L::kMaskY);
+  float2* pl = reinterpret_cast<float2*>(sm + L::kPlane);
+  const int tid = threadIdx.x;
+  const float2 one = make_float2(1.f, 0.f);
+  const float2 z2 = make_float2(0.f, 0.f);
+  for (int i = tid; i < N; i += NT) {
+    tw[i] = twg[i];
+    rxt[i] = a.acyclic ? a.ramp[0][i] : one;
+    ryt[i] = a.acyclic ? a.ramp[1][i] : one;
+    mxt[i] = a.mask[0][i];
+    myt[i] = a.mask[1][i];
+  }
+  __syncthreads();
+
+  constexpr bool kInv = KIND != kXYFirst;   // transforms T back (update of jj-1)
+  constexpr bool kFwd = KIND != kXYFinal;   // forms the source and transforms it
+  const int e = jj - 1;                     // iteration whose update completes here
+  const long long plane_n = (long long)N * N;
+  const long long est = (long long)a.rx * a.ry * a.rz;
+  const float2 cc = make_float2(0.f, a.c_im);
+  // Field_n / Field are read by the update from iteration 3 on (and Field by
+  // the final pass of a 2-iteration series); the incident field by the
+  // source of iteration 1 and 2 and by the final pass
+  const bool need_fn = kInv && e >= 3;
+  const bool need_f = kInv && (e >= 3 || (KIND == kXYFinal && e == 2));
+  const bool need_e = KIND == kXYFinal || ((KIND == kXYFirst || KIND == kXYEarly) && jj <= 2);
+
+  for (int p = blockIdx.x; p < nplanes; p += gridDim.x) {
+    const int b = p % a.nbatch;
+    const int z = p / a.nbatch;
+    const long long g0 = plane_n * (z + (long long)a.pz * b);   // plane (z, b) of T / Field_n / Field
+    const long long v0 = plane_n * z;
+    const int pn = p + gridDim.x;
+    const long long gn = pn < nplanes ? plane_n * (pn / a.nbatch + (long long)a.pz * (pn % a.nbatch)) : -1;
+    const float mz = a.mask[2][z];
+    const float2 rz = a.acyclic ? a.ramp[2][z] : one;
+    const bool zroi = (unsigned)(z - a.rz0) < (unsigned)a.rz;
+
+    if constexpr (kInv) {
+      // ---- 1: y-F3^-1 (R-point over k2 at rows R k1 + k2), twiddles, from T
+      for (int i = tid; i < 8 * N; i += NT) {
+        const int x = i % N, k1 = i / N;
+        float2 v[R];
+        if constexpr (ST == 0) {
+          const float2* src = a.T + g0 + (long long)(R * k1) * N + x;
+#pragma unroll
+          for (int r = 0; r < R; ++r) v[r] = src[(long long)r * N];
+        } else {
+          const long long o = g0 + (long long)(R * k1) * N + x;
+          const short2* src = a.T16 + o;
+          const signed char* se = a.Te + (o >> 3);
+#pragma unroll
+          for (int r = 0; r < R; ++r) v[r] = b16_decode(src[(long long)r * N], se[r * (N >> 3)]);
+        }
+        Butterfly<R, true>::run(v, tw, N);
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], cconj(tw[r * k1]));
+#pragma unroll
+        for (int r = 0; r < R; ++r) pl[(R * k1 + r) * N + x] = v[r];
+      }
+      __syncthreads();
+      // ---- 2: y-F1^-1 (8-point over k1 at rows R k1 + n2) -> natural y
+      for (int i = tid; i < R * N; i += NT) {
+        const int x = i % N, n2 = i / N;
+        float2 v[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = pl[(R * r + n2) * N + x];
+        Butterfly<8, true>::run(v, tw, N);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) pl[(R * r + n2) * N + x] = v[r];
+      }
+      __syncthreads();
+      // ---- 3: x-F3^-1 + F2^-1 on the contiguous groups R k1 .. R k1 + R-1
+      for (int i = tid; i < 8 * N; i += NT) {
+        const int k1 = i & 7, y = i >> 3;
+        float2* row = pl + y * N + R * k1;
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = row[r];
+        Butterfly<R, true>::run(v, tw, N);
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], cconj(tw[r * k1]));
+#pragma unroll
+        for (int r = 0; r < R; ++r) row[r] = v[r];
+      }
+      __syncthreads();
+    }
+    if (kInv && tid == 0 && gn >= 0) {
+      if constexpr (ST == 0) prefetch_l2(a.T + gn, (uint32_t)(plane_n * sizeof(float2)));
+      else prefetch_l2(a.T16 + gn, (uint32_t)(plane_n * sizeof(short2)));
+    }
+
+    // ---- 4: x-F1^-1 -> update of iteration jj-1 and source of jj -> x-F1
+    for (int i = tid; i < R * N; i += NT) {
+      const int n2 = i % R, y = i / R;
+      float2* row = pl + y * N;
+      const long long gy = g0 + (long long)y * N;
+      const long long vy = v0 + (long long)y * N;
+      const bool yzroi = zroi && (unsigned)(y - a.ry0) < (unsigned)a.ry;
+      const long long ebase = (long long)b * est + (long long)(y - a.ry0) * a.rx +
+                              (long long)(z - a.rz0) * a.rx * a.ry - a.rx0;
+      const float my = myt[y];
+      float2 V[8], Fo[8], Fp[8], Ei[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int x = R * r + n2;
+        const bool in_roi = yzroi && (unsigned)(x - a.rx0) < (unsigned)a.rx;
+        V[r] = a.V[vy + x];
+        if constexpr (ST == 0) {
+          Fo[r] = need_fn ? a.Fn[gy + x] : z2;
+        } else {
+          Fo[r] = need_fn ? b16_decode(a.Fn16[gy + x], a.Fe[(g0 >> 3) + r * R * R + (i >> 3)]) : z2;
+        }
+        Fp[r] = need_f ? a.F[gy + x] : z2;
+        Ei[r] = (need_e && in_roi) ? a.Einc[ebase + x] : z2;
+      }
+      // Field_n of element (x, y) of the item's r-th value (the 8 lanes of a
+      // group take 8 consecutive items, so they share Field_n's blocks)
+      auto store_fn = [&](int r, int x, float2 f) {
+        if constexpr (ST == 0) {
+          a.Fn[gy + x] = f;
+        } else {
+          const int ex = b16_group_exponent(f, __activemask());
+          a.Fn16[gy + x] = b16_encode(f, ex);
+          if ((i & 7) == 0) a.Fe[(g0 >> 3) + r * R * R + (i >> 3)] = (signed char)ex;
+        }
+      };
+      float2 v[8];
+      if constexpr (kInv) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = row[R * r + n2];
+        Butterfly<8, true>::run(v, tw, N);
+      }
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int x = R * r + n2;
+        const float2 Vr = V[r];
+        const float2 r0 = a.acyclic ? cmul(cmul(rxt[x], ryt[y]), rz) : one;
+        const bool in_roi = yzroi && (unsigned)(x - a.rx0) < (unsigned)a.rx;
+        float2 fn_new = z2, ftot = z2;
+        if constexpr (kInv) {
+          // PSI .* conj(phase ramp of iteration e)
+          float2 P = v[r];
+          if (a.acyclic) P = cmul(P, (e & 1) ? r0 : cconj(r0));
+          const float m = (mxt[x] * my) * mz;
+          const float2 vP = cmul(Vr, P);
+          if (KIND != kXYSteady && e <= 2) {   // Field_n = (0 + V .* PSI) .* mask
+            fn_new = cscale(vP, m);
+            // Field = 0 + Field_n after iteration 1; after iteration 2 Field
+            // keeps Field_n(1) until the e == 3 update
+            ftot = e == 1 ? fn_new : cadd(Fp[r], fn_new);
+            if (KIND != kXYFinal) {
+              store_fn(r, x, fn_new);
+              if (e == 1) a.F[gy + x] = fn_new;
+            }
+          } else {
+            const float2 fo = Fo[r];
+            const float2 fp = Fp[r];
+            const float2 psi = cmul(cmul(cc, fo), Vr);
+            const float2 fn = cscale(cadd(csub(fo, psi), vP), m);
+            if (e == 3) {  // Field = (Field_n1 + Field_n2) + Field_n3; Field_n = Field_n3 + Field_n1
+              ftot = cadd(cadd(fp, fo), fn);
+              fn_new = cadd(fn, fp);
+            } else {
+              ftot = cadd(fp, fn);
+              fn_new = fn;
+            }
+            if (KIND != kXYFinal) {
+              a.F[gy + x] = ftot;
+              store_fn(r, x, fn_new);
+            }
+          }
+        }
+        if constexpr (KIND == kXYFinal) {
+          if (in_roi) a.Fout[ebase + x] = cadd(ftot, Ei[r]);
+        } else {
+          float2 src;
+          if (jj <= 2) {  // (1i/eps) .* ((V(ROI) + 1i*eps) .* E_inc) / 2 inside the ROI
+            src = in_roi ? cscale(cmul(cc, cmul(make_float2(Vr.x, Vr.y + a.eps), Ei[r])), 0.5f) : z2;
+          } else {        // (1i/eps) .* Field_n .* V
+            src = cmul(cmul(cc, fn_new), Vr);
+          }
+          if (a.acyclic) src = cmul(src, (jj & 1) ? cconj(r0) : r0);
+          v[r] = src;
+        }
+      }
+      if constexpr (kFwd) {
+        Butterfly<8, false>::run(v, tw, N);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) row[R * r + n2] = v[r];
+      }
+    }
+    if constexpr (!kFwd) {
+      __syncthreads();   // the next plane's step 1 overwrites the plane
+      continue;
+    }
+    __syncthreads();
+    // ---- 5: x-F2 + F3 on the contiguous groups
+    for (int i = tid; i < 8 * N; i += NT) {
+      const int k1 = i & 7, y = i >> 3;
+      float2* row = pl + y * N + R * k1;
+      float2 v[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = row[r];
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tw[r * k1]);
+      Butterfly<R, false>::run(v, tw, N);
+#pragma unroll
+      for (int r = 0; r < R; ++r) row[r] = v[r];
+    }
+    __syncthreads();
+    if (tid == 0 && gn >= 0 && need_fn) {
+      if constexpr (ST == 0) prefetch_l2(a.Fn + gn, (uint32_t)(plane_n * sizeof(float2)));
+      else prefetch_l2(a.Fn16 + gn, (uint32_t)(plane_n * sizeof(short2)));
+      prefetch_l2(a.F + gn, (uint32_t)(plane_n * sizeof(float2)));
+    }
+    // ---- 6: y-F1 (8-point over n1 at rows R n1 + n2)
+    for (int i = tid; i < R * N; i += NT) {
+      const int x = i % N, n2 = i / N;
+      float2 v[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) v[r] = pl[(R * r + n2) * N + x];
+      Butterfly<8, false>::run(v, tw, N);
+#pragma unroll
+      for (int r = 0; r < 8; ++r) pl[(R * r + n2) * N + x] = v[r];
+    }
+    __syncthreads();
+    // ---- 7: y-F2 + F3 -> T
+    for (int i = tid; i < 8 * N; i += NT) {
+      const int x = i % N, k1 = i / N;
+      float2 v[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = pl[(R * k1 + r) * N + x];
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tw[r * k1]);
+      Butterfly<R, false>::run(v, tw, N);
+      if constexpr (ST == 0) {
+        float2* dst = a.T + g0 + (long long)(R * k1) * N + x;
+#pragma unroll
+        for (int r = 0; r < R; ++r) dst[(long long)r * N] = v[r];
+      } else {   // the 8 lanes of a group hold 8 consecutive x of the same rows
+        const long long o = g0 + (long long)(R * k1) * N + x;
+        short2* dst = a.T16 + o;
+        signed char* de = a.Te + (o >> 3);
+        const unsigned mask = __activemask();
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int ex = b16_group_exponent(v[r], mask);
+          dst[(long long)r * N] = b16_encode(v[r], ex);
+          if ((x & 7) == 0) de[r * (N >> 3)] = (signed char)ex;
+        }
+      }
+    }
+    __syncthreads();
+  }
+#endif
+}
+
+template <int R, int KIND, int ST>
+cudaError_t launch_r(const BornArgs& a, int jj, const float2* tw, cudaStream_t s) {
+  using L = XYSmem<R>;
+  static DeviceFlags configured;   // attribute raised once per device
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (!configured.test(dev)) {
+    e = cudaFuncSetAttribute(born_xy_kernel<R, KIND, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)L::kTotal);
+    if (e != cudaSuccess) return e;
+    configured.set(dev);
+  }
+  int nsm = 0;
+  e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  const long long nplanes = (long long)a.pz * a.nbatch;
+  const int grid = (int)(nplanes < nsm ? nplanes : nsm);
+  born_xy_kernel<R, KIND, ST><<<grid, 32 * R, L::kTotal, s>>>(a, jj, tw, (int)nplanes);
+  return cudaGetLastError();
+}
+
+template <int R, int ST>
+cudaError_t launch_kind_st(const BornArgs& a, int kind, int jj, const float2* tw, cudaStream_t s) {
+  switch (kind) {
+    case kXYSteady: return launch_r<R, kXYSteady, ST>(a, jj, tw, s);
+    case kXYEarly: return launch_r<R, kXYEarly, ST>(a, jj, tw, s);
+    case kXYFinal: return launch_r<R, kXYFinal, ST>(a, jj, tw, s);
+    default: return launch_r<R, kXYFirst, ST>(a, jj, tw, s);
+  }
+}
+
+template <int R>
+cudaError_t launch_kind(const BornArgs& a, int kind, int jj, const float2* tw, cudaStream_t s) {
+  return a.storage ? launch_kind_st<R, 1>(a, kind, jj, tw, s) : launch_kind_st<R, 0>(a, kind, jj, tw, s);
+}
+
+}  // namespace
+
+bool born_xy_supported(const BornArgs& a, int max_smem) {
+  if (a.px != a.py || a.px % 8 != 0) return false;
+  const int r = a.px / 8;
+  size_t need = 0;
+  switch (r) {
+    case 11: need = XYSmem<11>::kTotal; break;
+    case 12: need = XYSmem<12>::kTotal; break;
+    case 15: need = XYSmem<15>::kTotal; break;
+    case 19: need = XYSmem<19>::kTotal; break;
+    default: return false;
+  }
+  return need <= (size_t)max_smem && (long long)a.pz * a.nbatch < (1LL << 31);
+}
+
+int born_xy_perm_radix(const BornArgs& a) { return a.px / 8; }
+
+cudaError_t launch_born_xy(const BornArgs& a, int mode, int jj, const DevFft& fx, cudaStream_t s) {
+  int kind;
+  if (mode == kBornFirst) kind = kXYFirst;
+  else if (mode == kBornLast) kind = kXYFinal;
+  else kind = jj <= 3 ? kXYEarly : kXYSteady;
+  if ((mode == kBornFirst) != (jj == 1)) return cudaErrorInvalidValue;
+  switch (a.px / 8) {
+    case 11: return launch_kind<11>(a, kind, jj, fx.tw, s);
+    case 12: return launch_kind<12>(a, kind, jj, fx.tw, s);
+    case 15: return launch_kind<15>(a, kind, jj, fx.tw, s);
+    case 19: return launch_kind<19>(a, kind, jj, fx.tw, s);
+    default: return cudaErrorNotSupported;
+  }
+}
+
+}  // namespace odt

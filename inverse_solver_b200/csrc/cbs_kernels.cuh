@@ -38,6 +38,20 @@ struct BornArgs {
   const float2* V;         // potential            [nvox]
   const float2* Einc;      // incident field       [rx*ry*rz, nbatch]
   float2* Fout;            // Field(ROI)+incident  [rx*ry*rz, nbatch]
+  long long wait_limit;    // clock cycles a pipelined kernel's steady mbarrier wait may take
+  // T's x-y spectrum is in the fused xy-pass's order (launch_born_xy): along
+  // an axis of length 8 R, spectral index k1 + 8 k2 (k1 < 8, k2 < R) sits at
+  // position R k1 + k2
+  int perm_xy;
+  // reduced-precision storage (storage = 1): T and Field_n as 16-bit block
+  // floating point (b16.cuh) -- int16 (re, im) mantissas in T16 / Fn16 with
+  // the layouts of T / Field_n, one exponent byte per 8 values in Te / Fe;
+  // Field stays complex64 in F
+  int storage;
+  short2* T16;
+  signed char* Te;
+  short2* Fn16;
+  signed char* Fe;
 };
 
 enum BornXMode { kBornFirst = 0, kBornMid = 1, kBornLast = 2 };
@@ -90,6 +104,14 @@ cudaError_t launch_fft_y_pipe(const BornArgs& a, bool inverse, const DevFft& fy,
                               cudaStream_t s);
 cudaError_t launch_born_z_pipe(const BornArgs& a, int jj, const DevFft& fz, int* fault,
                                cudaStream_t s);
+// Fused xy-pass (born_xy.cu): the whole x-y plane of one z and illumination
+// in shared memory -- inverse y- and x-FFT of T, update of iteration jj-1,
+// source of iteration jj, forward x- and y-FFT -- for px == py = 8 * {11, 12,
+// 15, 19}; replaces launch_born_x and both y-FFTs (modes as launch_born_x;
+// the z-pass must run with a.perm_xy = 1).  Same results as the separate passes
+// up to the order of the FFT arithmetic.
+bool born_xy_supported(const BornArgs& a, int max_smem);
+cudaError_t launch_born_xy(const BornArgs& a, int mode, int jj, const DevFft& fx, cudaStream_t s);
 // z-pass of iteration jj: forward z-FFT, Green's multiply, inverse z-FFT.
 cudaError_t launch_born_z(const BornArgs& a, int jj, const DevFft& fz, cudaStream_t s);
 

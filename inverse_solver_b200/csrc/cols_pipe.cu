@@ -4,16 +4,21 @@
 // FORWARD_SOLVER_CONVERGENT_BORN.m:606-615) -- the same transforms as
 // fft_cols_body / born_z_body, restructured like the pipelined x-pass:
 //
-//   * persistent CTAs (three per SM) walk tiles of 16 adjacent columns;
+//   * persistent CTAs (as many per SM as shared memory and registers allow:
+//     three for the y-FFTs, five for the z-pass at n <= 152) walk tiles of
+//     16 adjacent columns;
 //   * a tile (16 columns x n rows, each row a 128-byte segment at a stride of
 //     px or px*py elements) arrives in shared memory through one tiled TMA
 //     copy (cp.async.bulk.tensor, 3D map for y, 4D for z) on an mbarrier,
 //     while the CTA computes the previous tile from the other stage;
-//   * fixed plan: radix-R2 pass in place in the landing buffer (one butterfly
+//   * y-FFTs: radix-R2 pass in place in the landing buffer (one butterfly
 //     per thread held in registers across a barrier), then radix-8 with
-//     twiddles (y: straight to global memory; z: Green's multiply and the
-//     first inverse radix-8 pass into a second buffer, then the inverse
-//     radix-R2 pass to global memory).
+//     twiddles straight to global memory;
+//   * z-pass: with z = R2 n1 + n2 and kz = k1 + 8 k2, an 8-point DFT over n1
+//     with twiddles, then per (column, k1) the R2-point DFT, the Green's
+//     multiply at kz and the inverse R2-point DFT in registers, then the
+//     inverse 8-point DFT to global memory; every step writes the rows it
+//     read, so the landing buffer is the only buffer.
 //
 // Layout in shared memory: [row][column], 16 columns = 128 bytes per row; the
 // column index is the fastest thread index, so every access of a half-warp
@@ -25,6 +30,7 @@
 
 #include <string>
 
+#include "b16.cuh"
 #include "cbs_kernels.cuh"
 #include "fft_core.cuh"
 #include "tma.cuh"
@@ -51,8 +57,15 @@ struct ColSmem {
   static constexpr size_t kS0 = a1k(kGxy + a16(sizeof(float) * kW));
   static constexpr size_t kS1 = kS0 + kTile;
   static constexpr size_t kB = kS1 + kTile;
-  static constexpr size_t kTotalY = kB;                             // y-pass: no second buffer
-  static constexpr size_t kTotalZ = kB + kTile;
+  static constexpr size_t kTotalY = kB;                             // both kinds: two stages only
+  static constexpr size_t kTotalZ = kB;
+  // z-pass on 16-bit block floating-point storage: two landing stages of
+  // int16 (re, im) pairs, one complex64 work tile, the tile's exponents
+  static constexpr size_t kTile16 = sizeof(short2) * N * kW;
+  static constexpr size_t kS1_16 = kS0 + kTile16;
+  static constexpr size_t kW16 = a1k(kS1_16 + kTile16);
+  static constexpr size_t kEx16 = kW16 + kTile;
+  static constexpr size_t kTotalZ16 = kEx16 + a16(2 * N);
 };
 
 #if defined(__CUDA_ARCH__)
@@ -82,17 +95,21 @@ __device__ __forceinline__ float rcp_approx(float x) {
 }
 #endif
 
-// KIND 0: forward y-FFT, 1: inverse y-FFT, 2: z-pass with Green's multiply.
+// KIND 0: forward y-FFT, 1: inverse y-FFT, 2: z-pass with Green's multiply,
+// 3: the z-pass on 16-bit block floating-point storage (a.T16 / a.Te: the
+// tile lands as int16 pairs, is decoded into a complex64 work tile and the
+// result is encoded again with one exponent per 8 columns of a row).
 // Tile t -> (x-tile fastest, then the outer index o): y-pass o = z + pz*b
 // (3D map {px, py, pz*nb}), z-pass o = y + py*b (4D map {px, py, pz, nb}).
 template <int R2, int KIND>
-__global__ void __launch_bounds__(kThreads, 3)
+__global__ void __launch_bounds__(kThreads, KIND >= 2 ? 5 : 3)
     cols_pipe_kernel(const __grid_constant__ CUtensorMap map, const BornArgs a, const int jj,
                      const float2* __restrict__ twg, const int nxt, const int ntiles,
                      int* __restrict__ fault) {
 #if defined(__CUDA_ARCH__)
   constexpr int N = kR1 * R2;
-  constexpr bool kZ = KIND == 2;
+  constexpr bool kZ = KIND >= 2;
+  constexpr bool k16 = KIND == 3;
   constexpr bool kInvFirst = KIND == 1;  // direction of the first transform
   using L = ColSmem<N>;
   extern __shared__ __align__(128) unsigned char sm[];
@@ -101,8 +118,9 @@ __global__ void __launch_bounds__(kThreads, 3)
   float* kz = reinterpret_cast<float*>(sm + L::kKz);
   float* gxy = reinterpret_cast<float*>(sm + L::kGxy);
   float2* const s0 = reinterpret_cast<float2*>(sm + L::kS0);
-  float2* const s1 = reinterpret_cast<float2*>(sm + L::kS1);
-  float2* const sB = reinterpret_cast<float2*>(sm + L::kB);
+  float2* const s1 = reinterpret_cast<float2*>(sm + (k16 ? L::kS1_16 : L::kS1));
+  float2* const w16 = reinterpret_cast<float2*>(sm + L::kW16);     // k16: work tile
+  signed char* const ex16 = reinterpret_cast<signed char*>(sm + L::kEx16);  // k16: [row][2]
   const int tid = threadIdx.x;
   const bool flip = kZ && a.acyclic && (jj & 1);
   if ((smem_addr(s0) & 127u) != 0u || (smem_addr(s1) & 127u) != 0u) {  // never issue a misaligned copy
@@ -123,12 +141,13 @@ __global__ void __launch_bounds__(kThreads, 3)
   int tile = blockIdx.x;
   if (tile >= ntiles) return;
   const long long rstride = kZ ? (long long)a.px * a.py : a.px;   // element stride between rows
-  constexpr uint32_t kBytes = (uint32_t)(sizeof(float2) * N * kW);
+  constexpr uint32_t kBytes = (uint32_t)((k16 ? sizeof(short2) : sizeof(float2)) * N * kW);
   auto issue = [&](int t, int stage) {
     const int xt = t % nxt, o = t / nxt;
     mbar_arrive_expect_tx(&bar[stage], kBytes);
     float2* dst = stage ? s1 : s0;
-    if (kZ) tma_load_4d(dst, &map, 2 * kW * xt, o % a.py, 0, o / a.py, &bar[stage]);
+    if (k16) tma_load_4d(dst, &map, kW * xt, o % a.py, 0, o / a.py, &bar[stage]);
+    else if (kZ) tma_load_4d(dst, &map, 2 * kW * xt, o % a.py, 0, o / a.py, &bar[stage]);
     else tma_load_3d(dst, &map, 2 * kW * xt, 0, o, &bar[stage]);
   };
   if (tid == 0) issue(tile, 0);
@@ -146,33 +165,37 @@ __global__ void __launch_bounds__(kThreads, 3)
     const int x0 = kW * xt;
     const int ncol = min(kW, a.px - x0);
     if (kZ && tid < kW) {
-      const int y = o % a.py;
-      const int kx = min(x0 + tid, a.px - 1);
+      int y = o % a.py;
+      int kx = min(x0 + tid, a.px - 1);
+      if (a.perm_xy) {   // position R k1 + k2 holds spectral index k1 + 8 k2
+        const int rx = a.px >> 3, ry = a.py >> 3;
+        kx = kx / rx + 8 * (kx % rx);
+        y = y / ry + 8 * (y % ry);
+      }
       const int ix = flip ? (kx == 0 ? 0 : a.px - kx) : kx;
       const int iy = flip ? (y == 0 ? 0 : a.py - y) : y;
       gxy[tid] = a.kq2[0][ix] + a.kq2[1][iy];
     }
-    const bool ok = mbar_wait(&bar[s], s ? ph1 : ph0);
-    if (s) ph1 ^= 1; else ph0 ^= 1;
+    if constexpr (k16) {   // the tile's two exponents per row (blocks x0 .. x0+7, x0+8 .. x0+15)
+      const int y = o % a.py, b = o / a.py;
+      const long long e0 = ((long long)b * a.nvox + (long long)y * a.px + x0) >> 3;
+      const long long es = ((long long)a.px * a.py) >> 3;
+      for (int i = tid; i < 2 * N; i += kThreads) {
+        const int row = i >> 1, h = i & 1;
+        ex16[i] = (h == 0 || x0 + 8 < a.px) ? a.Te[e0 + row * es + h] : (signed char)0;
+      }
+    }
+    const bool ok = mbar_wait(&bar[s], s ? ph1 : ph0, a.wait_limit);
     if (__syncthreads_or(!ok)) {
-      if (tid == 0) {  // give up; let the copy in flight land first
+      if (tid == 0) {  // give up; let the copies in flight land first
         atomicCAS(fault, 0, kFaultTimeout);
+        mbar_wait(&bar[s], s ? ph1 : ph0);
         if (next < ntiles) mbar_wait(&bar[s ^ 1], s ? ph0 : ph1);
       }
       return;
     }
+    if (s) ph1 ^= 1; else ph0 ^= 1;
     float2* S = s ? s1 : s0;
-    // ---- radix-R2 pass (ns = 1), in place: rows jr + 8r -> rows jr*R2 + r
-    {
-      float2 v[R2];
-#pragma unroll
-      for (int r = 0; r < R2; ++r) v[r] = S[(jr + kR1 * r) * kW + c];
-      Butterfly<R2, kInvFirst>::run(v, tw, N);
-      __syncthreads();
-#pragma unroll
-      for (int r = 0; r < R2; ++r) S[(jr * R2 + r) * kW + c] = v[r];
-    }
-    __syncthreads();
     // global address of (row, column) of this tile
     long long gbase;
     if (kZ) {
@@ -181,64 +204,115 @@ __global__ void __launch_bounds__(kThreads, 3)
     } else {
       gbase = (long long)o * a.px * a.py + x0;
     }
-    // ---- radix-8 pass (ns = R2): rows j + R2 r, twiddles tw[r j]
-    for (int idx = tid; idx < kW * R2; idx += kThreads) {
-      const int j = idx >> 4;  // c is idx & 15 == tid & 15
-      float2 v[kR1];
+    if constexpr (kZ) {
+      // z-pass with z = R2 n1 + n2, kz = k1 + 8 k2 (k1 < 8, k2 < R2), every
+      // step in place on the landing buffer:
+      //   A  8-point DFT over n1 at rows R2 n1 + n2, times W_N^(n2 k1)
+      //   B  R2-point DFT over n2 at rows R2 k1 + n2 (kz = k1 + 8 k2), Green's
+      //      multiply, inverse R2-point DFT, times conj W_N^(n2 k1)
+      //   C  inverse 8-point DFT over k1 -> rows R2 n1 + n2 of T
+      float2* const Wt = k16 ? w16 : S;   // the tile the steps work on
+      for (int idx = tid; idx < kW * R2; idx += kThreads) {
+        const int n2 = idx >> 4;  // column c is idx & 15 == tid & 15
+        float2 v[kR1];
+        if constexpr (k16) {
+          const short2* S16 = reinterpret_cast<const short2*>(S);
 #pragma unroll
-      for (int r = 0; r < kR1; ++r) v[r] = S[(j + R2 * r) * kW + c];
+          for (int r = 0; r < kR1; ++r) {
+            const int row = R2 * r + n2;
+            v[r] = b16_decode(S16[row * kW + c], ex16[2 * row + (c >> 3)]);
+          }
+        } else {
 #pragma unroll
-      for (int r = 1; r < kR1; ++r) {
-        float2 w = tw[r * j];
-        if (kInvFirst) w.y = -w.y;
-        v[r] = cmul(v[r], w);
-      }
-      Butterfly<kR1, kInvFirst>::run(v, tw, N);
-      if (!kZ) {
-        if (c < ncol) {
-          float2* out = a.T + gbase + c;
-#pragma unroll
-          for (int r = 0; r < kR1; ++r) out[(j + R2 * r) * rstride] = v[r];
+          for (int r = 0; r < kR1; ++r) v[r] = S[(R2 * r + n2) * kW + c];
         }
-      } else {
-        // Green's multiply at kz = j + R2 r, then the first inverse radix-8
-        // pass (ns = 1) into rows 8 j + r of the second buffer
+        Butterfly<kR1, false>::run(v, tw, N);
+#pragma unroll
+        for (int r = 1; r < kR1; ++r) v[r] = cmul(v[r], tw[r * n2]);
+#pragma unroll
+        for (int r = 0; r < kR1; ++r) Wt[(R2 * r + n2) * kW + c] = v[r];
+      }
+      __syncthreads();
+      {
+        const int k1 = jr;   // tid >> 4
+        float2 v[R2];
+#pragma unroll
+        for (int r = 0; r < R2; ++r) v[r] = Wt[(R2 * k1 + r) * kW + c];
+        Butterfly<R2, false>::run(v, tw, N);
         const float qxy = gxy[c];
 #pragma unroll
-        for (int r = 0; r < kR1; ++r) {
-          float q = qxy + kz[j + R2 * r];
+        for (int r = 0; r < R2; ++r) {
+          float q = qxy + kz[k1 + kR1 * r];
           q = a.g_scale * q - a.g_off;
           const float rden = rcp_approx(q * q + a.eps * a.eps) * a.inv_n;
           const float2 G = make_float2(q * rden, a.eps * rden);  // (1 / (q - i eps)) / N
           v[r] = cmul(G, v[r]);
         }
-        Butterfly<kR1, true>::run(v, tw, N);
+        Butterfly<R2, true>::run(v, tw, N);
 #pragma unroll
-        for (int r = 0; r < kR1; ++r) sB[(j * kR1 + r) * kW + c] = v[r];
+        for (int r = 1; r < R2; ++r) v[r] = cmul(v[r], cconj(tw[r * k1]));
+#pragma unroll
+        for (int r = 0; r < R2; ++r) Wt[(R2 * k1 + r) * kW + c] = v[r];
       }
-    }
-    if (kZ) {
       __syncthreads();
-      // ---- inverse radix-R2 pass (ns = 8): rows jr + 8 r, twiddles conj(tw[r jr])
-      float2 v[R2];
+      for (int idx = tid; idx < kW * R2; idx += kThreads) {
+        const int n2 = idx >> 4;
+        float2 v[kR1];
 #pragma unroll
-      for (int r = 0; r < R2; ++r) v[r] = sB[(jr + kR1 * r) * kW + c];
+        for (int r = 0; r < kR1; ++r) v[r] = Wt[(R2 * r + n2) * kW + c];
+        Butterfly<kR1, true>::run(v, tw, N);
+        if constexpr (k16) {   // lanes 8j .. 8j+7 hold columns 8h .. 8h+7 of the same rows
+          const unsigned mask = __activemask();
+          short2* out = a.T16 + gbase + c;
 #pragma unroll
-      for (int r = 1; r < R2; ++r) {
-        float2 w = tw[r * jr];
-        w.y = -w.y;
-        v[r] = cmul(v[r], w);
+          for (int r = 0; r < kR1; ++r) {
+            const int ex = b16_group_exponent(v[r], mask);
+            const long long off = (long long)(R2 * r + n2) * rstride;
+            if (c < ncol) {
+              out[off] = b16_encode(v[r], ex);
+              if ((c & 7) == 0) a.Te[(gbase + c + off) >> 3] = (signed char)ex;
+            }
+          }
+        } else if (c < ncol) {
+          float2* out = a.T + gbase + c;
+#pragma unroll
+          for (int r = 0; r < kR1; ++r) out[(R2 * r + n2) * rstride] = v[r];
+        }
       }
-      Butterfly<R2, true>::run(v, tw, N);
-      if (c < ncol) {
-        float2* out = a.T + gbase + c;
-#pragma unroll
-        for (int r = 0; r < R2; ++r) out[(jr + kR1 * r) * rstride] = v[r];
-      }
+      // the next iteration's copy refills the stage just read
+      __syncthreads();
     } else {
-      // the next iteration's copy refills the stage just read; the z-pass
-      // reads its stage only before the barrier above, and its next writes
-      // to sB follow the barriers of the next radix-R2 pass
+      // ---- radix-R2 pass (ns = 1), in place: rows jr + 8r -> rows jr*R2 + r
+      {
+        float2 v[R2];
+#pragma unroll
+        for (int r = 0; r < R2; ++r) v[r] = S[(jr + kR1 * r) * kW + c];
+        Butterfly<R2, kInvFirst>::run(v, tw, N);
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < R2; ++r) S[(jr * R2 + r) * kW + c] = v[r];
+      }
+      __syncthreads();
+      // ---- radix-8 pass (ns = R2): rows j + R2 r, twiddles tw[r j], to global
+      for (int idx = tid; idx < kW * R2; idx += kThreads) {
+        const int j = idx >> 4;  // c is idx & 15 == tid & 15
+        float2 v[kR1];
+#pragma unroll
+        for (int r = 0; r < kR1; ++r) v[r] = S[(j + R2 * r) * kW + c];
+#pragma unroll
+        for (int r = 1; r < kR1; ++r) {
+          float2 w = tw[r * j];
+          if (kInvFirst) w.y = -w.y;
+          v[r] = cmul(v[r], w);
+        }
+        Butterfly<kR1, kInvFirst>::run(v, tw, N);
+        if (c < ncol) {
+          float2* out = a.T + gbase + c;
+#pragma unroll
+          for (int r = 0; r < kR1; ++r) out[(j + R2 * r) * rstride] = v[r];
+        }
+      }
+      // the next iteration's copy refills the stage just read
       __syncthreads();
     }
   }
@@ -258,8 +332,10 @@ PFN_cuTensorMapEncodeTiled_v12000 encoder() {
 }
 
 // T viewed as float32 pairs: dims (inner first) {2*px, py, pz*nb} (y-pass) or
-// {2*px, py, pz, nb} (z-pass); box 32 floats = 16 complex columns.
-bool make_map(const BornArgs& a, bool zpass, CUtensorMap* m) {
+// {2*px, py, pz, nb} (z-pass); box 32 floats = 16 complex columns.  With
+// 16-bit storage (b16) the map covers T16 viewed as 32-bit (re, im) int16
+// pairs: dims {px, py, pz, nb}, box 16 columns (64 bytes).
+bool make_map(const BornArgs& a, bool zpass, CUtensorMap* m, bool b16 = false) {
   auto enc = encoder();
   if (!enc) return false;
   const cuuint64_t px2 = 2ull * a.px;
@@ -267,7 +343,15 @@ bool make_map(const BornArgs& a, bool zpass, CUtensorMap* m) {
   const cuuint64_t planeb = rowb * a.py;
   const cuuint32_t estr[4] = {1, 1, 1, 1};
   CUresult r;
-  if (!zpass) {
+  if (b16) {
+    const cuuint64_t rowb16 = (cuuint64_t)a.px * sizeof(short2);
+    const cuuint64_t dims[4] = {(cuuint64_t)a.px, (cuuint64_t)a.py, (cuuint64_t)a.pz, (cuuint64_t)a.nbatch};
+    const cuuint64_t strides[3] = {rowb16, rowb16 * a.py, rowb16 * a.py * a.pz};
+    const cuuint32_t box[4] = {kW, 1, (cuuint32_t)a.pz, 1};
+    r = enc(m, CU_TENSOR_MAP_DATA_TYPE_INT32, 4, a.T16, dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  } else if (!zpass) {
     const cuuint64_t dims[3] = {px2, (cuuint64_t)a.py, (cuuint64_t)a.pz * a.nbatch};
     const cuuint64_t strides[2] = {rowb, planeb};
     const cuuint32_t box[3] = {2 * kW, (cuuint32_t)a.py, 1};
@@ -288,7 +372,7 @@ bool make_map(const BornArgs& a, bool zpass, CUtensorMap* m) {
 template <int R2, int KIND>
 cudaError_t launch_kind(const BornArgs& a, int jj, const DevFft& f, int* fault, cudaStream_t s) {
   using L = ColSmem<kR1 * R2>;
-  constexpr size_t smem = KIND == 2 ? L::kTotalZ : L::kTotalY;
+  constexpr size_t smem = KIND == 3 ? L::kTotalZ16 : KIND == 2 ? L::kTotalZ : L::kTotalY;
   static DeviceFlags configured;   // attribute raised once per device
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -300,14 +384,19 @@ cudaError_t launch_kind(const BornArgs& a, int jj, const DevFft& f, int* fault, 
     configured.set(dev);
   }
   CUtensorMap map;
-  if (!make_map(a, KIND == 2, &map)) return cudaErrorInvalidValue;
+  if (!make_map(a, KIND >= 2, &map, KIND == 3)) return cudaErrorInvalidValue;
   int nsm = 0;
   e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
   const int nxt = (a.px + kW - 1) / kW;
-  const long long nout = KIND == 2 ? (long long)a.py * a.nbatch : (long long)a.pz * a.nbatch;
+  const long long nout = KIND >= 2 ? (long long)a.py * a.nbatch : (long long)a.pz * a.nbatch;
   const long long ntiles = nout * nxt;
-  const int grid = (int)(ntiles < 3LL * nsm ? ntiles : 3LL * nsm);
+  int per_sm = 0;   // resident CTAs per SM (shared memory and registers allowing)
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cols_pipe_kernel<R2, KIND>, kThreads, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  const long long cap = (long long)per_sm * nsm;
+  const int grid = (int)(ntiles < cap ? ntiles : cap);
   cols_pipe_kernel<R2, KIND><<<grid, kThreads, smem, s>>>(map, a, jj, f.tw, nxt, (int)ntiles, fault);
   return cudaGetLastError();
 }
@@ -316,6 +405,9 @@ template <int KIND>
 cudaError_t dispatch(const BornArgs& a, int jj, const DevFft& f, int* fault, cudaStream_t s) {
   switch (f.plan.n / kR1) {
     case 11: return launch_kind<11, KIND>(a, jj, f, fault, s);
+    case 12:   // z-pass only (96 = 8 x 12, the fused passes' even length)
+      if constexpr (KIND >= 2) return launch_kind<12, KIND>(a, jj, f, fault, s);
+      return cudaErrorNotSupported;
     case 15: return launch_kind<15, KIND>(a, jj, f, fault, s);
     case 19: return launch_kind<19, KIND>(a, jj, f, fault, s);
     case 25: return launch_kind<25, KIND>(a, jj, f, fault, s);
@@ -330,7 +422,7 @@ bool cols_pipe_supported(const BornArgs& a, const DevFft& f, bool zpass) {
   const int n = f.plan.n;
   if (n != (zpass ? a.pz : a.py) || n % kR1 != 0) return false;
   const int r2 = n / kR1;
-  if (r2 != 11 && r2 != 15 && r2 != 19 && r2 != 25 && r2 != 27) return false;
+  if (r2 != 11 && r2 != 15 && r2 != 19 && r2 != 25 && r2 != 27 && !(zpass && r2 == 12)) return false;
   if (a.px % 2 != 0 || !encoder()) return false;   // row strides must be multiples of 16 bytes
   const long long nout = zpass ? (long long)a.py * a.nbatch : (long long)a.pz * a.nbatch;
   return nout * ((a.px + kW - 1) / kW) < (1LL << 31);
@@ -342,6 +434,10 @@ cudaError_t launch_fft_y_pipe(const BornArgs& a, bool inverse, const DevFft& fy,
 }
 
 cudaError_t launch_born_z_pipe(const BornArgs& a, int jj, const DevFft& fz, int* fault, cudaStream_t s) {
+  if (a.storage) {
+    if (a.px % 8 != 0) return cudaErrorInvalidValue;   // 8-column exponent blocks, 16-byte rows
+    return dispatch<3>(a, jj, fz, fault, s);
+  }
   return dispatch<2>(a, jj, fz, fault, s);
 }
 

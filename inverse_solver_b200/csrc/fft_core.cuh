@@ -106,6 +106,45 @@ struct Butterfly<8, INV> {
   }
 };
 
+// R = 12 = 4 x 3 in registers (for the fused passes on lengths 96 = 8 x 12):
+// n = 3 n1 + n2, k = k1 + 4 k2; 4-point DFTs over n1, twiddles W_12^(n2 k1)
+// from the length-n table, 3-point DFTs over n2.
+template <bool INV>
+struct Butterfly<12, INV> {
+  ODT_HD static void run(float2* v, const float2* tw, int n) {
+    const int step = n / 12;
+    float2 t[3][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 3; ++n2) {
+      float2 q[4] = {v[n2], v[3 + n2], v[6 + n2], v[9 + n2]};
+      Butterfly<4, INV>::run(q, nullptr, 0);
+#pragma unroll
+      for (int k1 = 0; k1 < 4; ++k1) {
+        if (n2 * k1 == 0) {
+          t[n2][k1] = q[k1];
+        } else {
+          float2 w = tw[n2 * k1 * step];
+          if (INV) w.y = -w.y;
+          t[n2][k1] = cmul(q[k1], w);
+        }
+      }
+    }
+    // 3-point DFT: c = cos(2 pi / 3) = -1/2, s = sin(2 pi / 3)
+    const float s3 = 0.86602540378443864676f;
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+      const float2 a0 = t[0][k1], a1 = t[1][k1], a2 = t[2][k1];
+      const float2 sum = cadd(a1, a2), dif = csub(a1, a2);
+      const float2 m = make_float2(a0.x - 0.5f * sum.x, a0.y - 0.5f * sum.y);
+      // forward: X1 = m - i s dif, X2 = m + i s dif
+      const float2 j = make_float2(-s3 * dif.y, s3 * dif.x);   // i s dif
+      v[k1] = cadd(a0, sum);
+      v[k1 + 4] = INV ? cadd(m, j) : csub(m, j);
+      v[k1 + 8] = INV ? csub(m, j) : cadd(m, j);
+    }
+  }
+};
+
 // Odd R: X[k] = v0 + sum_m a_m cos(2 pi m k / R) -/+ i sum_m b_m sin(2 pi m k / R)
 // with a_m = v[m] + v[R-m], b_m = v[m] - v[R-m]; the cosines and sines are
 // read from the transform's table at multiples of n / R.

@@ -13,6 +13,7 @@
 #include "../../include/odt.h"
 #include "cbs_kernels.cuh"
 #include "fft_plan.h"
+#include "tma.cuh"
 
 namespace odt {
 const char* set_last_error(const std::string& msg);  // odt_api.cu
@@ -31,9 +32,15 @@ static __device__ __align__(256) float2 g_noalloc_scratch[kNoallocElems];
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 float2* g_noalloc_ptr[kMaxDevices] = {nullptr};
+// padded grid whose twiddle tables the scratch array holds on each device
+// (they sit right after T | Field_n | Field, so a call on another grid size
+// overwrites or moves them; a call on the same size finds them in place)
+int g_noalloc_tw[kMaxDevices][3] = {};
 
 // Device address of the scratch array on the current device; looked up once
-// per device (the first call on a device does this).
+// per device (the first call on a device does this).  The address is not
+// looked up again, so the entry point must not be called on a device after
+// cudaDeviceReset has run on it.
 cudaError_t noalloc_scratch(float2** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -65,8 +72,10 @@ extern "C" odt_status odt_born_series_noalloc(const odt_noalloc_born_args* a) {
     const int lo = a->roi[2 * i], hi = a->roi[2 * i + 1];
     if (lo < 1 || hi > a->sim_size[i] || hi < lo)
       return fail(ODT_ERR_INVALID_ARGUMENT, "odt_born_series_noalloc: ROI outside sim_size");
-    if (!a->mask[i] || !a->kq2[i] || (a->acyclic && !a->ramp[i]))
-      return fail(ODT_ERR_INVALID_ARGUMENT, "odt_born_series_noalloc: NULL table");
+    if (!a->mask[i] || !a->kq2[i] || !a->ramp[i])
+      return fail(ODT_ERR_INVALID_ARGUMENT,
+                  "odt_born_series_noalloc: NULL table (mask, ramp and kq2 are all required; "
+                  "pass ones as the ramp when acyclic = 0)");
   }
   if (!a->V || !a->einc || !a->fout)
     return fail(ODT_ERR_INVALID_ARGUMENT, "odt_born_series_noalloc: NULL V / einc / fout");
@@ -80,12 +89,6 @@ extern "C" odt_status odt_born_series_noalloc(const odt_noalloc_born_args* a) {
                     " voxels needs " + std::to_string(need * 8) + " bytes of scratch, more than the " +
                     std::to_string(kNoallocBytes) + "-byte fixed array (at most " +
                     std::to_string((kNoallocElems - 3 * 1024) / 3) + " voxels)");
-  if (!a->acyclic) {
-    for (int i = 0; i < 3; ++i)
-      if (!a->ramp[i])
-        return fail(ODT_ERR_INVALID_ARGUMENT,
-                    "odt_born_series_noalloc: ramp tables are required (pass ones when acyclic = 0)");
-  }
   float2* scratch = nullptr;
   cudaError_t e = noalloc_scratch(&scratch);
   if (e != cudaSuccess) {
@@ -105,22 +108,32 @@ extern "C" odt_status odt_born_series_noalloc(const odt_noalloc_born_args* a) {
   for (int i = 0; i < 3; ++i) {
     const int n = a->sim_size[i];
     std::string why;
-    if (!make_plan(n, &f[i].plan, &why, i == 0 ? kSmallFirst : kLargeFirst) || f[i].plan.rclass > 2)
+    if (!make_plan(n, &f[i].plan, &why, i == 0 ? kSmallFirst : kLargeFirst))
       return fail(ODT_ERR_UNSUPPORTED, "odt_born_series_noalloc: sim_size(" + std::to_string(i + 1) +
-                                           ") = " + std::to_string(n) + " has an unsupported prime factor");
+                                           ") = " + std::to_string(n) + ": " + why);
     f[i].lgW = n <= 512 ? 4 : 3;
     f[i].W = 1 << f[i].lgW;
     f[i].nthr = 128;
     if (fft_smem_bytes(n, f[i].W, kinds[i]) > (size_t)max_smem)
       return fail(ODT_ERR_UNSUPPORTED, "odt_born_series_noalloc: length too large for shared memory");
   }
-  // The twiddle tables are copied from pageable host memory, which makes the
-  // copies synchronous with the host; that is fine for a call that is
-  // synchronous anyway (see below).
+  // The twiddle tables are uploaded (from pageable host memory, so the copies
+  // are synchronous with the host) only when this device's scratch does not
+  // already hold them: the first call, and the first call after a call on
+  // another grid size.
+  bool have_tw;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    have_tw = std::memcmp(g_noalloc_tw[dev], a->sim_size, sizeof(g_noalloc_tw[dev])) == 0;
+    if (!have_tw) std::memset(g_noalloc_tw[dev], 0, sizeof(g_noalloc_tw[dev]));
+  }
   for (int i = 0; i < 3; ++i) {
-    const std::vector<float2> tw = make_twiddles(a->sim_size[i]);
-    e = cudaMemcpyAsync(twbase, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) return fail(ODT_ERR_CUDA, std::string("odt_born_series_noalloc: ") + cudaGetErrorString(e));
+    if (!have_tw) {
+      const std::vector<float2> tw = make_twiddles(a->sim_size[i]);
+      e = cudaMemcpyAsync(twbase, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess)
+        return fail(ODT_ERR_CUDA, std::string("odt_born_series_noalloc: ") + cudaGetErrorString(e));
+    }
     f[i].tw = twbase;
     twbase += a->sim_size[i];
   }
@@ -153,6 +166,7 @@ extern "C" odt_status odt_born_series_noalloc(const odt_noalloc_born_args* a) {
   b.V = reinterpret_cast<const float2*>(a->V);
   b.Einc = reinterpret_cast<const float2*>(a->einc);
   b.Fout = reinterpret_cast<float2*>(a->fout);
+  b.wait_limit = kWaitLimitCycles;
   const int B = a->bornmax;
   for (int jj = 1; jj <= B && e == cudaSuccess; ++jj) {
     if ((e = launch_born_x(b, jj == 1 ? kBornFirst : kBornMid, jj, f[0], s)) != cudaSuccess) break;
@@ -165,6 +179,10 @@ extern "C" odt_status odt_born_series_noalloc(const odt_noalloc_born_args* a) {
   if (e != cudaSuccess) {
     cudaGetLastError();
     return fail(ODT_ERR_CUDA, std::string("odt_born_series_noalloc: ") + cudaGetErrorString(e));
+  }
+  if (!have_tw) {  // the tables are in place from now on
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    std::memcpy(g_noalloc_tw[dev], a->sim_size, sizeof(g_noalloc_tw[dev]));
   }
   odt::set_last_error("");
   return ODT_OK;

@@ -26,6 +26,7 @@
 #include "../../include/odt.h"
 #include "cbs_kernels.cuh"
 #include "fft_plan.h"
+#include "tma.cuh"
 
 namespace odt {
 
@@ -84,11 +85,14 @@ struct DeviceGuard {
 };
 
 const char* const kKindNames[] = {"born_x", "born_y", "born_z", "io_fft", "io_elementwise",
-                                  "born_x_pipe", "born_y_pipe", "born_z_pipe", "born_x_pipe_edge"};
+                                  "born_x_pipe", "born_y_pipe", "born_z_pipe", "born_x_pipe_edge",
+                                  "born_xy", "born_xy_edge"};
 // born_x_pipe_edge: the pipelined x-pass of iterations 2, 3 and of the final
-// pass (incident-field source / output), timed apart from the steady state
+// pass (incident-field source / output), timed apart from the steady state;
+// born_xy / born_xy_edge: the fused xy-pass, steady (iterations 4..Bornmax)
+// and edge (iterations 1-3 and the final pass)
 enum Kind { kKBornX = 0, kKBornY, kKBornZ, kKIoFft, kKIoElem, kKBornXPipe, kKBornYPipe, kKBornZPipe,
-            kKBornXPipeEdge, kNumKinds };
+            kKBornXPipeEdge, kKBornXY, kKBornXYEdge, kNumKinds };
 
 struct Handle {
   odt_geometry g{};
@@ -154,6 +158,15 @@ struct Handle {
   // kernel selection: the pipelined x-pass where it applies (ODT_KERNELS=generic
   // in the environment at odt_create selects the generic tile kernels)
   bool use_pipe = true;
+  // clock cycles a pipelined kernel's steady mbarrier wait may take before it
+  // reports a timeout (ODT_WAIT_LIMIT_CYCLES in the environment at odt_create;
+  // default about a second)
+  long long wait_limit = kWaitLimitCycles;
+  // the fused xy-pass where it applies (ODT_XY=0 in the environment at
+  // odt_create keeps the separate x- and y-passes)
+  bool use_xy = true;
+  // storage of T and Field_n in the Born loop (ODT_STORAGE_*)
+  int storage = ODT_STORAGE_COMPLEX64;
 
   // CUDA graphs of a batch's whole solve (run_chunk), keyed by batch size,
   // outputs and potential slot; captured the second time a key is seen (the
@@ -468,6 +481,7 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
   a.V = P.V;
   a.Einc = H.einc;
   a.Fout = fout;
+  a.wait_limit = H.wait_limit;
   const int B = P.pp.bornmax;
   const bool pipe_x = !ten && H.use_pipe && born_x_pipe_supported(a, H.fx);
   const bool pipe_y = H.use_pipe && cols_pipe_supported(a, H.fy, false);
@@ -478,7 +492,46 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
     dy.absorb = make_float2(P.pp.absorb.re, P.pp.absorb.im);
   }
   const long long xlines = (long long)a.py * a.pz * nbp;
-  for (int jj = 1; jj <= B; ++jj) {
+  // fused xy-pass (x- and both y-passes in one kernel; the z-pass, pipelined
+  // or generic, reads its permuted x-y spectrum): scalar potentials
+  const bool fused_xy = !ten && !vec && H.use_pipe && H.use_xy && B >= 1 && born_xy_supported(a, H.max_smem);
+  a.perm_xy = fused_xy ? 1 : 0;
+  if (H.storage == ODT_STORAGE_B16) {
+    if (!fused_xy || !pipe_z)
+      raise(ODT_ERR_UNSUPPORTED,
+            "16-bit block storage (ODT_STORAGE_B16) needs the fused xy-pass: a scalar potential on a grid "
+            "with equal x and y lengths of 88, 96, 120 or 152 and a z length of 8 * {11, 12, 15, 19, 25, 27}");
+    // T16 | Field_n16 | Field | exponents of T | exponents of Field_n in the
+    // work block (16.25 of its 24 bytes per voxel)
+    const size_t n = (size_t)a.nvox * (size_t)nbp;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    char* w = reinterpret_cast<char*>(H.work);
+    a.storage = 1;
+    a.T16 = reinterpret_cast<short2*>(w);
+    a.Fn16 = reinterpret_cast<short2*>(w + al(4 * n));
+    a.F = reinterpret_cast<float2*>(w + 2 * al(4 * n));
+    a.Te = reinterpret_cast<signed char*>(w + 2 * al(4 * n) + al(8 * n));
+    a.Fe = a.Te + al(n / 8);
+    a.T = nullptr;
+    a.Fn = nullptr;
+  }
+  for (int jj = 1; fused_xy && jj <= B; ++jj) {
+    H.mark_begin(jj <= 3 ? kKBornXYEdge : kKBornXY, s);
+    ODT_CUDA(launch_born_xy(a, jj == 1 ? kBornFirst : kBornMid, jj, H.fx, s));
+    H.mark_end(s);
+    H.mark_begin(pipe_z ? kKBornZPipe : kKBornZ, s);
+    if (pipe_z)
+      ODT_CUDA(launch_born_z_pipe(a, jj, H.fz, H.d_fault, s));
+    else
+      ODT_CUDA(launch_born_z(a, jj, H.fz, s));
+    H.mark_end(s);
+  }
+  if (fused_xy) {
+    H.mark_begin(kKBornXYEdge, s);
+    ODT_CUDA(launch_born_xy(a, kBornLast, B + 1, H.fx, s));
+    H.mark_end(s);
+  }
+  for (int jj = 1; !fused_xy && jj <= B; ++jj) {
     if (ten) {  // plain x-FFTs around the component-coupling pointwise kernel
       H.mark_begin(kKBornX, s);
       if (jj >= 2) ODT_CUDA(launch_fft_lines(a.T, a.T, xlines, 0, 0, 1.0f, true, H.fx, s));
@@ -513,18 +566,20 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
       ODT_CUDA(launch_fft_cols(a.T, a.T, a.px, (long long)a.pz * nbp, 0, 0, 1.0f, true, H.fy, s));
     H.mark_end(s);
   }
-  if (ten) {
-    H.mark_begin(kKBornX, s);
-    if (B >= 1) ODT_CUDA(launch_fft_lines(a.T, a.T, xlines, 0, 0, 1.0f, true, H.fx, s));
-    ODT_CUDA(launch_born_tensor_point(a, P.V9, kBornLast, B + 1, s));
-  } else if (pipe_x && B + 1 >= 2) {
-    H.mark_begin(kKBornXPipeEdge, s);
-    ODT_CUDA(launch_born_x_pipe(a, kBornLast, B + 1, H.fx, H.d_fault, s));
-  } else {
-    H.mark_begin(kKBornX, s);
-    ODT_CUDA(launch_born_x(a, kBornLast, B + 1, H.fx, s));
+  if (!fused_xy) {
+    if (ten) {
+      H.mark_begin(kKBornX, s);
+      if (B >= 1) ODT_CUDA(launch_fft_lines(a.T, a.T, xlines, 0, 0, 1.0f, true, H.fx, s));
+      ODT_CUDA(launch_born_tensor_point(a, P.V9, kBornLast, B + 1, s));
+    } else if (pipe_x && B + 1 >= 2) {
+      H.mark_begin(kKBornXPipeEdge, s);
+      ODT_CUDA(launch_born_x_pipe(a, kBornLast, B + 1, H.fx, H.d_fault, s));
+    } else {
+      H.mark_begin(kKBornX, s);
+      ODT_CUDA(launch_born_x(a, kBornLast, B + 1, H.fx, s));
+    }
+    H.mark_end(s);
   }
-  H.mark_end(s);
 
   // ---- output projection (:445-511)
   if (want_t || want_r) {
@@ -746,6 +801,15 @@ odt_status odt_create(const odt_geometry* geom, const odt_cfloat* refocus,
     ODT_CUDA(cudaDeviceGetAttribute(&H->max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, g.device));
     if (const char* k = std::getenv("ODT_KERNELS")) H->use_pipe = std::string(k) != "generic";
     if (const char* k = std::getenv("ODT_GRAPHS")) H->use_graphs = std::string(k) != "0";
+    if (const char* k = std::getenv("ODT_XY")) H->use_xy = std::string(k) != "0";
+    if (const char* k = std::getenv("ODT_WAIT_LIMIT_CYCLES")) {
+      char* end = nullptr;
+      const long long v = std::strtoll(k, &end, 10);
+      if (end == k || *end != '\0' || v < 0)
+        raise(ODT_ERR_INVALID_ARGUMENT, std::string("ODT_WAIT_LIMIT_CYCLES must be a non-negative integer, got '") +
+                                            k + "'");
+      H->wait_limit = v;
+    }
     ODT_CUDA(cudaStreamCreateWithFlags(&H->own_stream, cudaStreamNonBlocking));
     H->fx = make_dev_fft(*H, g.sim_size[0], kKindBornX, "sim_size(1)");
     H->fy = make_dev_fft(*H, g.sim_size[1], kKindCols, "sim_size(2)");
@@ -1223,6 +1287,20 @@ odt_status odt_get_batch(odt_handle h, int32_t* batch) {
     auto H = lookup(h);
     if (!batch) raise(ODT_ERR_INVALID_ARGUMENT, "odt_get_batch: NULL");
     *batch = H->batch;
+  });
+}
+
+odt_status odt_set_field_storage(odt_handle h, int32_t storage) {
+  return guarded([&] {
+    auto H = lookup(h);
+    if (storage != ODT_STORAGE_COMPLEX64 && storage != ODT_STORAGE_B16)
+      raise(ODT_ERR_INVALID_ARGUMENT, "odt_set_field_storage: storage must be ODT_STORAGE_COMPLEX64 (0) "
+                                      "or ODT_STORAGE_B16 (1), got " + std::to_string(storage));
+    if (H->storage != storage) {
+      DeviceGuard dg(H->g.device);
+      H->drop_graphs();   // captured launches carry the storage layout
+      H->storage = storage;
+    }
   });
 }
 

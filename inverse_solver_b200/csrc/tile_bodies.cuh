@@ -271,7 +271,12 @@ ODT_HD void born_z_body(const BornArgs& a, int jj, const FftPlan& plan, const fl
   const bool flip = a.acyclic && (jj & 1);
   for (int c = th.tid; c < W; c += th.nthr) {
     const long long i0 = lmin(i00 + c, n0 - 1);
-    const int kx = (int)(i0 % a.px), ky = (int)(i0 / a.px);
+    int kx = (int)(i0 % a.px), ky = (int)(i0 / a.px);
+    if (a.perm_xy) {   // fused xy-pass order: position R k1 + k2 holds index k1 + 8 k2
+      const int rx = a.px >> 3, ry = a.py >> 3;
+      kx = kx / rx + 8 * (kx % rx);
+      ky = ky / ry + 8 * (ky % ry);
+    }
     const int ix = flip ? wrap_neg(kx, a.px) : kx;
     const int iy = flip ? wrap_neg(ky, a.py) : ky;
     gxy[c] = a.kq2[0][ix] + a.kq2[1][iy];

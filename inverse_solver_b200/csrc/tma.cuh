@@ -14,6 +14,13 @@
 
 namespace odt {
 
+// Default bound of every mbarrier wait: 2^31 clock cycles (about a second).
+// The steady waits of the pipelined Born kernels take the handle's limit
+// instead (ODT_WAIT_LIMIT_CYCLES at odt_create); the waits that drain a
+// CTA's copies in flight before it gives up always keep this one, so no bulk
+// copy is still writing shared memory when the CTA exits.
+constexpr long long kWaitLimitCycles = 1LL << 31;
+
 #if defined(__CUDA_ARCH__)
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -62,12 +69,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for phase `parity` of `bar`; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait for phase `parity` of `bar`; false once `limit` clock cycles
+// have passed without the phase completing.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit = kWaitLimitCycles) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - t0 > (1LL << 31)) return false;
+    if (clock64() - t0 > limit) return false;
   }
   return true;
 }

@@ -40,14 +40,17 @@ class CBSHostSetup:
     def get_default_parameters(init_params=None):
         """FORWARD_SOLVER.m:9-20 + FORWARD_SOLVER_CONVERGENT_BORN.m:32-45, plus
         the CUDA class's ``used_gpu`` (device ordinal) and this library's
-        ``max_batch`` (illuminations resident per launch, 0 = automatic) and
-        ``mem_budget`` (bytes, 0 = half of free HBM)."""
+        ``max_batch`` (illuminations resident per launch, 0 = automatic),
+        ``mem_budget`` (bytes, 0 = half of free HBM) and ``field_storage``
+        ("complex64", the reference's precision, or "b16": the Born loop's
+        spectral array and Field_n in 16-bit block floating point, see
+        odt_set_field_storage)."""
         p = basic_optical_parameter()
         p.update(return_transmission=True, return_reflection=False, return_3D=False,
                  use_GPU=True)
         p.update(iterations_number=-1, boundary_thickness=[6, 6, 6], boundary_sharpness=1,
                  verbose=False, acyclic=True, RI_xy_size=[0, 0], RI_center=[0, 0])
-        p.update(used_gpu=0, max_batch=0, mem_budget=0)
+        p.update(used_gpu=0, max_batch=0, mem_budget=0, field_storage="complex64")
         return update_struct(p, init_params) if init_params else p
 
     # ------------------------------------------------------------ ctor
@@ -337,6 +340,7 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
         _lib.check(self.lib.odt_create(C.byref(g), *[_lib.ptr(a) for a in self._keep], C.byref(h)))
         self._handle = h.value
         self._keep = None
+        self.set_field_storage(p.get("field_storage", "complex64"))
         if self.vector:
             rad, perp, tan, km = self.polarisation
             keep = [_f32(rad), _f32(perp), _f32(tan), np.asfortranarray(km.astype(np.uint8))]
@@ -600,6 +604,16 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
         b = C.c_int32(0)
         _lib.check(self.lib.odt_get_batch(self._handle, C.byref(b)))
         return b.value
+
+    def set_field_storage(self, storage):
+        """Storage of the Born loop's spectral array and Field_n: "complex64"
+        (default) or "b16" (16-bit block floating point, odt_set_field_storage;
+        square x-y grids of 88, 120 or 152 with a scalar potential)."""
+        modes = {"complex64": _lib.ODT_STORAGE_COMPLEX64, "b16": _lib.ODT_STORAGE_B16}
+        if storage not in modes:
+            raise ValueError('field_storage must be "complex64" or "b16", got %r' % (storage,))
+        _lib.check(self.lib.odt_set_field_storage(self._handle, modes[storage]))
+        self.parameters["field_storage"] = storage
 
     def set_profiling(self, on: bool):
         _lib.check(self.lib.odt_set_profiling(self._handle, 1 if on else 0))

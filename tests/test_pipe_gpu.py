@@ -27,9 +27,14 @@ def worst(a, b):
 
 
 def _solve(p, RI, fields, kernels=None):
+    """Solve with ODT_KERNELS=kernels; the fused xy-pass is off (ODT_XY=0) so
+    that these tests exercise the separate pipelined x-, y- and z-passes
+    (tests/test_xy_gpu.py covers the fused pass)."""
     from inverse_solver_b200 import FORWARD_SOLVER_CONVERGENT_BORN
 
     old = os.environ.get("ODT_KERNELS")
+    old_xy = os.environ.get("ODT_XY")
+    os.environ["ODT_XY"] = "0"
     if kernels:
         os.environ["ODT_KERNELS"] = kernels
     try:
@@ -43,6 +48,10 @@ def _solve(p, RI, fields, kernels=None):
             os.environ.pop("ODT_KERNELS", None)
         else:
             os.environ["ODT_KERNELS"] = old
+        if old_xy is None:
+            os.environ.pop("ODT_XY", None)
+        else:
+            os.environ["ODT_XY"] = old_xy
     return out, info
 
 

@@ -20,13 +20,26 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-5
 
 
-def test_noalloc_born_series_matches_solve_on_two_calls():
+def _small_case():
+    p = cases.small_params(return_transmission=False, return_3D=True)
+    return p, cases.small_RI()
+
+
+def _large_radix_case():
+    """Padded grid 46 x 48 x 29 (radices 23 and 29)."""
+    size = [22, 24, 5]
+    p = cases.params(size, [6, 6, 6], return_transmission=False, return_3D=True)
+    RI = cases.sphere_phantom(size, [0.1] * 3, cases.NM, seed=sum(size), n_spheres=2, radius_um=(0.1, 0.2))
+    return p, RI
+
+
+@pytest.mark.parametrize("make_case", [_small_case, _large_radix_case], ids=["small", "radix23_29"])
+def test_noalloc_born_series_matches_solve_on_two_calls(make_case):
     import torch
 
     from inverse_solver_b200 import FORWARD_SOLVER_CONVERGENT_BORN, _lib
 
-    p = cases.small_params(return_transmission=False, return_3D=True)
-    RI = cases.small_RI()
+    p, RI = make_case()
     fields = cases.circle_fields(p, 2)
     s = FORWARD_SOLVER_CONVERGENT_BORN(p)
     s.set_RI(RI)
