@@ -321,6 +321,36 @@ typedef struct odt_green_args {
 odt_status odt_green_planes(const odt_green_args* args);
 
 /*
+ * The cropped discrete Hankel transform pair of truncated_green_plus
+ * (sub_code/truncated_green_plus.m:33-66 with
+ * hankel_transform/discrete_hankel_croped_fourier.m:19-47, order 0, unit
+ * radius) applied to a radial profile, on the GPU: with c_0 .. c_{n-1} the
+ * first n positive zeros of J_0 and C the (n+1)-th (single precision, as the
+ * reference rounds them), I_j = |J_1(c_j)|, the transform matrix
+ *   F[i, j] = (s_i s_j) J_0((c_i / C) c_j),  s = sqrt(2 / C) / I,  i < pos,
+ * is built on the device (the reference's besselj matrices, one
+ * single-precision product per element as the reference forms them), and
+ *   out = Rv .* (F^T ((band .* ((F (values ./ Rv)) .* K)) ./ K)),
+ *   K = 2 pi I / C,  Rv = I,
+ * the forward transform, the band-limiting window and the inverse transform
+ * (:45-53), with double-precision accumulation of the two products.
+ * values / out: [n, nz] complex (column-major), band: [pos]; roots: the
+ * n + 1 zeros (double, host).  All arrays are host memory; synchronous.
+ */
+typedef struct odt_hankel_args {
+  const double* roots;        /* [n + 1] positive zeros of J_0                 */
+  int32_t n;                  /* samples                                       */
+  int32_t pos;                /* rows of the low-k band kept (<= n)            */
+  int32_t nz;                 /* profile columns                               */
+  const odt_cfloat* values;   /* [n, nz]                                       */
+  const float* band;          /* [pos]                                         */
+  odt_cfloat* out;            /* [n, nz]                                       */
+  int32_t device;             /* CUDA device (-1: the current one)             */
+} odt_hankel_args;
+
+odt_status odt_hankel_filter(const odt_hankel_args* args);
+
+/*
  * Field retrieval from off-axis holograms, the transform part of get_fields
  * (FIELD_EXPERIMENTAL_RETRIEVAL.m:110-178): centred 2D FFT of each background
  * and sample hologram; the sideband = the first maximum of |F_bg(:,:,1)|

@@ -252,6 +252,19 @@ class GreenArgs(C.Structure):
     ]
 
 
+class HankelArgs(C.Structure):
+    _fields_ = [
+        ("roots", C.c_void_p),
+        ("n", C.c_int32),
+        ("pos", C.c_int32),
+        ("nz", C.c_int32),
+        ("values", C.c_void_p),
+        ("band", C.c_void_p),
+        ("out", C.c_void_p),
+        ("device", C.c_int32),
+    ]
+
+
 class BPMArgs(C.Structure):
     _fields_ = [
         ("size", C.c_int32 * 3),
@@ -349,6 +362,7 @@ SIGNATURES = {
     "odt_get_batch": (C.c_int, [C.c_uint32, C.POINTER(C.c_int32)]),
     "odt_set_profiling": (C.c_int, [C.c_uint32, C.c_int32]),
     "odt_set_field_storage": (C.c_int, [C.c_uint32, C.c_int32]),
+    "odt_hankel_filter": (C.c_int, [C.POINTER(HankelArgs)]),
     "odt_get_kernel_times": (C.c_int, [C.c_uint32, C.POINTER(C.c_char_p),
                                        C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                        C.c_int32, C.POINTER(C.c_int32)]),

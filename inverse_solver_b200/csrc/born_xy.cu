@@ -26,7 +26,7 @@
 // Space-domain data is in natural order, so the pointwise work reads and
 // writes Field_n / Field / V / the incident field in their global layout.
 //
-// Seven steps per plane separated by CTA barriers:
+// Seven steps per plane:
 //   1 y-F3^-1 + F2^-1  read T from global (one R-point column group per item)
 //   2 y-F1^-1          shared memory
 //   3 x-F3^-1 + F2^-1  shared memory
@@ -36,8 +36,13 @@
 //   6 y-F1             shared memory
 //   7 y-F2 + F3        write T to global
 // One CTA per SM (the plane takes 8 N^2 bytes: 185 KB for N = 152) with 32 R
-// threads, persistent over the planes (illumination fastest, so concurrent
-// CTAs share V's planes in L2).  The next plane's T and Field_n / Field are
+// threads -- R warps -- persistent over the planes (illumination fastest, so
+// concurrent CTAs share V's planes in L2).  Steps 2-6 touch, for one n2, only
+// the 8 rows R n1 + n2 (step 2 and 6 combine exactly those rows, steps 3-5
+// work along rows), so warp w takes n2 = w and runs steps 2-6 on its own rows
+// with warp-level synchronisation only: a plane needs three CTA barriers
+// (after steps 1 and 6, and after step 7), and the warps drift apart so that
+// one warp's global loads in step 4 overlap other warps' transforms.  The next plane's T and Field_n / Field are
 // prefetched into L2 (cp.async.bulk.prefetch) during steps 4 and 6 of the
 // current one, so their DRAM reads overlap the shared-memory steps.
 //
@@ -83,9 +88,9 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
 #endif
 
 // ST: storage of T and Field_n, 0 = complex64, 1 = 16-bit block floating
-// point (b16.cuh; T's blocks are 8 consecutive x of a row, Field_n's are 8
-// consecutive step-4 work items of one n1, exponent index
-// plane * N^2/8 + n1 * R^2 + item / 8)
+// point (b16.cuh; T's blocks are 8 consecutive x of a row, Field_n's are the
+// values of one n1 in 8 consecutive step-4 work items of a warp, exponent
+// index plane * N^2/8 + n1 * R^2 + w * R + item / 8)
 template <int R, int KIND, int ST>
 __global__ void __launch_bounds__(32 * R, 1)
     born_xy_kernel(const BornArgs a, const int jj, const float2* __restrict__ twg, const int nplanes) {
@@ -101,6 +106,7 @@ __global__ void __launch_bounds__(32 * R, 1)
   float* myt = reinterpret_cast<float*>(sm + L::kMaskY);
   float2* pl = reinterpret_cast<float2*>(sm + L::kPlane);
   const int tid = threadIdx.x;
+  const int w = tid >> 5, lane = tid & 31;   // warp w owns the rows R n1 + w in steps 2-6
   const float2 one = make_float2(1.f, 0.f);
   const float2 z2 = make_float2(0.f, 0.f);
   for (int i = tid; i < N; i += NT) {
@@ -159,20 +165,19 @@ __global__ void __launch_bounds__(32 * R, 1)
         for (int r = 0; r < R; ++r) pl[(R * k1 + r) * N + x] = v[r];
       }
       __syncthreads();
-      // ---- 2: y-F1^-1 (8-point over k1 at rows R k1 + n2) -> natural y
-      for (int i = tid; i < R * N; i += NT) {
-        const int x = i % N, n2 = i / N;
+      // ---- 2: y-F1^-1 (8-point over k1 at rows R k1 + w) -> natural rows R n1 + w
+      for (int x = lane; x < N; x += 32) {
         float2 v[8];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = pl[(R * r + n2) * N + x];
+        for (int r = 0; r < 8; ++r) v[r] = pl[(R * r + w) * N + x];
         Butterfly<8, true>::run(v, tw, N);
 #pragma unroll
-        for (int r = 0; r < 8; ++r) pl[(R * r + n2) * N + x] = v[r];
+        for (int r = 0; r < 8; ++r) pl[(R * r + w) * N + x] = v[r];
       }
-      __syncthreads();
-      // ---- 3: x-F3^-1 + F2^-1 on the contiguous groups R k1 .. R k1 + R-1
-      for (int i = tid; i < 8 * N; i += NT) {
-        const int k1 = i & 7, y = i >> 3;
+      __syncwarp();
+      // ---- 3: x-F3^-1 + F2^-1 on the contiguous groups R k1 .. R k1 + R-1 of the warp's rows
+      for (int it = lane; it < 64; it += 32) {
+        const int k1 = it & 7, y = R * (it >> 3) + w;
         float2* row = pl + y * N + R * k1;
         float2 v[R];
 #pragma unroll
@@ -183,16 +188,20 @@ __global__ void __launch_bounds__(32 * R, 1)
 #pragma unroll
         for (int r = 0; r < R; ++r) row[r] = v[r];
       }
-      __syncthreads();
+      __syncwarp();
     }
     if (kInv && tid == 0 && gn >= 0) {
       if constexpr (ST == 0) prefetch_l2(a.T + gn, (uint32_t)(plane_n * sizeof(float2)));
       else prefetch_l2(a.T16 + gn, (uint32_t)(plane_n * sizeof(short2)));
     }
 
-    // ---- 4: x-F1^-1 -> update of iteration jj-1 and source of jj -> x-F1
-    for (int i = tid; i < R * N; i += NT) {
-      const int n2 = i % R, y = i / R;
+    // ---- 4: x-F1^-1 -> update of iteration jj-1 and source of jj -> x-F1, on
+    //      the warp's rows (item it: row R (it / R) + w, n2 = it % R)
+    for (int it = lane; it < 8 * R; it += 32) {
+      const int n2 = it % R, y = R * (it / R) + w;
+      // Field_n's exponent block of this item's n1 = r value: the 8 lanes of a
+      // group (8 consecutive it) share one; block w R + it / 8 of n1's R^2
+      const long long fe = (g0 >> 3) + w * R + (it >> 3);
       float2* row = pl + y * N;
       const long long gy = g0 + (long long)y * N;
       const long long vy = v0 + (long long)y * N;
@@ -209,7 +218,7 @@ __global__ void __launch_bounds__(32 * R, 1)
         if constexpr (ST == 0) {
           Fo[r] = need_fn ? a.Fn[gy + x] : z2;
         } else {
-          Fo[r] = need_fn ? b16_decode(a.Fn16[gy + x], a.Fe[(g0 >> 3) + r * R * R + (i >> 3)]) : z2;
+          Fo[r] = need_fn ? b16_decode(a.Fn16[gy + x], a.Fe[fe + r * R * R]) : z2;
         }
         Fp[r] = need_f ? a.F[gy + x] : z2;
         Ei[r] = (need_e && in_roi) ? a.Einc[ebase + x] : z2;
@@ -222,7 +231,7 @@ __global__ void __launch_bounds__(32 * R, 1)
         } else {
           const int ex = b16_group_exponent(f, __activemask());
           a.Fn16[gy + x] = b16_encode(f, ex);
-          if ((i & 7) == 0) a.Fe[(g0 >> 3) + r * R * R + (i >> 3)] = (signed char)ex;
+          if ((it & 7) == 0) a.Fe[fe + r * R * R] = (signed char)ex;
         }
       };
       float2 v[8];
@@ -294,10 +303,10 @@ __global__ void __launch_bounds__(32 * R, 1)
       __syncthreads();   // the next plane's step 1 overwrites the plane
       continue;
     }
-    __syncthreads();
-    // ---- 5: x-F2 + F3 on the contiguous groups
-    for (int i = tid; i < 8 * N; i += NT) {
-      const int k1 = i & 7, y = i >> 3;
+    __syncwarp();
+    // ---- 5: x-F2 + F3 on the contiguous groups of the warp's rows
+    for (int it = lane; it < 64; it += 32) {
+      const int k1 = it & 7, y = R * (it >> 3) + w;
       float2* row = pl + y * N + R * k1;
       float2 v[R];
 #pragma unroll
@@ -308,21 +317,20 @@ __global__ void __launch_bounds__(32 * R, 1)
 #pragma unroll
       for (int r = 0; r < R; ++r) row[r] = v[r];
     }
-    __syncthreads();
+    __syncwarp();
     if (tid == 0 && gn >= 0 && need_fn) {
       if constexpr (ST == 0) prefetch_l2(a.Fn + gn, (uint32_t)(plane_n * sizeof(float2)));
       else prefetch_l2(a.Fn16 + gn, (uint32_t)(plane_n * sizeof(short2)));
       prefetch_l2(a.F + gn, (uint32_t)(plane_n * sizeof(float2)));
     }
-    // ---- 6: y-F1 (8-point over n1 at rows R n1 + n2)
-    for (int i = tid; i < R * N; i += NT) {
-      const int x = i % N, n2 = i / N;
+    // ---- 6: y-F1 (8-point over n1 at the warp's rows R n1 + w)
+    for (int x = lane; x < N; x += 32) {
       float2 v[8];
 #pragma unroll
-      for (int r = 0; r < 8; ++r) v[r] = pl[(R * r + n2) * N + x];
+      for (int r = 0; r < 8; ++r) v[r] = pl[(R * r + w) * N + x];
       Butterfly<8, false>::run(v, tw, N);
 #pragma unroll
-      for (int r = 0; r < 8; ++r) pl[(R * r + n2) * N + x] = v[r];
+      for (int r = 0; r < 8; ++r) pl[(R * r + w) * N + x] = v[r];
     }
     __syncthreads();
     // ---- 7: y-F2 + F3 -> T

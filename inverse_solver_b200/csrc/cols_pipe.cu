@@ -65,7 +65,8 @@ struct ColSmem {
   static constexpr size_t kS1_16 = kS0 + kTile16;
   static constexpr size_t kW16 = a1k(kS1_16 + kTile16);
   static constexpr size_t kEx16 = kW16 + kTile;
-  static constexpr size_t kTotalZ16 = kEx16 + a16(2 * N);
+  static constexpr size_t kExStage = a16(2 * N);                  // one stage of [row][2] exponents
+  static constexpr size_t kTotalZ16 = kEx16 + 2 * kExStage;
 };
 
 #if defined(__CUDA_ARCH__)
@@ -176,15 +177,34 @@ __global__ void __launch_bounds__(kThreads, KIND >= 2 ? 5 : 3)
       const int iy = flip ? (y == 0 ? 0 : a.py - y) : y;
       gxy[tid] = a.kq2[0][ix] + a.kq2[1][iy];
     }
-    if constexpr (k16) {   // the tile's two exponents per row (blocks x0 .. x0+7, x0+8 .. x0+15)
-      const int y = o % a.py, b = o / a.py;
-      const long long e0 = ((long long)b * a.nvox + (long long)y * a.px + x0) >> 3;
+    // k16: the two exponents per row of a tile (blocks x0 .. x0+7 and
+    // x0+8 .. x0+15), loaded one tile ahead into registers and stored to the
+    // next stage's exponent buffer after this tile's last step
+    constexpr int kExPer = (2 * N + kThreads - 1) / kThreads;
+    signed char exn[k16 ? kExPer : 1];
+    auto ex_load = [&](int t, signed char* dst_regs, signed char* dst_smem) {
+      const int txt = t % nxt, to = t / nxt;
+      const int tx0 = kW * txt, y = to % a.py, b = to / a.py;
+      const long long e0 = ((long long)b * a.nvox + (long long)y * a.px + tx0) >> 3;
       const long long es = ((long long)a.px * a.py) >> 3;
-      for (int i = tid; i < 2 * N; i += kThreads) {
+#pragma unroll
+      for (int q = 0; q < kExPer; ++q) {
+        const int i = tid + q * kThreads;
         const int row = i >> 1, h = i & 1;
-        ex16[i] = (h == 0 || x0 + 8 < a.px) ? a.Te[e0 + row * es + h] : (signed char)0;
+        signed char e = 0;
+        if (i < 2 * N && (h == 0 || tx0 + 8 < a.px)) e = a.Te[e0 + row * es + h];
+        if (dst_smem) {
+          if (i < 2 * N) dst_smem[i] = e;
+        } else {
+          dst_regs[q] = e;
+        }
       }
+    };
+    if constexpr (k16) {
+      if (it == 0) ex_load(tile, nullptr, ex16);   // the first tile's, exposed once
+      if (next < ntiles) ex_load(next, exn, nullptr);
     }
+    signed char* const exs = ex16 + s * L::kExStage;   // this tile's exponents
     const bool ok = mbar_wait(&bar[s], s ? ph1 : ph0, a.wait_limit);
     if (__syncthreads_or(!ok)) {
       if (tid == 0) {  // give up; let the copies in flight land first
@@ -220,7 +240,7 @@ __global__ void __launch_bounds__(kThreads, KIND >= 2 ? 5 : 3)
 #pragma unroll
           for (int r = 0; r < kR1; ++r) {
             const int row = R2 * r + n2;
-            v[r] = b16_decode(S16[row * kW + c], ex16[2 * row + (c >> 3)]);
+            v[r] = b16_decode(S16[row * kW + c], exs[2 * row + (c >> 3)]);
           }
         } else {
 #pragma unroll
@@ -277,6 +297,16 @@ __global__ void __launch_bounds__(kThreads, KIND >= 2 ? 5 : 3)
           float2* out = a.T + gbase + c;
 #pragma unroll
           for (int r = 0; r < kR1; ++r) out[(R2 * r + n2) * rstride] = v[r];
+        }
+      }
+      if constexpr (k16) {
+        if (next < ntiles) {
+          signed char* nx = ex16 + (s ^ 1) * L::kExStage;
+#pragma unroll
+          for (int q = 0; q < kExPer; ++q) {
+            const int i = tid + q * kThreads;
+            if (i < 2 * N) nx[i] = exn[q];
+          }
         }
       }
       // the next iteration's copy refills the stage just read

@@ -146,7 +146,206 @@ odt_status gfail(odt_status st, const std::string& m) {
     }                                                                                      \
   } while (0)
 
+// ------------------------------------------------------------------ Hankel
+// The cropped order-0 Hankel transform pair (discrete_hankel_croped_fourier.m
+// :19-47, as truncated_green_plus.m:33-66 uses it) with the single-precision
+// rounding of the reference's besselj matrices and scalings: c (zeros of J_0)
+// and C rounded to float, I = |J_1(c)|, s = sqrt(2/C) / I, K = (2 pi / C) I,
+// F[i, j] = (s_i s_j) J_0((c_i / C) c_j).
+
+__global__ void hankel_scalars_kernel(const double* __restrict__ roots, int n, float* __restrict__ c,
+                                      float* __restrict__ I, float* __restrict__ sc, float* __restrict__ K) {
+  const float C = (float)roots[n];
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const float cj = (float)roots[j];
+    const float ij = fabsf((float)j1((double)cj));
+    c[j] = cj;
+    I[j] = ij;
+    sc[j] = __fdiv_rn(__fsqrt_rn(__fdiv_rn(2.0f, C)), ij);
+    K[j] = __fmul_rn(__fdiv_rn(6.28318548202514648f, C), ij);   // float(2 pi) / C * I
+  }
+}
+
+// F [pos, n] column-major
+__global__ void hankel_matrix_kernel(const float* __restrict__ c, const float* __restrict__ sc, float C, int pos,
+                                     long long n, float* __restrict__ F) {
+  const long long total = (long long)pos * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % pos);
+    const long long j = e / pos;
+    const float arg = __fmul_rn(__fdiv_rn(c[i], C), c[j]);
+    F[e] = __fmul_rn(__fmul_rn(sc[i], sc[j]), (float)j0((double)arg));
+  }
+}
+
+// A[j, z] = values[j, z] / I_j
+__global__ void hankel_div_rows_kernel(const float2* __restrict__ v, const float* __restrict__ d, long long n,
+                                       int nz, float2* __restrict__ out) {
+  const long long total = n * nz;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const float q = d[e % n];
+    out[e] = make_float2(__fdiv_rn(v[e].x, q), __fdiv_rn(v[e].y, q));
+  }
+}
+
+// Partial products of out[m, nn] = sum_k f(m, k) * B[k, nn] over one k-chunk
+// per blockIdx.z, double accumulation: f(m, k) = F[m + ldf k] (F [M, K]) or,
+// transF, F[k + ldf m] (F [K, M]); B complex [K, N] (ldb).  Tiles of 32 x 32
+// outputs, 256 threads with 2 x 2 outputs each, k in slices of 32.
+__global__ void __launch_bounds__(256) rc_gemm_part_kernel(int M, int N, int K, int kchunk,
+                                                           const float* __restrict__ F, int ldf, int transF,
+                                                           const float2* __restrict__ B, int ldb,
+                                                           double2* __restrict__ part) {
+  __shared__ float Fs[32][33];     // [k][m]
+  __shared__ float2 Bs[32][33];    // [k][n]
+  const int m0 = blockIdx.x * 32, n0 = blockIdx.y * 32;
+  const int k_lo = blockIdx.z * kchunk, k_hi = min(K, k_lo + kchunk);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double2 acc[2][2];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) acc[a][b] = make_double2(0.0, 0.0);
+  for (int k0 = k_lo; k0 < k_hi; k0 += 32) {
+    for (int e = threadIdx.x; e < 32 * 32; e += 256) {
+      const int r = e & 31, q = e >> 5;   // F: (m = r, k = q) or (k = r, m = q) so loads run along memory
+      int m, k;
+      if (transF) { k = r; m = q; } else { m = r; k = q; }
+      const int gm = m0 + m, gk = k0 + k;
+      float v = 0.f;
+      if (gm < M && gk < k_hi) v = transF ? F[gk + (long long)ldf * gm] : F[gm + (long long)ldf * gk];
+      Fs[k][m] = v;
+      const int bk = r, bn = q;           // B: (k = r, n = q)
+      const int gbk = k0 + bk, gbn = n0 + bn;
+      Bs[bk][bn] = (gbk < k_hi && gbn < N) ? B[gbk + (long long)ldb * gbn] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k) {
+      const double f0 = Fs[k][tx], f1 = Fs[k][tx + 16];
+      const float2 b0 = Bs[k][ty], b1 = Bs[k][ty + 16];
+      acc[0][0].x += f0 * b0.x; acc[0][0].y += f0 * b0.y;
+      acc[0][1].x += f0 * b1.x; acc[0][1].y += f0 * b1.y;
+      acc[1][0].x += f1 * b0.x; acc[1][0].y += f1 * b0.y;
+      acc[1][1].x += f1 * b1.x; acc[1][1].y += f1 * b1.y;
+    }
+    __syncthreads();
+  }
+  double2* P = part + (long long)blockIdx.z * M * N;
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      const int gm = m0 + tx + 16 * a, gn = n0 + ty + 16 * b;
+      if (gm < M && gn < N) P[gm + (long long)M * gn] = acc[a][b];
+    }
+}
+
+// out[m, n] = round(sum over the chunks, in order) -- then times post[m] if given
+__global__ void rc_gemm_reduce_kernel(const double2* __restrict__ part, int nchunk, long long MN, int M,
+                                      const float* __restrict__ post, float2* __restrict__ out) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < MN;
+       e += (long long)gridDim.x * blockDim.x) {
+    double x = 0.0, y = 0.0;
+    for (int c = 0; c < nchunk; ++c) {
+      x += part[c * MN + e].x;
+      y += part[c * MN + e].y;
+    }
+    float2 r = make_float2((float)x, (float)y);
+    if (post) {
+      const float q = post[e % M];
+      r = make_float2(__fmul_rn(r.x, q), __fmul_rn(r.y, q));
+    }
+    out[e] = r;
+  }
+}
+
+// V2[i, z] = ((T[i, z] * K_i) * band_i) / K_i, as forward(), the band window
+// and backward() round it
+__global__ void hankel_band_kernel(const float2* __restrict__ T, const float* __restrict__ K,
+                                   const float* __restrict__ band, int pos, int nz, float2* __restrict__ out) {
+  const long long total = (long long)pos * nz;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % pos);
+    const float k = K[i], b = band[i];
+    float2 v = make_float2(__fmul_rn(T[e].x, k), __fmul_rn(T[e].y, k));
+    v = make_float2(__fmul_rn(v.x, b), __fmul_rn(v.y, b));
+    out[e] = make_float2(__fdiv_rn(v.x, k), __fdiv_rn(v.y, k));
+  }
+}
+
 }  // namespace
+
+extern "C" odt_status odt_hankel_filter(const odt_hankel_args* a) {
+  if (!a || !a->roots || !a->values || !a->band || !a->out)
+    return gfail(ODT_ERR_INVALID_ARGUMENT, "odt_hankel_filter: NULL argument");
+  const int n = a->n, pos = a->pos, nz = a->nz;
+  if (n < 1 || pos < 1 || pos > n || nz < 1 || nz > 65535 || (long long)pos * n > (1LL << 31))
+    return gfail(ODT_ERR_INVALID_ARGUMENT, "odt_hankel_filter: bad sizes");
+  if (a->device >= 0) G_CHECK(cudaSetDevice(a->device));
+  cudaStream_t s = nullptr;
+  G_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  odt_status st = ODT_OK;
+  {
+    Scratch B;
+    B.s = s;
+    const int kchunk = 1024;
+    const int nsplit = (n + kchunk - 1) / kchunk;
+    const long long pn = (long long)pos * nz, nn = (long long)n * nz;
+    double* roots = B.get<double>((size_t)n + 1);
+    float* c = B.get<float>(n);
+    float* I = B.get<float>(n);
+    float* sc = B.get<float>(n);
+    float* K = B.get<float>(n);
+    float* band = B.get<float>(pos);
+    float* F = B.get<float>((size_t)pos * n);
+    float2* V = B.get<float2>(nn);
+    float2* A = B.get<float2>(nn);
+    float2* T = B.get<float2>(pn);
+    float2* V2 = B.get<float2>(pn);
+    double2* part = B.get<double2>((size_t)(nsplit > 1 ? nsplit : 1) * (size_t)(nn > pn ? nn : pn));
+    if (!roots || !c || !I || !sc || !K || !band || !F || !V || !A || !T || !V2 || !part) {
+      st = gfail(ODT_ERR_OUT_OF_MEMORY, "odt_hankel_filter: device allocation failed");
+    } else {
+      auto run = [&]() -> cudaError_t {
+        const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
+        cudaError_t e;
+        if ((e = cudaMemcpyAsync(roots, a->roots, ((size_t)n + 1) * sizeof(double), h2d, s)) ||
+            (e = cudaMemcpyAsync(band, a->band, (size_t)pos * sizeof(float), h2d, s)) ||
+            (e = cudaMemcpyAsync(V, a->values, (size_t)nn * sizeof(float2), h2d, s)))
+          return e;
+        const float C = (float)a->roots[n];
+        hankel_scalars_kernel<<<grid_for(n), kThreads, 0, s>>>(roots, n, c, I, sc, K);
+        hankel_matrix_kernel<<<grid_for((long long)pos * n), kThreads, 0, s>>>(c, sc, C, pos, n, F);
+        hankel_div_rows_kernel<<<grid_for(nn), kThreads, 0, s>>>(V, I, n, nz, A);
+        if ((e = cudaGetLastError())) return e;
+        // T = F A   [pos, nz], k = n split into chunks
+        rc_gemm_part_kernel<<<dim3((pos + 31) / 32, (nz + 31) / 32, nsplit), 256, 0, s>>>(
+            pos, nz, n, kchunk, F, pos, 0, A, n, part);
+        rc_gemm_reduce_kernel<<<grid_for(pn), kThreads, 0, s>>>(part, nsplit, pn, pos, nullptr, T);
+        hankel_band_kernel<<<grid_for(pn), kThreads, 0, s>>>(T, K, band, pos, nz, V2);
+        // out = (F^T V2) .* I   [n, nz], k = pos in one chunk
+        rc_gemm_part_kernel<<<dim3((n + 31) / 32, (nz + 31) / 32, 1), 256, 0, s>>>(
+            n, nz, pos, pos, F, pos, 1, V2, pos, part);
+        rc_gemm_reduce_kernel<<<grid_for(nn), kThreads, 0, s>>>(part, 1, nn, n, I, A);
+        if ((e = cudaGetLastError())) return e;
+        if ((e = cudaMemcpyAsync(a->out, A, (size_t)nn * sizeof(float2), cudaMemcpyDeviceToHost, s))) return e;
+        return cudaStreamSynchronize(s);
+      };
+      const cudaError_t e = run();
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        st = gfail(ODT_ERR_CUDA, std::string("odt_hankel_filter: ") + cudaGetErrorString(e));
+      }
+    }
+  }
+  cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  return st;
+}
 
 extern "C" odt_status odt_green_planes(const odt_green_args* a) {
   if (!a || !a->radial || !a->near1 || !a->near2 || !a->w || !a->m1 || !a->m2 || !a->mz || !a->out)

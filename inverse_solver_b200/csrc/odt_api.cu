@@ -97,6 +97,10 @@ enum Kind { kKBornX = 0, kKBornY, kKBornZ, kKIoFft, kKIoElem, kKBornXPipe, kKBor
 struct Handle {
   odt_geometry g{};
   cudaStream_t own_stream = nullptr;
+  // recorded after the work a device-memory solve leaves queued on the
+  // caller's stream; waited for before this handle's tables change
+  cudaEvent_t done_ev = nullptr;
+  bool done_pending = false;
   std::vector<void*> allocs;
   size_t static_bytes = 0;
   size_t batch_bytes = 0;
@@ -239,7 +243,19 @@ struct Handle {
     for (void* p : batch_allocs) cudaFree(p);
     for (void* p : allocs) cudaFree(p);
     for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    if (done_ev) cudaEventDestroy(done_ev);
     if (own_stream) cudaStreamDestroy(own_stream);
+  }
+
+  // The work of this handle still queued on the GPU has finished: its own
+  // stream and the last device-memory solve's stream (other handles' work
+  // keeps running, so concurrent solvers do not wait for each other).
+  void wait_idle() {
+    if (done_pending) {
+      ODT_CUDA(cudaEventSynchronize(done_ev));
+      done_pending = false;
+    }
+    ODT_CUDA(cudaStreamSynchronize(own_stream));
   }
 
   // ---- profiling helpers
@@ -706,7 +722,7 @@ void set_potential_slot(const std::shared_ptr<Handle>& Hp, int k, const odt_pote
     raise(ODT_ERR_INVALID_ARGUMENT, who + ": non-finite scalar");
   DeviceGuard dg(g.device);
   std::lock_guard<std::recursive_mutex> lk(g_device_mu);
-  ODT_CUDA(cudaDeviceSynchronize());  // a queued graph may still read the old tables
+  H.wait_idle();  // a queued solve or graph of this handle may still read the old tables
   H.drop_graphs();
   alloc_slot(H, k);
   Handle::PotSlot& P = H.pot[k];
@@ -811,6 +827,7 @@ odt_status odt_create(const odt_geometry* geom, const odt_cfloat* refocus,
       H->wait_limit = v;
     }
     ODT_CUDA(cudaStreamCreateWithFlags(&H->own_stream, cudaStreamNonBlocking));
+    ODT_CUDA(cudaEventCreateWithFlags(&H->done_ev, cudaEventDisableTiming));
     H->fx = make_dev_fft(*H, g.sim_size[0], kKindBornX, "sim_size(1)");
     H->fy = make_dev_fft(*H, g.sim_size[1], kKindCols, "sim_size(2)");
     H->fz = make_dev_fft(*H, g.sim_size[2], kKindBornZ, "sim_size(3)");
@@ -1003,6 +1020,10 @@ odt_status odt_solve(odt_handle h, const odt_solve_args* args) {
                                  (size_t)nb * nF * sizeof(float2), kout, s));
       if (!dev) ODT_CUDA(cudaStreamSynchronize(s));
       H->collect(s);
+    }
+    if (dev) {
+      ODT_CUDA(cudaEventRecord(H->done_ev, s));
+      H->done_pending = true;
     }
     if (!dev) {
       check_fault(*H);

@@ -299,7 +299,7 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
         Parameter ``green_on_device=False`` keeps the host path."""
         if not self.parameters.get("green_on_device", True):
             return super()._truncated_green(params, refocus_version)
-        r = truncated_green_radial(params, refocus_version)
+        r = truncated_green_radial(params, refocus_version, hankel_filter=self._device_hankel)
         keep = [np.asfortranarray(np.asarray(r["green"], dtype=C64)),
                 np.asfortranarray(np.asarray(r["near"], dtype=np.int32)),
                 np.asfortranarray(np.asarray(r["near2"], dtype=np.int32)),
@@ -317,6 +317,23 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
         a.out = _lib.ptr(out)
         a.device = int(self.parameters.get("used_gpu", 0))
         _lib.check(self.lib.odt_green_planes(C.byref(a)))
+        return out
+
+    def _device_hankel(self, hk, green, band):
+        """The cropped Hankel transform pair and band window of
+        truncated_green_plus (:33-66) on the GPU (odt_hankel_filter): the
+        Bessel matrix is built on the device from the zeros of J_0."""
+        if hk.order != 0 or float(hk.R) != 1.0:
+            raise ValueError("odt_hankel_filter covers the order-0, unit-radius transform only")
+        vals = np.asfortranarray(np.asarray(green, dtype=C64))
+        roots = np.ascontiguousarray(hk.roots64, dtype=np.float64)
+        b = np.ascontiguousarray(band, dtype=F32)
+        out = np.empty_like(vals, order="F")
+        a = _lib.HankelArgs()
+        a.roots, a.n, a.pos, a.nz = _lib.ptr(roots), len(hk.c), int(hk.pos), vals.shape[1]
+        a.values, a.band, a.out = _lib.ptr(vals), _lib.ptr(b), _lib.ptr(out)
+        a.device = int(self.parameters.get("used_gpu", 0))
+        _lib.check(self.lib.odt_hankel_filter(C.byref(a)))
         return out
 
     def _create_handle(self):

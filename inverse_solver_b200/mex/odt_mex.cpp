@@ -9,6 +9,7 @@
 //   odt_mex(uint32(5), id, Radial_2D, Perp_2D, ewald_TanVec, uint8(K_mask))   polarisation basis
 //   odt_mex(uint32(6), id, pot, single(V_adjoint))                             adjoint potential
 //   [grad, err] = odt_mex(uint32(7), id, input_field, output_field, RI_size)   fused gradient
+//   odt_mex(uint32(8), id, uint32(storage))   T / Field_n storage (0 complex64, 1 16-bit block float)
 //
 // geom: struct with simulation_size, RI_size, field_size, conv_size, used_gpu
 // (the CudaBorn names), optional max_batch and pol (3: dyadic Green's
@@ -161,6 +162,11 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
       a.memory = ODT_MEM_HOST;
       check(odt_gradient(id, &a));
       if (nlhs > 1) plhs[1] = mxCreateDoubleScalar(err);
+      break;
+    }
+    case 8: {
+      if (nrhs < 3) mexErrMsgIdAndTxt("odt:arg", "storage needs ODT_STORAGE_COMPLEX64 (0) or ODT_STORAGE_B16 (1)");
+      check(odt_set_field_storage(id, (int32_t)u32(prhs[2])));
       break;
     }
     case 3:

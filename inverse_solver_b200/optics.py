@@ -193,28 +193,39 @@ class CroppedHankel:
 
     def __init__(self, max_r, samples, order, cropping):
         R = F32(max_r)
-        roots = bessel_zeros(order, samples + 1).astype(F32)
+        self.roots64 = bessel_zeros(order, samples + 1)
+        roots = self.roots64.astype(F32)
         C = roots[-1]
         c = roots[:-1]
         self.r = R / C * c
         k = c / R
         self.pos = int(np.argmin(np.abs(k - k.max() * cropping))) + 1
-        p = self.pos
+        self.order, self.R, self.C, self.c = order, R, C, c
         I = np.abs(bessel_j(1 + order, c.astype(np.float64)).astype(F32))
         self.K = 2 * math.pi * R / C * I
         self.Rv = I / R
-        I = np.sqrt(F32(2) / C) / I
-        b1 = bessel_j(order, (c[:p, None] / C * c[None, :]).astype(np.float64)).astype(F32)
-        b2 = bessel_j(order, (c[:, None] / C * c[None, :p]).astype(np.float64)).astype(F32)
-        self.fwd = I[:p, None] * I[None, :] * b1
-        self.bwd = I[:, None] * I[None, :p] * b2
-        self.k = k[:p]
+        self.scale = np.sqrt(F32(2) / C) / I
+        self.k = k[:self.pos]
+        self._fwd = self._bwd = None
+
+    def _matrices(self):
+        """The Bessel matrices (:41-42), built on first use (most of the
+        set-up time on the host; the GPU path builds them on the device)."""
+        if self._fwd is None:
+            p, c, C, s = self.pos, self.c, self.C, self.scale
+            b1 = bessel_j(self.order, (c[:p, None] / C * c[None, :]).astype(np.float64)).astype(F32)
+            b2 = bessel_j(self.order, (c[:, None] / C * c[None, :p]).astype(np.float64)).astype(F32)
+            self._fwd = s[:p, None] * s[None, :] * b1
+            self._bwd = s[:, None] * s[None, :p] * b2
+        return self._fwd, self._bwd
 
     def forward(self, vals):
-        return (self.fwd @ (vals / self.Rv[:, None])) * self.K[:self.pos, None]
+        fwd, _ = self._matrices()
+        return (fwd @ (vals / self.Rv[:, None])) * self.K[:self.pos, None]
 
     def backward(self, vals):
-        return (self.bwd @ (vals / self.K[:self.pos, None])) * self.Rv[:, None]
+        _, bwd = self._matrices()
+        return (bwd @ (vals / self.K[:self.pos, None])) * self.Rv[:, None]
 
 
 _HANKEL_CACHE = {}
@@ -254,12 +265,13 @@ def _nearest_bins(value, grid):
     return near, near2, w
 
 
-def truncated_green_radial(params, refocus_version=False):
+def truncated_green_radial(params, refocus_version=False, hankel_filter=None):
     """The radial part of truncated_green_plus (sub_code/truncated_green_plus.m
     :1-66 and bin_search_nearest :111-129): the band-limited radial profile
     [samples, Nz] and the interpolation maps of the oversized xy grid.
     Returns a dict (green, near, near2, w, creation [S1, S2, Nz], out_px,
-    scale)."""
+    scale).  ``hankel_filter(hk, green, band)``, if given, replaces the host
+    forward transform / band window / backward transform (:45-53)."""
     req = basic_optical_parameter()
     req.update(use_GPU=True, oversize_z=10, oversample_xy=20000, oversample_xy_fourier=2,
                simultanous_process=30)
@@ -292,10 +304,13 @@ def truncated_green_radial(params, refocus_version=False):
     else:
         green = green * Hin[:, None] / (Hk3 + (~Hin))[:, None]
         green = green / (1j * 4 * math.pi)
-    img = hk.forward(green)
     nk = hk.k / hk.k.max()
-    band = (nk < 0.9) + (nk < 1) * (nk > 0.9) * (1 - nk) * 10
-    green = hk.backward(img * band.astype(F32)[:, None])
+    band = ((nk < 0.9) + (nk < 1) * (nk > 0.9) * (1 - nk) * 10).astype(F32)
+    if hankel_filter is not None:
+        green = hankel_filter(hk, green, band)
+    else:
+        img = hk.forward(green)
+        green = hk.backward(img * band[:, None])
     near, near2, w = _nearest_bins(u.coorxy, H)
     return dict(green=green, near=near, near2=near2, w=w, creation=[S1, S2, Nz], out_px=out_px,
                 scale=Nz / (u.image_res[0] * u.image_res[1]), simultanous_process=params["simultanous_process"])

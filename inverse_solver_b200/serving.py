@@ -138,6 +138,15 @@ class SolveServer:
             self._idle.clear()
             self._held = 0.0
 
+    def reset_stats(self):
+        """Start a new measurement (latencies, span, peaks) on a running server."""
+        with self._cv:
+            self._lat = []
+            self._done = 0
+            self._t0 = self._t1 = None
+            self._peak_bytes = 0
+            self._peak_running = 0
+
     def stats(self):
         with self._cv:
             lat = np.asarray(self._lat) * 1e3
@@ -231,7 +240,7 @@ class SolveServer:
         if isinstance(req, ForwardRequest):
             key, s, b = self._acquire(req.params, need)
             try:
-                s.set_RI(req.RI)
+                set_ri_on_device(s, req.RI)
                 return s.solve(req.fields)
             finally:
                 self._release(key, s, b)
@@ -248,6 +257,26 @@ class SolveServer:
             return bs.solve(req.fields_in, req.fields_out)
         finally:
             self._release(key, s, b)
+
+
+def set_ri_on_device(s, RI):
+    """set_RI with the potential built on the GPU (set_RI_device): the RI map
+    is uploaded once and eps_imag, Bornmax and the padded potential come from
+    device kernels, so a request's set-up does not run numpy sweeps under the
+    GIL while the other slots' solves wait for it.  Host set_RI where the
+    device path does not apply (RI tensors of the dyadic solver)."""
+    import torch
+
+    if s.vector or np.asarray(RI).ndim != 3:
+        s.set_RI(RI)
+        return
+    a = np.asarray(RI)
+    dt = np.complex64 if np.iscomplexobj(a) else np.float32
+    flat = np.ascontiguousarray(a.astype(dt).ravel(order="F"))
+    dev = torch.device("cuda", int(s.parameters.get("used_gpu", 0)))
+    t = torch.from_numpy(flat).to(dev)
+    s.set_RI_device(t)
+    torch.cuda.current_stream(dev).synchronize()
 
 
 def one_at_a_time(requests):
@@ -274,11 +303,17 @@ def one_at_a_time(requests):
 
 
 # ---------------------------------------------------------------- benchmark
+CONFIG5_SIZES = ((64, 64, 64), (96, 96, 64), (128, 128, 128), (192, 192, 96), (256, 256, 192))
+CONFIG5_RECON_SIZES = ((64, 64, 61), (128, 128, 127))
+
+
 def make_mix(n, seed, sizes=((64, 64, 64), (96, 96, 64), (128, 128, 128)), max_ill=16,
-             recon_every=0, recon_iters=10):
+             recon_every=0, recon_iters=10, recon_sizes=((64, 64, 61),)):
     """Seeded request mix: grids drawn from ``sizes``, 1..max_ill ring /
     circle illuminations, sphere phantoms; every ``recon_every``-th request
-    (0: none) is a reconstruction of ``recon_iters`` FISTA iterations."""
+    (0: none) is a reconstruction of ``recon_iters`` FISTA iterations on a
+    grid drawn from ``recon_sizes`` (odd z, as BACKWARD_SOLVER_MULTI.m:117-119
+    requires)."""
     from .backward import BACKWARD_SOLVER_MULTI
     from .forward import CBSHostSetup, FORWARD_SOLVER_CONVERGENT_BORN
     from .inputs import FIELD_GENERATOR, sphere_phantom
@@ -287,9 +322,8 @@ def make_mix(n, seed, sizes=((64, 64, 64), (96, 96, 64), (128, 128, 128)), max_i
     reqs = []
     for i in range(n):
         recon = bool(recon_every) and i % recon_every == recon_every - 1
-        # a reconstruction needs an odd z size (BACKWARD_SOLVER_MULTI.m:117-119);
-        # 61 pads to 85 = 5 * 17
-        size = [64, 64, 61] if recon else list(sizes[int(rng.integers(len(sizes)))])
+        size = (list(recon_sizes[int(rng.integers(len(recon_sizes)))]) if recon
+                else list(sizes[int(rng.integers(len(sizes)))]))
         n_ill = int(rng.integers(1, max_ill + 1))
         p = CBSHostSetup.get_default_parameters(dict(
             size=size, wavelength=0.532, NA=1.2, RI_bg=1.3355, resolution=[0.1] * 3,
@@ -316,13 +350,19 @@ def make_mix(n, seed, sizes=((64, 64, 64), (96, 96, 64), (128, 128, 128)), max_i
     return reqs
 
 
-def run_stream(reqs, rate_per_s, seed, budget_bytes=None, slots=4):
+def run_stream(reqs, rate_per_s, seed, budget_bytes=None, slots=4, srv=None):
     """Poisson arrivals at ``rate_per_s``: submit each request at its arrival
-    time, wait for all; returns (results, stats)."""
+    time, wait for all; returns (results, stats).  With ``srv`` the given
+    server (and its resident solvers) is used and left open; its statistics
+    cover this stream only."""
     rng = np.random.default_rng(seed)
     gaps = (np.zeros(len(reqs)) if not np.isfinite(rate_per_s)
             else rng.exponential(1.0 / rate_per_s, size=len(reqs)))
-    srv = SolveServer(budget_bytes=budget_bytes, slots=slots)
+    own = srv is None
+    if own:
+        srv = SolveServer(budget_bytes=budget_bytes, slots=slots)
+    else:
+        srv.reset_stats()
     t0 = time.perf_counter()
     futs = []
     t = 0.0
@@ -335,7 +375,8 @@ def run_stream(reqs, rate_per_s, seed, budget_bytes=None, slots=4):
         futs.append(srv.submit(r))
     res = [f.result() for f in futs]
     st = srv.stats()
-    srv.close()
+    if own:
+        srv.close()
     return res, st
 
 
@@ -352,15 +393,44 @@ def main():
     ap.add_argument("--uneven", action="store_true",
                     help="batched uneven solves: all requests submitted at once, forward only, "
                          "grids 64^3 / 96x96x64 / 128^3 / 192x192x96, 1-64 illuminations")
+    ap.add_argument("--config5", action="store_true",
+                    help="config 5: grids 64^3 .. 256x256x192 with 1-49 illuminations, every "
+                         "--recon-every-th request a 10-iteration reconstruction (64x64x61 or "
+                         "128x128x127); arrivals at --load times the measured capacity")
+    ap.add_argument("--load", type=float, default=0.7,
+                    help="with --config5: arrival rate as a fraction of the measured capacity")
+    ap.add_argument("--device", type=int, default=0)
     a = ap.parse_args()
+    capacity = None
     if a.uneven:
         reqs = make_mix(a.requests, a.seed, sizes=((64, 64, 64), (96, 96, 64), (128, 128, 128),
                                                    (192, 192, 96)), max_ill=64, recon_every=0)
         a.rate = float("inf")
+    elif a.config5:
+        reqs = make_mix(a.requests, a.seed, sizes=CONFIG5_SIZES, max_ill=49, recon_every=a.recon_every,
+                        recon_sizes=CONFIG5_RECON_SIZES)
+        # capacity: the same requests all submitted at once, on solvers made
+        # resident by a first pass (as a long-running server holds them)
+        server = SolveServer(slots=a.slots)
+        run_stream(reqs, float("inf"), a.seed + 1, srv=server)
+        _, cap = run_stream(reqs, float("inf"), a.seed + 1, srv=server)
+        capacity = cap["throughput_per_s"]
+        a.rate = a.load * capacity
     else:
         reqs = make_mix(a.requests, a.seed, recon_every=a.recon_every)
     serial = one_at_a_time(reqs)
-    _, st = run_stream(reqs, a.rate, a.seed + 1, slots=a.slots)
+    from .clocks import ClockSampler
+
+    clk = ClockSampler(a.device)
+    clk.start()
+    if capacity is not None:
+        _, st = run_stream(reqs, a.rate, a.seed + 2, srv=server)
+        server.close()
+    else:
+        _, st = run_stream(reqs, a.rate, a.seed + 1, slots=a.slots)
+    st["clocks"] = clk.stop()
+    if capacity is not None:
+        st.update(capacity_per_s=capacity, load=a.load)
     vox = 0
     for r in reqs:
         if isinstance(r, ForwardRequest):

@@ -107,4 +107,4 @@ def test_b16_unsupported_grid_is_rejected():
     p = cases.small_params(return_3D=True)
     with pytest.raises(OdtError) as ei:
         _solve(p, cases.small_RI(), cases.circle_fields(p, 1), "b16")
-    assert ei.value.args[0] == 6 and "B16" in str(ei.value)
+    assert ei.value.status == 6 and "B16" in str(ei.value)

@@ -44,7 +44,7 @@ def test_zero_wait_limit_reports_timeout_then_fresh_handle_solves(monkeypatch):
         s.set_RI(RI)
         with pytest.raises(OdtError) as ei:
             s.solve(fields)
-        assert ei.value.args[0] == 8, ei.value.args     # ODT_ERR_INTERNAL
+        assert ei.value.status == 8, ei.value.args     # ODT_ERR_INTERNAL
         assert "timed out" in str(ei.value)
     finally:
         s.delete()
@@ -72,4 +72,4 @@ def test_wait_limit_must_be_a_non_negative_integer(monkeypatch):
     monkeypatch.setenv("ODT_WAIT_LIMIT_CYCLES", "-5")
     with pytest.raises(OdtError) as ei:
         FORWARD_SOLVER_CONVERGENT_BORN(p)
-    assert ei.value.args[0] == 1 and "ODT_WAIT_LIMIT_CYCLES" in str(ei.value)
+    assert ei.value.status == 1 and "ODT_WAIT_LIMIT_CYCLES" in str(ei.value)
