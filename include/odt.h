@@ -658,6 +658,26 @@ odt_status odt_get_batch(odt_handle h, int32_t* batch);
 #define ODT_STORAGE_B16 1
 odt_status odt_set_field_storage(odt_handle h, int32_t storage);
 
+/* Plan autotuning (no counterpart in the reference): times one solve of
+ * n_ill plane waves (capped at the handle's batch) with each execution plan
+ * that applies to the handle -- the fused xy-pass with the pipelined z-pass,
+ * the separate pipelined x-, y-, z-passes, the generic tile kernels -- on
+ * the potential set last, keeps the fastest for the handle's later solves
+ * and caches the choice process-wide per (device, padded grid, batch,
+ * components, storage), so a later handle of the same shape takes it without
+ * timing.  The plans give the same results up to the order of the FFT
+ * arithmetic.  ms[i] is the time per solve of plan i (0: fused xy-pass, 1:
+ * separate pipelined passes, 2: generic tile kernels; -1 where a plan does
+ * not apply or was not timed).  Needs odt_set_potential first; synchronous. */
+typedef struct odt_tune_result {
+  int32_t fused_xy;    /* chosen: 1 fused xy-pass                              */
+  int32_t pipelined;   /* chosen: 1 pipelined kernels, 0 generic tile kernels   */
+  int32_t batch;       /* illuminations per launch of the timed solves          */
+  int32_t cached;      /* 1: the choice came from the cache (nothing timed)     */
+  double ms[3];
+} odt_tune_result;
+odt_status odt_autotune(odt_handle h, int32_t n_ill, odt_tune_result* out);
+
 /* Per-kernel timing (CUDA events around every launch on the solve stream).
  * When enabled, odt_get_kernel_times fills up to `cap` entries of names
  * (static strings), accumulated milliseconds and launch counts since the

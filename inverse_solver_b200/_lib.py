@@ -265,6 +265,16 @@ class HankelArgs(C.Structure):
     ]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [
+        ("fused_xy", C.c_int32),
+        ("pipelined", C.c_int32),
+        ("batch", C.c_int32),
+        ("cached", C.c_int32),
+        ("ms", C.c_double * 3),
+    ]
+
+
 class BPMArgs(C.Structure):
     _fields_ = [
         ("size", C.c_int32 * 3),
@@ -363,6 +373,7 @@ SIGNATURES = {
     "odt_set_profiling": (C.c_int, [C.c_uint32, C.c_int32]),
     "odt_set_field_storage": (C.c_int, [C.c_uint32, C.c_int32]),
     "odt_hankel_filter": (C.c_int, [C.POINTER(HankelArgs)]),
+    "odt_autotune": (C.c_int, [C.c_uint32, C.c_int32, C.POINTER(TuneResult)]),
     "odt_get_kernel_times": (C.c_int, [C.c_uint32, C.POINTER(C.c_char_p),
                                        C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                        C.c_int32, C.POINTER(C.c_int32)]),

@@ -40,9 +40,10 @@
 // concurrent CTAs share V's planes in L2).  Steps 2-6 touch, for one n2, only
 // the 8 rows R n1 + n2 (step 2 and 6 combine exactly those rows, steps 3-5
 // work along rows), so warp w takes n2 = w and runs steps 2-6 on its own rows
-// with warp-level synchronisation only: a plane needs three CTA barriers
-// (after steps 1 and 6, and after step 7), and the warps drift apart so that
-// one warp's global loads in step 4 overlap other warps' transforms.  The next plane's T and Field_n / Field are
+// with warp-level synchronisation only; step 7 of a plane and step 1 of the
+// next touch the same rows per item (see step1 below), so a plane needs two
+// CTA barriers (after steps 1 and 6), and the warps drift apart so that one
+// warp's global loads overlap other warps' transforms.  The next plane's T and Field_n / Field are
 // prefetched into L2 (cp.async.bulk.prefetch) during steps 4 and 6 of the
 // current one, so their DRAM reads overlap the shared-memory steps.
 //
@@ -91,8 +92,15 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
 // point (b16.cuh; T's blocks are 8 consecutive x of a row, Field_n's are the
 // values of one n1 in 8 consecutive step-4 work items of a warp, exponent
 // index plane * N^2/8 + n1 * R^2 + w * R + item / 8)
+// Registers per thread: all of the register file for the one CTA of 32 R
+// threads per SM (rounded down to the allocation granularity of 8), so that
+// the radix-R butterflies do not spill: 104 for R = 19.
+constexpr int xy_max_regs(int R) {
+  return ((65536 / (32 * R)) / 8) * 8 > 255 ? 255 : ((65536 / (32 * R)) / 8) * 8;
+}
+
 template <int R, int KIND, int ST>
-__global__ void __launch_bounds__(32 * R, 1)
+__global__ void __maxnreg__(xy_max_regs(R))
     born_xy_kernel(const BornArgs a, const int jj, const float2* __restrict__ twg, const int nplanes) {
 #if defined(__CUDA_ARCH__)
   constexpr int N = 8 * R;
@@ -131,6 +139,33 @@ __global__ void __launch_bounds__(32 * R, 1)
   const bool need_f = kInv && (e >= 3 || (KIND == kXYFinal && e == 2));
   const bool need_e = KIND == kXYFinal || ((KIND == kXYFirst || KIND == kXYEarly) && jj <= 2);
 
+  // ---- 1: y-F3^-1 (R-point over k2 at rows R k1 + k2) and twiddles of item
+  // i = (x, k1) of the plane at g0, from T into the plane buffer
+  auto step1 = [&](int i, long long g0) {
+    const int x = i % N, k1 = i / N;
+    float2 v[R];
+    if constexpr (ST == 0) {
+      const float2* src = a.T + g0 + (long long)(R * k1) * N + x;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = src[(long long)r * N];
+    } else {
+      const long long o = g0 + (long long)(R * k1) * N + x;
+      const short2* src = a.T16 + o;
+      const signed char* se = a.Te + (o >> 3);
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = b16_decode(src[(long long)r * N], se[r * (N >> 3)]);
+    }
+    Butterfly<R, true>::run(v, tw, N);
+#pragma unroll
+    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], cconj(tw[r * k1]));
+#pragma unroll
+    for (int r = 0; r < R; ++r) pl[(R * k1 + r) * N + x] = v[r];
+  };
+  // Step 7 of item (x, k1) reads the rows R k1 + r of column x and step 1 of
+  // the same item writes them, with the same item -> thread map: a thread
+  // goes from its step-7 item of one plane straight to its step-1 item of
+  // the next, with no CTA barrier in between.
+  bool loaded = false;   // step 1 of this plane done during the previous plane's step 7
   for (int p = blockIdx.x; p < nplanes; p += gridDim.x) {
     const int b = p % a.nbatch;
     const int z = p / a.nbatch;
@@ -143,27 +178,9 @@ __global__ void __launch_bounds__(32 * R, 1)
     const bool zroi = (unsigned)(z - a.rz0) < (unsigned)a.rz;
 
     if constexpr (kInv) {
-      // ---- 1: y-F3^-1 (R-point over k2 at rows R k1 + k2), twiddles, from T
-      for (int i = tid; i < 8 * N; i += NT) {
-        const int x = i % N, k1 = i / N;
-        float2 v[R];
-        if constexpr (ST == 0) {
-          const float2* src = a.T + g0 + (long long)(R * k1) * N + x;
-#pragma unroll
-          for (int r = 0; r < R; ++r) v[r] = src[(long long)r * N];
-        } else {
-          const long long o = g0 + (long long)(R * k1) * N + x;
-          const short2* src = a.T16 + o;
-          const signed char* se = a.Te + (o >> 3);
-#pragma unroll
-          for (int r = 0; r < R; ++r) v[r] = b16_decode(src[(long long)r * N], se[r * (N >> 3)]);
-        }
-        Butterfly<R, true>::run(v, tw, N);
-#pragma unroll
-        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], cconj(tw[r * k1]));
-#pragma unroll
-        for (int r = 0; r < R; ++r) pl[(R * k1 + r) * N + x] = v[r];
-      }
+      // ---- 1 (unless the previous plane's step 7 did it item by item)
+      if (!loaded)
+        for (int i = tid; i < 8 * N; i += NT) step1(i, g0);
       __syncthreads();
       // ---- 2: y-F1^-1 (8-point over k1 at rows R k1 + w) -> natural rows R n1 + w
       for (int x = lane; x < N; x += 32) {
@@ -301,6 +318,7 @@ __global__ void __launch_bounds__(32 * R, 1)
     }
     if constexpr (!kFwd) {
       __syncthreads();   // the next plane's step 1 overwrites the plane
+      loaded = false;
       continue;
     }
     __syncwarp();
@@ -359,7 +377,10 @@ __global__ void __launch_bounds__(32 * R, 1)
         }
       }
     }
-    __syncthreads();
+    if (kInv && gn >= 0)   // the same items as this thread's step 7: no barrier needed
+      for (int i = tid; i < 8 * N; i += NT) step1(i, gn);
+    loaded = kInv && gn >= 0;
+    if (!loaded) __syncthreads();   // the next plane's step 4 (first kind) writes other threads' rows
   }
 #endif
 }

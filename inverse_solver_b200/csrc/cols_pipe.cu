@@ -40,7 +40,12 @@ namespace {
 
 constexpr int kW = 16;               // columns per tile
 constexpr int kR1 = 8;
-constexpr int kThreads = kW * kR1;   // one radix-R2 butterfly per thread
+constexpr int kThreads = kW * kR1;   // y-FFTs: one radix-R2 butterfly per thread
+// z-pass: 160 threads, so its steps A and C (16 R2 radix-8 items) take two
+// rounds for R2 <= 19 instead of three; step B uses the first 128
+constexpr int kThreadsZ = 160;
+template <int KIND>
+__host__ __device__ constexpr int threads_of() { return KIND >= 2 ? kThreadsZ : kThreads; }
 
 constexpr size_t a16(size_t b) { return (b + 15) & ~(size_t)15; }
 constexpr size_t a1k(size_t b) { return (b + 1023) & ~(size_t)1023; }
@@ -103,7 +108,7 @@ __device__ __forceinline__ float rcp_approx(float x) {
 // Tile t -> (x-tile fastest, then the outer index o): y-pass o = z + pz*b
 // (3D map {px, py, pz*nb}), z-pass o = y + py*b (4D map {px, py, pz, nb}).
 template <int R2, int KIND>
-__global__ void __launch_bounds__(kThreads, KIND >= 2 ? 5 : 3)
+__global__ void __launch_bounds__(threads_of<KIND>(), KIND >= 2 ? (R2 <= 19 ? 5 : 4) : 3)
     cols_pipe_kernel(const __grid_constant__ CUtensorMap map, const BornArgs a, const int jj,
                      const float2* __restrict__ twg, const int nxt, const int ntiles,
                      int* __restrict__ fault) {
@@ -111,6 +116,7 @@ __global__ void __launch_bounds__(kThreads, KIND >= 2 ? 5 : 3)
   constexpr int N = kR1 * R2;
   constexpr bool kZ = KIND >= 2;
   constexpr bool k16 = KIND == 3;
+  constexpr int kT = threads_of<KIND>();
   constexpr bool kInvFirst = KIND == 1;  // direction of the first transform
   using L = ColSmem<N>;
   extern __shared__ __align__(128) unsigned char sm[];
@@ -129,7 +135,7 @@ __global__ void __launch_bounds__(kThreads, KIND >= 2 ? 5 : 3)
     return;
   }
 
-  for (int i = tid; i < N; i += kThreads) {
+  for (int i = tid; i < N; i += kT) {
     tw[i] = twg[i];
     if (kZ) kz[i] = a.kq2[2][flip ? (i == 0 ? 0 : N - i) : i];
   }
@@ -180,7 +186,7 @@ __global__ void __launch_bounds__(kThreads, KIND >= 2 ? 5 : 3)
     // k16: the two exponents per row of a tile (blocks x0 .. x0+7 and
     // x0+8 .. x0+15), loaded one tile ahead into registers and stored to the
     // next stage's exponent buffer after this tile's last step
-    constexpr int kExPer = (2 * N + kThreads - 1) / kThreads;
+    constexpr int kExPer = (2 * N + kT - 1) / kT;
     signed char exn[k16 ? kExPer : 1];
     auto ex_load = [&](int t, signed char* dst_regs, signed char* dst_smem) {
       const int txt = t % nxt, to = t / nxt;
@@ -189,7 +195,7 @@ __global__ void __launch_bounds__(kThreads, KIND >= 2 ? 5 : 3)
       const long long es = ((long long)a.px * a.py) >> 3;
 #pragma unroll
       for (int q = 0; q < kExPer; ++q) {
-        const int i = tid + q * kThreads;
+        const int i = tid + q * kT;
         const int row = i >> 1, h = i & 1;
         signed char e = 0;
         if (i < 2 * N && (h == 0 || tx0 + 8 < a.px)) e = a.Te[e0 + row * es + h];
@@ -232,7 +238,7 @@ __global__ void __launch_bounds__(kThreads, KIND >= 2 ? 5 : 3)
       //      multiply, inverse R2-point DFT, times conj W_N^(n2 k1)
       //   C  inverse 8-point DFT over k1 -> rows R2 n1 + n2 of T
       float2* const Wt = k16 ? w16 : S;   // the tile the steps work on
-      for (int idx = tid; idx < kW * R2; idx += kThreads) {
+      for (int idx = tid; idx < kW * R2; idx += kT) {
         const int n2 = idx >> 4;  // column c is idx & 15 == tid & 15
         float2 v[kR1];
         if constexpr (k16) {
@@ -253,7 +259,7 @@ __global__ void __launch_bounds__(kThreads, KIND >= 2 ? 5 : 3)
         for (int r = 0; r < kR1; ++r) Wt[(R2 * r + n2) * kW + c] = v[r];
       }
       __syncthreads();
-      {
+      if (tid < kW * kR1) {   // step B: (column, k1) items on the first 128 threads
         const int k1 = jr;   // tid >> 4
         float2 v[R2];
 #pragma unroll
@@ -275,7 +281,7 @@ __global__ void __launch_bounds__(kThreads, KIND >= 2 ? 5 : 3)
         for (int r = 0; r < R2; ++r) Wt[(R2 * k1 + r) * kW + c] = v[r];
       }
       __syncthreads();
-      for (int idx = tid; idx < kW * R2; idx += kThreads) {
+      for (int idx = tid; idx < kW * R2; idx += kT) {
         const int n2 = idx >> 4;
         float2 v[kR1];
 #pragma unroll
@@ -304,7 +310,7 @@ __global__ void __launch_bounds__(kThreads, KIND >= 2 ? 5 : 3)
           signed char* nx = ex16 + (s ^ 1) * L::kExStage;
 #pragma unroll
           for (int q = 0; q < kExPer; ++q) {
-            const int i = tid + q * kThreads;
+            const int i = tid + q * kT;
             if (i < 2 * N) nx[i] = exn[q];
           }
         }
@@ -422,12 +428,13 @@ cudaError_t launch_kind(const BornArgs& a, int jj, const DevFft& f, int* fault, 
   const long long nout = KIND >= 2 ? (long long)a.py * a.nbatch : (long long)a.pz * a.nbatch;
   const long long ntiles = nout * nxt;
   int per_sm = 0;   // resident CTAs per SM (shared memory and registers allowing)
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cols_pipe_kernel<R2, KIND>, kThreads, smem);
+  constexpr int nthr = threads_of<KIND>();
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cols_pipe_kernel<R2, KIND>, nthr, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   const long long cap = (long long)per_sm * nsm;
   const int grid = (int)(ntiles < cap ? ntiles : cap);
-  cols_pipe_kernel<R2, KIND><<<grid, kThreads, smem, s>>>(map, a, jj, f.tw, nxt, (int)ntiles, fault);
+  cols_pipe_kernel<R2, KIND><<<grid, nthr, smem, s>>>(map, a, jj, f.tw, nxt, (int)ntiles, fault);
   return cudaGetLastError();
 }
 

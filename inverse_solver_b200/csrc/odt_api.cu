@@ -21,6 +21,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 #include "../../include/odt.h"
@@ -1308,6 +1309,105 @@ odt_status odt_get_batch(odt_handle h, int32_t* batch) {
     auto H = lookup(h);
     if (!batch) raise(ODT_ERR_INVALID_ARGUMENT, "odt_get_batch: NULL");
     *batch = H->batch;
+  });
+}
+
+namespace {
+// process-wide plan choices of odt_autotune
+struct TuneKey {
+  int dev, px, py, pz, nb, np, storage;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(dev, px, py, pz, nb, np, storage) < std::tie(o.dev, o.px, o.py, o.pz, o.nb, o.np, o.storage);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, odt_tune_result> g_tune;
+}  // namespace
+
+odt_status odt_autotune(odt_handle h, int32_t n_ill, odt_tune_result* out) {
+  return guarded([&] {
+    auto H = lookup(h);
+    if (!out) raise(ODT_ERR_INVALID_ARGUMENT, "odt_autotune: NULL result");
+    if (n_ill < 1) raise(ODT_ERR_INVALID_ARGUMENT, "odt_autotune: n_ill < 1");
+    if (!H->pot[0].have) raise(ODT_ERR_NOT_READY, "odt_autotune: call odt_set_potential first");
+    if (H->np == 3 && !H->have_pol) raise(ODT_ERR_NOT_READY, "odt_autotune: set the polarisation basis first");
+    DeviceGuard dg(H->g.device);
+    const int nb = std::min<int>(n_ill, auto_batch(*H));
+    ensure_batch(*H, nb);
+    const TuneKey key{H->g.device, H->g.sim_size[0], H->g.sim_size[1], H->g.sim_size[2], nb, H->np, H->storage};
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tune.find(key);
+      if (it != g_tune.end()) {
+        *out = it->second;
+        out->cached = 1;
+        H->drop_graphs();
+        H->use_xy = out->fused_xy != 0;
+        H->use_pipe = out->pipelined != 0;
+        return;
+      }
+    }
+    // plane-wave inputs (ones) in the batch's input planes
+    const size_t nin = (size_t)H->nf() * H->npol * nb;
+    std::vector<float2> ones(nin, make_float2(1.f, 0.f));
+    cudaStream_t s = H->own_stream;
+    ODT_CUDA(cudaMemcpyAsync(H->in2d, ones.data(), nin * sizeof(float2), cudaMemcpyHostToDevice, s));
+    BornArgs probe{};
+    probe.px = H->g.sim_size[0];
+    probe.py = H->g.sim_size[1];
+    probe.pz = H->g.sim_size[2];
+    probe.nbatch = nb * H->np;
+    const bool xy_ok = H->np == 1 && !H->pot[0].tensor && born_xy_supported(probe, H->max_smem);
+    const bool saved_xy = H->use_xy, saved_pipe = H->use_pipe;
+    const bool want_t = H->ktrans != nullptr;
+    cudaEvent_t e0, e1;
+    ODT_CUDA(cudaEventCreate(&e0));
+    ODT_CUDA(cudaEventCreate(&e1));
+    odt_tune_result r{};
+    r.batch = nb;
+    int best = -1;
+    const bool plan_xy[3] = {true, false, false}, plan_pipe[3] = {true, true, false};
+    for (int c = 0; c < 3; ++c) {
+      r.ms[c] = -1.0;
+      if (c == 0 && !xy_ok) continue;
+      if (H->storage == ODT_STORAGE_B16 && c != 0) continue;   // 16-bit storage runs on the fused pass only
+      H->use_xy = plan_xy[c];
+      H->use_pipe = plan_pipe[c];
+      H->drop_graphs();
+      try {
+        run_chunk(*H, nb, s, want_t, false, 0, H->fout);   // warm-up (kernel attributes, caches)
+        ODT_CUDA(cudaEventRecord(e0, s));
+        for (int k = 0; k < 2; ++k) run_chunk(*H, nb, s, want_t, false, 0, H->fout);
+        ODT_CUDA(cudaEventRecord(e1, s));
+        ODT_CUDA(cudaEventSynchronize(e1));
+        check_fault(*H);
+      } catch (const ApiError&) {   // a plan that cannot run here is skipped
+        ODT_CUDA(cudaStreamSynchronize(s));
+        continue;
+      }
+      float ms = 0.f;
+      ODT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      r.ms[c] = ms / 2.0;
+      if (best < 0 || r.ms[c] < r.ms[best]) best = c;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    H->drop_graphs();
+    if (best < 0) {
+      H->use_xy = saved_xy;
+      H->use_pipe = saved_pipe;
+      raise(ODT_ERR_UNSUPPORTED, "odt_autotune: no plan applies to this handle");
+    }
+    H->use_xy = plan_xy[best];
+    H->use_pipe = plan_pipe[best];
+    r.fused_xy = plan_xy[best] ? 1 : 0;
+    r.pipelined = plan_pipe[best] ? 1 : 0;
+    r.cached = 0;
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      g_tune[key] = r;
+    }
+    *out = r;
   });
 }
 

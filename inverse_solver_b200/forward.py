@@ -632,6 +632,20 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
         _lib.check(self.lib.odt_set_field_storage(self._handle, modes[storage]))
         self.parameters["field_storage"] = storage
 
+    def autotune(self, n_ill=None):
+        """Time the execution plans that apply to this geometry (fused xy-pass,
+        separate pipelined passes, generic tile kernels) on one solve of
+        n_ill plane waves (default: the batch) with the current potential,
+        keep the fastest (odt_autotune; cached process-wide per shape) and
+        return {"plan", "batch", "cached", "ms": {plan: ms per solve}}."""
+        r = _lib.TuneResult()
+        n = int(n_ill) if n_ill else max(1, int(self.batch()) or int(self.parameters.get("max_batch") or 16))
+        _lib.check(self.lib.odt_autotune(self._handle, n, C.byref(r)))
+        names = ("fused_xy", "separate_pipelined", "generic")
+        plan = "fused_xy" if r.fused_xy else ("separate_pipelined" if r.pipelined else "generic")
+        return {"plan": plan, "batch": r.batch, "cached": bool(r.cached),
+                "ms": {nm: r.ms[i] for i, nm in enumerate(names) if r.ms[i] >= 0}}
+
     def set_profiling(self, on: bool):
         _lib.check(self.lib.odt_set_profiling(self._handle, 1 if on else 0))
 

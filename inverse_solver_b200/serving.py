@@ -53,8 +53,8 @@ def geometry_key(p):
     return tuple((k, repr(p.get(k))) for k in keys)
 
 
-def solver_bytes(p, n_ill):
-    """Device memory of one solver with a batch of min(n_ill, 16)
+def solver_bytes(p, n_ill, max_batch=16):
+    """Device memory of one solver with a batch of min(n_ill, max_batch)
     illuminations, estimated from the buffer layout of libodt (complex64):
     Green's / refocusing kernels 3 x conv-plane x z, V, and per illumination
     the Born state (3 x padded grid, or the conv volume if larger), the 3D
@@ -69,7 +69,7 @@ def solver_bytes(p, n_ill):
     nc2 = (2 * size[0]) * (2 * size[1])
     nc3 = nc2 * size[2]
     comp = 3 if p.get("vector_simulation", False) else 1
-    nb = min(int(n_ill), 16)
+    nb = min(int(n_ill), int(max_batch))
     static = 8 * (3 * nc3 + nvox)
     per = 8 * comp * (max(3 * nvox, nc3) + 2 * nri + 4 * nf + 2 * nc2)
     return static + nb * per
@@ -81,7 +81,7 @@ class SolveServer:
     may be replaced (the tests drive the scheduler with stand-ins); the
     defaults run the request on libodt."""
 
-    def __init__(self, budget_bytes=None, slots=4, execute=None, estimate=None):
+    def __init__(self, budget_bytes=None, slots=4, execute=None, estimate=None, max_batch=16, autotune=True):
         if budget_bytes is None:
             import torch
 
@@ -89,6 +89,9 @@ class SolveServer:
             budget_bytes = int(free * 0.8)
         self.budget = float(budget_bytes)
         self.slots = int(slots)
+        self.max_batch = int(max_batch)
+        self.autotune = bool(autotune)   # pick each new solver's execution plan by timing (odt_autotune)
+        self.plans = {}                  # geometry key -> the tuned plan
         self.execute = execute or self._execute
         self.estimate = estimate or self._estimate
         self._cv = threading.Condition()
@@ -203,9 +206,9 @@ class SolveServer:
     # ------------------------------------------------------------ execution
     def _estimate(self, req):
         if isinstance(req, ForwardRequest):
-            return solver_bytes(req.params, req.fields.shape[3])
+            return solver_bytes(req.params, req.fields.shape[3], self.max_batch)
         fp = req.params["forward_solver_parameters"]
-        return solver_bytes(fp, req.fields_in.shape[3])
+        return solver_bytes(fp, req.fields_in.shape[3], self.max_batch)
 
     def _acquire(self, p, need):
         """An idle solver of this geometry, or a new one; idle solvers of
@@ -227,8 +230,10 @@ class SolveServer:
                 self._held -= b
             self._held += need
         q = copy.deepcopy(p)
-        q["max_batch"] = 16
-        return key, FORWARD_SOLVER_CONVERGENT_BORN(q), need
+        q["max_batch"] = self.max_batch
+        s = FORWARD_SOLVER_CONVERGENT_BORN(q)
+        s._needs_tune = self.autotune
+        return key, s, need
 
     def _release(self, key, s, b):
         with self._pool_lock:
@@ -241,6 +246,9 @@ class SolveServer:
             key, s, b = self._acquire(req.params, need)
             try:
                 set_ri_on_device(s, req.RI)
+                if getattr(s, "_needs_tune", False):   # once per solver, after its first potential
+                    s._needs_tune = False
+                    self.plans[key] = s.autotune(min(req.fields.shape[3], self.max_batch))
                 return s.solve(req.fields)
             finally:
                 self._release(key, s, b)
@@ -380,6 +388,57 @@ def run_stream(reqs, rate_per_s, seed, budget_bytes=None, slots=4, srv=None):
     return res, st
 
 
+CONFIG4_SIZES = ((64, 64, 64), (96, 96, 64), (128, 128, 128), (192, 192, 96))
+
+
+def run_config4(a):
+    """Config 4: the seeded uneven batch through the request loop (all
+    requests at once, one resident solver per shape, its plan picked by
+    odt_autotune, up to 64 illuminations per launch, the shapes' solves
+    overlapping on the device), against the same solves one at a time with a
+    fresh default solver each.  Prints one JSON line with voxel-iter/s of
+    both, the plans chosen and the clocks."""
+    import json
+
+    from .clocks import ClockSampler
+    from .forward import CBSHostSetup
+
+    n = a.requests if a.requests != 24 else 256
+    reqs = make_mix(n, a.seed, sizes=CONFIG4_SIZES, max_ill=64, recon_every=0)
+    vox = 0
+    for r in reqs:
+        h = CBSHostSetup(r.params)
+        h.prepare_potential(r.RI)
+        vox += h.voxel_iterations(r.fields.shape[3])
+    server = SolveServer(slots=a.slots, max_batch=64)
+    first = {}
+    for r in reqs:   # one request of each shape makes its solver resident and tunes it
+        first.setdefault(geometry_key(r.params), r)
+    run_stream(list(first.values()), float("inf"), a.seed, srv=server)
+    clk = ClockSampler(a.device)
+    clk.start()
+    _, st = run_stream(reqs, float("inf"), a.seed + 1, srv=server)
+    st["clocks"] = clk.stop()
+    plans = {"x".join(str(v) for v in dict(k)["size"].strip("[]").split(", ")): pl
+             for k, pl in server.plans.items()} if server.plans else {}
+    server.close()
+    serial = one_at_a_time(reqs[: max(8, n // 8)])
+    serial_vox = 0
+    for r in reqs[: max(8, n // 8)]:
+        h = CBSHostSetup(r.params)
+        h.prepare_potential(r.RI)
+        serial_vox += h.voxel_iterations(r.fields.shape[3])
+    span = st["requests"] / st["throughput_per_s"]
+    out = {"workload": f"config 4: {n} seeded forward solves over 64^3 / 96x96x64 / 128^3 / 192x192x96, "
+                       "1-64 illuminations", "requests": n, "voxel_iterations": vox, "seconds": span,
+           "voxel_iter_per_s": vox / span,
+           "one_at_a_time_voxel_iter_per_s": serial_vox / serial,
+           "one_at_a_time_sample": f"first {max(8, n // 8)} requests, fresh default solver each",
+           "speedup": (vox / span) / (serial_vox / serial), "plans": plans, "slots": a.slots,
+           "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "clocks": st["clocks"]}
+    print(json.dumps(out))
+
+
 def main():
     import argparse
     import json
@@ -400,8 +459,14 @@ def main():
     ap.add_argument("--load", type=float, default=0.7,
                     help="with --config5: arrival rate as a fraction of the measured capacity")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--config4", action="store_true",
+                    help="config 4: 256 seeded forward solves over 64^3 / 96x96x64 / 128^3 / 192x192x96 "
+                         "with 1-64 illuminations, submitted at once to resident, autotuned solvers "
+                         "(batches of up to 64 illuminations)")
     a = ap.parse_args()
     capacity = None
+    if a.config4:
+        return run_config4(a)
     if a.uneven:
         reqs = make_mix(a.requests, a.seed, sizes=((64, 64, 64), (96, 96, 64), (128, 128, 128),
                                                    (192, 192, 96)), max_ill=64, recon_every=0)
