@@ -82,6 +82,10 @@ struct XYSmem {
 // kernel carries none of the other cases' work)
 enum XYKind { kXYSteady = 0, kXYEarly = 1, kXYFinal = 2, kXYFirst = 3 };
 
+// (i c) * v for real c: (-c v.y, c v.x), two products (a complex product
+// with (0, c) would also form 0 * v.x and 0 * v.y)
+__device__ __forceinline__ float2 mul_i(float c, float2 v) { return make_float2(-(c * v.y), c * v.x); }
+
 #if defined(__CUDA_ARCH__)
 __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
@@ -92,15 +96,12 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
 // point (b16.cuh; T's blocks are 8 consecutive x of a row, Field_n's are the
 // values of one n1 in 8 consecutive step-4 work items of a warp, exponent
 // index plane * N^2/8 + n1 * R^2 + w * R + item / 8)
-// Registers per thread: all of the register file for the one CTA of 32 R
-// threads per SM (rounded down to the allocation granularity of 8), so that
-// the radix-R butterflies do not spill: 104 for R = 19.
-constexpr int xy_max_regs(int R) {
-  return ((65536 / (32 * R)) / 8) * 8 > 255 ? 255 : ((65536 / (32 * R)) / 8) * 8;
-}
-
+// __launch_bounds__ lets the compiler fit the R warps of the one CTA per SM
+// into the register file, which is split into four quarters of 16384
+// registers (one per warp scheduler): 19 warps put five warps on a quarter,
+// so at most 96 registers per thread for R = 19 (104 did not launch).
 template <int R, int KIND, int ST>
-__global__ void __maxnreg__(xy_max_regs(R))
+__global__ void __launch_bounds__(32 * R, 1)
     born_xy_kernel(const BornArgs a, const int jj, const float2* __restrict__ twg, const int nplanes) {
 #if defined(__CUDA_ARCH__)
   constexpr int N = 8 * R;
@@ -131,7 +132,6 @@ __global__ void __maxnreg__(xy_max_regs(R))
   const int e = jj - 1;                     // iteration whose update completes here
   const long long plane_n = (long long)N * N;
   const long long est = (long long)a.rx * a.ry * a.rz;
-  const float2 cc = make_float2(0.f, a.c_im);
   // Field_n / Field are read by the update from iteration 3 on (and Field by
   // the final pass of a 2-iteration series); the incident field by the
   // source of iteration 1 and 2 and by the final pass
@@ -225,7 +225,10 @@ __global__ void __maxnreg__(xy_max_regs(R))
       const bool yzroi = zroi && (unsigned)(y - a.ry0) < (unsigned)a.ry;
       const long long ebase = (long long)b * est + (long long)(y - a.ry0) * a.rx +
                               (long long)(z - a.rz0) * a.rx * a.ry - a.rx0;
-      const float my = myt[y];
+      // the row's factors of the separable mask and phase ramp (mask(x) my mz,
+      // ramp(x) ry rz: per element one product with the x factor)
+      const float myz = myt[y] * mz;
+      const float2 ryz = a.acyclic ? cmul(ryt[y], rz) : one;
       float2 V[8], Fo[8], Fp[8], Ei[8];
 #pragma unroll
       for (int r = 0; r < 8; ++r) {
@@ -261,14 +264,14 @@ __global__ void __maxnreg__(xy_max_regs(R))
       for (int r = 0; r < 8; ++r) {
         const int x = R * r + n2;
         const float2 Vr = V[r];
-        const float2 r0 = a.acyclic ? cmul(cmul(rxt[x], ryt[y]), rz) : one;
+        const float2 r0 = a.acyclic ? cmul(rxt[x], ryz) : one;
         const bool in_roi = yzroi && (unsigned)(x - a.rx0) < (unsigned)a.rx;
         float2 fn_new = z2, ftot = z2;
         if constexpr (kInv) {
           // PSI .* conj(phase ramp of iteration e)
           float2 P = v[r];
           if (a.acyclic) P = cmul(P, (e & 1) ? r0 : cconj(r0));
-          const float m = (mxt[x] * my) * mz;
+          const float m = mxt[x] * myz;
           const float2 vP = cmul(Vr, P);
           if (KIND != kXYSteady && e <= 2) {   // Field_n = (0 + V .* PSI) .* mask
             fn_new = cscale(vP, m);
@@ -282,7 +285,7 @@ __global__ void __maxnreg__(xy_max_regs(R))
           } else {
             const float2 fo = Fo[r];
             const float2 fp = Fp[r];
-            const float2 psi = cmul(cmul(cc, fo), Vr);
+            const float2 psi = cmul(mul_i(a.c_im, fo), Vr);
             const float2 fn = cscale(cadd(csub(fo, psi), vP), m);
             if (e == 3) {  // Field = (Field_n1 + Field_n2) + Field_n3; Field_n = Field_n3 + Field_n1
               ftot = cadd(cadd(fp, fo), fn);
@@ -302,9 +305,9 @@ __global__ void __maxnreg__(xy_max_regs(R))
         } else {
           float2 src;
           if (jj <= 2) {  // (1i/eps) .* ((V(ROI) + 1i*eps) .* E_inc) / 2 inside the ROI
-            src = in_roi ? cscale(cmul(cc, cmul(make_float2(Vr.x, Vr.y + a.eps), Ei[r])), 0.5f) : z2;
+            src = in_roi ? cscale(mul_i(a.c_im, cmul(make_float2(Vr.x, Vr.y + a.eps), Ei[r])), 0.5f) : z2;
           } else {        // (1i/eps) .* Field_n .* V
-            src = cmul(cmul(cc, fn_new), Vr);
+            src = cmul(mul_i(a.c_im, fn_new), Vr);
           }
           if (a.acyclic) src = cmul(src, (jj & 1) ? cconj(r0) : r0);
           v[r] = src;
@@ -401,6 +404,10 @@ cudaError_t launch_r(const BornArgs& a, int jj, const float2* tw, cudaStream_t s
   int nsm = 0;
   e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
+  int per_sm = 0;   // the kernel needs one resident CTA per SM
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, born_xy_kernel<R, KIND, ST>, 32 * R, L::kTotal);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorLaunchOutOfResources;
   const long long nplanes = (long long)a.pz * a.nbatch;
   const int grid = (int)(nplanes < nsm ? nplanes : nsm);
   born_xy_kernel<R, KIND, ST><<<grid, 32 * R, L::kTotal, s>>>(a, jj, tw, (int)nplanes);

@@ -145,6 +145,43 @@ struct Butterfly<12, INV> {
   }
 };
 
+// cos(2 pi t / R) and sin(2 pi t / R) at compile time, in double: the angle
+// reduced to [-pi, pi] and Taylor series of 26 terms (the largest term is
+// below 2^3, so the result is within a few units of 1e-16), rounded to float
+// once -- the values the double-precision twiddle tables hold.
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+constexpr double ce_sin_red(double x) {
+  double term = x, sum = x;
+  for (int k = 1; k < 26; ++k) {
+    term *= -x * x / ((2.0 * k) * (2.0 * k + 1.0));
+    sum += term;
+  }
+  return sum;
+}
+constexpr double ce_cos_red(double x) {
+  double term = 1.0, sum = 1.0;
+  for (int k = 1; k < 26; ++k) {
+    term *= -x * x / ((2.0 * k - 1.0) * (2.0 * k));
+    sum += term;
+  }
+  return sum;
+}
+constexpr double ce_angle(int t, int R) {   // 2 pi t / R reduced to [-pi, pi]
+  const int u = ((t % R) + R) % R;
+  return 2 * u > R ? kTwoPi * (double)(u - R) / (double)R : kTwoPi * (double)u / (double)R;
+}
+template <int R>
+struct UnitRoots {   // cos / sin of 2 pi t / R, t < R, as float
+  float c[R];
+  float s[R];
+  constexpr UnitRoots() : c(), s() {
+    for (int t = 0; t < R; ++t) {
+      c[t] = (float)ce_cos_red(ce_angle(t, R));
+      s[t] = (float)ce_sin_red(ce_angle(t, R));
+    }
+  }
+};
+
 // Odd R: X[k] = v0 + sum_m a_m cos(2 pi m k / R) -/+ i sum_m b_m sin(2 pi m k / R)
 // with a_m = v[m] + v[R-m], b_m = v[m] - v[R-m]; the cosines and sines are
 // read from the transform's table at multiples of n / R.
@@ -152,15 +189,16 @@ template <int R, bool INV>
 struct OddButterfly {
   ODT_HD static void run(float2* v, const float2* tw, int n) {
     constexpr int H = (R - 1) / 2;
-    const int step = n / R;
+    constexpr UnitRoots<R> ur{};   // compile-time coefficients (no table loads)
+    (void)tw;
+    (void)n;
     float cs[H + 1], sn[H + 1];
     cs[0] = 1.f;  // m*k can be a multiple of R when R is composite (9, 15, ...)
     sn[0] = 0.f;
 #pragma unroll
     for (int t = 1; t <= H; ++t) {
-      float2 w = tw[t * step];  // exp(-2 pi i t / R)
-      cs[t] = w.x;
-      sn[t] = -w.y;
+      cs[t] = ur.c[t];   // exp(-2 pi i t / R) = cs - i sn
+      sn[t] = ur.s[t];
     }
     float2 a[H + 1], b[H + 1];
     float2 x0 = v[0];
