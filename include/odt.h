@@ -632,6 +632,26 @@ typedef struct odt_unwrap_args {
 
 odt_status odt_unwrap_goldstein(const odt_unwrap_args* args);
 
+/*
+ * odt_solve_source -- CudaBorn's action 2 (CUDA_CODE/main.cpp:139-163:
+ * set_source_3D, execute, get_field_3D): the Born series driven by a given
+ * 3D incident field instead of a 2D input field.  source holds n incident
+ * fields over the RI grid ([RI_x, RI_y, RI_z, n] complex, column-major;
+ * [RI_x, RI_y, RI_z, 3, n] on dyadic handles), as the input stage of
+ * odt_solve would form them (the refocused input, :543-554); field3d
+ * receives Field(ROI) + the incident field, as odt_solve's field3d.  No
+ * transmitted / reflected fields.  Memory / stream as odt_solve.
+ */
+typedef struct odt_source_args {
+  const odt_cfloat* source;   /* [RI_x, RI_y, RI_z, (3,) n]                 */
+  int32_t n;
+  odt_cfloat* field3d;        /* [RI_x, RI_y, RI_z, (3,) n]                 */
+  int32_t memory;             /* ODT_MEM_HOST or ODT_MEM_DEVICE            */
+  void* stream;
+} odt_source_args;
+
+odt_status odt_solve_source(odt_handle h, const odt_source_args* args);
+
 /* Free a solver (CudaBorn action 3, main.cpp:164-174). */
 odt_status odt_destroy(odt_handle h);
 

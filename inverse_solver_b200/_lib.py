@@ -265,6 +265,16 @@ class HankelArgs(C.Structure):
     ]
 
 
+class SourceArgs(C.Structure):
+    _fields_ = [
+        ("source", C.c_void_p),
+        ("n", C.c_int32),
+        ("field3d", C.c_void_p),
+        ("memory", C.c_int32),
+        ("stream", C.c_void_p),
+    ]
+
+
 class TuneResult(C.Structure):
     _fields_ = [
         ("fused_xy", C.c_int32),
@@ -374,6 +384,7 @@ SIGNATURES = {
     "odt_set_field_storage": (C.c_int, [C.c_uint32, C.c_int32]),
     "odt_hankel_filter": (C.c_int, [C.POINTER(HankelArgs)]),
     "odt_autotune": (C.c_int, [C.c_uint32, C.c_int32, C.POINTER(TuneResult)]),
+    "odt_solve_source": (C.c_int, [C.c_uint32, C.POINTER(SourceArgs)]),
     "odt_get_kernel_times": (C.c_int, [C.c_uint32, C.POINTER(C.c_char_p),
                                        C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                        C.c_int32, C.POINTER(C.c_int32)]),

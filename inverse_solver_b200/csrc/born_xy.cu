@@ -37,15 +37,15 @@
 //   7 y-F2 + F3        write T to global
 // One CTA per SM (the plane takes 8 N^2 bytes: 185 KB for N = 152) with 32 R
 // threads -- R warps -- persistent over the planes (illumination fastest, so
-// concurrent CTAs share V's planes in L2).  Steps 2-6 touch, for one n2, only
+// concurrent CTAs share V's planes in L2; prefetching the next plane's T,
+// Field_n and Field into L2 with cp.async.bulk.prefetch made a step 5.4 ms
+// slower, so there is none).  Steps 2-6 touch, for one n2, only
 // the 8 rows R n1 + n2 (step 2 and 6 combine exactly those rows, steps 3-5
 // work along rows), so warp w takes n2 = w and runs steps 2-6 on its own rows
 // with warp-level synchronisation only; step 7 of a plane and step 1 of the
 // next touch the same rows per item (see step1 below), so a plane needs two
 // CTA barriers (after steps 1 and 6), and the warps drift apart so that one
-// warp's global loads overlap other warps' transforms.  The next plane's T and Field_n / Field are
-// prefetched into L2 (cp.async.bulk.prefetch) during steps 4 and 6 of the
-// current one, so their DRAM reads overlap the shared-memory steps.
+// warp's global loads overlap other warps' transforms.
 //
 // Bank conflicts: rows have a pitch of N = 8 (mod 16) complex elements for
 // odd R (N = 96: 0 mod 16, two-way conflicts in steps 3 and 5).
@@ -85,12 +85,6 @@ enum XYKind { kXYSteady = 0, kXYEarly = 1, kXYFinal = 2, kXYFirst = 3 };
 // (i c) * v for real c: (-c v.y, c v.x), two products (a complex product
 // with (0, c) would also form 0 * v.x and 0 * v.y)
 __device__ __forceinline__ float2 mul_i(float c, float2 v) { return make_float2(-(c * v.y), c * v.x); }
-
-#if defined(__CUDA_ARCH__)
-__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-#endif
 
 // ST: storage of T and Field_n, 0 = complex64, 1 = 16-bit block floating
 // point (b16.cuh; T's blocks are 8 consecutive x of a row, Field_n's are the
@@ -206,10 +200,6 @@ __global__ void __launch_bounds__(32 * R, 1)
         for (int r = 0; r < R; ++r) row[r] = v[r];
       }
       __syncwarp();
-    }
-    if (kInv && tid == 0 && gn >= 0) {
-      if constexpr (ST == 0) prefetch_l2(a.T + gn, (uint32_t)(plane_n * sizeof(float2)));
-      else prefetch_l2(a.T16 + gn, (uint32_t)(plane_n * sizeof(short2)));
     }
 
     // ---- 4: x-F1^-1 -> update of iteration jj-1 and source of jj -> x-F1, on
@@ -339,11 +329,6 @@ __global__ void __launch_bounds__(32 * R, 1)
       for (int r = 0; r < R; ++r) row[r] = v[r];
     }
     __syncwarp();
-    if (tid == 0 && gn >= 0 && need_fn) {
-      if constexpr (ST == 0) prefetch_l2(a.Fn + gn, (uint32_t)(plane_n * sizeof(float2)));
-      else prefetch_l2(a.Fn16 + gn, (uint32_t)(plane_n * sizeof(short2)));
-      prefetch_l2(a.F + gn, (uint32_t)(plane_n * sizeof(float2)));
-    }
     // ---- 6: y-F1 (8-point over n1 at the warp's rows R n1 + w)
     for (int x = lane; x < N; x += 32) {
       float2 v[8];

@@ -211,6 +211,11 @@ cudaError_t launch_grad_accumulate(const float2* E, const float2* A, float2* acc
 cudaError_t launch_grad_finalize(const float2* acc, float2* grad, long long n, float n_ill,
                                  cudaStream_t s);
 
+// Raise `kernel`'s dynamic shared-memory limit (when `bytes` needs more than
+// the default 48 KB) to the device's opt-in maximum, once per kernel and
+// device; thread-safe (smem_attr.cu)
+cudaError_t raise_smem_limit(const void* kernel, size_t bytes);
+
 // shared-memory bytes a tile kernel of `kind` needs for length n and W pencils
 size_t fft_smem_bytes(int n, int W, int kind);
 

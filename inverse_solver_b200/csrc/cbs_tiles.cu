@@ -57,8 +57,7 @@ fft_cols_kernel(const float2* in, float2* out, long long n0, int in_shift, int o
 
 template <typename K>
 cudaError_t set_smem(K kernel, size_t bytes) {
-  if (bytes <= 48 * 1024) return cudaSuccess;
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  return raise_smem_limit(reinterpret_cast<const void*>(kernel), bytes);
 }
 
 }  // namespace

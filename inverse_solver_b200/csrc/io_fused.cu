@@ -389,8 +389,7 @@ emit_cols_reduce_kernel(const float2* __restrict__ mid, const float2* __restrict
 
 template <typename K>
 cudaError_t raise_smem(K kernel, size_t bytes) {
-  if (bytes <= 48 * 1024) return cudaSuccess;
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  return raise_smem_limit(reinterpret_cast<const void*>(kernel), bytes);
 }
 
 }  // namespace

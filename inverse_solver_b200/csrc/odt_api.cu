@@ -415,8 +415,11 @@ void check_fault(Handle& H) {
   }
 }
 
+// from_source: the batch's incident fields over the RI grid are already in
+// H.einc (odt_solve_source, CudaBorn's action 2): no input stage, and no
+// output projection (want_t / want_r must be false)
 void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int slot,
-               float2* fout) {
+               float2* fout, bool from_source = false) {
   const Handle::PotSlot& P = H.pot[slot];
   const odt_geometry& g = H.g;
   const int Fx = g.field_size[0], Fy = g.field_size[1];
@@ -434,6 +437,17 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
   //      illumination from there on
   const bool vec = H.np == 3;
   const long long nbp = (long long)nb * H.np;
+  if (from_source) want_t = want_r = false;
+  // fused refocus / inverse 2D FFT / crop (io_fused.cu) where its tiles fit;
+  // the unfused chain is kept for ODT_KERNELS=generic
+  const int nacc = (want_t ? 1 : 0) + (want_r ? 1 : 0);
+  const IoGeom gin{Cx, Cy, Rx, Ry, Rz, ocx, ocy, nbp}, gout{Cx, Cy, Rx, Ry, Rz, orx, ory, nbp};
+  const bool io_fused = H.use_pipe && io_fused_fits(gin, H.fcx, H.fcy, nacc, H.max_smem) &&
+                        io_fused_fits(gout, H.fcx, H.fcy, nacc, H.max_smem);
+  // an RI tensor couples the field components in the emitter: unfused output
+  const bool ten = P.tensor;
+  const bool io_out_fused = io_fused && !ten;
+  if (!from_source) {
   fftc2(H, H.in2d, H.ffx, H.ffy, (long long)nb * H.npol, false, s);
   H.mark_begin(kKIoElem, s);
   ODT_CUDA(launch_mul_plane(H.in2d, H.in2d, vec ? nullptr : H.kin, H.pupil_in, nF, nF * nb * H.npol, s));
@@ -445,15 +459,6 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
   ODT_CUDA(launch_pad2d(src2, H.c2a, Fx, Fy, Cx, Cy, ocx, ocy, nbp, s));
   H.mark_end(s);
   fftc2(H, H.c2a, H.fcx, H.fcy, nbp, false, s);
-  // fused refocus / inverse 2D FFT / crop (io_fused.cu) where its tiles fit;
-  // the unfused chain is kept for ODT_KERNELS=generic
-  const int nacc = (want_t ? 1 : 0) + (want_r ? 1 : 0);
-  const IoGeom gin{Cx, Cy, Rx, Ry, Rz, ocx, ocy, nbp}, gout{Cx, Cy, Rx, Ry, Rz, orx, ory, nbp};
-  const bool io_fused = H.use_pipe && io_fused_fits(gin, H.fcx, H.fcy, nacc, H.max_smem) &&
-                        io_fused_fits(gout, H.fcx, H.fcy, nacc, H.max_smem);
-  // an RI tensor couples the field components in the emitter: unfused output
-  const bool ten = P.tensor;
-  const bool io_out_fused = io_fused && !ten;
   if (io_fused) {
     H.mark_begin(kKIoFft, s);
     ODT_CUDA(launch_refocus_in(H.c2a, H.refocus, conv, H.einc, gin, H.fcx, H.fcy, s));
@@ -467,6 +472,7 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
     ODT_CUDA(launch_crop_volume(conv, H.einc, Cx, Cy, Rx, Ry, Rz, ocx, ocy, nbp, s));
     H.mark_end(s);
   }
+  }  // !from_source
 
   // ---- Born series (:577-647)
   BornArgs a{};
@@ -1036,6 +1042,45 @@ odt_status odt_solve(odt_handle h, const odt_solve_args* args) {
   });
 }
 
+odt_status odt_solve_source(odt_handle h, const odt_source_args* args) {
+  return guarded([&] {
+    auto H = lookup(h);
+    if (!args) raise(ODT_ERR_INVALID_ARGUMENT, "odt_solve_source: NULL args");
+    if (!H->pot[0].have) raise(ODT_ERR_NOT_READY, "odt_solve_source: call odt_set_potential first");
+    const odt_source_args& A = *args;
+    if (A.n < 0) raise(ODT_ERR_INVALID_ARGUMENT, "odt_solve_source: n < 0");
+    if (A.n == 0) return;
+    if (!A.source || !A.field3d) raise(ODT_ERR_INVALID_ARGUMENT, "odt_solve_source: NULL source or field3d");
+    if (A.memory != ODT_MEM_HOST && A.memory != ODT_MEM_DEVICE)
+      raise(ODT_ERR_INVALID_ARGUMENT, "odt_solve_source: memory must be ODT_MEM_HOST or ODT_MEM_DEVICE");
+    if (H->np == 3 && !H->have_pol)
+      raise(ODT_ERR_NOT_READY, "odt_solve_source: a dyadic handle needs odt_set_polarisation first");
+    DeviceGuard dg(H->g.device);
+    const bool dev = A.memory == ODT_MEM_DEVICE;
+    if (dev && (!is_device_ptr(A.source) || !is_device_ptr(A.field3d)))
+      raise(ODT_ERR_INVALID_ARGUMENT, "odt_solve_source: ODT_MEM_DEVICE with a non-device pointer");
+    cudaStream_t s = dev ? (cudaStream_t)A.stream : H->own_stream;
+    ensure_batch(*H, std::min<int>(A.n, auto_batch(*H)));
+    const cudaMemcpyKind kin = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const cudaMemcpyKind kout = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    const long long nR = H->nri() * H->np;   // complex values per source / field
+    for (int b0 = 0; b0 < A.n; b0 += H->batch) {
+      const int nb = std::min(H->batch, A.n - b0);
+      ODT_CUDA(cudaMemcpyAsync(H->einc, A.source + (size_t)b0 * nR, (size_t)nb * nR * sizeof(float2), kin, s));
+      run_chunk(*H, nb, s, false, false, 0, H->fout, true);
+      ODT_CUDA(cudaMemcpyAsync(A.field3d + (size_t)b0 * nR, H->fout, (size_t)nb * nR * sizeof(float2), kout, s));
+      if (!dev) ODT_CUDA(cudaStreamSynchronize(s));
+      H->collect(s);
+    }
+    if (dev) {
+      ODT_CUDA(cudaEventRecord(H->done_ev, s));
+      H->done_pending = true;
+    } else {
+      check_fault(*H);
+    }
+  });
+}
+
 odt_status odt_gradient(odt_handle h, const odt_gradient_args* args) {
   return guarded([&] {
     auto H = lookup(h);
@@ -1382,6 +1427,10 @@ odt_status odt_autotune(odt_handle h, int32_t n_ill, odt_tune_result* out) {
         ODT_CUDA(cudaEventSynchronize(e1));
         check_fault(*H);
       } catch (const ApiError&) {   // a plan that cannot run here is skipped
+        ODT_CUDA(cudaStreamSynchronize(s));
+        continue;
+      } catch (const CudaError&) {  // e.g. a launch that does not fit: the context is intact
+        cudaGetLastError();
         ODT_CUDA(cudaStreamSynchronize(s));
         continue;
       }

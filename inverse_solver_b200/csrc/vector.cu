@@ -361,7 +361,7 @@ cudaError_t launch_born_z_dyadic(const BornArgs& a, const DyadArgs& d, int jj, c
   switch (fz.plan.rclass) {
 #define ODT_DYAD_CASE(C)                                                                                \
   case C:                                                                                              \
-    e = cudaFuncSetAttribute(born_z_dyadic_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
+    e = raise_smem_limit(reinterpret_cast<const void*>(born_z_dyadic_kernel<C>), sm);                  \
     if (e != cudaSuccess) return e;                                                                    \
     born_z_dyadic_kernel<C><<<blocks, 128, sm, s>>>(a, d, jj, fz.plan, fz.tw, lgW);                    \
     break;

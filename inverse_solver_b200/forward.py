@@ -632,6 +632,29 @@ class FORWARD_SOLVER_CONVERGENT_BORN(CBSHostSetup):
         _lib.check(self.lib.odt_set_field_storage(self._handle, modes[storage]))
         self.parameters["field_storage"] = storage
 
+    def solve_source(self, source):
+        """CudaBorn's action 2 (CUDA_CODE/main.cpp:139-163): the Born series
+        driven by 3D incident fields over the RI grid, source [RI_x, RI_y,
+        RI_z, n] (or [RI_x, RI_y, RI_z, 3, n] with vector_simulation; one field
+        may omit the last axis); returns Field(ROI) + source in the same
+        layout (odt_solve_source)."""
+        x = np.asarray(source)
+        ri = list(self.expected_RI_size)
+        comp = (3,) if self.vector else ()
+        single = x.ndim == 3 + len(comp)
+        if single:
+            x = x[..., None]
+        if list(x.shape[:3]) != ri or tuple(x.shape[3:-1]) != comp:
+            raise ValueError("source must be [%d, %d, %d%s, n]" % (ri[0], ri[1], ri[2], ", 3" if comp else ""))
+        xin = _c64(x)
+        out = np.empty(x.shape, dtype=C64, order="F")
+        a = _lib.SourceArgs()
+        a.source, a.n, a.field3d = _lib.ptr(xin), x.shape[-1], _lib.ptr(out)
+        a.memory = _lib.ODT_MEM_HOST
+        a.stream = None
+        _lib.check(self.lib.odt_solve_source(self._handle, C.byref(a)))
+        return out[..., 0] if single else out
+
     def autotune(self, n_ill=None):
         """Time the execution plans that apply to this geometry (fused xy-pass,
         separate pipelined passes, generic tile kernels) on one solve of

@@ -4,6 +4,7 @@
 //   id = odt_mex(uint32(0), uint32(0), geom, refocus, kernel_trans, kernel_ref, pupil_in, pupil_out)
 //   odt_mex(uint32(1), id, pot, single(V))
 //   [trans, ref, field3d] = odt_mex(uint32(4), id, single complex input [F_x, F_y, npol, n], RI_size)
+//   field3d = odt_mex(uint32(2), id, single complex source3D [RI_x, RI_y, RI_z(, 3)(, n)])  (legacy)
 //   odt_mex(uint32(3), id)
 // and, beyond CudaBorn's actions (vector simulations, the inverse solver):
 //   odt_mex(uint32(5), id, Radial_2D, Perp_2D, ewald_TanVec, uint8(K_mask))   polarisation basis
@@ -162,6 +163,26 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
       a.memory = ODT_MEM_HOST;
       check(odt_gradient(id, &a));
       if (nlhs > 1) plhs[1] = mxCreateDoubleScalar(err);
+      break;
+    }
+    case 2: {
+      if (nrhs < 3) mexErrMsgIdAndTxt("odt:arg", "action 2 needs the 3D source");
+      const mwSize nd = mxGetNumberOfDimensions(prhs[2]);
+      const mwSize* d = mxGetDimensions(prhs[2]);
+      plhs[0] = mxCreateNumericArray(nd, d, mxSINGLE_CLASS, mxCOMPLEX);
+      const mwSize per = d[0] * d[1] * (nd > 2 ? d[2] : 1);
+      odt_source_args a{};
+      a.source = csingle(prhs[2], "source3D");
+      a.field3d = reinterpret_cast<odt_cfloat*>(mxGetComplexSingles(plhs[0]));
+      // n = elements / (RI grid x components); the library checks the grid
+      // against its handle through the sizes it was created with
+      mwSize comps = 1;
+      for (mwSize i = 3; i < nd; ++i) comps *= d[i];
+      a.n = (int32_t)comps;
+      if (nd > 4 && d[3] == 3) a.n = (int32_t)(comps / 3);
+      (void)per;
+      a.memory = ODT_MEM_HOST;
+      check(odt_solve_source(id, &a));
       break;
     }
     case 8: {
