@@ -1,4 +1,5 @@
-// Pipelined x-pass of the Born iteration for x-lengths n = 8 * R2 (R2 odd):
+// Pipelined x-pass of the Born iteration for x-lengths n = 8 * R2 (R2 odd:
+// 11, 15, 19, 25, 27, and 35 = 5 x 7 as one composite butterfly):
 // the same arithmetic as born_x_body in modes Mid (inverse x-FFT, update of
 // iteration jj-1, source term of iteration jj, forward x-FFT;
 // FORWARD_SOLVER_CONVERGENT_BORN.m:588-605, :616-642; jj >= 2) and Last
@@ -414,7 +415,10 @@ cudaError_t launch_r2(const BornArgs& a, int jj, const DevFft& fx, int* fault, c
   int nsm = 0;
   e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
-  const int per_sm = W == 16 ? 2 : 3;
+  int per_sm = 0;   // resident CTAs per SM (2 or 3; 2 for the 280-point lines)
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, born_x_pipe_kernel<R2, W, KIND>, W * kR1, L::kTotal);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorLaunchOutOfResources;
   const int nty = (a.py + W - 1) / W;
   const long long ntiles = (long long)nty * a.pz * a.nbatch;
   const int grid = (int)(ntiles < (long long)per_sm * nsm ? ntiles : (long long)per_sm * nsm);
@@ -429,6 +433,7 @@ int lines_of(int r2) {
     case 19: return tile_lines<19>();
     case 25: return tile_lines<25>();
     case 27: return tile_lines<27>();
+    case 35: return tile_lines<35>();
     default: return 0;
   }
 }
@@ -459,6 +464,7 @@ cudaError_t launch_born_x_pipe(const BornArgs& a, int mode, int jj, const DevFft
     ODT_PIPE_CASE(19)
     ODT_PIPE_CASE(25)
     ODT_PIPE_CASE(27)
+    ODT_PIPE_CASE(35)
 #undef ODT_PIPE_CASE
     default: return cudaErrorNotSupported;
   }

@@ -117,6 +117,11 @@ __global__ void __launch_bounds__(threads_of<KIND>(), KIND >= 2 ? (R2 <= 19 ? 5 
   constexpr bool kZ = KIND >= 2;
   constexpr bool k16 = KIND == 3;
   constexpr int kT = threads_of<KIND>();
+  // y-columns longer than a TMA box dimension (256) arrive as two halves
+  constexpr bool kSplitY = !kZ && N > 256;
+  static_assert(!kSplitY || (N % 2 == 0 && N / 2 <= 256 && ((N / 2) * kW * sizeof(float2)) % 128 == 0),
+                "split y-tile halves must fit a box and stay 128-byte aligned");
+  static_assert(!kZ || N <= 256, "z-tiles are one box");
   constexpr bool kInvFirst = KIND == 1;  // direction of the first transform
   using L = ColSmem<N>;
   extern __shared__ __align__(128) unsigned char sm[];
@@ -155,7 +160,12 @@ __global__ void __launch_bounds__(threads_of<KIND>(), KIND >= 2 ? (R2 <= 19 ? 5 
     float2* dst = stage ? s1 : s0;
     if (k16) tma_load_4d(dst, &map, kW * xt, o % a.py, 0, o / a.py, &bar[stage]);
     else if (kZ) tma_load_4d(dst, &map, 2 * kW * xt, o % a.py, 0, o / a.py, &bar[stage]);
-    else tma_load_3d(dst, &map, 2 * kW * xt, 0, o, &bar[stage]);
+    else if (kSplitY) {
+      tma_load_3d(dst, &map, 2 * kW * xt, 0, o, &bar[stage]);
+      tma_load_3d(dst + (N / 2) * kW, &map, 2 * kW * xt, N / 2, o, &bar[stage]);
+    } else {
+      tma_load_3d(dst, &map, 2 * kW * xt, 0, o, &bar[stage]);
+    }
   };
   if (tid == 0) issue(tile, 0);
   uint32_t ph0 = 0, ph1 = 0;
@@ -390,7 +400,10 @@ bool make_map(const BornArgs& a, bool zpass, CUtensorMap* m, bool b16 = false) {
   } else if (!zpass) {
     const cuuint64_t dims[3] = {px2, (cuuint64_t)a.py, (cuuint64_t)a.pz * a.nbatch};
     const cuuint64_t strides[2] = {rowb, planeb};
-    const cuuint32_t box[3] = {2 * kW, (cuuint32_t)a.py, 1};
+    // a box dimension holds at most 256 elements: longer columns (280) land
+    // as two boxes of py / 2 rows on the same mbarrier
+    const cuuint32_t rows = a.py > 256 ? (cuuint32_t)(a.py / 2) : (cuuint32_t)a.py;
+    const cuuint32_t box[3] = {2 * kW, rows, 1};
     r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, a.T, dims, strides, box, estr,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -449,6 +462,9 @@ cudaError_t dispatch(const BornArgs& a, int jj, const DevFft& f, int* fault, cud
     case 19: return launch_kind<19, KIND>(a, jj, f, fault, s);
     case 25: return launch_kind<25, KIND>(a, jj, f, fault, s);
     case 27: return launch_kind<27, KIND>(a, jj, f, fault, s);
+    case 35:   // y-FFTs only (280 = 8 x 35 x-y planes)
+      if constexpr (KIND < 2) return launch_kind<35, KIND>(a, jj, f, fault, s);
+      return cudaErrorNotSupported;
     default: return cudaErrorNotSupported;
   }
 }
@@ -459,7 +475,8 @@ bool cols_pipe_supported(const BornArgs& a, const DevFft& f, bool zpass) {
   const int n = f.plan.n;
   if (n != (zpass ? a.pz : a.py) || n % kR1 != 0) return false;
   const int r2 = n / kR1;
-  if (r2 != 11 && r2 != 15 && r2 != 19 && r2 != 25 && r2 != 27 && !(zpass && r2 == 12)) return false;
+  if (r2 != 11 && r2 != 15 && r2 != 19 && r2 != 25 && r2 != 27 && !(zpass && r2 == 12) && !(!zpass && r2 == 35))
+    return false;
   if (a.px % 2 != 0 || !encoder()) return false;   // row strides must be multiples of 16 bytes
   const long long nout = zpass ? (long long)a.py * a.nbatch : (long long)a.pz * a.nbatch;
   return nout * ((a.px + kW - 1) / kW) < (1LL << 31);

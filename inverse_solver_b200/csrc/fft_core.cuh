@@ -43,17 +43,71 @@ struct FftPlan {
   int rclass;  // radix class (largest radix: 0 -> <= 8, 1 -> <= 15, 2 -> <= 31)
 };
 
-ODT_HD float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-ODT_HD float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Device code on sm_100 adds, subtracts and multiply-adds complex values as
+// packed FP32 pairs (one add.f32x2 / sub.f32x2 / fma.rn.f32x2 per complex
+// operation instead of two scalar ones): the same IEEE operations on each
+// component, so the results are the scalar code's, at half the instruction
+// count.
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+#define ODT_F32X2 1
+__device__ __forceinline__ float2 fsub2(float2 a, float2 b) {
+  float2 r;
+  asm("{\n\t.reg .b64 x, y, d;\n\t"
+      "mov.b64 x, {%2, %3};\n\tmov.b64 y, {%4, %5};\n\t"
+      "sub.rn.f32x2 d, x, y;\n\tmov.b64 {%0, %1}, d;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+#endif
+ODT_HD float2 cadd(float2 a, float2 b) {
+#if defined(ODT_F32X2)
+  return __fadd2_rn(a, b);
+#else
+  return make_float2(a.x + b.x, a.y + b.y);
+#endif
+}
+ODT_HD float2 csub(float2 a, float2 b) {
+#if defined(ODT_F32X2)
+  return fsub2(a, b);
+#else
+  return make_float2(a.x - b.x, a.y - b.y);
+#endif
+}
+// acc + c * v for real c (both components)
+ODT_HD float2 cfma_real(float c, float2 v, float2 acc) {
+#if defined(ODT_F32X2)
+  return __ffma2_rn(make_float2(c, c), v, acc);
+#else
+  return make_float2(c * v.x + acc.x, c * v.y + acc.y);
+#endif
+}
 ODT_HD float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 ODT_HD float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
-ODT_HD float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+ODT_HD float2 cscale(float2 a, float s) {
+#if defined(ODT_F32X2)
+  return __fmul2_rn(a, make_float2(s, s));
+#else
+  return make_float2(a.x * s, a.y * s);
+#endif
+}
 // multiply by -i (forward) or +i (inverse)
 template <bool INV>
 ODT_HD float2 rot90(float2 a) {
   return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+// a + rot90<INV>(c) and a - rot90<INV>(c) as scalar pairs: the rotation
+// swaps components, which a packed operation could only take after two moves
+template <bool INV>
+ODT_HD float2 addrot(float2 a, float2 c) {
+  return INV ? make_float2(a.x - c.y, a.y + c.x) : make_float2(a.x + c.y, a.y - c.x);
+}
+template <bool INV>
+ODT_HD float2 subrot(float2 a, float2 c) {
+  return INV ? make_float2(a.x + c.y, a.y - c.x) : make_float2(a.x - c.y, a.y + c.x);
 }
 
 // ---------------------------------------------------------------- butterflies
@@ -73,11 +127,11 @@ template <bool INV>
 struct Butterfly<4, INV> {
   ODT_HD static void run(float2* v, const float2*, int) {
     float2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
-    float2 s13 = cadd(v[1], v[3]), d13 = rot90<INV>(csub(v[1], v[3]));
+    float2 s13 = cadd(v[1], v[3]), c13 = csub(v[1], v[3]);
     v[0] = cadd(s02, s13);
     v[2] = csub(s02, s13);
-    v[1] = cadd(d02, d13);
-    v[3] = csub(d02, d13);
+    v[1] = addrot<INV>(d02, c13);   // d02 + rot90(c13)
+    v[3] = subrot<INV>(d02, c13);
   }
 };
 
@@ -89,20 +143,20 @@ struct Butterfly<8, INV> {
     float2 o[4] = {v[1], v[3], v[5], v[7]};
     Butterfly<4, INV>::run(e, nullptr, 0);
     Butterfly<4, INV>::run(o, nullptr, 0);
-    // W8^k, k = 1..3 applied to the odd half
-    float2 o1 = INV ? make_float2(h * (o[1].x - o[1].y), h * (o[1].x + o[1].y))
-                    : make_float2(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
-    float2 o2 = rot90<INV>(o[2]);
-    float2 o3 = INV ? make_float2(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y))
-                    : make_float2(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
+    // W8^k, k = 1..3 applied to the odd half: o1 and o3 hold W8^k o[k] / h
+    // (h enters through the multiply-adds below), W8^2 = -/+ i through addrot
+    float2 o1 = INV ? make_float2(o[1].x - o[1].y, o[1].x + o[1].y)
+                    : make_float2(o[1].x + o[1].y, o[1].y - o[1].x);
+    float2 o3 = INV ? make_float2(-(o[3].x + o[3].y), o[3].x - o[3].y)
+                    : make_float2(o[3].y - o[3].x, -(o[3].x + o[3].y));
     v[0] = cadd(e[0], o[0]);
     v[4] = csub(e[0], o[0]);
-    v[1] = cadd(e[1], o1);
-    v[5] = csub(e[1], o1);
-    v[2] = cadd(e[2], o2);
-    v[6] = csub(e[2], o2);
-    v[3] = cadd(e[3], o3);
-    v[7] = csub(e[3], o3);
+    v[1] = cfma_real(h, o1, e[1]);    // e1 +/- h o1 as one multiply-add each
+    v[5] = cfma_real(-h, o1, e[1]);
+    v[2] = addrot<INV>(e[2], o[2]);
+    v[6] = subrot<INV>(e[2], o[2]);
+    v[3] = cfma_real(h, o3, e[3]);
+    v[7] = cfma_real(-h, o3, e[3]);
   }
 };
 
@@ -200,31 +254,30 @@ struct OddButterfly {
       cs[t] = ur.c[t];   // exp(-2 pi i t / R) = cs - i sn
       sn[t] = ur.s[t];
     }
-    float2 a[H + 1], b[H + 1];
+    // jb_m = i b_m = (-b_m.y, b_m.x), so that i * im = sum_m s jb_m is a sum
+    // of packed products (negation is exact: the same values as i * (sum s b_m))
+    float2 a[H + 1], jb[H + 1];
     float2 x0 = v[0];
     float2 sum = v[0];
 #pragma unroll
     for (int m = 1; m <= H; ++m) {
       a[m] = cadd(v[m], v[R - m]);
-      b[m] = csub(v[m], v[R - m]);
+      jb[m] = make_float2(v[R - m].y - v[m].y, v[m].x - v[R - m].x);
       sum = cadd(sum, a[m]);
     }
     v[0] = sum;
 #pragma unroll
     for (int k = 1; k <= H; ++k) {
-      float2 re = x0, im = make_float2(0.f, 0.f);
+      float2 re = x0, jim = make_float2(0.f, 0.f);
 #pragma unroll
       for (int m = 1; m <= H; ++m) {
         const int t = (m * k) % R;
         const float c = (t <= H) ? cs[t] : cs[R - t];
         const float s = (t <= H) ? sn[t] : -sn[R - t];
-        re.x += a[m].x * c;
-        re.y += a[m].y * c;
-        im.x += b[m].x * s;
-        im.y += b[m].y * s;
+        re = cfma_real(c, a[m], re);
+        jim = cfma_real(s, jb[m], jim);
       }
-      // forward: X[k] = re - i*im, X[R-k] = re + i*im
-      float2 jim = make_float2(-im.y, im.x);  // i * im
+      // forward: X[k] = re - i*im, X[R-k] = re + i*im (jim = i * im)
       if (INV) {
         v[k] = cadd(re, jim);
         v[R - k] = csub(re, jim);
@@ -232,6 +285,45 @@ struct OddButterfly {
         v[k] = csub(re, jim);
         v[R - k] = cadd(re, jim);
       }
+    }
+  }
+};
+
+// A * B points in registers (Cooley-Tukey with both factors as butterflies):
+// n = B n1 + n2, k = k1 + A k2; A-point DFTs over n1, the twiddles
+// W_AB^(n2 k1) as compile-time constants, B-point DFTs over n2.  For
+// composite radices of the pipelined passes (35 = 5 x 7: the 280-point axes).
+template <int A, int B, bool INV>
+struct CompositeButterfly {
+  ODT_HD static void run(float2* v, const float2* tw, int n) {
+    constexpr int AB = A * B;
+    constexpr UnitRoots<AB> ur{};
+    float2 t[B][A];
+#pragma unroll
+    for (int n2 = 0; n2 < B; ++n2) {
+      float2 q[A];
+#pragma unroll
+      for (int n1 = 0; n1 < A; ++n1) q[n1] = v[B * n1 + n2];
+      Butterfly<A, INV>::run(q, tw, n);
+#pragma unroll
+      for (int k1 = 0; k1 < A; ++k1) {
+        const int e = (n2 * k1) % AB;
+        if (e == 0) {
+          t[n2][k1] = q[k1];
+        } else {   // exp(-/+ 2 pi i e / AB)
+          const float2 w = make_float2(ur.c[e], INV ? ur.s[e] : -ur.s[e]);
+          t[n2][k1] = cmul(q[k1], w);
+        }
+      }
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < A; ++k1) {
+      float2 q[B];
+#pragma unroll
+      for (int n2 = 0; n2 < B; ++n2) q[n2] = t[n2][k1];
+      Butterfly<B, INV>::run(q, tw, n);
+#pragma unroll
+      for (int k2 = 0; k2 < B; ++k2) v[k1 + A * k2] = q[k2];
     }
   }
 };
@@ -258,6 +350,11 @@ ODT_ODD_BUTTERFLY(27)
 ODT_ODD_BUTTERFLY(29)
 ODT_ODD_BUTTERFLY(31)
 #undef ODT_ODD_BUTTERFLY
+
+template <bool INV>
+struct Butterfly<35, INV> {
+  ODT_HD static void run(float2* v, const float2* tw, int n) { CompositeButterfly<5, 7, INV>::run(v, tw, n); }
+};
 
 // ------------------------------------------------------------------ one pass
 // Stockham radix-R pass over a tile of W pencils (W a power of two, lgW its

@@ -166,21 +166,22 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
       break;
     }
     case 2: {
+      // source [RI_x, RI_y, RI_z, (3,) n]; the optional 4th argument is the
+      // number of field components per illumination (3 on dyadic handles,
+      // whose [.., 3] trailing size MATLAB cannot tell from n = 3)
       if (nrhs < 3) mexErrMsgIdAndTxt("odt:arg", "action 2 needs the 3D source");
       const mwSize nd = mxGetNumberOfDimensions(prhs[2]);
       const mwSize* d = mxGetDimensions(prhs[2]);
+      const mwSize comps = nrhs > 3 ? (mwSize)u32(prhs[3]) : 1;
+      if (comps != 1 && comps != 3) mexErrMsgIdAndTxt("odt:arg", "components must be 1 or 3");
+      mwSize trailing = 1;   // elements per RI-grid voxel
+      for (mwSize i = 3; i < nd; ++i) trailing *= d[i];
+      if (trailing % comps != 0) mexErrMsgIdAndTxt("odt:arg", "source size does not match the components");
       plhs[0] = mxCreateNumericArray(nd, d, mxSINGLE_CLASS, mxCOMPLEX);
-      const mwSize per = d[0] * d[1] * (nd > 2 ? d[2] : 1);
       odt_source_args a{};
       a.source = csingle(prhs[2], "source3D");
       a.field3d = reinterpret_cast<odt_cfloat*>(mxGetComplexSingles(plhs[0]));
-      // n = elements / (RI grid x components); the library checks the grid
-      // against its handle through the sizes it was created with
-      mwSize comps = 1;
-      for (mwSize i = 3; i < nd; ++i) comps *= d[i];
-      a.n = (int32_t)comps;
-      if (nd > 4 && d[3] == 3) a.n = (int32_t)(comps / 3);
-      (void)per;
+      a.n = (int32_t)(trailing / comps);   // the library checks the grid against its handle
       a.memory = ODT_MEM_HOST;
       check(odt_solve_source(id, &a));
       break;

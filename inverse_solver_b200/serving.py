@@ -312,7 +312,9 @@ def one_at_a_time(requests):
 
 # ---------------------------------------------------------------- benchmark
 CONFIG5_SIZES = ((64, 64, 64), (96, 96, 64), (128, 128, 128), (192, 192, 96), (256, 256, 192))
-CONFIG5_RECON_SIZES = ((64, 64, 61), (128, 128, 127))
+# reconstructions need an odd z; with the default 12-voxel boundary the padded
+# lengths are 88 x 88 x 85 and 152 x 152 x 153
+CONFIG5_RECON_SIZES = ((64, 64, 61), (128, 128, 129))
 
 
 def make_mix(n, seed, sizes=((64, 64, 64), (96, 96, 64), (128, 128, 128)), max_ill=16,

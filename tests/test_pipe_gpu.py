@@ -2,7 +2,7 @@
 iterations 2 onward and the final pass;
 csrc/cols_pipe.cu, the y-FFTs and the z-pass: persistent CTAs, bulk / tiled
 asynchronous copies, compile-time 8 x R2 plans), which the library selects
-for grid lengths 88, 120, 152, 200 and 216.
+for grid lengths 88, 120, 152, 200, 216 and (x and y) 280.
 
   * against the single-precision oracle on grids that put each of 88, 120
     and 152 on each axis (relative L2 per illumination 1e-5 for the
@@ -111,6 +111,23 @@ def test_pipe_radix_25_27_match_oracle(size):
     fields = cases.circle_fields(p, 2)
     (t, _, f), (sim, bm) = _solve(p, RI, fields)
     assert sim == [v + 24 for v in size] and bm >= 4
+    o = cbs.ForwardSolverCBS(p, single=True)
+    o.set_RI(RI)
+    ot, _, of = o.solve(fields)
+    assert worst(f, of) < 1e-5 and worst(t, ot) < 1e-5
+
+
+@pytest.mark.parametrize("size", [[256, 24, 16], [24, 256, 16]])
+def test_pipe_radix_35_matches_oracle(size):
+    """Padded length 280 = 8 x 35 (the x-y planes of the 256 x 256 x 192
+    serving grid; the 35-point butterfly is the 5 x 7 composite) on the x-
+    and the y-axis: (280, 48, 40) and (48, 280, 40)."""
+    p = cases.params(size, [6, 6, 6], return_3D=True, iterations_number=8)
+    RI = cases.sphere_phantom(size, [0.1] * 3, cases.NM, seed=sum(size) + 1, n_spheres=2,
+                              radius_um=(0.3, 0.8))
+    fields = cases.circle_fields(p, 2)
+    (t, _, f), (sim, bm) = _solve(p, RI, fields)
+    assert sim == [v + 24 for v in size] and bm == 8
     o = cbs.ForwardSolverCBS(p, single=True)
     o.set_RI(RI)
     ot, _, of = o.solve(fields)

@@ -61,7 +61,9 @@ def test_mixed_requests_equal_alone_results():
             alone.append(b.solve(r.fields_in, r.fields_out))
             b.delete()
 
-    srv = SolveServer(budget_bytes=16e9, slots=3)
+    # the alone solves use the default plan; an autotuned server could pick
+    # another (results then agree to 1e-5, tests/test_autotune_gpu.py)
+    srv = SolveServer(budget_bytes=16e9, slots=3, autotune=False)
     futs = []
     for r in reqs:
         r.arrival = time.perf_counter()
