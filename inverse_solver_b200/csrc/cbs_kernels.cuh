@@ -114,6 +114,13 @@ bool born_xy_supported(const BornArgs& a, int max_smem);
 cudaError_t launch_born_xy(const BornArgs& a, int mode, int jj, const DevFft& fx, cudaStream_t s);
 // z-pass of iteration jj: forward z-FFT, Green's multiply, inverse z-FFT.
 cudaError_t launch_born_z(const BornArgs& a, int jj, const DevFft& fz, cudaStream_t s);
+// Unfused Born loop for grids with a length outside the radix tiles
+// (born_any.cu): the pointwise work of the x-pass on T in natural order
+// (modes as launch_born_x; T holds the inverse transform of iteration jj-1's
+// spectrum, and receives the source of iteration jj), and the Green's
+// multiply G / N of iteration jj on T's spectrum.
+cudaError_t launch_born_point(const BornArgs& a, int mode, int jj, cudaStream_t s);
+cudaError_t launch_born_green(const BornArgs& a, int jj, cudaStream_t s);
 
 // Batched FFT along contiguous lines of an [n, nlines] array.  Input element
 // i is gathered from (i + in_shift) % n, output element k scattered to

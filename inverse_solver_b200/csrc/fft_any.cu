@@ -111,13 +111,25 @@ bool five_smooth(int m) {
 
 cudaError_t bluestein(Scratch& B, float2* x, int n0, int n, long long n2, bool inv, const AnyFft& f,
                       cudaStream_t s) {
-  const int m = f.m;
+  float2* tmp = B.get<float2>((long long)n0 * f.m * n2);
+  if (!tmp) return cudaErrorMemoryAllocation;
+  return bluestein_axis(x, n0, n2, inv, n / 2, inv ? 1.0f / (float)n : 1.0f, f, tmp, s);
+}
+
+}  // namespace
+
+int bluestein_length(int n) {
+  int m = 2 * n - 1;
+  while (!five_smooth(m)) ++m;
+  return m;
+}
+
+cudaError_t bluestein_axis(float2* x, int n0, long long n2, bool inv, int sh, float scale, const AnyFft& f,
+                           float2* tmp, cudaStream_t s) {
+  const int n = f.n, m = f.m;
   const bool lines = n0 == 1;
   const long long total = (long long)n0 * m * n2;
-  float2* tmp = B.get<float2>(total);
-  if (!tmp) return cudaErrorMemoryAllocation;
-  const int cj = inv ? 1 : 0, sh = n / 2;
-  const float scale = inv ? 1.0f / (float)n : 1.0f;
+  const int cj = inv ? 1 : 0;
   cudaError_t e;
   if (lines) bs_gather_lines<<<grid_for(total), kThreads, 0, s>>>(x, n, m, n2, sh, f.chirp, cj, tmp);
   else bs_gather_cols<<<grid_for(total), kThreads, 0, s>>>(x, n0, n, m, n2, sh, f.chirp, cj, tmp);
@@ -136,21 +148,7 @@ cudaError_t bluestein(Scratch& B, float2* x, int n0, int n, long long n2, bool i
   return cudaGetLastError();
 }
 
-}  // namespace
-
-bool scratch_fft_any(Scratch& B, int n, AnyFft* f, std::string* why) {
-  f->n = n;
-  FftPlan probe{};
-  std::string w2;
-  if (make_plan(n, &probe, &w2, kLargeFirst)) {
-    f->direct = true;
-    return scratch_fft(B, n, &f->f, why);
-  }
-  f->direct = false;
-  int m = 2 * n - 1;
-  while (!five_smooth(m)) ++m;
-  f->m = m;
-  if (!scratch_fft(B, m, &f->f, why)) return false;
+cudaError_t bluestein_tables(int n, int m, const DevFft& inner, float2* dw, float2* db, cudaStream_t s) {
   std::vector<float2> w(n), b(2 * (size_t)m, make_float2(0.f, 0.f));
   const double pi = 3.14159265358979323846;
   for (int j = 0; j < n; ++j) {
@@ -165,22 +163,37 @@ bool scratch_fft_any(Scratch& B, int n, AnyFft* f, std::string* why) {
       b[2 * (size_t)m - j] = w[j];
     }
   }
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(dw, w.data(), n * sizeof(float2), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(db, b.data(), 2 * (size_t)m * sizeof(float2), cudaMemcpyHostToDevice, s)) !=
+          cudaSuccess ||
+      (e = launch_fft_lines(db, db, 2, 0, 0, 1.f, false, inner, s)) != cudaSuccess)
+    return e;
+  bs_scale<<<grid_for(2LL * m), kThreads, 0, s>>>(db, 2LL * m, 1.0f / (float)m);
+  // (copies from pageable host memory have read their source when they return)
+  return cudaGetLastError();
+}
+
+bool scratch_fft_any(Scratch& B, int n, AnyFft* f, std::string* why) {
+  f->n = n;
+  FftPlan probe{};
+  std::string w2;
+  if (make_plan(n, &probe, &w2, kLargeFirst)) {
+    f->direct = true;
+    return scratch_fft(B, n, &f->f, why);
+  }
+  f->direct = false;
+  const int m = bluestein_length(n);
+  f->m = m;
+  if (!scratch_fft(B, m, &f->f, why)) return false;
   float2* dw = B.get<float2>(n);
   float2* db = B.get<float2>(2 * (size_t)m);
   if (!dw || !db) {
     *why = "device allocation failed";
     return false;
   }
-  cudaError_t e;
-  if ((e = cudaMemcpyAsync(dw, w.data(), n * sizeof(float2), cudaMemcpyHostToDevice, B.s)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(db, b.data(), 2 * (size_t)m * sizeof(float2), cudaMemcpyHostToDevice, B.s)) !=
-          cudaSuccess ||
-      (e = launch_fft_lines(db, db, 2, 0, 0, 1.f, false, f->f, B.s)) != cudaSuccess) {
-    *why = std::string("Bluestein tables: ") + cudaGetErrorString(e);
-    return false;
-  }
-  bs_scale<<<grid_for(2LL * m), kThreads, 0, B.s>>>(db, 2LL * m, 1.0f / (float)m);
-  if ((e = cudaGetLastError()) != cudaSuccess) {
+  const cudaError_t e = bluestein_tables(n, m, f->f, dw, db, B.s);
+  if (e != cudaSuccess) {
     *why = std::string("Bluestein tables: ") + cudaGetErrorString(e);
     return false;
   }

@@ -29,6 +29,22 @@ struct AnyFft {
 // Plan for length n on B's stream (tables in B's scratch).
 bool scratch_fft_any(Scratch& B, int n, AnyFft* f, std::string* why);
 
+// Smallest 5-smooth m >= 2 n - 1 (the convolution length of Bluestein's
+// algorithm for length n).
+int bluestein_length(int n);
+
+// Fills the tables of a Bluestein plan of length n whose length-m transforms
+// run through `inner`: chirp [n] and bhat [2 m] (forward, then inverse), on
+// stream s.
+cudaError_t bluestein_tables(int n, int m, const DevFft& inner, float2* chirp, float2* bhat, cudaStream_t s);
+
+// DFT of length n = f.n (not direct) along the middle axis of x [n0, n, n2]
+// in place, with index shift sh on input and output (0: plain transform;
+// n / 2: centred) and the result multiplied by scale.  tmp holds
+// n0 * f.m * n2 elements.
+cudaError_t bluestein_axis(float2* x, int n0, long long n2, bool inv, int sh, float scale, const AnyFft& f,
+                           float2* tmp, cudaStream_t s);
+
 // fftshift(fft2(ifftshift(x))) (or the normalised inverse) of every [N1, N2]
 // plane of x [N1, N2, nsl], in place.  With both lengths direct this is
 // fftc2; otherwise each axis is transformed on its own (the Bluestein axes

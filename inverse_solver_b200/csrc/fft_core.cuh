@@ -160,45 +160,6 @@ struct Butterfly<8, INV> {
   }
 };
 
-// R = 12 = 4 x 3 in registers (for the fused passes on lengths 96 = 8 x 12):
-// n = 3 n1 + n2, k = k1 + 4 k2; 4-point DFTs over n1, twiddles W_12^(n2 k1)
-// from the length-n table, 3-point DFTs over n2.
-template <bool INV>
-struct Butterfly<12, INV> {
-  ODT_HD static void run(float2* v, const float2* tw, int n) {
-    const int step = n / 12;
-    float2 t[3][4];
-#pragma unroll
-    for (int n2 = 0; n2 < 3; ++n2) {
-      float2 q[4] = {v[n2], v[3 + n2], v[6 + n2], v[9 + n2]};
-      Butterfly<4, INV>::run(q, nullptr, 0);
-#pragma unroll
-      for (int k1 = 0; k1 < 4; ++k1) {
-        if (n2 * k1 == 0) {
-          t[n2][k1] = q[k1];
-        } else {
-          float2 w = tw[n2 * k1 * step];
-          if (INV) w.y = -w.y;
-          t[n2][k1] = cmul(q[k1], w);
-        }
-      }
-    }
-    // 3-point DFT: c = cos(2 pi / 3) = -1/2, s = sin(2 pi / 3)
-    const float s3 = 0.86602540378443864676f;
-#pragma unroll
-    for (int k1 = 0; k1 < 4; ++k1) {
-      const float2 a0 = t[0][k1], a1 = t[1][k1], a2 = t[2][k1];
-      const float2 sum = cadd(a1, a2), dif = csub(a1, a2);
-      const float2 m = make_float2(a0.x - 0.5f * sum.x, a0.y - 0.5f * sum.y);
-      // forward: X1 = m - i s dif, X2 = m + i s dif
-      const float2 j = make_float2(-s3 * dif.y, s3 * dif.x);   // i s dif
-      v[k1] = cadd(a0, sum);
-      v[k1 + 4] = INV ? cadd(m, j) : csub(m, j);
-      v[k1 + 8] = INV ? csub(m, j) : cadd(m, j);
-    }
-  }
-};
-
 // cos(2 pi t / R) and sin(2 pi t / R) at compile time, in double: the angle
 // reduced to [-pi, pi] and Taylor series of 26 terms (the largest term is
 // below 2^3, so the result is within a few units of 1e-16), rounded to float
@@ -232,6 +193,47 @@ struct UnitRoots {   // cos / sin of 2 pi t / R, t < R, as float
     for (int t = 0; t < R; ++t) {
       c[t] = (float)ce_cos_red(ce_angle(t, R));
       s[t] = (float)ce_sin_red(ce_angle(t, R));
+    }
+  }
+};
+
+// R = 12 = 4 x 3 in registers (for the fused passes on lengths 96 = 8 x 12):
+// n = 3 n1 + n2, k = k1 + 4 k2; 4-point DFTs over n1, twiddles W_12^(n2 k1)
+// as compile-time constants, 3-point DFTs over n2.
+template <bool INV>
+struct Butterfly<12, INV> {
+  ODT_HD static void run(float2* v, const float2* tw, int n) {
+    constexpr UnitRoots<12> ur{};
+    (void)tw;
+    (void)n;
+    float2 t[3][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 3; ++n2) {
+      float2 q[4] = {v[n2], v[3 + n2], v[6 + n2], v[9 + n2]};
+      Butterfly<4, INV>::run(q, nullptr, 0);
+#pragma unroll
+      for (int k1 = 0; k1 < 4; ++k1) {
+        const int e = n2 * k1;
+        if (e == 0) {
+          t[n2][k1] = q[k1];
+        } else {   // exp(-/+ 2 pi i e / 12)
+          const float2 w = make_float2(ur.c[e], INV ? ur.s[e] : -ur.s[e]);
+          t[n2][k1] = cmul(q[k1], w);
+        }
+      }
+    }
+    // 3-point DFT: c = cos(2 pi / 3) = -1/2, s = sin(2 pi / 3)
+    const float s3 = 0.86602540378443864676f;
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+      const float2 a0 = t[0][k1], a1 = t[1][k1], a2 = t[2][k1];
+      const float2 sum = cadd(a1, a2), dif = csub(a1, a2);
+      const float2 m = make_float2(a0.x - 0.5f * sum.x, a0.y - 0.5f * sum.y);
+      // forward: X1 = m - i s dif, X2 = m + i s dif
+      const float2 j = make_float2(-s3 * dif.y, s3 * dif.x);   // i s dif
+      v[k1] = cadd(a0, sum);
+      v[k1 + 4] = INV ? cadd(m, j) : csub(m, j);
+      v[k1 + 8] = INV ? csub(m, j) : cadd(m, j);
     }
   }
 };

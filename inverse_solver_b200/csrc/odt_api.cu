@@ -26,6 +26,7 @@
 
 #include "../../include/odt.h"
 #include "cbs_kernels.cuh"
+#include "fft_any.cuh"
 #include "fft_plan.h"
 #include "tma.cuh"
 
@@ -109,6 +110,25 @@ struct Handle {
 
   // transform lengths
   DevFft fx{}, fy{}, fz{}, ffx{}, ffy{}, fcx{}, fcy{};
+  // Bluestein plans of the lengths the radix tiles do not cover (direct =
+  // true for the others; the DevFft of such a length has no passes) and
+  // their work buffer (bs_elems elements per field plane of a batch)
+  AnyFft bsx{}, bsy{}, bsz{}, bsfx{}, bsfy{}, bscx{}, bscy{};
+  float2* bs_work = nullptr;
+  long long bs_elems = 0;
+  bool any_loop() const { return !bsx.direct || !bsy.direct || !bsz.direct; }
+  bool any_io() const { return !bsfx.direct || !bsfy.direct || !bscx.direct || !bscy.direct; }
+  const AnyFft& bs_of(const DevFft& f) const {
+    static const AnyFft kDirect{};
+    if (&f == &fx) return bsx;
+    if (&f == &fy) return bsy;
+    if (&f == &fz) return bsz;
+    if (&f == &ffx) return bsfx;
+    if (&f == &ffy) return bsfy;
+    if (&f == &fcx) return bscx;
+    if (&f == &fcy) return bscy;
+    return kDirect;
+  }
 
   // dyadic (vector) handles: np = 3 field components per illumination (batch
   // entries 3 b + i), npol = 2 input / output polarisations
@@ -202,7 +222,22 @@ struct Handle {
   long long nc3() const { return nc2() * g.ri_size[2]; }
   long long work_elems() const { return std::max(3 * nvox(), nc3()); }
   size_t slot_bytes() const {
-    return sizeof(float2) * (size_t)np * (size_t)(work_elems() + 2 * nri() + 4 * nf() + 2 * nc2());
+    return sizeof(float2) * (size_t)np * (size_t)(work_elems() + 2 * nri() + 4 * nf() + 2 * nc2() + bs_elems);
+  }
+  // Bluestein work per field plane: the largest of the axes' n0 * m * n2 / nb
+  long long bluestein_elems() const {
+    long long e = 0;
+    const long long px = g.sim_size[0], py = g.sim_size[1], pz = g.sim_size[2];
+    const long long Fx = g.field_size[0], Fy = g.field_size[1], Cx = g.conv_size[0], Cy = g.conv_size[1];
+    const long long Rz = g.ri_size[2];
+    if (!bsx.direct) e = std::max(e, bsx.m * py * pz);
+    if (!bsy.direct) e = std::max(e, px * bsy.m * pz);
+    if (!bsz.direct) e = std::max(e, px * py * bsz.m);
+    if (!bsfx.direct) e = std::max(e, bsfx.m * Fy);
+    if (!bsfy.direct) e = std::max(e, Fx * bsfy.m);
+    if (!bscx.direct) e = std::max(e, bscx.m * Cy * Rz);
+    if (!bscy.direct) e = std::max(e, Cx * bscy.m * Rz);
+    return e;
   }
   PolTables pol_tables() const {
     const long long n = nf();
@@ -350,6 +385,37 @@ DevFft make_dev_fft(Handle& H, int n, int kind, const char* what) {
   return f;
 }
 
+// make_dev_fft for any length: a length with a prime factor above 31 gets a
+// Bluestein plan in *bs (tables on the device, transforms of the 5-smooth
+// length m >= 2 n - 1 through the line / column tiles) and a DevFft with no
+// passes, which no tile kernel accepts.
+DevFft make_handle_fft(Handle& H, int n, int kind, const char* what, AnyFft* bs) {
+  *bs = AnyFft{};
+  bs->n = n;
+  FftPlan probe{};
+  std::string why;
+  if (n < 1) raise(ODT_ERR_INVALID_ARGUMENT, std::string(what) + ": length must be positive");
+  if (make_plan(n, &probe, &why, kLargeFirst)) return make_dev_fft(H, n, kind, what);
+  const int m = bluestein_length(n);
+  bs->direct = false;
+  bs->m = m;
+  bs->f = make_dev_fft(H, m, kKindCols, what);
+  if (fft_smem_bytes(m, bs->f.W, kKindLines) > (size_t)H.max_smem)
+    raise(ODT_ERR_UNSUPPORTED, std::string(what) + ": Bluestein length " + std::to_string(m) +
+                                   " needs more shared memory than the device offers");
+  float2* chirp = H.dalloc<float2>(n, false);
+  float2* bhat = H.dalloc<float2>(2 * (size_t)m, false);
+  ODT_CUDA(bluestein_tables(n, m, bs->f, chirp, bhat, H.own_stream));
+  ODT_CUDA(cudaStreamSynchronize(H.own_stream));
+  bs->chirp = chirp;
+  bs->bhat_f = bhat;
+  bs->bhat_i = bhat + m;
+  DevFft f{};
+  f.plan.n = n;
+  f.plan.npass = 0;
+  return f;
+}
+
 bool is_device_ptr(const void* p) {
   cudaPointerAttributes at{};
   if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
@@ -375,6 +441,7 @@ void ensure_batch(Handle& H, int nb) {
   H.out_r = H.dalloc<float2>((size_t)H.nf() * nbp, true);
   H.c2a = H.dalloc<float2>((size_t)H.nc2() * nbp, true);
   H.c2b = H.dalloc<float2>((size_t)H.nc2() * nbp, true);
+  if (H.bs_elems > 0) H.bs_work = H.dalloc<float2>((size_t)H.bs_elems * nbp, true);
   H.d_count = H.dalloc<unsigned int>(1, true);
   H.d_fault = H.dalloc<int>(1, true);
   ODT_CUDA(cudaMemset(H.d_fault, 0, sizeof(int)));
@@ -394,13 +461,29 @@ int auto_batch(Handle& H) {
 }
 
 // centred 2D FFT on [n0, n1, nslices] in place (MATLAB fftshift(fft2(ifftshift(x))))
+// (Bluestein on an axis whose length has a prime factor above 31; the
+// inverse then normalises axis by axis)
 void fftc2(Handle& H, float2* x, const DevFft& f0, const DevFft& f1, long long nslices,
            bool inverse, cudaStream_t s) {
   const int n0 = f0.plan.n, n1 = f1.plan.n;
-  const float sc = inverse ? 1.0f / ((float)n0 * (float)n1) : 1.0f;
+  const AnyFft& b0 = H.bs_of(f0);
+  const AnyFft& b1 = H.bs_of(f1);
   H.mark_begin(kKIoFft, s);
-  ODT_CUDA(launch_fft_lines(x, x, (long long)n1 * nslices, n0 / 2, n0 / 2, 1.0f, inverse, f0, s));
-  ODT_CUDA(launch_fft_cols(x, x, n0, nslices, n1 / 2, n1 / 2, sc, inverse, f1, s));
+  if (b0.direct && b1.direct) {
+    const float sc = inverse ? 1.0f / ((float)n0 * (float)n1) : 1.0f;
+    ODT_CUDA(launch_fft_lines(x, x, (long long)n1 * nslices, n0 / 2, n0 / 2, 1.0f, inverse, f0, s));
+    ODT_CUDA(launch_fft_cols(x, x, n0, nslices, n1 / 2, n1 / 2, sc, inverse, f1, s));
+  } else {
+    const float s0 = inverse ? 1.0f / (float)n0 : 1.0f, s1 = inverse ? 1.0f / (float)n1 : 1.0f;
+    if (b0.direct)
+      ODT_CUDA(launch_fft_lines(x, x, (long long)n1 * nslices, n0 / 2, n0 / 2, s0, inverse, f0, s));
+    else
+      ODT_CUDA(bluestein_axis(x, 1, (long long)n1 * nslices, inverse, n0 / 2, s0, b0, H.bs_work, s));
+    if (b1.direct)
+      ODT_CUDA(launch_fft_cols(x, x, n0, nslices, n1 / 2, n1 / 2, s1, inverse, f1, s));
+    else
+      ODT_CUDA(bluestein_axis(x, n0, nslices, inverse, n1 / 2, s1, b1, H.bs_work, s));
+  }
   H.mark_end(s);
 }
 
@@ -442,7 +525,7 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
   // the unfused chain is kept for ODT_KERNELS=generic
   const int nacc = (want_t ? 1 : 0) + (want_r ? 1 : 0);
   const IoGeom gin{Cx, Cy, Rx, Ry, Rz, ocx, ocy, nbp}, gout{Cx, Cy, Rx, Ry, Rz, orx, ory, nbp};
-  const bool io_fused = H.use_pipe && io_fused_fits(gin, H.fcx, H.fcy, nacc, H.max_smem) &&
+  const bool io_fused = H.use_pipe && !H.any_io() && io_fused_fits(gin, H.fcx, H.fcy, nacc, H.max_smem) &&
                         io_fused_fits(gout, H.fcx, H.fcy, nacc, H.max_smem);
   // an RI tensor couples the field components in the emitter: unfused output
   const bool ten = P.tensor;
@@ -506,9 +589,49 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
   a.Fout = fout;
   a.wait_limit = H.wait_limit;
   const int B = P.pp.bornmax;
-  const bool pipe_x = !ten && H.use_pipe && born_x_pipe_supported(a, H.fx);
-  const bool pipe_y = H.use_pipe && cols_pipe_supported(a, H.fy, false);
-  const bool pipe_z = !vec && H.use_pipe && cols_pipe_supported(a, H.fz, true);
+  if (H.any_loop()) {
+    // unfused loop with Bluestein transforms along the uncovered axes
+    if (ten || vec) raise(ODT_ERR_UNSUPPORTED, "RI tensors and dyadic solves need padded lengths whose prime "
+                                               "factors are at most 31");
+    const long long xl = (long long)a.py * a.pz * nbp, yl = (long long)a.pz * nbp;
+    const long long pxy = (long long)a.px * a.py;
+    auto fft3 = [&](bool inv) {
+      auto ax = [&]() {
+        if (H.bsx.direct) ODT_CUDA(launch_fft_lines(a.T, a.T, xl, 0, 0, 1.0f, inv, H.fx, s));
+        else ODT_CUDA(bluestein_axis(a.T, 1, xl, inv, 0, 1.0f, H.bsx, H.bs_work, s));
+      };
+      auto ay = [&]() {
+        if (H.bsy.direct) ODT_CUDA(launch_fft_cols(a.T, a.T, a.px, yl, 0, 0, 1.0f, inv, H.fy, s));
+        else ODT_CUDA(bluestein_axis(a.T, a.px, yl, inv, 0, 1.0f, H.bsy, H.bs_work, s));
+      };
+      auto az = [&]() {
+        if (pxy > INT32_MAX) raise(ODT_ERR_UNSUPPORTED, "x-y plane too large for the column transforms");
+        if (H.bsz.direct) ODT_CUDA(launch_fft_cols(a.T, a.T, (int)pxy, nbp, 0, 0, 1.0f, inv, H.fz, s));
+        else ODT_CUDA(bluestein_axis(a.T, (int)pxy, nbp, inv, 0, 1.0f, H.bsz, H.bs_work, s));
+      };
+      H.mark_begin(kKBornY, s);
+      if (inv) { az(); ay(); ax(); } else { ax(); ay(); az(); }
+      H.mark_end(s);
+    };
+    for (int jj = 1; jj <= B; ++jj) {
+      if (jj >= 2) fft3(true);
+      H.mark_begin(kKBornX, s);
+      ODT_CUDA(launch_born_point(a, jj == 1 ? kBornFirst : kBornMid, jj, s));
+      H.mark_end(s);
+      fft3(false);
+      H.mark_begin(kKBornZ, s);
+      ODT_CUDA(launch_born_green(a, jj, s));
+      H.mark_end(s);
+    }
+    if (B >= 1) fft3(true);
+    H.mark_begin(kKBornX, s);
+    ODT_CUDA(launch_born_point(a, kBornLast, B + 1, s));
+    H.mark_end(s);
+  }
+  const bool any = H.any_loop();
+  const bool pipe_x = !any && !ten && H.use_pipe && born_x_pipe_supported(a, H.fx);
+  const bool pipe_y = !any && H.use_pipe && cols_pipe_supported(a, H.fy, false);
+  const bool pipe_z = !any && !vec && H.use_pipe && cols_pipe_supported(a, H.fz, true);
   DyadArgs dy{};
   if (vec) {
     for (int i = 0; i < 3; ++i) dy.rad[i] = P.rad[i];
@@ -517,7 +640,7 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
   const long long xlines = (long long)a.py * a.pz * nbp;
   // fused xy-pass (x- and both y-passes in one kernel; the z-pass, pipelined
   // or generic, reads its permuted x-y spectrum): scalar potentials
-  const bool fused_xy = !ten && !vec && H.use_pipe && H.use_xy && B >= 1 && born_xy_supported(a, H.max_smem);
+  const bool fused_xy = !any && !ten && !vec && H.use_pipe && H.use_xy && B >= 1 && born_xy_supported(a, H.max_smem);
   a.perm_xy = fused_xy ? 1 : 0;
   if (H.storage == ODT_STORAGE_B16) {
     if (!fused_xy || !pipe_z)
@@ -554,7 +677,7 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
     ODT_CUDA(launch_born_xy(a, kBornLast, B + 1, H.fx, s));
     H.mark_end(s);
   }
-  for (int jj = 1; !fused_xy && jj <= B; ++jj) {
+  for (int jj = 1; !any && !fused_xy && jj <= B; ++jj) {
     if (ten) {  // plain x-FFTs around the component-coupling pointwise kernel
       H.mark_begin(kKBornX, s);
       if (jj >= 2) ODT_CUDA(launch_fft_lines(a.T, a.T, xlines, 0, 0, 1.0f, true, H.fx, s));
@@ -589,7 +712,7 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
       ODT_CUDA(launch_fft_cols(a.T, a.T, a.px, (long long)a.pz * nbp, 0, 0, 1.0f, true, H.fy, s));
     H.mark_end(s);
   }
-  if (!fused_xy) {
+  if (!any && !fused_xy) {
     if (ten) {
       H.mark_begin(kKBornX, s);
       if (B >= 1) ODT_CUDA(launch_fft_lines(a.T, a.T, xlines, 0, 0, 1.0f, true, H.fx, s));
@@ -835,13 +958,17 @@ odt_status odt_create(const odt_geometry* geom, const odt_cfloat* refocus,
     }
     ODT_CUDA(cudaStreamCreateWithFlags(&H->own_stream, cudaStreamNonBlocking));
     ODT_CUDA(cudaEventCreateWithFlags(&H->done_ev, cudaEventDisableTiming));
-    H->fx = make_dev_fft(*H, g.sim_size[0], kKindBornX, "sim_size(1)");
-    H->fy = make_dev_fft(*H, g.sim_size[1], kKindCols, "sim_size(2)");
-    H->fz = make_dev_fft(*H, g.sim_size[2], kKindBornZ, "sim_size(3)");
-    H->ffx = make_dev_fft(*H, g.field_size[0], kKindLines, "field_size(1)");
-    H->ffy = make_dev_fft(*H, g.field_size[1], kKindCols, "field_size(2)");
-    H->fcx = make_dev_fft(*H, g.conv_size[0], kKindLines, "conv_size(1)");
-    H->fcy = make_dev_fft(*H, g.conv_size[1], kKindCols, "conv_size(2)");
+    H->fx = make_handle_fft(*H, g.sim_size[0], kKindBornX, "sim_size(1)", &H->bsx);
+    H->fy = make_handle_fft(*H, g.sim_size[1], kKindCols, "sim_size(2)", &H->bsy);
+    H->fz = make_handle_fft(*H, g.sim_size[2], kKindBornZ, "sim_size(3)", &H->bsz);
+    H->ffx = make_handle_fft(*H, g.field_size[0], kKindLines, "field_size(1)", &H->bsfx);
+    H->ffy = make_handle_fft(*H, g.field_size[1], kKindCols, "field_size(2)", &H->bsfy);
+    H->fcx = make_handle_fft(*H, g.conv_size[0], kKindLines, "conv_size(1)", &H->bscx);
+    H->fcy = make_handle_fft(*H, g.conv_size[1], kKindCols, "conv_size(2)", &H->bscy);
+    if ((H->any_loop() || H->any_io()) && H->np == 3)
+      raise(ODT_ERR_UNSUPPORTED, "dyadic (vector) solves need simulation, field and convolution lengths whose "
+                                 "prime factors are at most 31");
+    H->bs_elems = H->bluestein_elems();
     const size_t n3 = (size_t)H->nc3();
     H->refocus = H->dalloc<float2>(n3, false);
     ODT_CUDA(cudaMemcpy(H->refocus, refocus, n3 * sizeof(float2), cudaMemcpyHostToDevice));
