@@ -74,7 +74,11 @@ struct XYSmem {
   static constexpr size_t kRampY = kRampX + a16(sizeof(float2) * N);  // ramp along y
   static constexpr size_t kMaskX = kRampY + a16(sizeof(float2) * N);
   static constexpr size_t kMaskY = kMaskX + a16(sizeof(float) * N);
-  static constexpr size_t kPlane = a128(kMaskY + a16(sizeof(float) * N));
+  // W_N^(r k1) at twk[k1 * kTkS + r] (steps 3 and 5, whose lanes take 8
+  // different k1): an odd stride puts the 8 addresses on distinct bank pairs
+  static constexpr int kTkS = R | 1;
+  static constexpr size_t kTk = kMaskY + a16(sizeof(float) * N);
+  static constexpr size_t kPlane = a128(kTk + a16(sizeof(float2) * 8 * kTkS));
   static constexpr size_t kTotal = kPlane + sizeof(float2) * N * N;
 };
 
@@ -107,6 +111,7 @@ __global__ void __launch_bounds__(32 * R, 1)
   float2* ryt = reinterpret_cast<float2*>(sm + L::kRampY);
   float* mxt = reinterpret_cast<float*>(sm + L::kMaskX);
   float* myt = reinterpret_cast<float*>(sm + L::kMaskY);
+  float2* twk = reinterpret_cast<float2*>(sm + L::kTk);
   float2* pl = reinterpret_cast<float2*>(sm + L::kPlane);
   const int tid = threadIdx.x;
   const int w = tid >> 5, lane = tid & 31;   // warp w owns the rows R n1 + w in steps 2-6
@@ -118,6 +123,10 @@ __global__ void __launch_bounds__(32 * R, 1)
     ryt[i] = a.acyclic ? a.ramp[1][i] : one;
     mxt[i] = a.mask[0][i];
     myt[i] = a.mask[1][i];
+  }
+  for (int i = tid; i < 8 * L::kTkS; i += NT) {   // r k1 < 8 R = N
+    const int k1 = i / L::kTkS, r = i - k1 * L::kTkS;
+    twk[i] = r < R ? twg[r * k1] : make_float2(0.f, 0.f);
   }
   __syncthreads();
 
@@ -194,8 +203,9 @@ __global__ void __launch_bounds__(32 * R, 1)
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = row[r];
         Butterfly<R, true>::run(v, tw, N);
+        const float2* tk = twk + k1 * L::kTkS;
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], cconj(tw[r * k1]));
+        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], cconj(tk[r]));
 #pragma unroll
         for (int r = 0; r < R; ++r) row[r] = v[r];
       }
@@ -322,8 +332,9 @@ __global__ void __launch_bounds__(32 * R, 1)
       float2 v[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) v[r] = row[r];
+      const float2* tk = twk + k1 * L::kTkS;
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tw[r * k1]);
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tk[r]);
       Butterfly<R, false>::run(v, tw, N);
 #pragma unroll
       for (int r = 0; r < R; ++r) row[r] = v[r];

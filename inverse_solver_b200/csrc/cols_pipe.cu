@@ -28,7 +28,6 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
-#include <cstdlib>
 #include <string>
 
 #include "b16.cuh"
@@ -366,219 +365,6 @@ __global__ void __launch_bounds__(threads_of<KIND>(), KIND >= 2 ? (R2 <= 19 ? 5 
 #endif
 }
 
-// ------------------------------------------------------------------------
-// z-pass with warp-owned columns (the z-pass of complex64 storage).  The same
-// steps A, B, C as cols_pipe_kernel<R2, 2>, but each of the 4 warps of a CTA
-// takes 4 of the tile's 16 columns through all three steps, so the steps are
-// separated by warp synchronisation only and the warps drift apart: one
-// warp's global stores and table loads overlap the other warps' transforms.
-// A stage is handed back to the copy engine through an "empty" mbarrier that
-// every warp arrives on after its step C; thread 0, which issues the copies,
-// waits on it before refilling the stage.
-//
-// The tile lands with the copy engine's 128-byte swizzle: the 16-byte chunk
-// j of row r (two complex values) is stored at chunk j ^ (r mod 8), so that a
-// warp's accesses -- 4 columns (2 chunks) of 8 rows whose indices differ mod
-// 8 -- spread over all 32 banks.
-constexpr int kThreadsZW = 128;   // 4 warps x 4 columns
-
-// Twiddles in two tables laid out for the warps' access patterns: step A's
-// lanes take 8 different n2 and read W^(r n2) at twA[9 n2 + r], step B's 8
-// different k1 read W^(r k1) at twB[R2 k1 + r] (R2 odd): both strides put
-// the 8 addresses of an instruction on distinct bank pairs.
-template <int N>
-struct ZwSmem {
-  static constexpr int R2 = N / 8;
-  static constexpr size_t kTwA = 64;   // after the full[2] and empty[2] mbarriers
-  static constexpr size_t kTwB = kTwA + a16(sizeof(float2) * 9 * R2);
-  static constexpr size_t kKz = kTwB + a16(sizeof(float2) * 8 * R2);
-  static constexpr size_t kTile = sizeof(float2) * N * kW;   // 1024 R2 bytes: stages stay 1024-aligned
-  static constexpr size_t kS0 = a1k(kKz + a16(sizeof(float) * N));
-  static constexpr size_t kS1 = kS0 + kTile;
-  static constexpr size_t kTotal = kS1 + kTile;
-};
-
-// complex64 index of (row, column) in a swizzled tile
-__host__ __device__ __forceinline__ int zw_idx(int row, int c) {
-  return row * kW + ((((c >> 1) ^ (row & 7))) << 1) + (c & 1);
-}
-
-template <int R2>
-__global__ void __launch_bounds__(kThreadsZW, R2 <= 19 ? 5 : 4)
-    born_z_warp_kernel(const __grid_constant__ CUtensorMap map, const BornArgs a, const int jj,
-                       const float2* __restrict__ twg, const int nxt, const int ntiles,
-                       int* __restrict__ fault) {
-#if defined(__CUDA_ARCH__)
-  constexpr int N = kR1 * R2;
-  using L = ZwSmem<N>;
-  extern __shared__ __align__(1024) unsigned char smz[];
-  uint64_t* full = reinterpret_cast<uint64_t*>(smz);
-  uint64_t* empty = full + 2;
-  float2* twA = reinterpret_cast<float2*>(smz + L::kTwA);
-  float2* twB = reinterpret_cast<float2*>(smz + L::kTwB);
-  float* kz = reinterpret_cast<float*>(smz + L::kKz);
-  float2* const s0 = reinterpret_cast<float2*>(smz + L::kS0);
-  float2* const s1 = reinterpret_cast<float2*>(smz + L::kS1);
-  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
-  const bool flip = a.acyclic && (jj & 1);
-  // the swizzle pattern is a function of the address: stages on 1024 bytes
-  if ((smem_addr(s0) & 1023u) != 0u || (smem_addr(s1) & 1023u) != 0u) {
-    if (tid == 0) atomicCAS(fault, 0, kFaultAlign);
-    return;
-  }
-  for (int i = tid; i < N; i += kThreadsZW) kz[i] = a.kq2[2][flip ? (i == 0 ? 0 : N - i) : i];
-  for (int i = tid; i < 9 * R2; i += kThreadsZW) {   // r n2 < 8 R2 = N
-    const int n2 = i / 9, r = i - 9 * n2;
-    twA[i] = r < kR1 ? twg[r * n2] : make_float2(0.f, 0.f);
-  }
-  for (int i = tid; i < 8 * R2; i += kThreadsZW) {   // r k1 < 8 R2 = N
-    const int k1 = i / R2, r = i - R2 * k1;
-    twB[i] = twg[r * k1];
-  }
-  if (tid == 0) {
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
-    mbar_init(&empty[0], kThreadsZW / 32);
-    mbar_init(&empty[1], kThreadsZW / 32);
-    mbar_fence_init();
-  }
-  __syncthreads();
-  int tile = blockIdx.x;
-  if (tile >= ntiles) return;
-  const long long rstride = (long long)a.px * a.py;   // element stride between z-rows
-  constexpr uint32_t kBytes = (uint32_t)(sizeof(float2) * N * kW);
-  auto issue = [&](int t, int stage) {
-    const int xt = t % nxt, o = t / nxt;
-    mbar_arrive_expect_tx(&full[stage], kBytes);
-    tma_load_4d(stage ? s1 : s0, &map, 2 * kW * xt, o % a.py, 0, o / a.py, &full[stage]);
-  };
-  // thread 0: the copies it issued and has not yet seen land -- bit s of
-  // `pending` for stage s, bit s of `pend_par` the phase parity to wait for
-  int pending = 0, pend_par = 0;
-  if (tid == 0) {
-    issue(tile, 0);
-    pending = 1;
-  }
-  const int cl = lane & 3;      // the lane's column within its warp's four
-  // The lane's row index within a group of 8: 64-bit accesses are served a
-  // half-warp at a time, so lanes 0-15 take the even rows 0, 2, 4, 6 and
-  // lanes 16-31 the odd ones; for odd R2 the four rows of a half-warp then
-  // differ by 2 mod 8 and, with the two column pairs, fill all 8 swizzled
-  // chunks (conflict-free).
-  const int j8 = (((lane >> 2) & 3) << 1) | (lane >> 4);
-  // swizzled offsets within a row for the lane's column: steps A and C read
-  // rows R2 r + n2 with n2 = 8 q + j8 (row mod 8 fixed per r), step B rows
-  // R2 k1 + r with k1 = j8 (row mod 8 periodic in r)
-  const int cc = ((4 * w + cl) >> 1), c1 = cl & 1;
-  int offA[kR1], offB[8];
-#pragma unroll
-  for (int r = 0; r < kR1; ++r) offA[r] = (((cc ^ ((R2 * r + j8) & 7))) << 1) | c1;
-#pragma unroll
-  for (int r = 0; r < 8; ++r) offB[r] = (((cc ^ ((R2 * j8 + r) & 7))) << 1) | c1;
-  for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
-    const int s = it & 1;
-    const uint32_t par = (uint32_t)(it >> 1) & 1u;
-    const int next = tile + gridDim.x;
-    bool ok = true;
-    if (tid == 0 && next < ntiles) {
-      // stage s ^ 1 held tile it - 1: every warp must have released it
-      if (it >= 1) ok = mbar_wait(&empty[s ^ 1], (uint32_t)((it - 1) >> 1) & 1u, a.wait_limit);
-      if (ok) {
-        fence_proxy_async();
-        issue(next, s ^ 1);
-        pending |= 1 << (s ^ 1);
-        pend_par = (pend_par & ~(1 << (s ^ 1))) | ((((it + 1) >> 1) & 1) << (s ^ 1));
-      }
-    }
-    ok = ok && mbar_wait(&full[s], par, a.wait_limit);
-    if (!__all_sync(0xffffffffu, ok)) {
-      if (lane == 0) atomicCAS(fault, 0, kFaultTimeout);
-      break;
-    }
-    if (tid == 0) pending &= ~(1 << s);
-    const float2* Sc = s ? s1 : s0;
-    float2* S = const_cast<float2*>(Sc);
-    const int xt = tile % nxt, o = tile / nxt;
-    const int x0 = kW * xt;
-    const int ncol = min(kW, a.px - x0);
-    const int cb = 4 * w;   // the warp's first column
-    if (cb < ncol) {
-      const int y = o % a.py, b = o / a.py;
-      const long long gbase = (long long)b * a.nvox + (long long)y * a.px + x0;
-      // A: 8-point DFT over n1 at rows R2 n1 + n2, times W_N^(n2 k1); items
-      //    (column, n2), lane -> column lane % 4, n2 = j8 + 8 q
-      for (int n2 = j8; n2 < R2; n2 += 8) {
-        float2* col = S + n2 * kW;
-        float2 v[kR1];
-#pragma unroll
-        for (int r = 0; r < kR1; ++r) v[r] = col[R2 * r * kW + offA[r]];
-        Butterfly<kR1, false>::run(v, twA, N);
-#pragma unroll
-        for (int r = 1; r < kR1; ++r) v[r] = cmul(v[r], twA[9 * n2 + r]);
-#pragma unroll
-        for (int r = 0; r < kR1; ++r) col[R2 * r * kW + offA[r]] = v[r];
-      }
-      __syncwarp();
-      // B: per (column, k1) the R2-point DFT over n2 at rows R2 k1 + n2
-      //    (kz = k1 + 8 k2), the Green's multiply, the inverse R2-point DFT
-      //    and the conjugate twiddles; lane -> column lane % 4, k1 = j8
-      {
-        const int c = cb + cl, k1 = j8;
-        int kx = min(x0 + c, a.px - 1), ky = y;
-        if (a.perm_xy) {   // position R k1 + k2 holds spectral index k1 + 8 k2
-          const int rx = a.px >> 3, ry = a.py >> 3;
-          kx = kx / rx + 8 * (kx % rx);
-          ky = ky / ry + 8 * (ky % ry);
-        }
-        const int ix = flip ? (kx == 0 ? 0 : a.px - kx) : kx;
-        const int iy = flip ? (ky == 0 ? 0 : a.py - ky) : ky;
-        const float qxy = a.kq2[0][ix] + a.kq2[1][iy];
-        float2* col = S + R2 * k1 * kW;
-        float2 v[R2];
-#pragma unroll
-        for (int r = 0; r < R2; ++r) v[r] = col[r * kW + offB[r & 7]];
-        Butterfly<R2, false>::run(v, twA, N);
-#pragma unroll
-        for (int r = 0; r < R2; ++r) {
-          float q = qxy + kz[k1 + kR1 * r];
-          q = a.g_scale * q - a.g_off;
-          const float rden = rcp_approx(q * q + a.eps * a.eps) * a.inv_n;
-          const float2 G = make_float2(q * rden, a.eps * rden);  // (1 / (q - i eps)) / N
-          v[r] = cmul(G, v[r]);
-        }
-        Butterfly<R2, true>::run(v, twA, N);
-        const float2* tk = twB + R2 * k1;
-#pragma unroll
-        for (int r = 1; r < R2; ++r) v[r] = cmul(v[r], cconj(tk[r]));
-#pragma unroll
-        for (int r = 0; r < R2; ++r) col[r * kW + offB[r & 7]] = v[r];
-      }
-      __syncwarp();
-      // C: inverse 8-point DFT over k1 -> rows R2 n1 + n2 of T
-      for (int n2 = j8; n2 < R2; n2 += 8) {
-        const int c = cb + cl;
-        const float2* col = S + n2 * kW;
-        float2 v[kR1];
-#pragma unroll
-        for (int r = 0; r < kR1; ++r) v[r] = col[R2 * r * kW + offA[r]];
-        Butterfly<kR1, true>::run(v, twA, N);
-        if (c < ncol) {
-          float2* out = a.T + gbase + c;
-#pragma unroll
-          for (int r = 0; r < kR1; ++r) out[(R2 * r + n2) * rstride] = v[r];
-        }
-      }
-    }
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[s]);   // this warp is done with the stage
-  }
-  if (tid == 0) {   // no copy may still be writing shared memory when the CTA exits
-    if (pending & 1) mbar_wait(&full[0], (uint32_t)(pend_par & 1));
-    if (pending & 2) mbar_wait(&full[1], (uint32_t)((pend_par >> 1) & 1));
-  }
-#endif
-}
-
 PFN_cuTensorMapEncodeTiled_v12000 encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -595,7 +381,7 @@ PFN_cuTensorMapEncodeTiled_v12000 encoder() {
 // {2*px, py, pz, nb} (z-pass); box 32 floats = 16 complex columns.  With
 // 16-bit storage (b16) the map covers T16 viewed as 32-bit (re, im) int16
 // pairs: dims {px, py, pz, nb}, box 16 columns (64 bytes).
-bool make_map(const BornArgs& a, bool zpass, CUtensorMap* m, bool b16 = false, bool swizzle = false) {
+bool make_map(const BornArgs& a, bool zpass, CUtensorMap* m, bool b16 = false) {
   auto enc = encoder();
   if (!enc) return false;
   const cuuint64_t px2 = 2ull * a.px;
@@ -626,8 +412,8 @@ bool make_map(const BornArgs& a, bool zpass, CUtensorMap* m, bool b16 = false, b
     const cuuint64_t strides[3] = {rowb, planeb, planeb * a.pz};
     const cuuint32_t box[4] = {2 * kW, 1, (cuuint32_t)a.pz, 1};
     r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, a.T, dims, strides, box, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
-            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   }
   return r == CUDA_SUCCESS;
 }
@@ -663,48 +449,6 @@ cudaError_t launch_kind(const BornArgs& a, int jj, const DevFft& f, int* fault, 
   const int grid = (int)(ntiles < cap ? ntiles : cap);
   cols_pipe_kernel<R2, KIND><<<grid, nthr, smem, s>>>(map, a, jj, f.tw, nxt, (int)ntiles, fault);
   return cudaGetLastError();
-}
-
-template <int R2>
-cudaError_t launch_zw(const BornArgs& a, int jj, const DevFft& f, int* fault, cudaStream_t s) {
-  using L = ZwSmem<kR1 * R2>;
-  static DeviceFlags configured;   // attribute raised once per device
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  if (!configured.test(dev)) {
-    e = cudaFuncSetAttribute(born_z_warp_kernel<R2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)L::kTotal);
-    if (e != cudaSuccess) return e;
-    configured.set(dev);
-  }
-  CUtensorMap map;
-  if (!make_map(a, true, &map, false, true)) return cudaErrorInvalidValue;
-  int nsm = 0;
-  e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  if (e != cudaSuccess) return e;
-  const int nxt = (a.px + kW - 1) / kW;
-  const long long ntiles = (long long)a.py * a.nbatch * nxt;
-  int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, born_z_warp_kernel<R2>, kThreadsZW, L::kTotal);
-  if (e != cudaSuccess) return e;
-  if (per_sm < 1) return cudaErrorInvalidConfiguration;
-  const long long cap = (long long)per_sm * nsm;
-  const int grid = (int)(ntiles < cap ? ntiles : cap);
-  born_z_warp_kernel<R2><<<grid, kThreadsZW, L::kTotal, s>>>(map, a, jj, f.tw, nxt, (int)ntiles, fault);
-  return cudaGetLastError();
-}
-
-cudaError_t dispatch_zw(const BornArgs& a, int jj, const DevFft& f, int* fault, cudaStream_t s) {
-  switch (f.plan.n / kR1) {
-    case 11: return launch_zw<11>(a, jj, f, fault, s);
-    case 12: return launch_kind<12, 2>(a, jj, f, fault, s);   // even R2: rows of a half-warp would share chunks
-    case 15: return launch_zw<15>(a, jj, f, fault, s);
-    case 19: return launch_zw<19>(a, jj, f, fault, s);
-    case 25: return launch_zw<25>(a, jj, f, fault, s);
-    case 27: return launch_zw<27>(a, jj, f, fault, s);
-    default: return cudaErrorNotSupported;
-  }
 }
 
 template <int KIND>
@@ -748,12 +492,7 @@ cudaError_t launch_born_z_pipe(const BornArgs& a, int jj, const DevFft& fz, int*
     if (a.px % 8 != 0) return cudaErrorInvalidValue;   // 8-column exponent blocks, 16-byte rows
     return dispatch<3>(a, jj, fz, fault, s);
   }
-  // warp-owned columns by default; ODT_ZPASS=block selects the CTA-step kernel
-  static const bool block_steps = [] {
-    const char* e = std::getenv("ODT_ZPASS");
-    return e && std::string(e) == "block";
-  }();
-  return block_steps ? dispatch<2>(a, jj, fz, fault, s) : dispatch_zw(a, jj, fz, fault, s);
+  return dispatch<2>(a, jj, fz, fault, s);
 }
 
 }  // namespace odt

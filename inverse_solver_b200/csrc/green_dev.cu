@@ -17,6 +17,7 @@
 // reference's formula (ceil(1.556 n + 10), often prime).
 #include <cuda_runtime.h>
 
+#include <cstdlib>
 #include <string>
 
 #include "../../include/odt.h"
@@ -25,6 +26,10 @@
 
 namespace odt {
 const char* set_last_error(const std::string& msg);  // odt_api.cu
+// tcgen05 (TF32 split) complex GEMM, tc_gemm.cu
+cudaError_t tc_cgemm(int M, int N, int K, const float2* A, int lda, long long sA, const float2* B, int ldb,
+                     long long sB, bool transB, float2* C, int ldc, long long sC, int batch, int* fault,
+                     cudaStream_t s);
 }
 
 using namespace odt;
@@ -374,7 +379,8 @@ extern "C" odt_status odt_green_planes(const odt_green_args* a) {
     float2* T = B.get<float2>((size_t)o0 * S2 * nz);
     float2* Z = B.get<float2>(o01 * nz);
     float2* D = B.get<float2>(o01 * o2);
-    if (!g || !n1 || !n2 || !w || !m1 || !m2 || !mz || !G || !T || !Z || !D) {
+    int* fault = B.get<int>(1);
+    if (!g || !n1 || !n2 || !w || !m1 || !m2 || !mz || !G || !T || !Z || !D || !fault) {
       st = gfail(ODT_ERR_OUT_OF_MEMORY, "odt_green_planes: device allocation failed");
     } else {
       auto run = [&]() -> cudaError_t {
@@ -390,13 +396,26 @@ extern "C" odt_status odt_green_planes(const odt_green_args* a) {
           return e;
         radial_interp_kernel<<<grid_for(S * nz), kThreads, 0, s>>>(g, nr, n1, n2, w, S, nz, a->scale, G);
         if ((e = cudaGetLastError())) return e;
-        // T_z = M1 G_z ; Z_z = T_z M2^T ; D = Z Mz^T (Z viewed as [o0 o1, nz])
-        if ((e = cgemm(o0, S2, S1, m1, o0, 0, G, S1, S, false, T, o0, (long long)o0 * S2, nz, s)) ||
-            (e = cgemm(o0, o1, S2, T, o0, (long long)o0 * S2, m2, o1, 0, true, Z, o0, o01, nz, s)) ||
-            (e = cgemm((int)o01, o2, nz, Z, (int)o01, 0, mz, o2, 0, true, D, (int)o01, 0, 1, s)))
+        // T_z = M1 G_z ; Z_z = T_z M2^T ; D = Z Mz^T (Z viewed as [o0 o1, nz]):
+        // on the tensor cores (TF32 split, FP32 accuracy) unless
+        // ODT_GREEN_GEMM=simt selects the FP32 SIMT kernel
+        const char* gm = std::getenv("ODT_GREEN_GEMM");
+        const bool simt = gm && std::string(gm) == "simt";
+        if ((e = cudaMemsetAsync(fault, 0, sizeof(int), s))) return e;
+        auto gemm = [&](int M, int N, int K, const float2* A, int lda, long long sA, const float2* Bm, int ldb,
+                        long long sB, bool tB, float2* C, int ldc, long long sC, int nb) {
+          return simt ? cgemm(M, N, K, A, lda, sA, Bm, ldb, sB, tB, C, ldc, sC, nb, s)
+                      : tc_cgemm(M, N, K, A, lda, sA, Bm, ldb, sB, tB, C, ldc, sC, nb, fault, s);
+        };
+        if ((e = gemm(o0, S2, S1, m1, o0, 0, G, S1, S, false, T, o0, (long long)o0 * S2, nz)) ||
+            (e = gemm(o0, o1, S2, T, o0, (long long)o0 * S2, m2, o1, 0, true, Z, o0, o01, nz)) ||
+            (e = gemm((int)o01, o2, nz, Z, (int)o01, 0, mz, o2, 0, true, D, (int)o01, 0, 1)))
           return e;
         if ((e = cudaMemcpyAsync(a->out, D, o01 * o2 * sizeof(float2), cudaMemcpyDeviceToHost, s))) return e;
-        return cudaStreamSynchronize(s);
+        int f = 0;
+        if ((e = cudaMemcpyAsync(&f, fault, sizeof(int), cudaMemcpyDeviceToHost, s))) return e;
+        if ((e = cudaStreamSynchronize(s))) return e;
+        return f ? cudaErrorLaunchTimeout : cudaSuccess;
       };
       const cudaError_t e = run();
       if (e != cudaSuccess) {
