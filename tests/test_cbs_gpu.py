@@ -177,14 +177,20 @@ def test_nan_input_is_reported():
     s.delete()
 
 
-def test_unsupported_length_is_rejected():
+def test_prime_length_dyadic_solve_is_rejected():
+    """A padded length with a prime factor above 31 (29 + 2 * 4 = 37 along x)
+    runs through Bluestein transforms for scalar solves
+    (tests/test_any_length_gpu.py); the dyadic branch has no such path and is
+    refused with ODT_ERR_UNSUPPORTED, while the scalar solver of the same grid
+    is created."""
     from inverse_solver_b200 import OdtError
 
-    # 29 + 2*4 = 37 (prime) along x
     p = cases.params([29, 24, 16], [2, 2, 2])
+    _solver(p).delete()
+    pv = dict(p, vector_simulation=True)
     with pytest.raises(OdtError) as e:
-        _solver(p)
-    assert e.value.status == 6
+        _solver(pv)
+    assert e.value.status == 6 and "dyadic" in str(e.value)
 
 
 def test_solve_before_set_RI_and_bad_shapes():
