@@ -383,6 +383,8 @@ def run_fista(args):
                                   "multi-sphere phantom, %d ring illuminations, inner_itt 100, "
                                   "tv_param 7.5e-3" % fields.shape[3], "grid": grid,
                       "n_ill": int(fields.shape[3])}}
+    clk = ClockSampler(0)
+    clk.start()
     for device_loop in (True, False):
         bp = BACKWARD_SOLVER_MULTI.get_default_parameters(dict(
             RI_bg=nm, wavelength=0.532, NA=1.2, resolution=[0.1] * 3, size=grid,
@@ -400,6 +402,7 @@ def run_fista(args):
             times.append(time.perf_counter() - t0)
             b.delete()
         out["device_loop" if device_loop else "host_loop"] = (times[1] - times[0]) / args.steps
+    out["clocks"] = clk.stop()
     out["value"] = out["device_loop"]
     out["steps"] = args.steps
     print(json.dumps(out), flush=True)
@@ -425,6 +428,8 @@ def run_bpm(args):
     s.set_RI(RI)
     for _ in range(args.warmup):
         s.solve(fields)
+    clk = ClockSampler(0)
+    clk.start()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         s.solve(fields)
@@ -446,6 +451,7 @@ def run_bpm(args):
         s.solve_device(fin, tout, stream)
     e1.record(stream)
     torch.cuda.synchronize()
+    clocks = clk.stop()
     dev_ms = e0.elapsed_time(e1) / args.steps
     o = obpm.ForwardSolverBPM(p, single=True)
     o.set_RI(RI)
@@ -454,7 +460,7 @@ def run_bpm(args):
     dtc = time.perf_counter() - t0
     print(json.dumps({
         "metric": "BPM voxel-steps/s", "value": units / dt, "unit": "voxel-steps/s", "higher_is_better": True,
-        "ms_per_solve": dt * 1e3, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_solve": dt * 1e3, "steps": args.steps, "warmup": args.warmup, "clocks": clocks,
         "device_resident": {"value": units / (dev_ms / 1e3), "unit": "voxel-steps/s", "ms_per_solve": dev_ms},
         "config": {"workload": "FORWARD_SOLVER_BPM: 128^3 RI grid, 0.1 um voxels, seeded multi-sphere "
                                "phantom, %d ring illuminations, cos_correction, host API" % fields.shape[3]},
@@ -515,10 +521,13 @@ def run_retrieval(args):
     r = FIELD_EXPERIMENTAL_RETRIEVAL(p)
     for _ in range(args.warmup):
         r.get_fields(bg, sp)
+    clk = ClockSampler(0)
+    clk.start()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         r.get_fields(bg, sp)
     dt = (time.perf_counter() - t0) / args.steps
+    clocks = clk.stop()
 
     def unwrap(ph):
         out = goldstein.unwrapp2(ph)
@@ -552,7 +561,7 @@ def run_retrieval(args):
     side["get_aberration_pattern"]["cpu_port_fields_per_s"] = 7 / (time.perf_counter() - t0)
     print(json.dumps({
         "metric": "holograms/s", "value": n / dt, "unit": "holograms/s", "higher_is_better": True,
-        "ms_per_stack": dt * 1e3, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_stack": dt * 1e3, "steps": args.steps, "warmup": args.warmup, "clocks": clocks,
         "config": {"workload": "FIELD_EXPERIMENTAL_RETRIEVAL.get_fields: %d background / sample off-axis "
                                "holograms of %d x %d, 0.0625 um camera pixel, 0.1 um output" % (n, N, N)},
         "cpu_baseline": {"value": 2 / dtc, "unit": "holograms/s", "cores": os.cpu_count(), "kind": "port",

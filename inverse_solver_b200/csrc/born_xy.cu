@@ -86,6 +86,13 @@ struct XYSmem {
 // kernel carries none of the other cases' work)
 enum XYKind { kXYSteady = 0, kXYEarly = 1, kXYFinal = 2, kXYFirst = 3 };
 
+// *p += v component-wise in L2 (red.global.add.v2.f32: round to nearest;
+// subnormal inputs and results flush to zero, which the Born fields never
+// reach), with no value returned, so the thread does not wait for it
+__device__ __forceinline__ void red_add2(float2* p, float2 v) {
+  asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(v.x), "f"(v.y) : "memory");
+}
+
 // (i c) * v for real c: (-c v.y, c v.x), two products (a complex product
 // with (0, c) would also form 0 * v.x and 0 * v.y)
 __device__ __forceinline__ float2 mul_i(float c, float2 v) { return make_float2(-(c * v.y), c * v.x); }
@@ -139,7 +146,9 @@ __global__ void __launch_bounds__(32 * R, 1)
   // the final pass of a 2-iteration series); the incident field by the
   // source of iteration 1 and 2 and by the final pass
   const bool need_fn = kInv && e >= 3;
-  const bool need_f = kInv && (e >= 3 || (KIND == kXYFinal && e == 2));
+  // the steady kind only adds Field_n to Field, with a reduction in L2
+  // (red.global.add: no load of Field on the way)
+  const bool need_f = KIND != kXYSteady && kInv && (e >= 3 || (KIND == kXYFinal && e == 2));
   const bool need_e = KIND == kXYFinal || ((KIND == kXYFirst || KIND == kXYEarly) && jj <= 2);
 
   // ---- 1: y-F3^-1 (R-point over k2 at rows R k1 + k2) and twiddles of item
@@ -287,16 +296,22 @@ __global__ void __launch_bounds__(32 * R, 1)
             const float2 fp = Fp[r];
             const float2 psi = cmul(mul_i(a.c_im, fo), Vr);
             const float2 fn = cscale(cadd(csub(fo, psi), vP), m);
-            if (e == 3) {  // Field = (Field_n1 + Field_n2) + Field_n3; Field_n = Field_n3 + Field_n1
-              ftot = cadd(cadd(fp, fo), fn);
-              fn_new = cadd(fn, fp);
-            } else {
-              ftot = cadd(fp, fn);
+            if (KIND == kXYSteady) {   // e >= 4: Field += Field_n (the same IEEE add, done in L2)
               fn_new = fn;
-            }
-            if (KIND != kXYFinal) {
-              a.F[gy + x] = ftot;
+              red_add2(a.F + gy + x, fn);
               store_fn(r, x, fn_new);
+            } else {
+              if (e == 3) {  // Field = (Field_n1 + Field_n2) + Field_n3; Field_n = Field_n3 + Field_n1
+                ftot = cadd(cadd(fp, fo), fn);
+                fn_new = cadd(fn, fp);
+              } else {
+                ftot = cadd(fp, fn);
+                fn_new = fn;
+              }
+              if (KIND != kXYFinal) {
+                a.F[gy + x] = ftot;
+                store_fn(r, x, fn_new);
+              }
             }
           }
         }
@@ -447,7 +462,7 @@ cudaError_t launch_born_xy(const BornArgs& a, int mode, int jj, const DevFft& fx
   int kind;
   if (mode == kBornFirst) kind = kXYFirst;
   else if (mode == kBornLast) kind = kXYFinal;
-  else kind = jj <= 3 ? kXYEarly : kXYSteady;
+  else kind = jj <= 4 ? kXYEarly : kXYSteady;   // steady: e = jj - 1 >= 4 (Field += Field_n only)
   if ((mode == kBornFirst) != (jj == 1)) return cudaErrorInvalidValue;
   switch (a.px / 8) {
     case 11: return launch_kind<11>(a, kind, jj, fx.tw, s);

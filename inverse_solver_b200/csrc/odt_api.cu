@@ -662,7 +662,7 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
     a.Fn = nullptr;
   }
   for (int jj = 1; fused_xy && jj <= B; ++jj) {
-    H.mark_begin(jj <= 3 ? kKBornXYEdge : kKBornXY, s);
+    H.mark_begin(jj <= 4 ? kKBornXYEdge : kKBornXY, s);
     ODT_CUDA(launch_born_xy(a, jj == 1 ? kBornFirst : kBornMid, jj, H.fx, s));
     H.mark_end(s);
     H.mark_begin(pipe_z ? kKBornZPipe : kKBornZ, s);

@@ -56,7 +56,11 @@ constexpr int kEpiWarps = 4;                    // warps reading the accumulator
 constexpr int kThreads = 32 * (kEpiWarps + 1);  // + one warp issuing copies and MMAs
 constexpr int kTmemCols = 2 * kTN;              // two FP32 accumulators of 128 columns
 constexpr uint32_t kOpBytes = kTM * kTK * 4;    // one operand tile: 16 KB
-constexpr int kParts = 3;                       // TF32 parts per operand
+#ifndef ODT_TC_PARTS
+#define ODT_TC_PARTS 3
+#endif
+constexpr int kParts = ODT_TC_PARTS;            // TF32 parts per operand (2 or 3)
+static_assert(kParts == 2 || kParts == 3, "two or three TF32 parts");
 constexpr uint32_t kStageBytes = 2 * kParts * kOpBytes;  // A h, m, l; B h, m, l
 constexpr size_t kSmem = 1024 + 2 * (size_t)kStageBytes + 1024;   // barriers, 2 stages, alignment slack
 
@@ -134,14 +138,14 @@ __device__ __forceinline__ float to_tf32(float x) {
   return __uint_as_float(r);
 }
 
-// the three TF32 parts of x into out[i], out[total + i], out[2 total + i]
+// the TF32 parts of x into out[i], out[total + i] (, out[2 total + i])
 __device__ __forceinline__ void split3(float x, float* out, long long i, long long total) {
   const float h = to_tf32(x);
   const float r = x - h;   // exact
   const float m = to_tf32(r);
   out[i] = h;
   out[total + i] = m;
-  out[2 * total + i] = to_tf32(r - m);
+  if (kParts == 3) out[2 * total + i] = to_tf32(r - m);
 }
 #endif
 
@@ -268,15 +272,20 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (!ok) break;
         tc_fence_after();
         const uint32_t acc = tmem + (uint32_t)(t * kTN);
-        const uint32_t a_h = smem_addr(stage(st, 0)), a_m = smem_addr(stage(st, 1)), a_l = smem_addr(stage(st, 2));
-        const uint32_t b_h = smem_addr(stage(st, 3)), b_m = smem_addr(stage(st, 4)), b_l = smem_addr(stage(st, 5));
+        const uint32_t a_h = smem_addr(stage(st, 0)), a_m = smem_addr(stage(st, 1));
+        const uint32_t b_h = smem_addr(stage(st, kParts)), b_m = smem_addr(stage(st, kParts + 1));
 #pragma unroll
         for (int ks = 0; ks < kTK / 8; ++ks) {   // 8 TF32 = 32 bytes of K per MMA
           const uint32_t o = 32u * ks;
-          umma_tf32(acc, sw128_desc(a_l + o), sw128_desc(b_h + o), ks > 0 ? 1u : 0u);
-          umma_tf32(acc, sw128_desc(a_h + o), sw128_desc(b_l + o), 1u);
-          umma_tf32(acc, sw128_desc(a_m + o), sw128_desc(b_m + o), 1u);
-          umma_tf32(acc, sw128_desc(a_m + o), sw128_desc(b_h + o), 1u);
+          if constexpr (kParts == 3) {   // l h + h l + m m + m h + h m + h h
+            const uint32_t a_l = smem_addr(stage(st, 2)), b_l = smem_addr(stage(st, 5));
+            umma_tf32(acc, sw128_desc(a_l + o), sw128_desc(b_h + o), ks > 0 ? 1u : 0u);
+            umma_tf32(acc, sw128_desc(a_h + o), sw128_desc(b_l + o), 1u);
+            umma_tf32(acc, sw128_desc(a_m + o), sw128_desc(b_m + o), 1u);
+            umma_tf32(acc, sw128_desc(a_m + o), sw128_desc(b_h + o), 1u);
+          } else {                       // m h + h m + h h (m is the second, last part)
+            umma_tf32(acc, sw128_desc(a_m + o), sw128_desc(b_h + o), ks > 0 ? 1u : 0u);
+          }
           umma_tf32(acc, sw128_desc(a_h + o), sw128_desc(b_m + o), 1u);
           umma_tf32(acc, sw128_desc(a_h + o), sw128_desc(b_h + o), 1u);
         }

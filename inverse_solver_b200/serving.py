@@ -18,6 +18,7 @@ are deterministic.  Latency = completion - arrival on the host clock.
 """
 from __future__ import annotations
 
+import contextlib
 import copy
 import threading
 import time
@@ -75,6 +76,49 @@ def solver_bytes(p, n_ill, max_batch=16):
     return static + nb * per
 
 
+class DeviceGate:
+    """Shared for ordinary device work, exclusive for timing.  Plan
+    autotuning (odt_autotune) measures kernel times, so it must have the GPU
+    to itself: exclusive() waits until the work already running in shared()
+    sections has finished (the solves are synchronous host calls) and holds
+    new shared sections back until it is done; a waiting exclusive section
+    goes before shared sections that arrive after it."""
+
+    def __init__(self):
+        self._cv = threading.Condition()
+        self._shared = 0
+        self._exclusive = False
+        self._waiting = 0
+
+    @contextlib.contextmanager
+    def shared(self):
+        with self._cv:
+            while self._exclusive or self._waiting:
+                self._cv.wait()
+            self._shared += 1
+        try:
+            yield
+        finally:
+            with self._cv:
+                self._shared -= 1
+                self._cv.notify_all()
+
+    @contextlib.contextmanager
+    def exclusive(self):
+        with self._cv:
+            self._waiting += 1
+            while self._exclusive or self._shared:
+                self._cv.wait()
+            self._waiting -= 1
+            self._exclusive = True
+        try:
+            yield
+        finally:
+            with self._cv:
+                self._exclusive = False
+                self._cv.notify_all()
+
+
 class SolveServer:
     """Admits requests by device-memory budget and runs up to ``slots`` of
     them at once.  ``execute(request)`` and ``estimate(request)`` (bytes)
@@ -109,6 +153,7 @@ class SolveServer:
         self._idle = []           # (key, solver, bytes) in release order, for eviction
         self._held = 0.0          # bytes of all live solvers, idle or busy
         self._pool_lock = threading.Lock()
+        self._gate = DeviceGate()   # requests run shared, autotuning exclusive
         self._threads = [threading.Thread(target=self._loop, daemon=True) for _ in range(self.slots)]
         for t in self._threads:
             t.start()
@@ -243,26 +288,34 @@ class SolveServer:
     def _execute(self, req):
         need = self._estimate(req)
         if isinstance(req, ForwardRequest):
-            key, s, b = self._acquire(req.params, need)
+            with self._gate.shared():
+                key, s, b = self._acquire(req.params, need)
             try:
-                set_ri_on_device(s, req.RI)
-                if getattr(s, "_needs_tune", False):   # once per solver, after its first potential
-                    s._needs_tune = False
-                    self.plans[key] = s.autotune(min(req.fields.shape[3], self.max_batch))
-                return s.solve(req.fields)
+                if getattr(s, "_needs_tune", False):   # once per solver, after its first potential,
+                    s._needs_tune = False               # with the GPU to itself
+                    with self._gate.exclusive():
+                        set_ri_on_device(s, req.RI)
+                        self.plans[key] = s.autotune(min(req.fields.shape[3], self.max_batch))
+                    with self._gate.shared():
+                        return s.solve(req.fields)
+                with self._gate.shared():
+                    set_ri_on_device(s, req.RI)
+                    return s.solve(req.fields)
             finally:
                 self._release(key, s, b)
         from .backward import BACKWARD_SOLVER_MULTI
 
         fp = req.params["forward_solver_parameters"]
-        key, s, b = self._acquire(fp, need)
+        with self._gate.shared():
+            key, s, b = self._acquire(fp, need)
         try:
             p = dict(req.params)
             RI0 = req.RI0
             p["init_solver"] = type("Init", (), {"solve": staticmethod(lambda a, b: RI0)})
             bs = BACKWARD_SOLVER_MULTI(p, init_solver=False)
             bs.forward_solver = s
-            return bs.solve(req.fields_in, req.fields_out)
+            with self._gate.shared():
+                return bs.solve(req.fields_in, req.fields_out)
         finally:
             self._release(key, s, b)
 

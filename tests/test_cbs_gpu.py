@@ -178,14 +178,14 @@ def test_nan_input_is_reported():
 
 
 def test_prime_length_dyadic_solve_is_rejected():
-    """A padded length with a prime factor above 31 (29 + 2 * 4 = 37 along x)
-    runs through Bluestein transforms for scalar solves
-    (tests/test_any_length_gpu.py); the dyadic branch has no such path and is
-    refused with ODT_ERR_UNSUPPORTED, while the scalar solver of the same grid
-    is created."""
+    """Padded lengths with a prime factor above 31 (29 + 2 * 4 = 37 along x
+    and y; the dyadic solver needs a square field) run through Bluestein
+    transforms for scalar solves (tests/test_any_length_gpu.py); the dyadic
+    branch has no such path and is refused with ODT_ERR_UNSUPPORTED, while
+    the scalar solver of the same grid is created."""
     from inverse_solver_b200 import OdtError
 
-    p = cases.params([29, 24, 16], [2, 2, 2])
+    p = cases.params([29, 29, 16], [2, 2, 2])
     _solver(p).delete()
     pv = dict(p, vector_simulation=True)
     with pytest.raises(OdtError) as e:

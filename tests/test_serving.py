@@ -73,3 +73,45 @@ def test_oversized_and_failing_requests():
     res, _, _, _ = _run(reqs, budget=5.0, slots=2)
     assert res[0] == 0 and res[3] == 30
     assert isinstance(res[1], MemoryError) and isinstance(res[2], RuntimeError)
+
+
+def test_device_gate_gives_autotuning_the_device_alone():
+    """DeviceGate: an exclusive section (plan autotuning) starts only after
+    the shared sections already running (requests) have ended, and shared
+    sections arriving while it waits or runs are held back until it ends."""
+    import threading
+    import time as _time
+
+    from inverse_solver_b200.serving import DeviceGate
+
+    g = DeviceGate()
+    log = []
+    lock = threading.Lock()
+
+    def note(x):
+        with lock:
+            log.append(x)
+
+    def shared(name, hold):
+        with g.shared():
+            note(name + "+")
+            _time.sleep(hold)
+            note(name + "-")
+
+    def exclusive():
+        with g.exclusive():
+            note("X+")
+            _time.sleep(0.05)
+            note("X-")
+
+    a = threading.Thread(target=shared, args=("a", 0.2))
+    a.start()
+    _time.sleep(0.05)                      # a is running
+    x = threading.Thread(target=exclusive)
+    x.start()
+    _time.sleep(0.05)                      # x waits for a
+    b = threading.Thread(target=shared, args=("b", 0.0))
+    b.start()                              # b arrives after x: waits for x
+    for t in (a, x, b):
+        t.join(5)
+    assert log == ["a+", "a-", "X+", "X-", "b+", "b-"], log
