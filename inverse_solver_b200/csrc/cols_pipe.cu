@@ -28,7 +28,6 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
-#include <cstdlib>
 #include <string>
 
 #include "b16.cuh"
@@ -366,183 +365,6 @@ __global__ void __launch_bounds__(threads_of<KIND>(), KIND >= 2 ? (R2 <= 19 ? 5 
 #endif
 }
 
-// ------------------------------------------------------------------------
-// z-pass (complex64 storage) with two CTA barriers per tile instead of
-// three: step C of tile t reads only its own stage and step A of tile t + 1
-// works only on the other one, so they run in the same phase:
-//   A(t0) | sync | B(t) | sync | C(t), A(t + 1) | sync | [refill stage of t] | B(t + 1) ...
-// The refill of a stage is issued as soon as its tile's step C is done, a
-// whole step B ahead of its step A.  Steps A, B and C are those of
-// cols_pipe_kernel<R2, 2> (same operations, same results).
-template <int R2>
-__global__ void __launch_bounds__(kThreadsZ, R2 <= 19 ? 5 : 4)
-    zpass_kernel(const __grid_constant__ CUtensorMap map, const BornArgs a, const int jj,
-                 const float2* __restrict__ twg, const int nxt, const int ntiles, int* __restrict__ fault) {
-#if defined(__CUDA_ARCH__)
-  constexpr int N = kR1 * R2;
-  constexpr int kT = kThreadsZ;
-  using L = ColSmem<N>;
-  extern __shared__ __align__(128) unsigned char sm[];
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
-  float2* tw = reinterpret_cast<float2*>(sm + L::kTw);
-  float* kz = reinterpret_cast<float*>(sm + L::kKz);
-  float* gxy = reinterpret_cast<float*>(sm + L::kGxy);
-  float2* const s0 = reinterpret_cast<float2*>(sm + L::kS0);
-  float2* const s1 = reinterpret_cast<float2*>(sm + L::kS1);
-  const int tid = threadIdx.x;
-  const bool flip = a.acyclic && (jj & 1);
-  if ((smem_addr(s0) & 127u) != 0u || (smem_addr(s1) & 127u) != 0u) {  // never issue a misaligned copy
-    if (tid == 0) atomicCAS(fault, 0, kFaultAlign);
-    return;
-  }
-  for (int i = tid; i < N; i += kT) {
-    tw[i] = twg[i];
-    kz[i] = a.kq2[2][flip ? (i == 0 ? 0 : N - i) : i];
-  }
-  if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-  int tile = blockIdx.x;
-  if (tile >= ntiles) return;
-  const long long rstride = (long long)a.px * a.py;   // element stride between z-rows
-  constexpr uint32_t kBytes = (uint32_t)(sizeof(float2) * N * kW);
-  auto issue = [&](int t, int stage) {
-    const int xt = t % nxt, o = t / nxt;
-    mbar_arrive_expect_tx(&bar[stage], kBytes);
-    tma_load_4d(stage ? s1 : s0, &map, 2 * kW * xt, o % a.py, 0, o / a.py, &bar[stage]);
-  };
-  const int c = tid & (kW - 1), jr = tid >> 4;
-  // per-column Green's factor kq2x + kq2y of tile t (threads 0-15)
-  auto green_xy = [&](int t) {
-    if (tid < kW) {
-      const int xt = t % nxt, o = t / nxt;
-      int y = o % a.py;
-      int kx = min(kW * xt + tid, a.px - 1);
-      if (a.perm_xy) {   // position R k1 + k2 holds spectral index k1 + 8 k2
-        const int rx = a.px >> 3, ry = a.py >> 3;
-        kx = kx / rx + 8 * (kx % rx);
-        y = y / ry + 8 * (y % ry);
-      }
-      const int ix = flip ? (kx == 0 ? 0 : a.px - kx) : kx;
-      const int iy = flip ? (y == 0 ? 0 : a.py - y) : y;
-      gxy[tid] = a.kq2[0][ix] + a.kq2[1][iy];
-    }
-  };
-  // A: 8-point DFT over n1 at rows R2 n1 + n2, times W_N^(n2 k1), in place
-  auto step_a = [&](float2* S) {
-    for (int idx = tid; idx < kW * R2; idx += kT) {
-      const int n2 = idx >> 4;  // column c is idx & 15 == tid & 15
-      float2 v[kR1];
-#pragma unroll
-      for (int r = 0; r < kR1; ++r) v[r] = S[(R2 * r + n2) * kW + c];
-      Butterfly<kR1, false>::run(v, tw, N);
-#pragma unroll
-      for (int r = 1; r < kR1; ++r) v[r] = cmul(v[r], tw[r * n2]);
-#pragma unroll
-      for (int r = 0; r < kR1; ++r) S[(R2 * r + n2) * kW + c] = v[r];
-    }
-  };
-  // tid 0: tiles whose copies it issued and has not yet seen land
-  int pend = 0;                  // bit s: stage s
-  const int t1 = tile + gridDim.x;
-  if (tid == 0) {
-    issue(tile, 0);
-    pend = 1;
-    if (t1 < ntiles) {
-      issue(t1, 1);
-      pend |= 2;
-    }
-  }
-  green_xy(tile);
-  bool ok = mbar_wait(&bar[0], 0u, a.wait_limit);
-  if (__syncthreads_or(!ok)) {
-    if (tid == 0) {   // give up; let the copies in flight land first
-      atomicCAS(fault, 0, kFaultTimeout);
-      mbar_wait(&bar[0], 0u);
-      if (pend & 2) mbar_wait(&bar[1], 0u);
-    }
-    return;
-  }
-  if (tid == 0) pend &= ~1;
-  step_a(s0);
-  __syncthreads();
-  for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
-    const int s = it & 1;
-    float2* S = s ? s1 : s0;
-    // B: per (column, k1) the R2-point DFT over n2 at rows R2 k1 + n2 (kz =
-    //    k1 + 8 k2), the Green's multiply, the inverse R2-point DFT
-    if (tid < kW * kR1) {
-      const int k1 = jr;
-      float2 v[R2];
-#pragma unroll
-      for (int r = 0; r < R2; ++r) v[r] = S[(R2 * k1 + r) * kW + c];
-      Butterfly<R2, false>::run(v, tw, N);
-      const float qxy = gxy[c];
-#pragma unroll
-      for (int r = 0; r < R2; ++r) {
-        float q = qxy + kz[k1 + kR1 * r];
-        q = a.g_scale * q - a.g_off;
-        const float rden = rcp_approx(q * q + a.eps * a.eps) * a.inv_n;
-        const float2 G = make_float2(q * rden, a.eps * rden);  // (1 / (q - i eps)) / N
-        v[r] = cmul(G, v[r]);
-      }
-      Butterfly<R2, true>::run(v, tw, N);
-#pragma unroll
-      for (int r = 1; r < R2; ++r) v[r] = cmul(v[r], cconj(tw[r * k1]));
-#pragma unroll
-      for (int r = 0; r < R2; ++r) S[(R2 * k1 + r) * kW + c] = v[r];
-    }
-    __syncthreads();
-    // C: inverse 8-point DFT over k1 -> rows R2 n1 + n2 of T
-    {
-      const int xt = tile % nxt, o = tile / nxt;
-      const int x0 = kW * xt;
-      const int ncol = min(kW, a.px - x0);
-      const int y = o % a.py, b = o / a.py;
-      const long long gbase = (long long)b * a.nvox + (long long)y * a.px + x0;
-      for (int idx = tid; idx < kW * R2; idx += kT) {
-        const int n2 = idx >> 4;
-        float2 v[kR1];
-#pragma unroll
-        for (int r = 0; r < kR1; ++r) v[r] = S[(R2 * r + n2) * kW + c];
-        Butterfly<kR1, true>::run(v, tw, N);
-        if (c < ncol) {
-          float2* out = a.T + gbase + c;
-#pragma unroll
-          for (int r = 0; r < kR1; ++r) out[(R2 * r + n2) * rstride] = v[r];
-        }
-      }
-    }
-    // ... and A of the next tile on the other stage
-    const int next = tile + gridDim.x;
-    ok = true;
-    if (next < ntiles) {
-      green_xy(next);   // gxy of tile t is no longer read (step B is done)
-      ok = mbar_wait(&bar[s ^ 1], (uint32_t)((it + 1) >> 1) & 1u, a.wait_limit);
-    }
-    if (__syncthreads_or(!ok)) {
-      if (tid == 0) {
-        atomicCAS(fault, 0, kFaultTimeout);
-        if (pend & (1 << (s ^ 1))) mbar_wait(&bar[s ^ 1], (uint32_t)((it + 1) >> 1) & 1u);
-      }
-      return;
-    }
-    if (tid == 0) pend &= ~(1 << (s ^ 1));
-    if (next < ntiles) step_a(s ? s0 : s1);
-    __syncthreads();   // C(t) and A(next) done: stage s is free again
-    const int after = next + gridDim.x;
-    if (tid == 0 && after < ntiles) {
-      fence_proxy_async();
-      issue(after, s);
-      pend |= 1 << s;
-    }
-  }
-#endif
-}
-
 PFN_cuTensorMapEncodeTiled_v12000 encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -629,48 +451,6 @@ cudaError_t launch_kind(const BornArgs& a, int jj, const DevFft& f, int* fault, 
   return cudaGetLastError();
 }
 
-template <int R2>
-cudaError_t launch_zpass(const BornArgs& a, int jj, const DevFft& f, int* fault, cudaStream_t s) {
-  using L = ColSmem<kR1 * R2>;
-  constexpr size_t smem = L::kTotalZ;
-  static DeviceFlags configured;   // attribute raised once per device
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  if (!configured.test(dev)) {
-    e = cudaFuncSetAttribute(zpass_kernel<R2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    configured.set(dev);
-  }
-  CUtensorMap map;
-  if (!make_map(a, true, &map, false)) return cudaErrorInvalidValue;
-  int nsm = 0;
-  e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  if (e != cudaSuccess) return e;
-  const int nxt = (a.px + kW - 1) / kW;
-  const long long ntiles = (long long)a.py * a.nbatch * nxt;
-  int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, zpass_kernel<R2>, kThreadsZ, smem);
-  if (e != cudaSuccess) return e;
-  if (per_sm < 1) return cudaErrorInvalidConfiguration;
-  const long long cap = (long long)per_sm * nsm;
-  const int grid = (int)(ntiles < cap ? ntiles : cap);
-  zpass_kernel<R2><<<grid, kThreadsZ, smem, s>>>(map, a, jj, f.tw, nxt, (int)ntiles, fault);
-  return cudaGetLastError();
-}
-
-cudaError_t dispatch_zpass(const BornArgs& a, int jj, const DevFft& f, int* fault, cudaStream_t s) {
-  switch (f.plan.n / kR1) {
-    case 11: return launch_zpass<11>(a, jj, f, fault, s);
-    case 12: return launch_zpass<12>(a, jj, f, fault, s);
-    case 15: return launch_zpass<15>(a, jj, f, fault, s);
-    case 19: return launch_zpass<19>(a, jj, f, fault, s);
-    case 25: return launch_zpass<25>(a, jj, f, fault, s);
-    case 27: return launch_zpass<27>(a, jj, f, fault, s);
-    default: return cudaErrorNotSupported;
-  }
-}
-
 template <int KIND>
 cudaError_t dispatch(const BornArgs& a, int jj, const DevFft& f, int* fault, cudaStream_t s) {
   switch (f.plan.n / kR1) {
@@ -712,12 +492,7 @@ cudaError_t launch_born_z_pipe(const BornArgs& a, int jj, const DevFft& fz, int*
     if (a.px % 8 != 0) return cudaErrorInvalidValue;   // 8-column exponent blocks, 16-byte rows
     return dispatch<3>(a, jj, fz, fault, s);
   }
-  // two barriers per tile; ODT_ZPASS=three selects the three-barrier kernel
-  static const bool three = [] {
-    const char* e = std::getenv("ODT_ZPASS");
-    return e && std::string(e) == "three";
-  }();
-  return three ? dispatch<2>(a, jj, fz, fault, s) : dispatch_zpass(a, jj, fz, fault, s);
+  return dispatch<2>(a, jj, fz, fault, s);
 }
 
 }  // namespace odt
