@@ -71,8 +71,10 @@ struct PipeSmem {
 // W = 16 x-lines per tile (two CTAs per SM) where the shared memory allows,
 // else 8 (n = 200, 216: three CTAs per SM).  KIND (compile time, so the
 // steady-state kernel carries none of the other cases' work):
-//   kSteady: jj >= 4 (update of iteration jj-1 >= 3, source V .* Field_n)
-//   kEarly:  jj = 2, 3 (first updates, incident-field source for jj = 2)
+//   kSteady: jj >= 5 (update of iteration jj-1 >= 4: Field += Field_n,
+//            reduced in L2; source V .* Field_n)
+//   kEarly:  jj = 2, 3, 4 (first updates, the e = 3 bookkeeping, incident-
+//            field source for jj = 2)
 //   kFinal:  the final pass (update of the last iteration, Field(ROI) +
 //            incident field into Fout, :646-647; no source, no forward FFT)
 enum PipeKind { kSteady = 0, kEarly = 1, kFinal = 2 };
@@ -136,14 +138,17 @@ __global__ void __launch_bounds__(W * 8, W == 16 ? 2 : 3)
     mbar_arrive_expect_tx(&bar[stage], bytes);
     bulk_g2s(stage ? sT1 : sT0, a.T + tile_off(b, y0, z), bytes, &bar[stage]);
   };
+  // the steady kind only adds Field_n to Field (red_add2 in L2): no copy of
+  // Field into shared memory
+  constexpr bool kLoadF = KIND != kSteady;
   auto issue_F = [&](int t) {
     int b, y0, z, nl;
     decode(t, b, y0, z, nl);
     const uint32_t bytes = (uint32_t)(nl * N * sizeof(float2));
     const long long o = tile_off(b, y0, z);
-    mbar_arrive_expect_tx(&bar[2], 2 * bytes);
+    mbar_arrive_expect_tx(&bar[2], kLoadF ? 2 * bytes : bytes);
     bulk_g2s(sFn, a.Fn + o, bytes, &bar[2]);
-    bulk_g2s(sF, a.F + o, bytes, &bar[2]);
+    if (kLoadF) bulk_g2s(sF, a.F + o, bytes, &bar[2]);
   };
   if (tid == 0) {
     issue_T(tile, 0);
@@ -320,6 +325,16 @@ __global__ void __launch_bounds__(W * 8, W == 16 ? 2 : 3)
             a.Fn[Ln.g + x] = fn_new;
             if (e == 1) a.F[Ln.g + x] = fn_new;
           }
+        } else if (KIND == kSteady) {   // e >= 4: Field += Field_n (the same IEEE add, done in L2)
+          const float2 fo = sFn[c * N + x];
+          const float2 psi = cmul(cmul(cc, fo), V);
+          const float2 fn = cscale(cadd(csub(fo, psi), vP), m);
+          fn_new = fn;
+          ftot = z2;   // not used by this kind
+          if (Ln.valid) {
+            red_add2(a.F + Ln.g + x, fn);
+            a.Fn[Ln.g + x] = fn_new;
+          }
         } else {
           const float2 fo = sFn[c * N + x];
           const float2 fp = sF[c * N + x];
@@ -452,7 +467,7 @@ bool born_x_pipe_supported(const BornArgs& a, const DevFft& fx) {
 cudaError_t launch_born_x_pipe(const BornArgs& a, int mode, int jj, const DevFft& fx, int* fault,
                                cudaStream_t s) {
   if (jj < 2 || (mode != kBornMid && mode != kBornLast)) return cudaErrorInvalidValue;
-  const int kind = mode == kBornLast ? kFinal : (jj <= 3 ? kEarly : kSteady);
+  const int kind = mode == kBornLast ? kFinal : (jj <= 4 ? kEarly : kSteady);
   switch (a.px / kR1) {
 #define ODT_PIPE_CASE(R)                                                     \
   case R:                                                                    \

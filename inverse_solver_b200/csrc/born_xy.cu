@@ -86,13 +86,6 @@ struct XYSmem {
 // kernel carries none of the other cases' work)
 enum XYKind { kXYSteady = 0, kXYEarly = 1, kXYFinal = 2, kXYFirst = 3 };
 
-// *p += v component-wise in L2 (red.global.add.v2.f32: round to nearest;
-// subnormal inputs and results flush to zero, which the Born fields never
-// reach), with no value returned, so the thread does not wait for it
-__device__ __forceinline__ void red_add2(float2* p, float2 v) {
-  asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(v.x), "f"(v.y) : "memory");
-}
-
 // (i c) * v for real c: (-c v.y, c v.x), two products (a complex product
 // with (0, c) would also form 0 * v.x and 0 * v.y)
 __device__ __forceinline__ float2 mul_i(float c, float2 v) { return make_float2(-(c * v.y), c * v.x); }

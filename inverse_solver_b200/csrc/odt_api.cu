@@ -684,7 +684,7 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
       ODT_CUDA(launch_born_tensor_point(a, P.V9, jj == 1 ? kBornFirst : kBornMid, jj, s));
       ODT_CUDA(launch_fft_lines(a.T, a.T, xlines, 0, 0, 1.0f, false, H.fx, s));
     } else if (pipe_x && jj >= 2) {
-      H.mark_begin(jj <= 3 ? kKBornXPipeEdge : kKBornXPipe, s);
+      H.mark_begin(jj <= 4 ? kKBornXPipeEdge : kKBornXPipe, s);
       ODT_CUDA(launch_born_x_pipe(a, kBornMid, jj, H.fx, H.d_fault, s));
     } else {
       H.mark_begin(kKBornX, s);

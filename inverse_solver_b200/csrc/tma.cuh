@@ -95,6 +95,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long l
   return true;
 }
 
+// *p += v component-wise in L2 (red.global.add.v2.f32: round to nearest;
+// subnormal inputs and results flush to zero, which the Born fields never
+// reach), with no value returned, so the thread does not wait for it: the
+// steady Born passes accumulate Field this way
+__device__ __forceinline__ void red_add2(float2* p, float2 v) {
+  asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(v.x), "f"(v.y) : "memory");
+}
+
 #endif  // __CUDA_ARCH__
 
 // Host side: one flag per (kernel instantiation, device) saying that the
