@@ -17,6 +17,7 @@
 // reference's formula (ceil(1.556 n + 10), often prime).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdlib>
 #include <string>
 
@@ -28,8 +29,9 @@ namespace odt {
 const char* set_last_error(const std::string& msg);  // odt_api.cu
 // tcgen05 (TF32 split) complex GEMM, tc_gemm.cu
 cudaError_t tc_cgemm(int M, int N, int K, const float2* A, int lda, long long sA, const float2* B, int ldb,
-                     long long sB, bool transB, float2* C, int ldc, long long sC, int batch, int* fault,
-                     cudaStream_t s);
+                     long long sB, bool transB, float2* C, int ldc, long long sC, int batch, float* work,
+                     long long work_floats, int* fault, cudaStream_t s);
+long long tc_cgemm_work(int M, int N, int K, bool batchedA, bool batchedB, int batch);
 }
 
 using namespace odt;
@@ -402,10 +404,20 @@ extern "C" odt_status odt_green_planes(const odt_green_args* a) {
         const char* gm = std::getenv("ODT_GREEN_GEMM");
         const bool simt = gm && std::string(gm) == "simt";
         if ((e = cudaMemsetAsync(fault, 0, sizeof(int), s))) return e;
+        // one operand workspace for the three tensor-core GEMMs
+        float* work = nullptr;
+        long long work_n = 0;
+        if (!simt) {
+          work_n = std::max(std::max(tc_cgemm_work(o0, S2, S1, false, true, nz),
+                                     tc_cgemm_work(o0, o1, S2, true, false, nz)),
+                            tc_cgemm_work((int)o01, o2, nz, false, false, 1));
+          work = B.get<float>((size_t)work_n);
+          if (!work) return cudaErrorMemoryAllocation;
+        }
         auto gemm = [&](int M, int N, int K, const float2* A, int lda, long long sA, const float2* Bm, int ldb,
                         long long sB, bool tB, float2* C, int ldc, long long sC, int nb) {
           return simt ? cgemm(M, N, K, A, lda, sA, Bm, ldb, sB, tB, C, ldc, sC, nb, s)
-                      : tc_cgemm(M, N, K, A, lda, sA, Bm, ldb, sB, tB, C, ldc, sC, nb, fault, s);
+                      : tc_cgemm(M, N, K, A, lda, sA, Bm, ldb, sB, tB, C, ldc, sC, nb, work, work_n, fault, s);
         };
         if ((e = gemm(o0, S2, S1, m1, o0, 0, G, S1, S, false, T, o0, (long long)o0 * S2, nz)) ||
             (e = gemm(o0, o1, S2, T, o0, (long long)o0 * S2, m2, o1, 0, true, Z, o0, o01, nz)) ||

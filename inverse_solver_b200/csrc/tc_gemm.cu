@@ -3,15 +3,14 @@
 // (green_dev.cu: the three chains of centred DFT maps of
 // truncated_green_plus.m:67-110).
 //
-// FP32 accuracy from TF32 operands: every operand is split into three TF32
-// parts x = h + m + l (h = tf32(x), m = tf32(x - h), l = tf32(x - h - m),
-// round to nearest; 33 significant bits), and the accumulator (FP32 in
-// tensor memory) takes the six products whose parts sum to at most 2^-22 of
-// the product, l*h + h*l + m*m + m*h + h*m + h*h, smallest first: the
-// dropped terms are below 2^-33 of each product, so FP32 accumulation sets
-// the accuracy, as in a SIMT FP32 GEMM (with two parts and three products
-// the results were 4x less accurate: 2.1e-6 against 5.6e-7 rel-L2 on the
-// Green's function planes).
+// FP32 accuracy from TF32 operands: every operand is split into two TF32
+// parts x = h + m (h = tf32(x), m = tf32(x - h), round to nearest; 22
+// significant bits) and the accumulator takes m*h + h*m + h*h, smallest
+// first (the dropped m*m and the split's remainder are near 2^-22 of each
+// product).  A three-part split (h, m, l = tf32(x - h - m)) with six products
+// is kept as a build option (ODT_TC_PARTS=3); it measured no more accurate
+// (8.3e-7 against 8.1e-7 - 8.6e-7 rel-L2 on the Green's function planes)
+// once the K sums are taken in FP32 registers (below).
 //
 // The complex product C = A B is one real GEMM of twice the size with the
 // interleaved complex layout kept on the A side:
@@ -19,19 +18,20 @@
 //   B'^T[2n + j][2k + c] = [[Re B, -Im B], [Im B, Re B]](k, n)[j][c] (2N x 2K)
 //   C'[m][2n + j]      = (Re, Im)(C(m, n))[j]
 // Both operands are K-major (rows of 2K reals), written by a conversion
-// kernel together with their three-part split, zero-padded to whole tiles.
+// kernel together with their TF32 split, zero-padded to whole tiles, into a
+// workspace the caller provides (tc_cgemm_work floats).
 //
 // The tensor cores' own accumulation over K is not IEEE-rounded FP32: over
 // the Green's function GEMMs (K up to 2 x 409 reals) it left 2.1e-6 rel-L2
 // against the host build, with two-part and with three-part operands alike,
 // where the FP32 SIMT GEMM leaves 5.6e-7.  So every 32-wide K block is
 // accumulated afresh in tensor memory and the blocks are added in FP32
-// registers: 8.3e-7.
+// registers: 8.1e-7 - 8.6e-7.
 //
 // Kernel: one CTA of 160 threads per 128 x 128 tile of C' (and batch
 // entry).  Warp 4 (one thread) issues the tiled copies (cp.async.bulk.tensor,
 // 128-byte swizzle, 128 rows x 32 reals per operand part and stage, two
-// stages) and the MMAs (M = 128, N = 128, K = 8 per instruction, 24 per K
+// stages) and the MMAs (M = 128, N = 128, K = 8 per instruction, 12 per K
 // block) into one of two 128 x 128 FP32 accumulators in tensor memory;
 // tcgen05.commit hands a stage back once its MMAs have read it and tells the
 // epilogue that the accumulator is complete.  Warps 0-3 (rows 32 w ..
@@ -57,11 +57,11 @@ constexpr int kThreads = 32 * (kEpiWarps + 1);  // + one warp issuing copies and
 constexpr int kTmemCols = 2 * kTN;              // two FP32 accumulators of 128 columns
 constexpr uint32_t kOpBytes = kTM * kTK * 4;    // one operand tile: 16 KB
 #ifndef ODT_TC_PARTS
-#define ODT_TC_PARTS 3
+#define ODT_TC_PARTS 2
 #endif
 constexpr int kParts = ODT_TC_PARTS;            // TF32 parts per operand (2 or 3)
 static_assert(kParts == 2 || kParts == 3, "two or three TF32 parts");
-constexpr uint32_t kStageBytes = 2 * kParts * kOpBytes;  // A h, m, l; B h, m, l
+constexpr uint32_t kStageBytes = 2 * kParts * kOpBytes;  // the parts of A, then of B
 constexpr size_t kSmem = 1024 + 2 * (size_t)kStageBytes + 1024;   // barriers, 2 stages, alignment slack
 
 // instruction descriptor: D FP32, A and B TF32, both K-major, N = 128, M = 128
@@ -387,46 +387,48 @@ int grid_for(long long n) {
 // SIMT cgemm (op(B) = B [K x N] with ldb, or transB: B stored [N x K]); a
 // batch stride of 0 shares the operand across the batch.  *fault (device
 // int) receives a timeout / alignment code.
+// Floats of operand workspace tc_cgemm needs for these sizes (the TF32 parts
+// of both operands, padded to whole tiles).
+long long tc_cgemm_work(int M, int N, int K, bool batchedA, bool batchedB, int batch) {
+  const long long Mp = (M + kTM - 1) / kTM * kTM;
+  const long long Np = (2LL * N + kTN - 1) / kTN * kTN;
+  const long long Kp = (2LL * K + kTK - 1) / kTK * kTK;
+  return kParts * ((batchedA ? batch : 1) * Mp * Kp + (batchedB ? batch : 1) * Np * Kp);
+}
+
 cudaError_t tc_cgemm(int M, int N, int K, const float2* A, int lda, long long sA, const float2* B, int ldb,
-                     long long sB, bool transB, float2* C, int ldc, long long sC, int batch, int* fault,
-                     cudaStream_t s) {
-  if (M < 1 || N < 1 || K < 1 || batch < 1 || batch > 65535) return cudaErrorInvalidValue;
+                     long long sB, bool transB, float2* C, int ldc, long long sC, int batch, float* work,
+                     long long work_floats, int* fault, cudaStream_t s) {
+  if (M < 1 || N < 1 || K < 1 || batch < 1 || batch > 65535 || !work) return cudaErrorInvalidValue;
   const int Mp = (M + kTM - 1) / kTM * kTM;
   const int Np = (2 * N + kTN - 1) / kTN * kTN;
   const int Kp = (2 * K + kTK - 1) / kTK * kTK;
   const int bA = sA ? batch : 1, bB = sB ? batch : 1;
   const long long na = (long long)bA * Mp * Kp, nb = (long long)bB * Np * Kp;
   if ((long long)bA * Mp > (1LL << 31) || (long long)bB * Np > (1LL << 31)) return cudaErrorInvalidValue;
-  float* buf = nullptr;
-  cudaError_t e = cudaMallocAsync(&buf, (size_t)(kParts * (na + nb)) * sizeof(float), s);
-  if (e != cudaSuccess) return e;
-  float *pa = buf, *pb = buf + kParts * na;   // parts h, m, l of each operand, one after the other
+  if (work_floats < kParts * (na + nb)) return cudaErrorInvalidValue;
+  float *pa = work, *pb = work + kParts * na;   // the parts of each operand, one after the other
   tc_split_a<<<grid_for(na), 256, 0, s>>>(A, M, K, lda, sA, Mp, Kp, na, pa);
   tc_split_b<<<grid_for(nb), 256, 0, s>>>(B, N, K, ldb, sB, transB ? 1 : 0, Np, Kp, nb, pb);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
   TcMaps maps;
   for (int q = 0; q < kParts; ++q) {
     if (!tc_map(&maps.a[q], pa + q * na, (long long)bA * Mp, Kp) ||
-        !tc_map(&maps.b[q], pb + q * nb, (long long)bB * Np, Kp)) {
-      cudaFreeAsync(buf, s);
+        !tc_map(&maps.b[q], pb + q * nb, (long long)bB * Np, Kp))
       return cudaErrorInvalidValue;
-    }
   }
   static DeviceFlags configured;
   int dev = 0;
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
   if (!configured.test(dev)) {
     e = cudaFuncSetAttribute(tc_cgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
-    if (e != cudaSuccess) {
-      cudaFreeAsync(buf, s);
-      return e;
-    }
+    if (e != cudaSuccess) return e;
     configured.set(dev);
   }
   const dim3 grid(Mp / kTM, Np / kTN, batch);
   tc_cgemm_kernel<<<grid, kThreads, kSmem, s>>>(maps, M, 2 * N, Kp / kTK, Mp, Np, bA, bB, C, ldc, sC, fault);
-  e = cudaGetLastError();
-  cudaFreeAsync(buf, s);
-  return e;
+  return cudaGetLastError();
 }
 
 }  // namespace odt
