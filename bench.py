@@ -468,6 +468,73 @@ def run_bpm(args):
                          "cores": os.cpu_count(), "kind": "port", "sample": "2 illuminations"}}), flush=True)
 
 
+GRID_LENGTH_CASES = (
+    (103, "127^3 padded: 127 is prime, Bluestein transforms on every axis, unfused Born loop"),
+    (104, "128^3 padded: radix tiles, separate x-, y-, z-passes"),
+    (128, "152^3 padded: fused xy-pass + pipelined z-pass"),
+)
+
+
+def run_grid_lengths(args):
+    """Born-loop speed against the padded grid's lengths: scalar CBS solves
+    of 16 ring illuminations (NA 1.2, 0.1 um voxels, seeded multi-sphere
+    phantom, default boundary) on RI grids of 103^3, 104^3 and 128^3, which
+    the default boundary pads to 127^3 (prime: Bluestein transforms), 128^3
+    and 152^3.  Device-resident solve_device calls timed with CUDA events;
+    each solve moves more than the L2 (16 fields of >= 127^3 complex64)."""
+    import torch
+
+    from inverse_solver_b200 import FORWARD_SOLVER_CONVERGENT_BORN
+    from inverse_solver_b200.forward import CBSHostSetup
+    from inverse_solver_b200.inputs import ring_illumination, sphere_phantom
+
+    n_ill = 16
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    cases = []
+    clk = ClockSampler(0)
+    clk.start()
+    known = [n for n, _ in GRID_LENGTH_CASES]
+    if any(n not in known for n in args.grid_lengths):
+        raise SystemExit("--grid-lengths takes RI sizes from %s" % known)
+    for n, what in GRID_LENGTH_CASES:
+        if args.grid_lengths and n not in args.grid_lengths:
+            continue
+        size = [n, n, n]
+        p = CBSHostSetup.get_default_parameters(dict(size=size, wavelength=0.532, NA=1.2, RI_bg=1.3355,
+                                                     resolution=[0.1] * 3, vector_simulation=False,
+                                                     return_transmission=True))
+        RI = sphere_phantom(size, [0.1] * 3, 1.3355, seed=SEED)
+        fields = np.ascontiguousarray(ring_illumination(p)[:, :, :, :n_ill])
+        s = FORWARD_SOLVER_CONVERGENT_BORN(dict(p, max_batch=n_ill))
+        try:
+            s.set_RI(RI)
+            F = s.field_size
+            fin = torch.from_numpy(np.ascontiguousarray(fields[:, :, 0, :].transpose(2, 1, 0))).to(dev)
+            tout = torch.empty((n_ill, F[1], F[0]), dtype=torch.complex64, device=dev)
+            for _ in range(args.warmup):
+                s.solve_device(fin, tout, stream=stream)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                s.solve_device(fin, tout, stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / args.steps
+            vox = int(np.prod(s.sim_size)) * n_ill * s.Bornmax
+            cases.append({"ri": size, "padded": list(s.sim_size), "path": what, "bornmax": s.Bornmax,
+                          "ms_per_solve": ms, "voxel_iter_per_s": vox / (ms / 1e3)})
+        finally:
+            s.delete()
+    clocks = clk.stop()
+    print(json.dumps({
+        "metric": "CBS Born iterations by padded-grid length", "unit": "voxel-iter/s", "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "clocks": clocks, "cases": cases,
+        "config": {"workload": "scalar CBS, %d ring illuminations (NA 1.2), 0.1 um voxels, seeded multi-sphere "
+                               "phantom, default boundary, solve_device (device-resident)" % n_ill}}), flush=True)
+
+
 def run_setup(args):
     """Solver construction time (Green's / refocusing kernels, pupils, device
     plans) for the benchmark geometry (128^3 RI grid, 256^2 conv plane), with
@@ -623,6 +690,9 @@ def main():
                     help="time the beam-propagation forward solver")
     ap.add_argument("--fista", action="store_true",
                     help="time FISTA outer iterations of the inverse solver (device vs host loop)")
+    ap.add_argument("--grid-lengths", nargs="*", type=int, default=None, metavar="RI_SIZE",
+                    help="time the Born loop on padded grids of 127^3 (Bluestein), 128^3 and 152^3 "
+                         "(RI sizes 103, 104, 128; give some of them to time only those)")
     ap.add_argument("--print-rank-env", action="store_true",
                     help="print each rank's RANK / LOCAL_RANK / WORLD_SIZE and exit (launcher check)")
     args = ap.parse_args()
@@ -649,6 +719,9 @@ def main():
         return
     if args.retrieval:
         run_retrieval(args)
+        return
+    if args.grid_lengths is not None:
+        run_grid_lengths(args)
         return
     if world > 1:
         import datetime

@@ -441,7 +441,7 @@ extern "C" odt_status odt_aberration_pattern(const odt_aberration_args* a) {
     // stitched pupil
     ratio_kernel<<<grid_for(tot), kThreads, 0, s>>>(in, out, tot, Q);
     A_CHECK(cudaGetLastError());
-    A_CHECK(fftc2_any(B, Q, N1, N2, n, false, f1, f2, s));
+    A_CHECK(fftc2_any(Q, N1, N2, n, false, f1, f2, s));
     stitch_kernel<<<grid_for(tot), kThreads, 0, s>>>(Q, N1, N2, tot, dsh, fm, na, P);
     A_CHECK(cudaGetLastError());
     for (int it = 1; it < n; ++it) {
@@ -474,10 +474,10 @@ extern "C" odt_status odt_aberration_pattern(const odt_aberration_args* a) {
     // low-passed pupil and the pattern
     approx_kernel<<<grid_for(plane), kThreads, 0, s>>>(P2, rk, plane, centre, d);
     A_CHECK(cudaGetLastError());
-    A_CHECK(fftc2_any(B, P2, N1, N2, 1, true, f1, f2, s));
+    A_CHECK(fftc2_any(P2, N1, N2, 1, true, f1, f2, s));
     box_kernel<<<grid_for(plane), kThreads, 0, s>>>(P2, N1, plane, r0, r1, c0, c1);
     A_CHECK(cudaGetLastError());
-    A_CHECK(fftc2_any(B, P2, N1, N2, 1, false, f1, f2, s));
+    A_CHECK(fftc2_any(P2, N1, N2, 1, false, f1, f2, s));
     approx_kernel<<<grid_for(plane), kThreads, 0, s>>>(P2, rk, plane, centre, d);
     float2* dpat = dev ? reinterpret_cast<float2*>(a->pattern) : pat;
     pattern_kernel<<<grid_for(plane), kThreads, 0, s>>>(P2, plane, centre, na, dpat, filt);
@@ -490,10 +490,10 @@ extern "C" odt_status odt_aberration_pattern(const odt_aberration_args* a) {
       A_CHECK(cudaMemcpyAsync(oo, out, tot * sizeof(float2), cudaMemcpyDeviceToDevice, s));
     }
     for (float2* x : {oi, oo}) {
-      A_CHECK(fftc2_any(B, x, N1, N2, n, false, f1, f2, s));
+      A_CHECK(fftc2_any(x, N1, N2, n, false, f1, f2, s));
       cmul_plane_np_kernel<<<grid_for(tot), kThreads, 0, s>>>(x, filt, plane, tot);
       A_CHECK(cudaGetLastError());
-      A_CHECK(fftc2_any(B, x, N1, N2, n, true, f1, f2, s));
+      A_CHECK(fftc2_any(x, N1, N2, n, true, f1, f2, s));
     }
     if (!dev) {
       const cudaMemcpyKind d2h = cudaMemcpyDeviceToHost;
@@ -532,7 +532,7 @@ extern "C" odt_status odt_fft2c(const odt_fft2c_args* a) {
     return afail(ODT_ERR_UNSUPPORTED, "odt_fft2c: " + why);
   auto run = [&]() -> cudaError_t {
     if (!dev) A_CHECK(cudaMemcpyAsync(x, a->data, tot * sizeof(float2), cudaMemcpyHostToDevice, s));
-    A_CHECK(fftc2_any(B, x, N1, N2, n, a->inverse != 0, f1, f2, s));
+    A_CHECK(fftc2_any(x, N1, N2, n, a->inverse != 0, f1, f2, s));
     if (!dev) A_CHECK(cudaMemcpyAsync(a->data, x, tot * sizeof(float2), cudaMemcpyDeviceToHost, s));
     return cudaStreamSynchronize(s);
   };

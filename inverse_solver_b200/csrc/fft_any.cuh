@@ -40,16 +40,16 @@ cudaError_t bluestein_tables(int n, int m, const DevFft& inner, float2* chirp, f
 
 // DFT of length n = f.n (not direct) along the middle axis of x [n0, n, n2]
 // in place, with index shift sh on input and output (0: plain transform;
-// n / 2: centred) and the result multiplied by scale.  tmp holds
-// n0 * f.m * n2 elements.
+// n / 2: centred) and the result multiplied by scale; one kernel, no work
+// array (bs_fused.cu).
 cudaError_t bluestein_axis(float2* x, int n0, long long n2, bool inv, int sh, float scale, const AnyFft& f,
-                           float2* tmp, cudaStream_t s);
+                           cudaStream_t s);
 
 // fftshift(fft2(ifftshift(x))) (or the normalised inverse) of every [N1, N2]
 // plane of x [N1, N2, nsl], in place.  With both lengths direct this is
 // fftc2; otherwise each axis is transformed on its own (the Bluestein axes
-// through work buffers taken from B).
-cudaError_t fftc2_any(Scratch& B, float2* x, int N1, int N2, long long nsl, bool inv, const AnyFft& f1,
+// by bluestein_axis, without work buffers).
+cudaError_t fftc2_any(float2* x, int N1, int N2, long long nsl, bool inv, const AnyFft& f1,
                       const AnyFft& f2, cudaStream_t s);
 
 }  // namespace odt

@@ -251,8 +251,8 @@ extern "C" odt_status odt_hologram_fields(const odt_hologram_args* a) {
     }
     to_complex_kernel<<<grid_for(nin), kThreads, 0, s>>>(db, Fb, nin);
     to_complex_kernel<<<grid_for(nin), kThreads, 0, s>>>(ds, Fs, nin);
-    if ((e = cudaGetLastError()) || (e = fftc2_any(B, Fb, N, N, nimg, false, fN, fN, s)) ||
-        (e = fftc2_any(B, Fs, N, N, nimg, false, fN, fN, s)))
+    if ((e = cudaGetLastError()) || (e = fftc2_any(Fb, N, N, nimg, false, fN, fN, s)) ||
+        (e = fftc2_any(Fs, N, N, nimg, false, fN, fN, s)))
       return e;
     // deleted bands (1-based): rows round(N cp):N; columns round(N cp):N, or
     // 1:round(N (1 - cp)) with other_corner
@@ -267,8 +267,8 @@ extern "C" odt_status odt_hologram_fields(const odt_hologram_args* a) {
     centre_crop_kernel<<<grid_for(nmid), kThreads, 0, s>>>(Fb, N, M, d, sb, dna, nimg, Gb);
     centre_crop_kernel<<<grid_for(nmid), kThreads, 0, s>>>(Fs, N, M, d, sb, dna, nimg, Gs);
     peak_kernel<<<nimg, 256, 0, s>>>(Gb, M, dev ? a->peaks : pk);
-    if ((e = cudaGetLastError()) || (e = fftc2_any(B, Gb, M, M, nimg, true, fM, fM, s)) ||
-        (e = fftc2_any(B, Gs, M, M, nimg, true, fM, fM, s)))
+    if ((e = cudaGetLastError()) || (e = fftc2_any(Gb, M, M, nimg, true, fM, fM, s)) ||
+        (e = fftc2_any(Gs, M, M, nimg, true, fM, fM, s)))
       return e;
     float2* outb = dev ? reinterpret_cast<float2*>(a->bg_field) : ob;
     float2* outs = dev ? reinterpret_cast<float2*>(a->sp_field) : os;
@@ -408,10 +408,10 @@ extern "C" odt_status odt_refocus_2d(const odt_refocus_args* a) {
     cudaError_t e;
     if ((e = cudaMemcpyAsync(x, a->field, tot * sizeof(float2), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(k, a->kernel, plane * sizeof(float2), cudaMemcpyHostToDevice, s)) ||
-        (e = fftc2_any(B, x, n1, n2, n, false, f1, f2, s)))
+        (e = fftc2_any(x, n1, n2, n, false, f1, f2, s)))
       return e;
     cmul_plane_kernel<<<grid_for(tot), kThreads, 0, s>>>(x, k, plane, tot);
-    if ((e = cudaGetLastError()) || (e = fftc2_any(B, x, n1, n2, n, true, f1, f2, s)) ||
+    if ((e = cudaGetLastError()) || (e = fftc2_any(x, n1, n2, n, true, f1, f2, s)) ||
         (e = cudaMemcpyAsync(a->out, x, tot * sizeof(float2), cudaMemcpyDeviceToHost, s)))
       return e;
     return cudaStreamSynchronize(s);

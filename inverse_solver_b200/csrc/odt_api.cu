@@ -111,11 +111,8 @@ struct Handle {
   // transform lengths
   DevFft fx{}, fy{}, fz{}, ffx{}, ffy{}, fcx{}, fcy{};
   // Bluestein plans of the lengths the radix tiles do not cover (direct =
-  // true for the others; the DevFft of such a length has no passes) and
-  // their work buffer (bs_elems elements per field plane of a batch)
+  // true for the others; the DevFft of such a length has no passes)
   AnyFft bsx{}, bsy{}, bsz{}, bsfx{}, bsfy{}, bscx{}, bscy{};
-  float2* bs_work = nullptr;
-  long long bs_elems = 0;
   bool any_loop() const { return !bsx.direct || !bsy.direct || !bsz.direct; }
   bool any_io() const { return !bsfx.direct || !bsfy.direct || !bscx.direct || !bscy.direct; }
   const AnyFft& bs_of(const DevFft& f) const {
@@ -222,22 +219,7 @@ struct Handle {
   long long nc3() const { return nc2() * g.ri_size[2]; }
   long long work_elems() const { return std::max(3 * nvox(), nc3()); }
   size_t slot_bytes() const {
-    return sizeof(float2) * (size_t)np * (size_t)(work_elems() + 2 * nri() + 4 * nf() + 2 * nc2() + bs_elems);
-  }
-  // Bluestein work per field plane: the largest of the axes' n0 * m * n2 / nb
-  long long bluestein_elems() const {
-    long long e = 0;
-    const long long px = g.sim_size[0], py = g.sim_size[1], pz = g.sim_size[2];
-    const long long Fx = g.field_size[0], Fy = g.field_size[1], Cx = g.conv_size[0], Cy = g.conv_size[1];
-    const long long Rz = g.ri_size[2];
-    if (!bsx.direct) e = std::max(e, bsx.m * py * pz);
-    if (!bsy.direct) e = std::max(e, px * bsy.m * pz);
-    if (!bsz.direct) e = std::max(e, px * py * bsz.m);
-    if (!bsfx.direct) e = std::max(e, bsfx.m * Fy);
-    if (!bsfy.direct) e = std::max(e, Fx * bsfy.m);
-    if (!bscx.direct) e = std::max(e, bscx.m * Cy * Rz);
-    if (!bscy.direct) e = std::max(e, Cx * bscy.m * Rz);
-    return e;
+    return sizeof(float2) * (size_t)np * (size_t)(work_elems() + 2 * nri() + 4 * nf() + 2 * nc2());
   }
   PolTables pol_tables() const {
     const long long n = nf();
@@ -441,7 +423,6 @@ void ensure_batch(Handle& H, int nb) {
   H.out_r = H.dalloc<float2>((size_t)H.nf() * nbp, true);
   H.c2a = H.dalloc<float2>((size_t)H.nc2() * nbp, true);
   H.c2b = H.dalloc<float2>((size_t)H.nc2() * nbp, true);
-  if (H.bs_elems > 0) H.bs_work = H.dalloc<float2>((size_t)H.bs_elems * nbp, true);
   H.d_count = H.dalloc<unsigned int>(1, true);
   H.d_fault = H.dalloc<int>(1, true);
   ODT_CUDA(cudaMemset(H.d_fault, 0, sizeof(int)));
@@ -478,11 +459,11 @@ void fftc2(Handle& H, float2* x, const DevFft& f0, const DevFft& f1, long long n
     if (b0.direct)
       ODT_CUDA(launch_fft_lines(x, x, (long long)n1 * nslices, n0 / 2, n0 / 2, s0, inverse, f0, s));
     else
-      ODT_CUDA(bluestein_axis(x, 1, (long long)n1 * nslices, inverse, n0 / 2, s0, b0, H.bs_work, s));
+      ODT_CUDA(bluestein_axis(x, 1, (long long)n1 * nslices, inverse, n0 / 2, s0, b0, s));
     if (b1.direct)
       ODT_CUDA(launch_fft_cols(x, x, n0, nslices, n1 / 2, n1 / 2, s1, inverse, f1, s));
     else
-      ODT_CUDA(bluestein_axis(x, n0, nslices, inverse, n1 / 2, s1, b1, H.bs_work, s));
+      ODT_CUDA(bluestein_axis(x, n0, nslices, inverse, n1 / 2, s1, b1, s));
   }
   H.mark_end(s);
 }
@@ -598,16 +579,16 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
     auto fft3 = [&](bool inv) {
       auto ax = [&]() {
         if (H.bsx.direct) ODT_CUDA(launch_fft_lines(a.T, a.T, xl, 0, 0, 1.0f, inv, H.fx, s));
-        else ODT_CUDA(bluestein_axis(a.T, 1, xl, inv, 0, 1.0f, H.bsx, H.bs_work, s));
+        else ODT_CUDA(bluestein_axis(a.T, 1, xl, inv, 0, 1.0f, H.bsx, s));
       };
       auto ay = [&]() {
         if (H.bsy.direct) ODT_CUDA(launch_fft_cols(a.T, a.T, a.px, yl, 0, 0, 1.0f, inv, H.fy, s));
-        else ODT_CUDA(bluestein_axis(a.T, a.px, yl, inv, 0, 1.0f, H.bsy, H.bs_work, s));
+        else ODT_CUDA(bluestein_axis(a.T, a.px, yl, inv, 0, 1.0f, H.bsy, s));
       };
       auto az = [&]() {
         if (pxy > INT32_MAX) raise(ODT_ERR_UNSUPPORTED, "x-y plane too large for the column transforms");
         if (H.bsz.direct) ODT_CUDA(launch_fft_cols(a.T, a.T, (int)pxy, nbp, 0, 0, 1.0f, inv, H.fz, s));
-        else ODT_CUDA(bluestein_axis(a.T, (int)pxy, nbp, inv, 0, 1.0f, H.bsz, H.bs_work, s));
+        else ODT_CUDA(bluestein_axis(a.T, (int)pxy, nbp, inv, 0, 1.0f, H.bsz, s));
       };
       H.mark_begin(kKBornY, s);
       if (inv) { az(); ay(); ax(); } else { ax(); ay(); az(); }
@@ -968,7 +949,6 @@ odt_status odt_create(const odt_geometry* geom, const odt_cfloat* refocus,
     if ((H->any_loop() || H->any_io()) && H->np == 3)
       raise(ODT_ERR_UNSUPPORTED, "dyadic (vector) solves need simulation, field and convolution lengths whose "
                                  "prime factors are at most 31");
-    H->bs_elems = H->bluestein_elems();
     const size_t n3 = (size_t)H->nc3();
     H->refocus = H->dalloc<float2>(n3, false);
     ODT_CUDA(cudaMemcpy(H->refocus, refocus, n3 * sizeof(float2), cudaMemcpyHostToDevice));
