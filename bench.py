@@ -481,7 +481,11 @@ def run_grid_lengths(args):
     phantom, default boundary) on RI grids of 103^3, 104^3 and 128^3, which
     the default boundary pads to 127^3 (prime: Bluestein transforms), 128^3
     and 152^3.  Device-resident solve_device calls timed with CUDA events;
-    each solve moves more than the L2 (16 fields of >= 127^3 complex64)."""
+    each solve moves more than the L2 (16 fields of >= 127^3 complex64).
+    "kinds_one_solve" is one further solve with events around each kind of
+    launch; on the 127^3 grid the unfused loop books born_point under
+    born_x, each 3D FFT (three axis transforms) under born_y and born_green
+    under born_z."""
     import torch
 
     from inverse_solver_b200 import FORWARD_SOLVER_CONVERGENT_BORN
@@ -523,8 +527,14 @@ def run_grid_lengths(args):
             torch.cuda.synchronize()
             ms = e0.elapsed_time(e1) / args.steps
             vox = int(np.prod(s.sim_size)) * n_ill * s.Bornmax
+            # one more solve with per-kind event timing (not in the timed region)
+            s.set_profiling(True)
+            s.solve_device(fin, tout, stream=stream)
+            torch.cuda.synchronize()
+            kt = {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in s.kernel_times().items() if v[1]}
+            s.set_profiling(False)
             cases.append({"ri": size, "padded": list(s.sim_size), "path": what, "bornmax": s.Bornmax,
-                          "ms_per_solve": ms, "voxel_iter_per_s": vox / (ms / 1e3)})
+                          "ms_per_solve": ms, "voxel_iter_per_s": vox / (ms / 1e3), "kinds_one_solve": kt})
         finally:
             s.delete()
     clocks = clk.stop()

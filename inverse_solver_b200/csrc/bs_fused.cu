@@ -171,29 +171,35 @@ __global__ void __launch_bounds__(kBsMaxThreads<CLS>, 2)
 
 namespace {
 
+// pencils per tile: at most 8 (the padded length m is about twice the
+// transform's, so 16 pencils of two stages would hold a third of an SM's
+// shared memory and leave 3 CTAs per SM)
+constexpr int kBsLgW = 3;
+
 template <int CLS>
 cudaError_t bs_launch(float2* x, int n0, long long n2, int cj, int sh, float scale, const AnyFft& f,
                       const float2* bh, int max_smem, cudaStream_t s) {
   const int n = f.n, m = f.m;
   const DevFft& g = f.f;
+  const int lgW = g.lgW < kBsLgW ? g.lgW : kBsLgW;
+  const int W = 1 << lgW;
   cudaError_t e;
   if (n0 == 1) {   // contiguous lines
-    const size_t sm = align16(sizeof(float2) * m) + 2 * sizeof(float2) * (size_t)g.W * smem_line_ld(m);
+    const size_t sm = align16(sizeof(float2) * m) + 2 * sizeof(float2) * (size_t)W * smem_line_ld(m);
     if (sm > (size_t)max_smem) return cudaErrorInvalidConfiguration;
     if ((e = raise_smem_limit(reinterpret_cast<const void*>(bs_lines_kernel<CLS>), sm)) != cudaSuccess) return e;
-    const long long blocks = (n2 + g.W - 1) / g.W;
+    const long long blocks = (n2 + W - 1) / W;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
     bs_lines_kernel<CLS><<<(unsigned)blocks, g.nthr, sm, s>>>(x, n2, n, sh, scale, cj, f.chirp, bh, g.plan, g.tw,
-                                                               g.W);
+                                                               W);
   } else {
-    const int W = 1 << g.lgW;
     const size_t sm = align16(sizeof(float2) * m) + 2 * sizeof(float2) * (size_t)m * (W + 1);
     if (sm > (size_t)max_smem) return cudaErrorInvalidConfiguration;
     if ((e = raise_smem_limit(reinterpret_cast<const void*>(bs_cols_kernel<CLS>), sm)) != cudaSuccess) return e;
     const long long blocks = ((long long)(n0 + W - 1) / W) * n2;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
     bs_cols_kernel<CLS><<<(unsigned)blocks, g.nthr, sm, s>>>(x, n0, n, sh, scale, cj, f.chirp, bh, g.plan, g.tw,
-                                                              g.lgW);
+                                                              lgW);
   }
   return cudaGetLastError();
 }
