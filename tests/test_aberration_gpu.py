@@ -134,9 +134,11 @@ def test_device_memory_matches_host():
 
 
 # sizes: radix tiles on both axes; Bluestein on both (2 * 37, 2 * 53); a
-# Bluestein line axis of padded length 1280 (8 pencils per tile); a Bluestein
+# Bluestein line axis and a Bluestein column axis of padded length 1280 (8
+# pencils per tile: the largest tiles of the Bluestein kernels); a Bluestein
 # column axis of padded length 2048 and direct lengths of 1536 (4 pencils)
-FFT_SIZES = [(60, 84, 3), (74, 106, 2), (37, 53, 1), (636, 96, 1), (64, 1016, 1), (1536, 8, 1), (8, 1536, 1)]
+FFT_SIZES = [(60, 84, 3), (74, 106, 2), (37, 53, 1), (636, 96, 1), (96, 636, 1), (64, 1016, 1), (1536, 8, 1),
+             (8, 1536, 1)]
 
 
 @pytest.mark.parametrize("inverse", [False, True])
