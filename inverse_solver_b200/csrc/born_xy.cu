@@ -11,7 +11,7 @@
 // The z-pass (cols_pipe.cu) does the z-FFT, the Green's multiply and the
 // inverse z-FFT in between.
 //
-// Transforms along an axis of length N = 8 R (R = 11, 12, 15, 19): index
+// Transforms along an axis of length N = 8 R (R = 11, 12, 15, 16, 19): index
 // n = R n1 + n2 (n1 < 8, n2 < R), k = k1 + 8 k2 (k1 < 8, k2 < R).
 //   forward  F1: 8-point DFT over n1 of the positions R n1 + n2 (stride R),
 //                result k1 stored at R k1 + n2;
@@ -48,11 +48,16 @@
 // warp's global loads overlap other warps' transforms.
 //
 // Bank conflicts: rows have a pitch of N = 8 (mod 16) complex elements for
-// odd R (N = 96: 0 mod 16, two-way conflicts in steps 3 and 5).
-// Steps 1, 2, 6, 7 put consecutive x on consecutive lanes; steps 3 and 5
-// take R consecutive elements at R k1 (lanes over k1 and rows: the stride of
-// 2R banks and the row pitch of 16 banks keep a half-warp's 8-byte accesses
-// on distinct bank pairs); step 4 takes consecutive n2 on consecutive lanes.
+// odd R.  Steps 1, 2, 6, 7 put consecutive x on consecutive lanes; steps 3
+// and 5 take R consecutive elements at R k1 (lanes over k1 and rows: the
+// stride of 2R banks and the row pitch of 16 banks keep a half-warp's 8-byte
+// accesses on distinct bank pairs); step 4 takes consecutive n2 on
+// consecutive lanes.  For even R (N = 96, 128) a stride of R elements puts
+// several k1 on the same banks (all eight at R = 16), so those planes carry
+// one pad element after every R elements of a row (XYSmem::sx): group k1
+// starts at (R + 1) k1, eight distinct bank pairs, and the pitch N + N / R
+// is 8 (mod 16); the four rows of a warp's step-3 / -5 access still share
+// banks (two wavefronts where one would do).
 #include <cuda_runtime.h>
 
 #include "b16.cuh"
@@ -79,7 +84,15 @@ struct XYSmem {
   static constexpr int kTkS = R | 1;
   static constexpr size_t kTk = kMaskY + a16(sizeof(float) * N);
   static constexpr size_t kPlane = a128(kTk + a16(sizeof(float2) * 8 * kTkS));
-  static constexpr size_t kTotal = kPlane + sizeof(float2) * N * N;
+  // plane rows: for odd R a pitch of N (= 8 mod 16) elements; for even R
+  // (N = 96, 128: 0 mod 16) one pad element after every R elements of a row,
+  // so that the groups R k1 .. R k1 + R-1 of steps 3 and 5 start on
+  // different banks ((R + 1) k1) and the pitch N + N / R is 8 mod 16 again
+  static constexpr bool kPad = R % 2 == 0;
+  static constexpr int P = kPad ? N + N / R : N;
+  static constexpr size_t kTotal = kPlane + sizeof(float2) * N * P;
+  // in-row position of x
+  static __device__ __forceinline__ int sx(int x) { return kPad ? x + x / R : x; }
 };
 
 // KIND: which Born iterations a launch serves (compile time, so the steady
@@ -164,7 +177,7 @@ __global__ void __launch_bounds__(32 * R, 1)
 #pragma unroll
     for (int r = 1; r < R; ++r) v[r] = cmul(v[r], cconj(tw[r * k1]));
 #pragma unroll
-    for (int r = 0; r < R; ++r) pl[(R * k1 + r) * N + x] = v[r];
+    for (int r = 0; r < R; ++r) pl[(R * k1 + r) * L::P + L::sx(x)] = v[r];
   };
   // Step 7 of item (x, k1) reads the rows R k1 + r of column x and step 1 of
   // the same item writes them, with the same item -> thread map: a thread
@@ -191,16 +204,16 @@ __global__ void __launch_bounds__(32 * R, 1)
       for (int x = lane; x < N; x += 32) {
         float2 v[8];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = pl[(R * r + w) * N + x];
+        for (int r = 0; r < 8; ++r) v[r] = pl[(R * r + w) * L::P + L::sx(x)];
         Butterfly<8, true>::run(v, tw, N);
 #pragma unroll
-        for (int r = 0; r < 8; ++r) pl[(R * r + w) * N + x] = v[r];
+        for (int r = 0; r < 8; ++r) pl[(R * r + w) * L::P + L::sx(x)] = v[r];
       }
       __syncwarp();
       // ---- 3: x-F3^-1 + F2^-1 on the contiguous groups R k1 .. R k1 + R-1 of the warp's rows
       for (int it = lane; it < 64; it += 32) {
         const int k1 = it & 7, y = R * (it >> 3) + w;
-        float2* row = pl + y * N + R * k1;
+        float2* row = pl + y * L::P + (R + (L::kPad ? 1 : 0)) * k1;
         float2 v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = row[r];
@@ -221,7 +234,7 @@ __global__ void __launch_bounds__(32 * R, 1)
       // Field_n's exponent block of this item's n1 = r value: the 8 lanes of a
       // group (8 consecutive it) share one; block w R + it / 8 of n1's R^2
       const long long fe = (g0 >> 3) + w * R + (it >> 3);
-      float2* row = pl + y * N;
+      float2* row = pl + y * L::P;
       const long long gy = g0 + (long long)y * N;
       const long long vy = v0 + (long long)y * N;
       const bool yzroi = zroi && (unsigned)(y - a.ry0) < (unsigned)a.ry;
@@ -259,7 +272,7 @@ __global__ void __launch_bounds__(32 * R, 1)
       float2 v[8];
       if constexpr (kInv) {
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = row[R * r + n2];
+        for (int r = 0; r < 8; ++r) v[r] = row[(R + (L::kPad ? 1 : 0)) * r + n2];
         Butterfly<8, true>::run(v, tw, N);
       }
 #pragma unroll
@@ -324,7 +337,7 @@ __global__ void __launch_bounds__(32 * R, 1)
       if constexpr (kFwd) {
         Butterfly<8, false>::run(v, tw, N);
 #pragma unroll
-        for (int r = 0; r < 8; ++r) row[R * r + n2] = v[r];
+        for (int r = 0; r < 8; ++r) row[(R + (L::kPad ? 1 : 0)) * r + n2] = v[r];
       }
     }
     if constexpr (!kFwd) {
@@ -336,7 +349,7 @@ __global__ void __launch_bounds__(32 * R, 1)
     // ---- 5: x-F2 + F3 on the contiguous groups of the warp's rows
     for (int it = lane; it < 64; it += 32) {
       const int k1 = it & 7, y = R * (it >> 3) + w;
-      float2* row = pl + y * N + R * k1;
+      float2* row = pl + y * L::P + (R + (L::kPad ? 1 : 0)) * k1;
       float2 v[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) v[r] = row[r];
@@ -352,10 +365,10 @@ __global__ void __launch_bounds__(32 * R, 1)
     for (int x = lane; x < N; x += 32) {
       float2 v[8];
 #pragma unroll
-      for (int r = 0; r < 8; ++r) v[r] = pl[(R * r + w) * N + x];
+      for (int r = 0; r < 8; ++r) v[r] = pl[(R * r + w) * L::P + L::sx(x)];
       Butterfly<8, false>::run(v, tw, N);
 #pragma unroll
-      for (int r = 0; r < 8; ++r) pl[(R * r + w) * N + x] = v[r];
+      for (int r = 0; r < 8; ++r) pl[(R * r + w) * L::P + L::sx(x)] = v[r];
     }
     __syncthreads();
     // ---- 7: y-F2 + F3 -> T
@@ -363,7 +376,7 @@ __global__ void __launch_bounds__(32 * R, 1)
       const int x = i % N, k1 = i / N;
       float2 v[R];
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[r] = pl[(R * k1 + r) * N + x];
+      for (int r = 0; r < R; ++r) v[r] = pl[(R * k1 + r) * L::P + L::sx(x)];
 #pragma unroll
       for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tw[r * k1]);
       Butterfly<R, false>::run(v, tw, N);
@@ -443,6 +456,7 @@ bool born_xy_supported(const BornArgs& a, int max_smem) {
     case 11: need = XYSmem<11>::kTotal; break;
     case 12: need = XYSmem<12>::kTotal; break;
     case 15: need = XYSmem<15>::kTotal; break;
+    case 16: need = XYSmem<16>::kTotal; break;
     case 19: need = XYSmem<19>::kTotal; break;
     default: return false;
   }
@@ -461,6 +475,7 @@ cudaError_t launch_born_xy(const BornArgs& a, int mode, int jj, const DevFft& fx
     case 11: return launch_kind<11>(a, kind, jj, fx.tw, s);
     case 12: return launch_kind<12>(a, kind, jj, fx.tw, s);
     case 15: return launch_kind<15>(a, kind, jj, fx.tw, s);
+    case 16: return launch_kind<16>(a, kind, jj, fx.tw, s);
     case 19: return launch_kind<19>(a, kind, jj, fx.tw, s);
     default: return cudaErrorNotSupported;
   }

@@ -459,6 +459,9 @@ cudaError_t dispatch(const BornArgs& a, int jj, const DevFft& f, int* fault, cud
       if constexpr (KIND >= 2) return launch_kind<12, KIND>(a, jj, f, fault, s);
       return cudaErrorNotSupported;
     case 15: return launch_kind<15, KIND>(a, jj, f, fault, s);
+    case 16:   // z-pass only (128 = 8 x 16 columns behind the fused xy-pass)
+      if constexpr (KIND >= 2) return launch_kind<16, KIND>(a, jj, f, fault, s);
+      return cudaErrorNotSupported;
     case 19: return launch_kind<19, KIND>(a, jj, f, fault, s);
     case 25: return launch_kind<25, KIND>(a, jj, f, fault, s);
     case 27: return launch_kind<27, KIND>(a, jj, f, fault, s);
@@ -475,7 +478,8 @@ bool cols_pipe_supported(const BornArgs& a, const DevFft& f, bool zpass) {
   const int n = f.plan.n;
   if (n != (zpass ? a.pz : a.py) || n % kR1 != 0) return false;
   const int r2 = n / kR1;
-  if (r2 != 11 && r2 != 15 && r2 != 19 && r2 != 25 && r2 != 27 && !(zpass && r2 == 12) && !(!zpass && r2 == 35))
+  if (r2 != 11 && r2 != 15 && r2 != 19 && r2 != 25 && r2 != 27 && !(zpass && (r2 == 12 || r2 == 16)) &&
+      !(!zpass && r2 == 35))
     return false;
   if (a.px % 2 != 0 || !encoder()) return false;   // row strides must be multiples of 16 bytes
   const long long nout = zpass ? (long long)a.py * a.nbatch : (long long)a.pz * a.nbatch;

@@ -358,6 +358,12 @@ struct Butterfly<35, INV> {
   ODT_HD static void run(float2* v, const float2* tw, int n) { CompositeButterfly<5, 7, INV>::run(v, tw, n); }
 };
 
+// 16 = 4 x 4 (the fused xy-pass and the pipelined z-pass on 128-point axes)
+template <bool INV>
+struct Butterfly<16, INV> {
+  ODT_HD static void run(float2* v, const float2* tw, int n) { CompositeButterfly<4, 4, INV>::run(v, tw, n); }
+};
+
 // ------------------------------------------------------------------ one pass
 // Stockham radix-R pass over a tile of W pencils (W a power of two, lgW its
 // log2).  ns = product of the radices of the passes already done.  Work item
