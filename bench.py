@@ -472,16 +472,19 @@ GRID_LENGTH_CASES = (
     (72, "96^3 padded: fused xy-pass (12-point butterflies) + pipelined z-pass"),
     (103, "127^3 padded: 127 is prime, Bluestein transforms on every axis, unfused Born loop"),
     (104, "128^3 padded: fused xy-pass + pipelined z-pass (16-point butterflies)"),
+    (112, "136^3 padded: fused xy-pass + pipelined z-pass (17-point butterflies)"),
     (128, "152^3 padded: fused xy-pass + pipelined z-pass"),
+    (136, "160^3 padded: fused xy-pass + pipelined z-pass (20-point butterflies)"),
 )
 
 
 def run_grid_lengths(args):
     """Born-loop speed against the padded grid's lengths: scalar CBS solves
     of 16 ring illuminations (NA 1.2, 0.1 um voxels, seeded multi-sphere
-    phantom, default boundary) on RI grids of 72^3, 103^3, 104^3 and 128^3,
-    which the default boundary pads to 96^3, 127^3 (prime: Bluestein
-    transforms), 128^3 and 152^3 (fused passes on all but 127^3).  Device-resident solve_device calls
+    phantom, default boundary) on RI grids of 72^3, 103^3, 104^3, 112^3,
+    128^3 and 136^3, which the default boundary pads to 96^3, 127^3 (prime:
+    Bluestein transforms), 128^3, 136^3, 152^3 and 160^3 (fused passes on all
+    but 127^3).  Device-resident solve_device calls
     timed with CUDA events;
     each solve moves more than the L2 (16 fields of >= 127^3 complex64).
     "kinds_one_solve" is one further solve with events around each kind of
@@ -703,8 +706,8 @@ def main():
     ap.add_argument("--fista", action="store_true",
                     help="time FISTA outer iterations of the inverse solver (device vs host loop)")
     ap.add_argument("--grid-lengths", nargs="*", type=int, default=None, metavar="RI_SIZE",
-                    help="time the Born loop on padded grids of 96^3, 127^3 (Bluestein), 128^3 and 152^3 "
-                         "(RI sizes 72, 103, 104, 128; give some of them to time only those)")
+                    help="time the Born loop on padded grids of 96^3, 127^3 (Bluestein), 128^3, 136^3, 152^3 "
+                         "and 160^3 (RI sizes 72, 103, 104, 112, 128, 136; give some of them to time only those)")
     ap.add_argument("--print-rank-env", action="store_true",
                     help="print each rank's RANK / LOCAL_RANK / WORLD_SIZE and exit (launcher check)")
     args = ap.parse_args()

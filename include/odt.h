@@ -671,7 +671,7 @@ odt_status odt_get_batch(odt_handle h, int32_t* batch);
  *     benchmark grid (the storage rounding of the early, largest Born terms
  *     dominates it, so every iteration uses the same format).
  * B16 needs the fused xy-pass: a scalar potential on a grid whose x and y
- * lengths are equal and one of 88, 96, 120, 128, 152 (z: 8 * {11, 12, 15, 16, 19, 25, 27});
+ * lengths are equal and 8 * R with 11 <= R <= 20 (z: 8 * R, 11 <= R <= 20, or 8 * {25, 27});
  * a solve on another grid fails with ODT_ERR_UNSUPPORTED.  Not to be called
  * while a solve on the same handle runs. */
 #define ODT_STORAGE_COMPLEX64 0

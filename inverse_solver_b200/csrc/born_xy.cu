@@ -11,7 +11,7 @@
 // The z-pass (cols_pipe.cu) does the z-FFT, the Green's multiply and the
 // inverse z-FFT in between.
 //
-// Transforms along an axis of length N = 8 R (R = 11, 12, 15, 16, 19): index
+// Transforms along an axis of length N = 8 R (11 <= R <= 20): index
 // n = R n1 + n2 (n1 < 8, n2 < R), k = k1 + 8 k2 (k1 < 8, k2 < R).
 //   forward  F1: 8-point DFT over n1 of the positions R n1 + n2 (stride R),
 //                result k1 stored at R k1 + n2;
@@ -455,9 +455,14 @@ bool born_xy_supported(const BornArgs& a, int max_smem) {
   switch (r) {
     case 11: need = XYSmem<11>::kTotal; break;
     case 12: need = XYSmem<12>::kTotal; break;
+    case 13: need = XYSmem<13>::kTotal; break;
+    case 14: need = XYSmem<14>::kTotal; break;
     case 15: need = XYSmem<15>::kTotal; break;
     case 16: need = XYSmem<16>::kTotal; break;
+    case 17: need = XYSmem<17>::kTotal; break;
+    case 18: need = XYSmem<18>::kTotal; break;
     case 19: need = XYSmem<19>::kTotal; break;
+    case 20: need = XYSmem<20>::kTotal; break;
     default: return false;
   }
   return need <= (size_t)max_smem && (long long)a.pz * a.nbatch < (1LL << 31);
@@ -474,9 +479,14 @@ cudaError_t launch_born_xy(const BornArgs& a, int mode, int jj, const DevFft& fx
   switch (a.px / 8) {
     case 11: return launch_kind<11>(a, kind, jj, fx.tw, s);
     case 12: return launch_kind<12>(a, kind, jj, fx.tw, s);
+    case 13: return launch_kind<13>(a, kind, jj, fx.tw, s);
+    case 14: return launch_kind<14>(a, kind, jj, fx.tw, s);
     case 15: return launch_kind<15>(a, kind, jj, fx.tw, s);
     case 16: return launch_kind<16>(a, kind, jj, fx.tw, s);
+    case 17: return launch_kind<17>(a, kind, jj, fx.tw, s);
+    case 18: return launch_kind<18>(a, kind, jj, fx.tw, s);
     case 19: return launch_kind<19>(a, kind, jj, fx.tw, s);
+    case 20: return launch_kind<20>(a, kind, jj, fx.tw, s);
     default: return cudaErrorNotSupported;
   }
 }

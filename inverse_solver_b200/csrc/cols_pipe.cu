@@ -458,10 +458,20 @@ cudaError_t dispatch(const BornArgs& a, int jj, const DevFft& f, int* fault, cud
     case 12:   // z-pass only (96 = 8 x 12, the fused passes' even length)
       if constexpr (KIND >= 2) return launch_kind<12, KIND>(a, jj, f, fault, s);
       return cudaErrorNotSupported;
-    case 15: return launch_kind<15, KIND>(a, jj, f, fault, s);
-    case 16:   // z-pass only (128 = 8 x 16 columns behind the fused xy-pass)
-      if constexpr (KIND >= 2) return launch_kind<16, KIND>(a, jj, f, fault, s);
+    case 13: case 14: case 16: case 17: case 18: case 20:
+      // z-pass only (104 - 160-point columns behind the fused xy-pass)
+      if constexpr (KIND >= 2) {
+        switch (f.plan.n / kR1) {
+          case 13: return launch_kind<13, KIND>(a, jj, f, fault, s);
+          case 14: return launch_kind<14, KIND>(a, jj, f, fault, s);
+          case 16: return launch_kind<16, KIND>(a, jj, f, fault, s);
+          case 17: return launch_kind<17, KIND>(a, jj, f, fault, s);
+          case 18: return launch_kind<18, KIND>(a, jj, f, fault, s);
+          default: return launch_kind<20, KIND>(a, jj, f, fault, s);
+        }
+      }
       return cudaErrorNotSupported;
+    case 15: return launch_kind<15, KIND>(a, jj, f, fault, s);
     case 19: return launch_kind<19, KIND>(a, jj, f, fault, s);
     case 25: return launch_kind<25, KIND>(a, jj, f, fault, s);
     case 27: return launch_kind<27, KIND>(a, jj, f, fault, s);
@@ -478,8 +488,8 @@ bool cols_pipe_supported(const BornArgs& a, const DevFft& f, bool zpass) {
   const int n = f.plan.n;
   if (n != (zpass ? a.pz : a.py) || n % kR1 != 0) return false;
   const int r2 = n / kR1;
-  if (r2 != 11 && r2 != 15 && r2 != 19 && r2 != 25 && r2 != 27 && !(zpass && (r2 == 12 || r2 == 16)) &&
-      !(!zpass && r2 == 35))
+  const bool zonly = r2 == 12 || r2 == 13 || r2 == 14 || r2 == 16 || r2 == 17 || r2 == 18 || r2 == 20;
+  if (r2 != 11 && r2 != 15 && r2 != 19 && r2 != 25 && r2 != 27 && !(zpass && zonly) && !(!zpass && r2 == 35))
     return false;
   if (a.px % 2 != 0 || !encoder()) return false;   // row strides must be multiples of 16 bytes
   const long long nout = zpass ? (long long)a.py * a.nbatch : (long long)a.pz * a.nbatch;

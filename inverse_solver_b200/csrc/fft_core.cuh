@@ -358,10 +358,24 @@ struct Butterfly<35, INV> {
   ODT_HD static void run(float2* v, const float2* tw, int n) { CompositeButterfly<5, 7, INV>::run(v, tw, n); }
 };
 
-// 16 = 4 x 4 (the fused xy-pass and the pipelined z-pass on 128-point axes)
+// even radices of the fused xy-pass and the pipelined z-pass (axes of
+// 8 R = 112, 128, 144, 160 points): 14 = 2 x 7, 16 = 4 x 4, 18 = 2 x 9,
+// 20 = 4 x 5
+template <bool INV>
+struct Butterfly<14, INV> {
+  ODT_HD static void run(float2* v, const float2* tw, int n) { CompositeButterfly<2, 7, INV>::run(v, tw, n); }
+};
 template <bool INV>
 struct Butterfly<16, INV> {
   ODT_HD static void run(float2* v, const float2* tw, int n) { CompositeButterfly<4, 4, INV>::run(v, tw, n); }
+};
+template <bool INV>
+struct Butterfly<18, INV> {
+  ODT_HD static void run(float2* v, const float2* tw, int n) { CompositeButterfly<2, 9, INV>::run(v, tw, n); }
+};
+template <bool INV>
+struct Butterfly<20, INV> {
+  ODT_HD static void run(float2* v, const float2* tw, int n) { CompositeButterfly<4, 5, INV>::run(v, tw, n); }
 };
 
 // ------------------------------------------------------------------ one pass

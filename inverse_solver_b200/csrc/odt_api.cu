@@ -627,8 +627,8 @@ void run_chunk(Handle& H, int nb, cudaStream_t s, bool want_t, bool want_r, int 
     if (!fused_xy || !pipe_z)
       raise(ODT_ERR_UNSUPPORTED,
             "16-bit block storage (ODT_STORAGE_B16) needs the fused xy-pass: a scalar potential on a grid "
-            "with equal x and y lengths of 88, 96, 120, 128 or 152 and a z length of 8 * {11, 12, 15, 16, 19, 25, "
-            "27}");
+            "with equal x and y lengths of 8 * R (11 <= R <= 20) and a z length of 8 * R (11 <= R <= 20, 25, "
+            "27)");
     // T16 | Field_n16 | Field | exponents of T | exponents of Field_n in the
     // work block (16.25 of its 24 bytes per voxel)
     const size_t n = (size_t)a.nvox * (size_t)nbp;

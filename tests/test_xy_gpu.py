@@ -2,12 +2,12 @@
 one z and illumination in shared memory -- inverse y- and x-FFT, update,
 source, forward x- and y-FFT -- with the spectrum in its permuted order for
 the z-pass), which the library selects for scalar solves on square x-y grids
-of 88, 96, 120, 128 or 152 (with the pipelined z-pass where the z length
+of 8 R points, 11 <= R <= 20 (with the pipelined z-pass where the z length
 allows it, else the generic one).
 
-  * against the single-precision oracle on (88, 88, 40), (120, 120, 88),
-    (152, 152, 40), (96, 96, 96), (128, 128, 64) and (128, 128, 128) grids,
-    for short series of 1-6 iterations (the first,
+  * against the single-precision oracle on grids covering every R of the
+    xy-pass and every z length of the pipelined z-pass (see
+    test_fused_xy_matches_oracle), for short series of 1-6 iterations (the first,
     early and final kinds) and without the phase ramp (acyclic = false):
     relative L2 per illumination 1e-5 (transmitted, 3D), 3e-5 (reflected);
   * against the separate pipelined passes (ODT_XY=0) on the benchmark's
@@ -52,12 +52,19 @@ def _solve(p, RI, fields, xy=True, profile=False):
     return out, info
 
 
+# z lengths 8 R2 of the pipelined z-pass
+Z_PIPE = {8 * r for r in (11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 25, 27)}
+
+
 @pytest.mark.parametrize("size", [[64, 64, 16], [96, 96, 64], [128, 128, 16], [72, 72, 72], [104, 104, 40],
-                                  [104, 104, 104]])
+                                  [104, 104, 104], [80, 80, 80], [88, 88, 16], [112, 112, 16], [120, 120, 16],
+                                  [136, 136, 16], [64, 64, 88], [64, 64, 112], [64, 64, 120], [64, 64, 136]])
 def test_fused_xy_matches_oracle(size):
-    """Padded grids (88, 88, 40), (152, 152, 40) and (128, 128, 64) with the
-    generic z-pass, (120, 120, 88), (96, 96, 96) (the 12-point butterfly)
-    and (128, 128, 128) (the 16-point one) with the pipelined one."""
+    """Padded x-y planes of 88, 96, 104, 112, 120, 128, 136, 144, 152 and
+    160 points (R = 11 ... 20; 12, 14, 16, 18, 20 are the composite even
+    butterflies with padded plane rows); z lengths with the generic z-pass
+    (40, 64) and the pipelined one (88, 96, 104, 112, 120, 128, 136, 144,
+    160)."""
     p = cases.params(size, [6, 6, 6], return_reflection=True, return_3D=True)
     RI = cases.sphere_phantom(size, [0.1] * 3, cases.NM, seed=size[0] + 5, n_spheres=3, radius_um=(0.3, 0.8))
     fields = cases.circle_fields(p, 3)
@@ -65,7 +72,7 @@ def test_fused_xy_matches_oracle(size):
     assert sim == [v + 24 for v in size] and bm >= 4
     used = {k for k, (ms, n) in kt.items() if n > 0}
     assert {"born_xy", "born_xy_edge"} <= used
-    assert ("born_z_pipe" if sim[2] in (88, 96, 128) else "born_z") in used
+    assert ("born_z_pipe" if sim[2] in Z_PIPE else "born_z") in used
     assert not used & {"born_x", "born_y", "born_x_pipe", "born_y_pipe", "born_x_pipe_edge"}
     o = cbs.ForwardSolverCBS(p, single=True)
     o.set_RI(RI)
