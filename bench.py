@@ -497,15 +497,15 @@ def run_grid_lengths(args):
     from inverse_solver_b200.forward import CBSHostSetup
     from inverse_solver_b200.inputs import ring_illumination, sphere_phantom
 
+    known = [n for n, _ in GRID_LENGTH_CASES]
+    if any(n not in known for n in args.grid_lengths):
+        raise SystemExit("--grid-lengths takes RI sizes from %s" % known)
     n_ill = 16
     dev = torch.device("cuda", 0)
     stream = torch.cuda.current_stream(dev)
     cases = []
     clk = ClockSampler(0)
     clk.start()
-    known = [n for n, _ in GRID_LENGTH_CASES]
-    if any(n not in known for n in args.grid_lengths):
-        raise SystemExit("--grid-lengths takes RI sizes from %s" % known)
     for n, what in GRID_LENGTH_CASES:
         if args.grid_lengths and n not in args.grid_lengths:
             continue

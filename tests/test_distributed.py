@@ -162,3 +162,14 @@ def test_bench_gpus_n_starts_n_ranks():
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [json.loads(ln) for ln in r.stdout.splitlines() if ln.startswith("{")]
     assert sorted((d["rank"], d["local_rank"], d["world"]) for d in lines) == [(0, 0, 2), (1, 1, 2)]
+
+
+def test_bench_grid_lengths_rejects_unknown_size():
+    """`python bench.py --grid-lengths 100`: the RI size is not one of the
+    timed cases, so the run stops with a message naming them, before any GPU
+    work."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--grid-lengths", "100"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode != 0
+    assert "--grid-lengths takes RI sizes from [72, 103, 104, 112, 128, 136]" in r.stderr
