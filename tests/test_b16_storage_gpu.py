@@ -15,6 +15,10 @@ North-star bar: relative L2 <= 1e-4 against the FP64 oracle.
     bound the FP32 path meets (2e-4: the single-precision Green's function
     set-up dominates the transmitted field's error, up to 1.1e-4 for the
     FP32 reference itself) and within 1e-4 of the FP32 path;
+  * on every other plane radix of the fused xy-pass (104, 112, 128, 136, 144
+    and 160-point cubes, with the pipelined z-pass on the same radix) the 3D
+    field is within 1e-4 of the FP32 path, which is checked against the
+    oracle on those radices in test_xy_gpu.py;
   * graph replays of a b16 solve give the same bits as its eager run;
   * a grid the mode does not cover fails with ODT_ERR_UNSUPPORTED."""
 import os
@@ -80,6 +84,20 @@ def test_b16_bench_grid_within_1e4_of_fp64():
         assert et < 2e-4, (sel[k], et)
         assert cbs.rel_l2(t16[..., k], t32[..., k]) < 1e-4
     print("bench grid, b16 field3d vs FP64 (illuminations 0, 37):", errs)
+
+
+@pytest.mark.parametrize("n", [80, 88, 104, 112, 120, 136])
+def test_b16_other_radices_within_1e4_of_fp32(n):
+    size = [n, n, n]
+    p = cases.params(size, [6, 6, 6], return_3D=True)
+    RI = cases.sphere_phantom(size, [0.1] * 3, cases.NM, seed=n, n_spheres=3, radius_um=(0.4, 0.9))
+    fields = cases.circle_fields(p, 2)
+    (t16, _, f16), (sim, _) = _solve(p, RI, fields, "b16")
+    (t32, _, f32), _ = _solve(p, RI, fields, "complex64")
+    assert sim == [n + 24] * 3
+    e3, et = cbs.rel_l2(f16, f32), cbs.rel_l2(t16, t32)
+    print("%d^3 padded, b16 vs FP32: field3d %.2e trans %.2e" % (n + 24, e3, et))
+    assert e3 < 1e-4 and et < 1e-4
 
 
 def test_b16_graph_replays_equal_eager():
